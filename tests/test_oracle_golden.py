@@ -1,0 +1,152 @@
+"""Pins the CPU oracle against the reference's own golden vectors and closed forms.
+
+Sources (paths inside the graphFlow project):
+  tests/unit/test_philox.cpp:48-61, 63-82, 141-151   keyed Philox streams and pinned literals
+  tests/unit/test_reservation.cpp:49-105, 220-285     outputChunkBound closed forms, exhaustive bound
+  tests/unit/test_dense_bin_table.cpp:18-59           planDenseBins / buildDenseTable
+  flow/Execution.hpp:113-124, 2377-2389              tileCount and the flatten loop
+"""
+import itertools
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+# ---- tests/unit/test_philox.cpp:141-151 ----
+PINNED = [((42, 7, 0, 0), 0xD0FD0CC6), ((42, 7, 0, 2), 0xFDA9155E), ((42, 7, 0, 4), 0x6F0157DF),
+          ((42, 7, 1, 4), 0xAB9FEF20), ((42, 7, 0, 6), 0xE0CBA29E), ((42, 7, 2, 6), 0x752FFE28)]
+
+
+@pytest.mark.parametrize("pos,expected", PINNED)
+def test_philox_pinned_literals(pos, expected):
+    assert O.draw(*pos) == expected
+
+
+def test_stream_keys_unique_within_packed_limits():
+    keys = {O.stream_key(42, i, e, p) for i in range(64) for e in range(64) for p in range(32)}
+    assert len(keys) == 64 * 64 * 32
+
+
+def test_engines_own_disjoint_streams():
+    base = O.draws(42, 7, 3, 6, 16)
+    same = O.draws(42, 7, 3, 6, 16)
+    assert np.array_equal(base, same)
+    for other in (O.draws(42, 8, 3, 6, 16), O.draws(42, 7, 4, 6, 16), O.draws(42, 7, 3, 7, 16)):
+        assert np.all(base != other)
+
+
+def test_unmix_is_inverse_of_mix():
+    rng = np.random.default_rng(1)
+    for v in rng.integers(0, 2**63, 200, dtype=np.uint64):
+        assert O.unmix64(O.mix64(int(v))) == int(v)
+
+
+def test_uniform_ranges():
+    assert O.uniform_f32(0) == 0.0 and O.uniform_f32(0xFFFFFFFF) < 1.0
+    assert O.uniform_f64(0) == 0.0 and O.uniform_f64(0xFFFFFFFF) < 1.0
+
+
+# ---- tests/unit/test_reservation.cpp:49-62 ----
+@pytest.mark.parametrize("n,c,b,expected", [(0, 128, 2, 0), (0, 1, 1, 0), (1, 1, 2, 1), (17, 127, 2, 2),
+                                            (128, 128, 2, 2), (4097, 128, 2, 34), (4097, 1, 2, 4097),
+                                            (64, 128, 64, 64), (1, 128, 64, 1)])
+def test_output_chunk_bound_closed_form(n, c, b, expected):
+    assert O.output_chunk_bound(n, c, b) == expected
+
+
+def test_output_chunk_bound_checked():
+    with pytest.raises(O.OracleError):
+        O.output_chunk_bound(4, 0, 2)
+    with pytest.raises(O.OracleError):
+        O.output_chunk_bound(4, 2, 0)
+    with pytest.raises(O.OracleError):
+        O.output_chunk_bound(2**64 - 1, 1, 2)
+    with pytest.raises(O.OracleError):
+        O.checked_output_chunk_bound(2**32 - 1 + 10, 1, 1)
+    with pytest.raises(O.OracleError):
+        O.checked_output_chunk_bound(2**64 - 1, 1, 2)
+
+
+def _distributions(n, bins):
+    if bins == 1:
+        yield (n,)
+        return
+    for i in range(n + 1):
+        for rest in _distributions(n - i, bins - 1):
+            yield (i,) + rest
+
+
+def test_bound_covers_every_distribution():
+    # tests/unit/test_reservation.cpp:74-105, exhaustive over small shapes
+    for n in range(0, 15):
+        for c in range(1, 7):
+            for b in range(1, 6):
+                bound = O.output_chunk_bound(n, c, b)
+                exact_max = max(sum(-(-t // c) for t in d) for d in _distributions(n, b))
+                assert exact_max <= bound, (n, c, b)
+
+
+def test_hash_credit_uses_max_bins():
+    # tests/unit/test_reservation.cpp:220-236
+    for max_bins in (1025, 4096, 65536):
+        assert O.output_chunk_bound(64, 64, max_bins) == 64
+        assert O.output_chunk_bound(1000, 64, max_bins) == 1000
+
+
+# ---- tests/unit/test_dense_bin_table.cpp:18-59 ----
+def test_dense_plan_consecutive_chunks():
+    base, fills, r = O.plan_dense([3, 0, 2], 2)
+    assert list(base) == [0, 2, 2] and r == 3 and list(fills) == [2, 1, 2]
+    assert list(O.build_dense_table(base, [10, 11, 12], r)) == [0, 2, 2, 10, 11, 12]
+
+
+def test_dense_plan_empty_and_single():
+    base, fills, r = O.plan_dense([0, 0], 8)
+    assert list(base) == [0, 0] and r == 0 and fills.size == 0
+    base, fills, r = O.plan_dense([5], 5)
+    assert list(base) == [0] and r == 1 and list(fills) == [5]
+    _, fills, r = O.plan_dense([4, 4], 4)
+    assert r == 2 and list(fills) == [4, 4]
+
+
+def test_dense_plan_bound_and_errors():
+    _, _, r = O.plan_dense([3, 2, 2], 2)
+    assert r == 4 and O.output_chunk_bound(7, 2, 3) == 6
+    with pytest.raises(O.OracleError):
+        O.plan_dense([], 1)
+    with pytest.raises(O.OracleError):
+        O.plan_dense([1], 0)
+    with pytest.raises(O.OracleError):
+        O.build_dense_table([0], [1, 2], 1)
+
+
+# ---- flow/Execution.hpp:113-124, 2377-2389 ----
+def test_tile_flattening():
+    assert O.tile_count(0, 128) == 0 and O.tile_count(1, 128) == 1 and O.tile_count(129, 128) == 2
+    with pytest.raises(O.OracleError):
+        O.tile_count(1, 0)
+    tiles = O.flatten_tiles([5, 9, 2], [300, 0, 128], 128)
+    assert tiles.tolist() == [[5, 0, 128], [5, 128, 128], [5, 256, 44], [2, 0, 128]]
+
+
+# ---- scalar particle model invariants: tests/integration/test_particle_feedback.cpp:281-349 ----
+def test_particle_scalar_invariants():
+    n, max_visits = 20000, 64
+    w, capped, ncap = O.particle_scalar(42, n, max_visits)
+    rows_w, rows_c = O.histogram_u32(w)
+    assert int(rows_c.sum()) == n
+    assert np.all(np.diff(rows_w.astype(np.int64)) > 0)
+    # a weight is 1000*a + b with a + b == visits <= maxVisits
+    visits = w // 1000 + w % 1000
+    assert visits.max() <= max_visits
+    assert int(capped.sum()) == ncap
+    # zero-weight row exists (sink at the first A/B decision)
+    assert rows_w[0] == 0
+
+
+def test_particle_scalar_max_visits_zero_caps_or_sinks():
+    w, capped, ncap = O.particle_scalar(7, 5000, 0)
+    assert np.all(w == 0)
+    assert ncap == int(capped.sum()) and ncap > 0
