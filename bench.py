@@ -1,0 +1,442 @@
+"""Benchmark of the B200 transform-batch hot path: dense classify + exact plan + scatter of
+N = 1e8 u32 keys into pooled output chunks (C = 8192), one whole-array batch per step.
+
+  value   fused single-pass form (one classify->scan->scatter launch + device finish), inputs
+          resident in HBM; particles/s summed over all ranks (weak scaling: every rank
+          partitions its own 1e8 keys; the path has no exchange step, so no collective).
+  plain   the reference's two-launch form (classify, host plan, scatter) on the same data.
+  e2e     the same step through the C ABI from pinned host buffers: H2D of the keys, fused
+          partition, D2H of the output chunks and descriptors, inside the timed region.
+
+``--impl reference`` times the reference algorithm's CPU restatement (the oracle's pool path:
+per-tile histogram -> plan -> scatter, OpenMP over all host threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_KEYS = 100_000_000
+CAPACITY = 8192
+SEED = 42
+HEADLINE_BINS = 64
+HEADLINE_DIST = "uniform"
+BYTES_PER_PARTICLE = 8  # read the 4-byte key once, write it once (algorithmic)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--tile", type=int, default=4096)
+    p.add_argument("--bins", type=int, default=HEADLINE_BINS)
+    p.add_argument("--dist", default=HEADLINE_DIST)
+    p.add_argument("--n", type=int, default=N_KEYS)
+    p.add_argument("--no-sweep", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.proc, self.path = index, None, None
+
+    def __enter__(self):
+        try:
+            self.path = f"/tmp/gf_clocks_{os.getpid()}.csv"
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU arms (oracle = the reference algorithm restated in C; test infrastructure, used here only
+# as the timed CPU baseline)
+# ------------------------------------------------------------------------------------------------
+def cpu_pool_pass(n, bins, dist, threads=0, reps=3):
+    import numpy as np
+    from oracle import oracle as O
+    keys = O.generate_keys_u32(dist, SEED, n, bins, zipf_s=1.1, threads=threads)
+    n_in = -(-n // CAPACITY)
+    bound = O.output_chunk_bound(n, CAPACITY, bins)
+    pool_in = np.zeros((n_in + bound) * CAPACITY, np.uint32)
+    pool_in[:n] = keys
+    fills = np.full(n_in, CAPACITY, np.uint32)
+    fills[-1] = n - CAPACITY * (n_in - 1)
+    tiles = O.flatten_tiles(np.arange(n_in, dtype=np.uint32), fills, 128)  # the reference's T = 128
+    free = np.arange(n_in, n_in + bound, dtype=np.uint32)
+    pool_out = pool_in.copy()
+    bin_ids = np.zeros_like(pool_in)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.partition_pool_u32(pool_in, CAPACITY, tiles, bins, free, threads=threads, pool_out=pool_out,
+                             bin_ids=bin_ids)
+        times.append(time.perf_counter() - t0)
+    return n / statistics.median(times), statistics.median(times)
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    threads = O.cpu_threads()
+    import numpy as np
+    n = args.n
+    keys = O.generate_keys_u32(args.dist, SEED, n, args.bins, zipf_s=1.1, threads=threads)
+    n_in = -(-n // CAPACITY)
+    bound = O.output_chunk_bound(n, CAPACITY, args.bins)
+    pool_in = np.zeros((n_in + bound) * CAPACITY, np.uint32)
+    pool_in[:n] = keys
+    fills = np.full(n_in, CAPACITY, np.uint32)
+    fills[-1] = n - CAPACITY * (n_in - 1)
+    tiles = O.flatten_tiles(np.arange(n_in, dtype=np.uint32), fills, 128)
+    free = np.arange(n_in, n_in + bound, dtype=np.uint32)
+    pool_out = pool_in.copy()
+    bin_ids = np.zeros_like(pool_in)
+    for _ in range(args.warmup):
+        O.partition_pool_u32(pool_in, CAPACITY, tiles, args.bins, free, threads=threads, pool_out=pool_out,
+                             bin_ids=bin_ids)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.partition_pool_u32(pool_in, CAPACITY, tiles, args.bins, free, threads=threads, pool_out=pool_out,
+                             bin_ids=bin_ids)
+    dt = (time.perf_counter() - t0) / max(args.steps, 1)
+    value = n / dt
+    sample = (f"full workload: {n} u32 keys, B={args.bins} {args.dist}, C={CAPACITY}, T=128 tiles, "
+              f"classify->plan->scatter over a chunk pool, per step")
+    print(json.dumps({
+        "impl": "reference", "metric": "particles/s", "value": value, "unit": "particles/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Philox keys)",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": "particles/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def workload_config(args):
+    return {"workload": f"dense classify+plan+scatter, N={args.n} u32 keys, B={args.bins}, {args.dist} keys, "
+                        f"C={CAPACITY}, one whole-array batch",
+            "n": args.n, "bins": args.bins, "dist": args.dist, "capacity": CAPACITY, "tile": args.tile,
+            "l2": "inputs 400 MB and outputs 400 MB exceed the 126 MB L2; no flush"}
+
+
+# ------------------------------------------------------------------------------------------------
+# GPU arm
+# ------------------------------------------------------------------------------------------------
+class DenseBench:
+    """Device-resident setup of one whole-array batch (input chunks 0..n_in-1, a contiguous
+    reservation of outputChunkBound chunks behind them)."""
+
+    def __init__(self, n, bins, dist, tile, device):
+        import numpy as np
+        import torch
+        from graphflow_b200 import capi
+        from graphflow_b200.partition import ChunkPool, FusedPartition, PlainPartition
+        self.torch, self.capi, self.np = torch, capi, np
+        self.n, self.bins, self.dist, self.tile = n, bins, dist, tile
+        self.n_in = -(-n // CAPACITY)
+        self.bound = capi.output_chunk_bound(n, CAPACITY, bins)
+        self.pool = ChunkPool(self.n_in + self.bound, CAPACITY, device=device)
+        cdf = torch.from_numpy(capi.zipf_cdf(1.1, bins)).to(device) if dist == "zipf" else None
+        capi.check(capi.lib().gf_generate_keys_u32(None, capi.DIST_NAMES[dist], SEED, 0, n, bins,
+                                                   cdf.data_ptr() if cdf is not None else None,
+                                                   self.pool.column.data_ptr()), "generate")
+        self.fills = np.full(self.n_in, CAPACITY, np.uint32)
+        self.fills[-1] = n - CAPACITY * (self.n_in - 1)
+        self.chunks = np.arange(self.n_in, dtype=np.uint32)
+        for _ in range(self.n_in):
+            self.pool.free.popleft()
+        self.fused = FusedPartition(self.pool, bins, tile_size=tile, max_batch_particles=n)
+        tiles, self.d_tiles = self.fused._tiles(self.chunks, self.fills)
+        self.n_tiles = len(tiles)
+        reserved = np.arange(self.n_in, self.n_in + self.bound, dtype=np.uint32)
+        self.fused.reserved[:self.bound].copy_(torch.from_numpy(reserved.view(np.int32)))
+        self.plain = PlainPartition(self.pool, bins, tile_size=tile)
+        torch.cuda.synchronize()
+
+    def fused_step(self, stream):
+        self.fused.enqueue(self.d_tiles, self.n_tiles, self.bound, stream)
+
+    def plain_step(self, stream):
+        totals, table, descs = self.plain.run(self.chunks, self.fills, stream)
+        self.pool.release([int(c) for c in descs[:, 0]])
+
+    def check_fused(self):
+        """Size-independent properties at full size: counts sum to N, each port's keys are
+        congruent to the port, the plan matches the totals, the output multiset is the input."""
+        np, torch = self.np, self.torch
+        st = int(self.fused.status.item())
+        totals = self.fused.totals.cpu().numpy().view(np.uint32)
+        r = int(self.fused.num_out.item())
+        descs = self.fused.descs.cpu().numpy().view(np.uint32)[:3 * r].reshape(-1, 3)
+        ok = st == 0 and int(totals.sum(dtype=np.uint64)) == self.n
+        col = self.pool.column
+        if ok and self.dist != "zipf":
+            # port check on device: key % B == port for every output slot
+            ch = torch.from_numpy(descs[:, 0].astype(np.int64)).to(col.device)
+            fl = torch.from_numpy(descs[:, 1].astype(np.int64)).to(col.device)
+            bn = torch.from_numpy(descs[:, 2].astype(np.int64)).to(col.device)
+            view = col.view(-1, CAPACITY)[ch]
+            idx = torch.arange(CAPACITY, device=col.device)[None, :]
+            valid = idx < fl[:, None]
+            keys = view.to(torch.int64) & 0xFFFFFFFF
+            ok &= bool(((keys % self.bins == bn[:, None]) | ~valid).all().item())
+            ok &= int(valid.sum().item()) == self.n
+            # checksum of checksums: sum of all output keys == sum of all input keys (mod 2^64)
+            out_sum = int((keys * valid).sum().item())
+            in_sum = int((col[: self.n_in * CAPACITY].view(-1, CAPACITY).to(torch.int64) & 0xFFFFFFFF).sum().item())
+            ok &= out_sum == in_sum
+        return ok
+
+
+def gpu_arm(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist_mod
+    from graphflow_b200 import capi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist_mod.init_process_group("nccl", device_id=dev, timeout=__import__("datetime").timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist_mod.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist_mod.all_reduce(t, op=dist_mod.ReduceOp.MAX)
+        return float(t.item())
+
+    stream = torch.cuda.Stream(device=dev)
+    bench = DenseBench(args.n, args.bins, args.dist, args.tile, dev)
+
+    # -------- fused (value) --------
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            bench.fused_step(stream)
+    stream.synchronize()
+    correct = bench.check_fused()
+    k_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    k_end = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            t_start.record(stream)
+            for i in range(args.steps):
+                k_start[i].record(stream)
+                capi.check(capi.lib().gf_partition_fused_u32(
+                    stream.cuda_stream, bench.pool.ptr(), bench.pool.ptr(), CAPACITY, bench.pool.slots,
+                    bench.d_tiles.data_ptr(), bench.n_tiles, args.tile, args.bins, capi.CLS_KEY_MOD,
+                    bench.fused.reserved.data_ptr(), bench.bound, bench.fused.totals.data_ptr(),
+                    bench.fused.port_chunks.data_ptr(), bench.fused.max_k, bench.fused.scratch.data_ptr(),
+                    bench.fused.scratch_bytes, bench.fused.next_epoch(), bench.fused.status.data_ptr()), "fused")
+                k_end[i].record(stream)
+                capi.check(capi.lib().gf_fused_finish(
+                    stream.cuda_stream, bench.fused.totals.data_ptr(), bench.fused.port_chunks.data_ptr(), args.bins,
+                    CAPACITY, bench.fused.max_k, bench.fused.epoch, bench.fused.table.data_ptr(),
+                    bench.fused.descs.data_ptr(), bench.fused.reserve_cap, bench.fused.num_out.data_ptr(),
+                    bench.fused.status.data_ptr()), "finish")
+            t_end.record(stream)
+        stream.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(t_start.elapsed_time(t_end) / args.steps)
+    kernel_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(k_start, k_end))
+    correct &= bench.check_fused()
+    value = world * args.n / (ms / 1e3)
+
+    # -------- plain (reference's two-launch form) --------
+    plain_ms = None
+    if rank == 0 or True:
+        for _ in range(max(1, args.warmup // 2)):
+            bench.plain_step(stream)
+        stream.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(3, args.steps // 4)
+        p0.record(stream)
+        for _ in range(reps):
+            bench.plain_step(stream)
+        p1.record(stream)
+        stream.synchronize()
+        plain_ms = max_over_ranks(p0.elapsed_time(p1) / reps)
+
+    # -------- e2e through the C ABI from pinned host buffers --------
+    host_keys = torch.empty(args.n, dtype=torch.int32, pin_memory=True)
+    host_keys.copy_(bench.pool.column[: args.n].cpu())
+    out_slots = bench.bound * CAPACITY
+    host_out = torch.empty(out_slots, dtype=torch.int32, pin_memory=True)
+    host_descs = torch.empty(3 * bench.fused.reserve_cap, dtype=torch.int32, pin_memory=True)
+    host_small = torch.empty(2, dtype=torch.int32, pin_memory=True)
+    out_view = bench.pool.column[bench.n_in * CAPACITY: bench.n_in * CAPACITY + out_slots]
+
+    def e2e_step():
+        bench.pool.column[: args.n].copy_(host_keys, non_blocking=True)
+        bench.fused_step(stream)
+        host_out.copy_(out_view, non_blocking=True)
+        host_descs.copy_(bench.fused.descs, non_blocking=True)
+        host_small[0:1].copy_(bench.fused.num_out, non_blocking=True)
+        host_small[1:2].copy_(bench.fused.status, non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            e2e_step()
+        stream.synchronize()
+        e_reps = max(3, args.steps // 4)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e_reps):
+            e2e_step()
+        e1.record(stream)
+        stream.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e_reps)
+    correct &= int(host_small[1].item()) == 0
+
+    # -------- sweep (fused, every B x distribution of the kernel-level config) --------
+    sweep = []
+    if not args.no_sweep:
+        del bench
+        torch.cuda.empty_cache()
+        for b in (2, 8, 32, 64):
+            for d in ("uniform", "zipf", "one_port", "round_robin"):
+                sb = DenseBench(args.n, b, d, args.tile, dev)
+                with torch.cuda.stream(stream):
+                    for _ in range(2):
+                        sb.fused_step(stream)
+                    stream.synchronize()
+                    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    s0.record(stream)
+                    for _ in range(5):
+                        sb.fused_step(stream)
+                    s1.record(stream)
+                    stream.synchronize()
+                sms = s0.elapsed_time(s1) / 5
+                ok = sb.check_fused()
+                sweep.append({"bins": b, "dist": d, "ms": round(sms, 4), "particles_per_s": args.n / (sms / 1e3),
+                              "hbm_frac": round(args.n * BYTES_PER_PARTICLE / (sms / 1e3) / 1e9 /
+                                                measured_peak()[0], 4), "correct": ok})
+                del sb
+                torch.cuda.empty_cache()
+
+    peak, peak_kind = measured_peak()
+    achieved = args.n * BYTES_PER_PARTICLE / (kernel_ms / 1e3) / 1e9
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        from oracle import oracle as O
+        threads = O.cpu_threads()
+        sample_n = min(args.n, 20_000_000)
+        v, t = cpu_pool_pass(sample_n, args.bins, args.dist, threads=threads)
+        cpu = {"value": v, "unit": "particles/s", "cores": threads, "kind": "port",
+               "sample": f"{sample_n} u32 keys (same B, distribution, C; T=128 tiles), median of 3 passes of "
+                         f"classify->plan->scatter over a chunk pool ({t:.3f} s each)"}
+    if world > 1:
+        dist_mod.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": "particles/s", "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Philox keys)",
+        "config": workload_config(args),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_kind, "kernel": "fused_partition_kernel",
+                     "kernel_ms": kernel_ms,
+                     "algorithmic_bytes": f"{BYTES_PER_PARTICLE} B/particle x {args.n} particles per launch"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * args.n / (e2e_ms / 1e3), "unit": "particles/s",
+                "h2d_bytes_per_step": args.n * 4,
+                "d2h_bytes_per_step": out_slots * 4 + 3 * 4 * bench_reserve_cap(args) + 8},
+        "clocks": clocks.summary(),
+        "gpu_launches": 2 * args.steps,
+        "plain": {"value": world * args.n / (plain_ms / 1e3), "ms_per_step": plain_ms,
+                  "form": "classify kernel + host plan + scatter kernel (reference structure)"},
+        "correct": bool(correct),
+        "sweep": sweep,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def bench_reserve_cap(args):
+    from graphflow_b200 import capi
+    return capi.output_chunk_bound(args.n, CAPACITY, args.bins)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,171 @@
+"""ctypes binding of the graphflow_b200 C ABI (include/graphflow_b200.h).
+
+The shared library is built in-tree (graphflow_b200/_build/libgraphflow_b200.so). Importing a
+kernel entry point without it raises immediately: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libgraphflow_b200.so")
+HEADER = os.path.join(os.path.dirname(_HERE), "include", "graphflow_b200.h")
+
+GF_OK, GF_INVALID, GF_OVERFLOW, GF_ERR_ARGUMENT, GF_ERR_RANGE, GF_ERR_LOGIC, GF_ERR_CUDA, GF_ERR_TIMEOUT, \
+    GF_ERR_TABLE_FULL = range(9)
+STATUS_NAMES = {0: "ok", 1: "invalid", 2: "overflow", 3: "invalid argument", 4: "range overflow", 5: "logic error",
+                6: "cuda error", 7: "timeout", 8: "hash table full"}
+
+CLS_KEY_MOD, CLS_ID_BALANCED, CLS_ID_ONEHOT, CLS_ID_SKEWED, CLS_KEY_UNMIX = range(5)
+SCATTER_SHARED, SCATTER_DIRECT = 0, 1
+DIST_UNIFORM, DIST_ZIPF, DIST_ONE_PORT, DIST_ROUND_ROBIN = range(4)
+DIST_NAMES = {"uniform": DIST_UNIFORM, "zipf": DIST_ZIPF, "one_port": DIST_ONE_PORT, "round_robin": DIST_ROUND_ROBIN}
+
+
+class GfError(RuntimeError):
+    def __init__(self, code, what):
+        super().__init__(f"{what}: {STATUS_NAMES.get(code, code)}")
+        self.code = code
+
+
+class Tile(C.Structure):
+    _fields_ = [("chunk_index", C.c_uint32), ("tile_offset", C.c_uint32), ("count", C.c_uint32)]
+
+
+class OutDesc(C.Structure):
+    _fields_ = [("chunk_index", C.c_uint32), ("fill", C.c_uint32), ("bin", C.c_uint32)]
+
+
+def build(force: bool = False) -> str:
+    """Compile the library with its Makefile (nvcc, sm_100a)."""
+    cmd = ["make", "-s", "-C", _HERE]
+    if force:
+        subprocess.run(cmd + ["clean"], check=True)
+    subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+_VP, _U32, _U64, _I32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
+_SIGS = {
+    "gf_output_chunk_bound": [_U64, _U64, _U64, C.POINTER(_U64)],
+    "gf_checked_output_chunk_bound": [_U64, _U64, _U64, C.POINTER(_U32)],
+    "gf_plan_dense": [_VP, _U32, _U32, _VP, _VP, _U32, C.POINTER(_U32)],
+    "gf_build_dense_table": [_VP, _U32, _VP, _U32, _VP],
+    "gf_tile_count": [_U32, _U32, C.POINTER(_U32)],
+    "gf_flatten_tiles": [_VP, _VP, _U32, _U32, _VP, _U32, C.POINTER(_U32)],
+    "gf_classify_dense_u32": [_VP, _VP, _U32, _U64, _VP, _U32, _U32, _U32, _I32, _VP, _VP, _VP],
+    "gf_scatter_dense_u32": [_VP, _VP, _VP, _U32, _U64, _VP, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _I32, _VP],
+    "gf_fused_scratch_bytes": [_U32, _U32, C.POINTER(_U64)],
+    "gf_partition_fused_u32": [_VP, _VP, _VP, _U32, _U64, _VP, _U32, _U32, _U32, _I32, _VP, _U32, _VP, _VP, _U32,
+                               _VP, _U64, _U32, _VP],
+    "gf_fused_finish": [_VP, _VP, _VP, _U32, _U32, _U32, _U32, _VP, _VP, _U32, _VP, _VP],
+    "gf_zipf_cdf": [C.c_double, _U32, _VP],
+    "gf_generate_keys_u32": [_VP, _I32, _U64, _U64, _U64, _U32, _VP, _VP],
+}
+
+
+def lib():
+    """The loaded library. Raises if it has not been built: the product has no fallback."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"graphflow_b200: native library missing at {LIB_PATH}; run graphflow_b200.capi.build()")
+        L = C.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_int
+        L.gf_supported_tile_sizes.argtypes = [_VP, _U32]
+        L.gf_supported_tile_sizes.restype = _U32
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str):
+    if rc != GF_OK:
+        raise GfError(rc, what)
+
+
+def declared_symbols(header: str = HEADER):
+    """Every function name the public header declares."""
+    import re
+    text = open(header).read()
+    return sorted(set(re.findall(r"^\s*(?:gf_status|uint32_t)\s+(gf_\w+)\s*\(", text, re.M)))
+
+
+# ---- host planning ------------------------------------------------------------------------------
+def output_chunk_bound(n, capacity, max_bins):
+    out = _U64()
+    check(lib().gf_output_chunk_bound(n, capacity, max_bins, C.byref(out)), "outputChunkBound")
+    return out.value
+
+
+def checked_output_chunk_bound(n, capacity, max_bins):
+    out = _U32()
+    check(lib().gf_checked_output_chunk_bound(n, capacity, max_bins, C.byref(out)), "checkedOutputChunkBound")
+    return out.value
+
+
+def plan_dense(totals, capacity):
+    import numpy as np
+    totals = np.ascontiguousarray(totals, np.uint32)
+    base = np.zeros(max(totals.size, 1), np.uint32)
+    cap = int(sum(-(-int(t) // capacity) for t in totals)) if capacity else 0
+    fills = np.zeros(max(cap, 1), np.uint32)
+    num = _U32()
+    check(lib().gf_plan_dense(totals.ctypes.data, totals.size, capacity, base.ctypes.data, fills.ctypes.data, cap,
+                              C.byref(num)), "planDenseBins")
+    return base[:totals.size], fills[:num.value], num.value
+
+
+def build_dense_table(bin_base, chunk_indices):
+    import numpy as np
+    bin_base = np.ascontiguousarray(bin_base, np.uint32)
+    chunk_indices = np.ascontiguousarray(chunk_indices, np.uint32)
+    table = np.zeros(bin_base.size + chunk_indices.size, np.uint32)
+    check(lib().gf_build_dense_table(bin_base.ctypes.data, bin_base.size, chunk_indices.ctypes.data,
+                                     chunk_indices.size, table.ctypes.data), "buildDenseTable")
+    return table
+
+
+def tile_count(fill, tile_size):
+    out = _U32()
+    check(lib().gf_tile_count(fill, tile_size, C.byref(out)), "tileCount")
+    return out.value
+
+
+def flatten_tiles(chunk_index, fills, tile_size):
+    """Flatten chunks into tile descriptors; returns an (n, 3) uint32 array."""
+    import numpy as np
+    chunk_index = np.ascontiguousarray(chunk_index, np.uint32)
+    fills = np.ascontiguousarray(fills, np.uint32)
+    cap = int(((fills.astype(np.int64) + tile_size - 1) // tile_size).sum()) if tile_size else 0
+    out = np.zeros((max(cap, 1), 3), np.uint32)
+    n = _U32()
+    check(lib().gf_flatten_tiles(chunk_index.ctypes.data, fills.ctypes.data, chunk_index.size, tile_size,
+                                 out.ctypes.data, cap, C.byref(n)), "flattenTiles")
+    return out[:n.value]
+
+
+def supported_tile_sizes():
+    import numpy as np
+    buf = np.zeros(16, np.uint32)
+    n = lib().gf_supported_tile_sizes(buf.ctypes.data, 16)
+    return [int(x) for x in buf[:n]]
+
+
+def zipf_cdf(s, k):
+    import numpy as np
+    cdf = np.zeros(k, np.float64)
+    check(lib().gf_zipf_cdf(s, k, cdf.ctypes.data), "zipfCdf")
+    return cdf
+
+
+def fused_scratch_bytes(n_tiles, bins):
+    out = _U64()
+    check(lib().gf_fused_scratch_bytes(n_tiles, bins, C.byref(out)), "fusedScratchBytes")
+    return out.value

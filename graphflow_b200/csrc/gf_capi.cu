@@ -1,0 +1,248 @@
+// C ABI of the dense partition kernels and the synthetic key source: argument validation on the
+// host, then dispatch to the tile-size instantiations of gf_partition.cuh.
+#include <cstdio>
+#include <mutex>
+
+#include "gf_partition.cuh"
+
+namespace gf {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kMaxDenseBins = 65535u;
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+gf_status cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess)
+        return GF_OK;
+    std::fprintf(stderr, "graphflow_b200: CUDA error %s\n", cudaGetErrorString(e));
+    return GF_ERR_CUDA;
+}
+
+int device_sms()
+{
+    static int sms = [] {
+        int dev = 0, n = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess)
+            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n;
+    }();
+    return sms;
+}
+
+template <typename Kernel>
+cudaError_t allow_smem(Kernel k, size_t bytes)
+{
+    if (bytes <= 48u * 1024u)
+        return cudaSuccess;
+    return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <typename Shape, typename P>
+size_t staged_smem(uint32_t B, uint32_t extra_bin_arrays)
+{
+    return sizeof(P) * Shape::kTile + sizeof(uint32_t) * Shape::kTile + sizeof(uint32_t) * Shape::kWarps * B +
+           sizeof(uint32_t) * B * extra_bin_arrays + sizeof(uint32_t) * (Shape::kWarps + 2) + 16;
+}
+
+bool valid_tile_size(uint32_t t) { return t == 1024u || t == 2048u || t == 4096u || t == 8192u; }
+
+// Calls f.template operator()<Shape>() for the instantiation of `tile_size`.
+template <typename F>
+gf_status with_shape(uint32_t tile_size, F&& f)
+{
+    switch (tile_size) {
+    case 1024u:
+        return f.template operator()<TileShape<kThreads, 4>>();
+    case 2048u:
+        return f.template operator()<TileShape<kThreads, 8>>();
+    case 4096u:
+        return f.template operator()<TileShape<kThreads, 16>>();
+    case 8192u:
+        return f.template operator()<TileShape<kThreads, 32>>();
+    default:
+        return GF_ERR_ARGUMENT;
+    }
+}
+
+KeyClassifier key_classifier(int cls, uint32_t bins)
+{
+    KeyClassifier k;
+    k.kind = cls;
+    k.bins = bins;
+    k.fd = FastDiv(bins);
+    k.salt = 0u;
+    return k;
+}
+
+bool valid_classifier(int cls)
+{
+    return cls == GF_CLS_KEY_MOD || cls == GF_CLS_ID_BALANCED || cls == GF_CLS_ID_ONEHOT || cls == GF_CLS_ID_SKEWED;
+}
+
+uint32_t launch_frames(uint32_t n_tiles, size_t smem_bytes)
+{
+    (void)smem_bytes;
+    return n_tiles;
+}
+
+} // namespace
+} // namespace gf
+
+using namespace gf;
+
+extern "C" {
+
+uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap)
+{
+    static const uint32_t sizes[] = {1024u, 2048u, 4096u, 8192u};
+    for (uint32_t i = 0; i < 4u && i < cap && h_sizes != nullptr; ++i)
+        h_sizes[i] = sizes[i];
+    return 4u;
+}
+
+gf_status gf_classify_dense_u32(void* stream, const uint32_t* d_keys, uint32_t capacity, uint64_t pool_slots,
+                                const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size, uint32_t bins,
+                                int classifier, uint32_t* d_bin_ids, uint32_t* d_counts, uint32_t* d_status)
+{
+    if (capacity == 0u || bins == 0u || bins > kMaxDenseBins || !valid_tile_size(tile_size) ||
+        !valid_classifier(classifier) || d_counts == nullptr || (n_tiles != 0u && (d_keys == nullptr ||
+                                                                                    d_tiles == nullptr ||
+                                                                                    d_bin_ids == nullptr)))
+        return GF_ERR_ARGUMENT;
+    if (n_tiles == 0u)
+        return GF_OK;
+    return with_shape(tile_size, [&]<typename Shape>() -> gf_status {
+        using Acc = U32Column;
+        auto kernel = classify_kernel<Shape, Acc, KeyClassify<Acc>>;
+        const size_t smem = sizeof(uint32_t) * bins;
+        cudaError_t e = allow_smem(kernel, smem);
+        if (e != cudaSuccess)
+            return cuda_status(e);
+        Acc acc{d_keys, nullptr};
+        KeyClassify<Acc> cls{key_classifier(classifier, bins)};
+        kernel<<<launch_frames(n_tiles, smem), Shape::kThreads, smem, as_stream(stream)>>>(
+            acc, cls, capacity, pool_slots, d_tiles, n_tiles, bins, d_bin_ids, d_counts, d_status);
+        return cuda_status(cudaGetLastError());
+    });
+}
+
+gf_status gf_scatter_dense_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out, uint32_t capacity,
+                               uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size,
+                               uint32_t bins, const uint32_t* d_bin_ids, const uint32_t* d_table, uint32_t* d_next,
+                               uint32_t* d_counts, int mode, uint32_t* d_status)
+{
+    if (capacity == 0u || bins == 0u || bins > kMaxDenseBins || !valid_tile_size(tile_size) ||
+        (mode != GF_SCATTER_SHARED && mode != GF_SCATTER_DIRECT) || d_counts == nullptr || d_next == nullptr ||
+        (n_tiles != 0u && (d_keys_in == nullptr || d_keys_out == nullptr || d_tiles == nullptr ||
+                           d_bin_ids == nullptr || d_table == nullptr)))
+        return GF_ERR_ARGUMENT;
+    if (n_tiles == 0u)
+        return GF_OK;
+    return with_shape(tile_size, [&]<typename Shape>() -> gf_status {
+        using Acc = U32Column;
+        Acc acc{d_keys_in, d_keys_out};
+        const FastDiv fdc(capacity);
+        if (mode == GF_SCATTER_DIRECT) {
+            auto kernel = scatter_direct_kernel<Shape, Acc, NoUpdate>;
+            kernel<<<n_tiles, Shape::kThreads, 0, as_stream(stream)>>>(acc, NoUpdate{}, 0u, capacity, fdc,
+                                                                        pool_slots, d_tiles, n_tiles, bins,
+                                                                        d_bin_ids, d_table, d_next, d_counts,
+                                                                        d_status);
+            return cuda_status(cudaGetLastError());
+        }
+        auto kernel = scatter_kernel<Shape, Acc, NoUpdate>;
+        const size_t smem = staged_smem<Shape, uint32_t>(bins, 3u);
+        cudaError_t e = allow_smem(kernel, smem);
+        if (e != cudaSuccess)
+            return cuda_status(e);
+        kernel<<<launch_frames(n_tiles, smem), Shape::kThreads, smem, as_stream(stream)>>>(
+            acc, NoUpdate{}, 0u, capacity, fdc, pool_slots, d_tiles, n_tiles, bins, d_bin_ids, d_table, d_next,
+            d_counts, d_status);
+        return cuda_status(cudaGetLastError());
+    });
+}
+
+gf_status gf_fused_scratch_bytes(uint32_t n_tiles, uint32_t bins, uint64_t* h_bytes)
+{
+    if (h_bytes == nullptr || bins == 0u)
+        return GF_ERR_ARGUMENT;
+    *h_bytes = sizeof(FusedCtl) + (uint64_t)n_tiles * bins * sizeof(unsigned long long);
+    return GF_OK;
+}
+
+gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out, uint32_t capacity,
+                                 uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size,
+                                 uint32_t bins, int classifier, const uint32_t* d_reserved, uint32_t n_reserved,
+                                 uint32_t* d_totals, unsigned long long* d_port_chunks, uint32_t max_chunks_per_port,
+                                 void* d_scratch, uint64_t scratch_bytes, uint32_t epoch, uint32_t* d_status)
+{
+    uint64_t need = 0;
+    if (gf_fused_scratch_bytes(n_tiles, bins, &need) != GF_OK || scratch_bytes < need || d_scratch == nullptr ||
+        (reinterpret_cast<uintptr_t>(d_scratch) & 15u) != 0u)
+        return GF_ERR_ARGUMENT;
+    if (capacity == 0u || bins > kMaxDenseBins || !valid_tile_size(tile_size) || !valid_classifier(classifier) ||
+        epoch == 0u || (epoch & 0x3FFFFFFFu) == 0u || d_totals == nullptr || d_status == nullptr ||
+        (n_tiles != 0u && (d_keys_in == nullptr || d_keys_out == nullptr || d_tiles == nullptr ||
+                           d_port_chunks == nullptr || max_chunks_per_port == 0u)))
+        return GF_ERR_ARGUMENT;
+    if (n_tiles == 0u)
+        return cuda_status(cudaMemsetAsync(d_totals, 0, sizeof(uint32_t) * bins, as_stream(stream)));
+    FusedCtl* ctl = static_cast<FusedCtl*>(d_scratch);
+    unsigned long long* desc = reinterpret_cast<unsigned long long*>(ctl + 1);
+    cudaError_t e = cudaMemsetAsync(ctl, 0, sizeof(FusedCtl), as_stream(stream));
+    if (e != cudaSuccess)
+        return cuda_status(e);
+    return with_shape(tile_size, [&]<typename Shape>() -> gf_status {
+        using Acc = U32Column;
+        auto kernel = fused_partition_kernel<Shape, Acc, KeyClassify<Acc>, NoUpdate>;
+        const size_t smem = staged_smem<Shape, uint32_t>(bins, 6u) + sizeof(uint32_t) * 2;
+        cudaError_t err = allow_smem(kernel, smem);
+        if (err != cudaSuccess)
+            return cuda_status(err);
+        Acc acc{d_keys_in, d_keys_out};
+        KeyClassify<Acc> cls{key_classifier(classifier, bins)};
+        kernel<<<n_tiles, Shape::kThreads, smem, as_stream(stream)>>>(
+            acc, cls, NoUpdate{}, 0u, capacity, FastDiv(capacity), pool_slots, d_tiles, n_tiles, bins, d_reserved,
+            n_reserved, d_totals, d_port_chunks, max_chunks_per_port, ctl, desc, epoch, d_status);
+        return cuda_status(cudaGetLastError());
+    });
+}
+
+gf_status gf_fused_finish(void* stream, const uint32_t* d_totals, const unsigned long long* d_port_chunks,
+                          uint32_t bins, uint32_t capacity, uint32_t max_chunks_per_port, uint32_t epoch,
+                          uint32_t* d_table, gf_out_desc* d_descs, uint32_t desc_cap, uint32_t* d_num_out,
+                          uint32_t* d_status)
+{
+    if (bins == 0u || capacity == 0u || d_totals == nullptr || d_table == nullptr || d_num_out == nullptr ||
+        (desc_cap != 0u && (d_descs == nullptr || d_port_chunks == nullptr)))
+        return GF_ERR_ARGUMENT;
+    constexpr int T = 1024;
+    const size_t smem = sizeof(uint32_t) * (4096u * 2u + T / 32 + 1);
+    cudaError_t e = allow_smem(fused_finish_kernel<T>, smem);
+    if (e != cudaSuccess)
+        return cuda_status(e);
+    fused_finish_kernel<T><<<1, T, smem, as_stream(stream)>>>(d_totals, d_port_chunks, bins, capacity,
+                                                              FastDiv(capacity), max_chunks_per_port, epoch, d_table,
+                                                              d_descs, desc_cap, d_num_out, d_status);
+    return cuda_status(cudaGetLastError());
+}
+
+gf_status gf_generate_keys_u32(void* stream, int dist, uint64_t seed, uint64_t first_id, uint64_t n, uint32_t bins,
+                               const double* d_cdf, uint32_t* d_keys)
+{
+    if (dist < GF_DIST_UNIFORM || dist > GF_DIST_ROUND_ROBIN || (dist == GF_DIST_ZIPF && (d_cdf == nullptr ||
+                                                                                       bins == 0u)) ||
+        (n != 0u && d_keys == nullptr))
+        return GF_ERR_ARGUMENT;
+    if (n == 0u)
+        return GF_OK;
+    const uint64_t blocks64 = (n + 255u) / 256u;
+    const unsigned blocks = (unsigned)(blocks64 < (uint64_t)device_sms() * 16u ? blocks64 : (uint64_t)device_sms() * 16u);
+    generate_keys_kernel<<<blocks, 256, 0, as_stream(stream)>>>(dist, mix64(seed), first_id, n, bins, d_cdf, d_keys);
+    return cuda_status(cudaGetLastError());
+}
+
+} // extern "C"

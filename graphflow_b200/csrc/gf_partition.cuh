@@ -1,0 +1,617 @@
+// Partition kernels of the transform-batch hot path (dense bins), templated over the payload
+// access policy, the classifier and the updater so that the C ABI (built-in classifiers) and
+// the C++ Flow front end (user functors) instantiate the same code.
+//
+// Reference behaviour restated (paths inside graphFlow's include/graphFlow):
+//   classify  flow/Execution.hpp:870-954, graph/ClassifyKernel.hpp:33-93
+//   scatter   flow/Execution.hpp:985-1189, graph/ScatterKernel.hpp:174-289 (shared) / :98-173 (direct)
+//   plan      graph/DenseBinTable.hpp:39-91 (host) and its device form in fused_finish_kernel
+//
+// Tile layout inside a CTA: warp w owns the contiguous slice [w*32*IPT, (w+1)*32*IPT) of the tile
+// and walks it in IPT rounds of 32 consecutive items, so every global access of a round is one
+// coalesced 128-byte (u32) or 512-byte (16 B record) transaction per warp.
+#pragma once
+
+#include "gf_device.cuh"
+
+namespace gf {
+
+// UpdateResult of flow/Concepts.hpp (success / overflow / invalid).
+enum : uint32_t { kUpdateSuccess = 0u, kUpdateOverflow = 1u, kUpdateInvalid = 2u };
+
+struct NoUpdate {
+    template <typename P>
+    GF_D uint32_t operator()(uint32_t, P&, uint64_t /*seed_mixed*/) const
+    {
+        return kUpdateSuccess;
+    }
+};
+
+// One u32 column (the kernel-level sweeps' key payload).
+struct U32Column {
+    using Payload = uint32_t;
+    const uint32_t* in;
+    uint32_t* out;
+    GF_D Payload load(uint64_t slot) const { return ld_stream(in + slot); }
+    GF_D void store(uint64_t slot, const Payload& p) const { out[slot] = p; }
+    GF_HD static uint64_t key(const Payload& p) { return p; }
+};
+
+template <typename Access>
+struct KeyClassify {
+    KeyClassifier cls;
+    GF_D uint32_t operator()(const typename Access::Payload& p) const { return cls(Access::key(p)); }
+};
+
+template <int THREADS, int IPT>
+struct TileShape {
+    static constexpr int kThreads = THREADS;
+    static constexpr int kIpt = IPT;
+    static constexpr int kWarps = THREADS / 32;
+    static constexpr int kTile = THREADS * IPT;
+    GF_D static uint32_t item(int w, int r, int lane) { return (uint32_t)(w * 32 * IPT + r * 32 + lane); }
+};
+
+constexpr uint32_t kNoBin = 0xFFFFFFFFu;
+constexpr uint32_t kNoChunk = 0xFFFFFFFFu;
+
+// Block-wide exclusive scan of n <= 65536 u32 values held in shared memory (in-place allowed).
+// `warp_tmp` needs kWarps + 1 words. Returns the total to every thread.
+template <int THREADS>
+GF_D uint32_t block_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* warp_tmp)
+{
+    constexpr int W = THREADS / 32;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const uint32_t per = (n + THREADS - 1) / THREADS;
+    const uint32_t lo = min(n, (uint32_t)tid * per), hi = min(n, lo + per);
+    uint32_t sum = 0;
+    for (uint32_t i = lo; i < hi; ++i)
+        sum += in[i];
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o)
+            incl += v;
+    }
+    if (lane == 31)
+        warp_tmp[w] = incl;
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t run = 0;
+        for (int i = 0; i < W; ++i) {
+            uint32_t c = warp_tmp[i];
+            warp_tmp[i] = run;
+            run += c;
+        }
+        warp_tmp[W] = run;
+    }
+    __syncthreads();
+    uint32_t run = warp_tmp[w] + incl - sum;
+    for (uint32_t i = lo; i < hi; ++i) {
+        uint32_t c = in[i];
+        out[i] = run;
+        run += c;
+    }
+    uint32_t total = warp_tmp[W];
+    __syncthreads();
+    return total;
+}
+
+// Stable in-tile ranking. bins[r] is the bin of item (w, r, lane) or kNoBin. On return pos[r] is
+// the item's rank among the items of its bin inside its warp's slice, and warp_cnt[w*B + b] holds
+// the number of items of bin b in warp w's slice.
+template <typename Shape>
+GF_D void warp_rank(const uint32_t (&bins)[Shape::kIpt], uint32_t (&pos)[Shape::kIpt], uint32_t* warp_cnt,
+                    uint32_t B)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t* cnt = warp_cnt + (size_t)w * B;
+    for (uint32_t b = lane; b < B; b += 32)
+        cnt[b] = 0u;
+    __syncwarp();
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int r = 0; r < Shape::kIpt; ++r) {
+        const uint32_t bin = bins[r];
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, bin);
+        uint32_t base = 0;
+        if (bin != kNoBin)
+            base = cnt[bin];
+        __syncwarp();
+        if (bin != kNoBin) {
+            pos[r] = base + __popc(peers & lt);
+            if (lane == 31 - __clz(peers))
+                cnt[bin] = base + __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
+// Per-bin warp offsets (exclusive over warps, in place) and tile totals.
+template <typename Shape>
+GF_D void warp_offsets(uint32_t* warp_cnt, uint32_t* bin_tot, uint32_t B)
+{
+    for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads) {
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < Shape::kWarps; ++w) {
+            uint32_t c = warp_cnt[(size_t)w * B + b];
+            warp_cnt[(size_t)w * B + b] = run;
+            run += c;
+        }
+        bin_tot[b] = run;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Classify: flow/Execution.hpp:870-954. Per tile: classify every payload, store its bin, count
+// bins in shared memory with warp-aggregated atomics, then one device atomic per (tile, bin).
+// counts[B] is the status slot.
+// ---------------------------------------------------------------------------------------------
+template <typename Shape, typename Access, typename Classify>
+__global__ void __launch_bounds__(Shape::kThreads) classify_kernel(Access acc, Classify classify, uint32_t capacity,
+                                                                   uint64_t pool_slots, const gf_tile* tiles,
+                                                                   uint32_t n_tiles, uint32_t B, uint32_t* bin_ids,
+                                                                   uint32_t* counts, uint32_t* status)
+{
+    extern __shared__ uint32_t smem[];
+    uint32_t* hist = smem; // [B]
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const gf_tile tile = tiles[t];
+        const uint64_t base = (uint64_t)tile.chunk_index * capacity + tile.tile_offset;
+        const bool tile_ok = tile.count <= (uint32_t)Shape::kTile && base + tile.count <= pool_slots &&
+                             tile.tile_offset + tile.count <= capacity;
+        for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads)
+            hist[b] = 0u;
+        __syncthreads();
+        if (!tile_ok) {
+            if (threadIdx.x == 0)
+                set_status(status, GF_INVALID);
+        } else {
+            typename Access::Payload p[Shape::kIpt];
+#pragma unroll
+            for (int r = 0; r < Shape::kIpt; ++r) {
+                const uint32_t i = Shape::item(w, r, lane);
+                if (i < tile.count)
+                    p[r] = acc.load(base + i);
+            }
+#pragma unroll
+            for (int r = 0; r < Shape::kIpt; ++r) {
+                const uint32_t i = Shape::item(w, r, lane);
+                uint32_t bin = kNoBin;
+                if (i < tile.count) {
+                    bin = classify(p[r]);
+                    if (bin >= B) {
+                        counts[B] = 1u;
+                        set_status(status, GF_INVALID);
+                        bin = kNoBin;
+                    } else {
+                        bin_ids[base + i] = bin;
+                    }
+                }
+                const uint32_t peers = __match_any_sync(0xFFFFFFFFu, bin);
+                if (bin != kNoBin && lane == 31 - __clz(peers))
+                    atomicAdd(&hist[bin], (uint32_t)__popc(peers));
+            }
+        }
+        __syncthreads();
+        for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads)
+            if (hist[b] != 0u)
+                atomicAdd(&counts[b], hist[b]);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Scatter (SharedStaging): flow/Execution.hpp:1096-1187. Per tile: recount from the stored bins,
+// reserve one range per bin with a device atomic on next[bin], rank inside the tile (stable),
+// apply the updater, stage the tile in shared memory in bin order and write it out coalesced:
+// out slot = table[B + table[bin] + j / C] * C + j % C.
+// ---------------------------------------------------------------------------------------------
+template <typename Shape, typename Access, typename Update>
+__global__ void __launch_bounds__(Shape::kThreads) scatter_kernel(Access acc, Update update, uint64_t seed_mixed,
+                                                                  uint32_t capacity, FastDiv fdc, uint64_t pool_slots,
+                                                                  const gf_tile* tiles, uint32_t n_tiles, uint32_t B,
+                                                                  const uint32_t* bin_ids, const uint32_t* table,
+                                                                  uint32_t* next, uint32_t* counts, uint32_t* status)
+{
+    using P = typename Access::Payload;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    P* stage = reinterpret_cast<P*>(smem_raw);
+    uint32_t* stage_bin = reinterpret_cast<uint32_t*>(stage + Shape::kTile);
+    uint32_t* warp_cnt = stage_bin + Shape::kTile;            // [W][B]
+    uint32_t* bin_tot = warp_cnt + (size_t)Shape::kWarps * B; // [B]
+    uint32_t* bin_excl = bin_tot + B;                         // [B]
+    uint32_t* gbase = bin_excl + B;                           // [B]
+    uint32_t* scan_tmp = gbase + B;                           // [W+1]
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+
+    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const gf_tile tile = tiles[t];
+        const uint64_t base = (uint64_t)tile.chunk_index * capacity + tile.tile_offset;
+        const bool tile_ok = tile.count <= (uint32_t)Shape::kTile && base + tile.count <= pool_slots &&
+                             tile.tile_offset + tile.count <= capacity;
+        uint32_t bins[Shape::kIpt], pos[Shape::kIpt];
+        P p[Shape::kIpt];
+#pragma unroll
+        for (int r = 0; r < Shape::kIpt; ++r) {
+            const uint32_t i = Shape::item(w, r, lane);
+            bins[r] = kNoBin;
+            if (tile_ok && i < tile.count) {
+                bins[r] = __ldg(bin_ids + base + i);
+                p[r] = acc.load(base + i);
+                if (bins[r] >= B) {
+                    counts[B] = 1u;
+                    set_status(status, GF_INVALID);
+                    bins[r] = kNoBin;
+                }
+            }
+        }
+        if (!tile_ok && threadIdx.x == 0)
+            set_status(status, GF_INVALID);
+        warp_rank<Shape>(bins, pos, warp_cnt, B);
+        __syncthreads();
+        warp_offsets<Shape>(warp_cnt, bin_tot, B);
+        __syncthreads();
+        const uint32_t n_valid = block_exclusive_scan<Shape::kThreads>(bin_tot, bin_excl, B, scan_tmp);
+        for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads)
+            if (bin_tot[b] != 0u)
+                gbase[b] = atomicAdd(&next[b], bin_tot[b]) - bin_excl[b];
+#pragma unroll
+        for (int r = 0; r < Shape::kIpt; ++r) {
+            if (bins[r] == kNoBin)
+                continue;
+            const uint32_t q = bin_excl[bins[r]] + warp_cnt[(size_t)w * B + bins[r]] + pos[r];
+            const uint32_t res = update(bins[r], p[r], seed_mixed);
+            if (res != kUpdateSuccess) {
+                counts[B] = 1u;
+                set_status(status, res == kUpdateOverflow ? GF_OVERFLOW : GF_INVALID);
+            }
+            stage[q] = p[r];
+            stage_bin[q] = bins[r];
+        }
+        __syncthreads();
+        for (uint32_t q = threadIdx.x; q < n_valid; q += Shape::kThreads) {
+            const uint32_t b = stage_bin[q];
+            const uint32_t j = gbase[b] + q;
+            const uint32_t k = fdc.div(j);
+            const uint32_t chunk = __ldg(table + B + __ldg(table + b) + k);
+            const uint64_t slot = (uint64_t)chunk * capacity + (j - k * capacity);
+            if (slot < pool_slots)
+                acc.store(slot, stage[q]);
+            else
+                set_status(status, GF_OVERFLOW);
+        }
+        __syncthreads();
+    }
+}
+
+// Scatter (Direct): flow/Execution.hpp:1034-1095, one device atomic per particle.
+template <typename Shape, typename Access, typename Update>
+__global__ void __launch_bounds__(Shape::kThreads) scatter_direct_kernel(Access acc, Update update,
+                                                                         uint64_t seed_mixed, uint32_t capacity,
+                                                                         FastDiv fdc, uint64_t pool_slots,
+                                                                         const gf_tile* tiles, uint32_t n_tiles,
+                                                                         uint32_t B, const uint32_t* bin_ids,
+                                                                         const uint32_t* table, uint32_t* next,
+                                                                         uint32_t* counts, uint32_t* status)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const gf_tile tile = tiles[t];
+        const uint64_t base = (uint64_t)tile.chunk_index * capacity + tile.tile_offset;
+        if (tile.count > (uint32_t)Shape::kTile || base + tile.count > pool_slots ||
+            tile.tile_offset + tile.count > capacity) {
+            if (threadIdx.x == 0)
+                set_status(status, GF_INVALID);
+            continue;
+        }
+#pragma unroll
+        for (int r = 0; r < Shape::kIpt; ++r) {
+            const uint32_t i = Shape::item(w, r, lane);
+            if (i >= tile.count)
+                continue;
+            const uint32_t b = __ldg(bin_ids + base + i);
+            if (b >= B) {
+                counts[B] = 1u;
+                set_status(status, GF_INVALID);
+                continue;
+            }
+            const uint32_t j = atomicAdd(&next[b], 1u);
+            const uint32_t k = fdc.div(j);
+            const uint32_t chunk = __ldg(table + B + __ldg(table + b) + k);
+            const uint64_t slot = (uint64_t)chunk * capacity + (j - k * capacity);
+            typename Access::Payload p = acc.load(base + i);
+            const uint32_t res = update(b, p, seed_mixed);
+            if (res != kUpdateSuccess) {
+                counts[B] = 1u;
+                set_status(status, res == kUpdateOverflow ? GF_OVERFLOW : GF_INVALID);
+            }
+            if (slot < pool_slots)
+                acc.store(slot, p);
+            else
+                set_status(status, GF_OVERFLOW);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused single-pass classify -> scan -> scatter.
+//
+// Scratch: a control block {tile counter, allocation cursor} that the host zeroes per launch,
+// followed by one 64-bit look-back descriptor per (tile, bin):
+//   bits 63..34 epoch, 33..32 flag (1 = tile aggregate, 2 = inclusive prefix), 31..0 value.
+// Descriptors of older launches carry an older epoch and read as "not ready", so the array
+// needs no clearing. Tiles take their index from the counter in launch order, so every tile a
+// CTA waits on belongs to a CTA that is already running; every wait is still bounded.
+// ---------------------------------------------------------------------------------------------
+struct FusedCtl {
+    uint32_t tile_counter;
+    uint32_t alloc_cursor;
+    uint32_t pad[14];
+};
+
+GF_HD unsigned long long make_desc(uint32_t epoch, uint32_t flag, uint32_t value)
+{
+    return ((unsigned long long)((epoch << 2) | flag) << 32) | value;
+}
+
+template <typename Shape, typename Access, typename Classify, typename Update>
+__global__ void __launch_bounds__(Shape::kThreads) fused_partition_kernel(
+    Access acc, Classify classify, Update update, uint64_t seed_mixed, uint32_t capacity, FastDiv fdc,
+    uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B, const uint32_t* reserved,
+    uint32_t n_reserved, uint32_t* totals, unsigned long long* port_chunks, uint32_t max_k, FusedCtl* ctl,
+    unsigned long long* desc, uint32_t epoch, uint32_t* status)
+{
+    using P = typename Access::Payload;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    P* stage = reinterpret_cast<P*>(smem_raw);
+    uint32_t* stage_bin = reinterpret_cast<uint32_t*>(stage + Shape::kTile);
+    uint32_t* warp_cnt = stage_bin + Shape::kTile;            // [W][B]
+    uint32_t* bin_tot = warp_cnt + (size_t)Shape::kWarps * B; // [B]
+    uint32_t* bin_excl = bin_tot + B;                         // [B]
+    uint32_t* gbase = bin_excl + B;                           // [B]
+    uint32_t* k0 = gbase + B;                                 // [B]
+    uint32_t* chunk_lo = k0 + B;                              // [B]
+    uint32_t* chunk_hi = chunk_lo + B;                        // [B]
+    uint32_t* scan_tmp = chunk_hi + B;                        // [W+1]
+    uint32_t* s_tile = scan_tmp + Shape::kWarps + 1;          // [1]
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t epoch_hi = epoch & 0x3FFFFFFFu;
+
+    if (threadIdx.x == 0)
+        *s_tile = atomicAdd(&ctl->tile_counter, 1u);
+    __syncthreads();
+    const uint32_t t = *s_tile;
+    if (t >= n_tiles)
+        return;
+
+    const gf_tile tile = tiles[t];
+    const uint64_t base = (uint64_t)tile.chunk_index * capacity + tile.tile_offset;
+    const bool tile_ok = tile.count <= (uint32_t)Shape::kTile && base + tile.count <= pool_slots &&
+                         tile.tile_offset + tile.count <= capacity;
+    if (!tile_ok && threadIdx.x == 0)
+        set_status(status, GF_INVALID);
+
+    // 1. load and classify
+    uint32_t bins[Shape::kIpt], pos[Shape::kIpt];
+    P p[Shape::kIpt];
+#pragma unroll
+    for (int r = 0; r < Shape::kIpt; ++r) {
+        const uint32_t i = Shape::item(w, r, lane);
+        bins[r] = kNoBin;
+        if (tile_ok && i < tile.count)
+            p[r] = acc.load(base + i);
+    }
+#pragma unroll
+    for (int r = 0; r < Shape::kIpt; ++r) {
+        const uint32_t i = Shape::item(w, r, lane);
+        if (tile_ok && i < tile.count) {
+            uint32_t b = classify(p[r]);
+            if (b >= B) {
+                set_status(status, GF_INVALID);
+                b = kNoBin;
+            }
+            bins[r] = b;
+        }
+    }
+    // 2. stable rank inside the tile, per-bin tile totals
+    warp_rank<Shape>(bins, pos, warp_cnt, B);
+    __syncthreads();
+    warp_offsets<Shape>(warp_cnt, bin_tot, B);
+    __syncthreads();
+
+    // 3. publish the tile aggregate, then look back for the exclusive prefix of every bin
+    unsigned long long* my_desc = desc + (size_t)t * B;
+    for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads)
+        st_relaxed_u64(my_desc + b, make_desc(epoch_hi, t == 0 ? 2u : 1u, bin_tot[b]));
+    const uint32_t n_valid = block_exclusive_scan<Shape::kThreads>(bin_tot, bin_excl, B, scan_tmp);
+    for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads) {
+        uint32_t excl = 0;
+        bool ok = true;
+        for (int64_t pred = (int64_t)t - 1; pred >= 0; --pred) {
+            const unsigned long long* d = desc + (size_t)pred * B + b;
+            unsigned long long v = 0;
+            ok = bounded_wait(
+                [&] {
+                    v = ld_relaxed_u64(d);
+                    return (uint32_t)(v >> 34) == epoch_hi && ((v >> 32) & 3u) != 0u;
+                },
+                status);
+            if (!ok)
+                break;
+            excl += (uint32_t)v;
+            if (((v >> 32) & 3u) == 2u)
+                break;
+        }
+        if (!ok) {
+            set_status(status, GF_ERR_TIMEOUT);
+            __threadfence();
+            excl = 0xFFFFFFFFu;
+        }
+        if (t != 0)
+            st_relaxed_u64(my_desc + b, make_desc(epoch_hi, 2u, excl + bin_tot[b]));
+        if (t + 1 == n_tiles)
+            totals[b] = excl + bin_tot[b];
+        gbase[b] = excl - bin_excl[b];
+
+        // 4. output chunks of this bin's range [excl, excl + tot): take on first touch
+        uint32_t lo = kNoChunk, hi = kNoChunk;
+        const uint32_t tot = bin_tot[b];
+        if (tot != 0u && ok) {
+            const uint32_t ka = fdc.div(excl), kb = fdc.div(excl + tot - 1u);
+            k0[b] = ka;
+            for (uint32_t k = ka; k <= kb; ++k) {
+                uint32_t chunk = kNoChunk;
+                if (k >= max_k) {
+                    set_status(status, GF_OVERFLOW);
+                } else if ((uint64_t)k * capacity >= excl) {
+                    const uint32_t idx = atomicAdd(&ctl->alloc_cursor, 1u);
+                    if (idx < n_reserved) {
+                        chunk = __ldg(reserved + idx);
+                        st_relaxed_u64(port_chunks + (size_t)b * max_k + k,
+                                       ((unsigned long long)epoch << 32) | chunk);
+                    } else {
+                        set_status(status, GF_OVERFLOW);
+                    }
+                } else {
+                    const unsigned long long* src = port_chunks + (size_t)b * max_k + k;
+                    unsigned long long v = 0;
+                    if (bounded_wait(
+                            [&] {
+                                v = ld_relaxed_u64(src);
+                                return (uint32_t)(v >> 32) == epoch;
+                            },
+                            status))
+                        chunk = (uint32_t)v;
+                    else
+                        set_status(status, GF_ERR_TIMEOUT);
+                }
+                if (k == ka)
+                    lo = chunk;
+                else
+                    hi = chunk;
+            }
+        }
+        chunk_lo[b] = lo;
+        chunk_hi[b] = hi;
+    }
+
+    // 5. apply the updater and stage the tile in bin order
+#pragma unroll
+    for (int r = 0; r < Shape::kIpt; ++r) {
+        if (bins[r] == kNoBin)
+            continue;
+        const uint32_t q = bin_excl[bins[r]] + warp_cnt[(size_t)w * B + bins[r]] + pos[r];
+        const uint32_t res = update(bins[r], p[r], seed_mixed);
+        if (res != kUpdateSuccess)
+            set_status(status, res == kUpdateOverflow ? GF_OVERFLOW : GF_INVALID);
+        stage[q] = p[r];
+        stage_bin[q] = bins[r];
+    }
+    if (threadIdx.x == 0)
+        *s_tile = ld_relaxed_u32(status);
+    __syncthreads();
+    if (*s_tile != 0u)
+        return; // the batch failed somewhere: write nothing, the host discards it
+
+    // 6. coalesced write-out
+    for (uint32_t q = threadIdx.x; q < n_valid; q += Shape::kThreads) {
+        const uint32_t b = stage_bin[q];
+        const uint32_t j = gbase[b] + q;
+        const uint32_t k = fdc.div(j);
+        const uint32_t chunk = k == k0[b] ? chunk_lo[b] : chunk_hi[b];
+        if (chunk == kNoChunk)
+            continue;
+        const uint64_t slot = (uint64_t)chunk * capacity + (j - k * capacity);
+        if (slot < pool_slots)
+            acc.store(slot, stage[q]);
+        else
+            set_status(status, GF_OVERFLOW);
+    }
+}
+
+// Device form of planDenseBins + buildDenseTable + the output-descriptor loop
+// (DenseBinTable.hpp:39-91, Execution.hpp:2558-2581) for a fused launch. One CTA.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) fused_finish_kernel(const uint32_t* totals,
+                                                               const unsigned long long* port_chunks, uint32_t B,
+                                                               uint32_t capacity, FastDiv fdc, uint32_t max_k,
+                                                               uint32_t epoch, uint32_t* table, gf_out_desc* descs,
+                                                               uint32_t desc_cap, uint32_t* num_out, uint32_t* status)
+{
+    extern __shared__ uint32_t smem[];
+    uint32_t* nck = smem;      // [seg]
+    uint32_t* base = nck + 4096; // [seg]
+    uint32_t* tmp = base + 4096;  // [W+1]
+    uint32_t carry = 0;
+    for (uint32_t seg = 0; seg < B; seg += 4096) {
+        const uint32_t n = min(4096u, B - seg);
+        for (uint32_t i = threadIdx.x; i < n; i += THREADS) {
+            const uint32_t tot = totals[seg + i];
+            nck[i] = fdc.div(tot) + (fdc.mod(tot) != 0u ? 1u : 0u);
+        }
+        __syncthreads();
+        const uint32_t sum = block_exclusive_scan<THREADS>(nck, base, n, tmp);
+        for (uint32_t i = threadIdx.x; i < n; i += THREADS) {
+            const uint32_t b = seg + i, bb = carry + base[i], tot = totals[b];
+            table[b] = bb;
+            for (uint32_t k = 0; k < nck[i]; ++k) {
+                const uint32_t f = bb + k;
+                if (f >= desc_cap || k >= max_k) {
+                    set_status(status, GF_OVERFLOW);
+                    break;
+                }
+                const unsigned long long v = port_chunks[(size_t)b * max_k + k];
+                const uint32_t chunk = (uint32_t)(v >> 32) == epoch ? (uint32_t)v : kNoChunk;
+                if (chunk == kNoChunk)
+                    set_status(status, GF_INVALID);
+                table[B + f] = chunk;
+                descs[f].chunk_index = chunk;
+                descs[f].fill = min(capacity, tot - k * capacity);
+                descs[f].bin = b;
+            }
+        }
+        carry += sum;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        *num_out = carry;
+}
+
+// Synthetic key source (uniform / Zipf / one port / round robin) at stream positions
+// (first_id + i, 0, 0x100 + dist).
+__global__ void generate_keys_kernel(int dist, uint64_t seed_mixed, uint64_t first_id, uint64_t n, uint32_t bins,
+                                     const double* cdf, uint32_t* keys)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t id = first_id + i;
+        uint32_t k;
+        if (dist == GF_DIST_UNIFORM || dist == GF_DIST_ZIPF) {
+            const uint32_t d = first_draws(stream_key(seed_mixed, id, 0u, 0x100u + (uint32_t)dist)).v[0];
+            if (dist == GF_DIST_UNIFORM) {
+                k = d;
+            } else {
+                const double u = uniform_f64(d);
+                uint32_t lo = 0, hi = bins - 1u;
+                while (lo < hi) {
+                    const uint32_t mid = lo + (hi - lo) / 2u;
+                    if (u < cdf[mid])
+                        hi = mid;
+                    else
+                        lo = mid + 1u;
+                }
+                k = lo;
+            }
+        } else if (dist == GF_DIST_ONE_PORT) {
+            k = 0u;
+        } else {
+            k = (uint32_t)id;
+        }
+        keys[i] = k;
+    }
+}
+
+} // namespace gf

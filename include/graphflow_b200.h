@@ -1,0 +1,157 @@
+/* graphflow_b200: C ABI of the B200-native transform-batch hot path of graphFlow.
+ *
+ * Plain pointers and sizes only. Device pointers are marked `d_`, host pointers `h_`.
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ * Every kernel entry point is stream-ordered and asynchronous: it validates its arguments on
+ * the host, enqueues its work and returns. Device-side failures (an invalid classifier result, a
+ * checked updater overflow, an exhausted reservation, a wait that ran out of polls) are written
+ * to the caller's device status word, which the caller zeroes before the batch and reads after
+ * it, exactly like the reference's `Status` word and `counts[B]` status slot
+ * (flow/Status.hpp:21-96, flow/Execution.hpp:2527-2547). No entry point throws.
+ *
+ * Reference paths below are inside the graphFlow project (include/graphFlow/...).
+ */
+#ifndef GRAPHFLOW_B200_H
+#define GRAPHFLOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------ */
+/* 0..2 are the device StatusCode values of flow/Status.hpp:21-26; the rest are host-side. */
+typedef enum gf_status {
+    GF_OK = 0,
+    GF_INVALID = 1,        /* StatusCode::invalid: bin >= B, bad payload                   */
+    GF_OVERFLOW = 2,       /* StatusCode::overflow: checked updater or capacity overflow   */
+    GF_ERR_ARGUMENT = 3,   /* std::invalid_argument of the reference (config/argument)     */
+    GF_ERR_RANGE = 4,      /* std::overflow_error of the reference (32-bit limits)         */
+    GF_ERR_LOGIC = 5,      /* std::logic_error of the reference (plan exceeds the bound)   */
+    GF_ERR_CUDA = 6,       /* a CUDA runtime call failed                                   */
+    GF_ERR_TIMEOUT = 7,    /* a bounded device wait gave up                                */
+    GF_ERR_TABLE_FULL = 8  /* hash table of a tile is full (HashClassifyKernel.hpp:35-41)  */
+} gf_status;
+
+/* ---- data layouts ------------------------------------------------------------------------ */
+/* One <= T slice of one pool chunk: graph/TileDescriptor.hpp:25-30. */
+typedef struct gf_tile {
+    uint32_t chunk_index;
+    uint32_t tile_offset;
+    uint32_t count;
+} gf_tile;
+
+/* One published output chunk: core/Chunk.hpp:33-37 (handle index, fill, bin). */
+typedef struct gf_out_desc {
+    uint32_t chunk_index;
+    uint32_t fill;
+    uint32_t bin;
+} gf_out_desc;
+
+/* Built-in classifiers. User functors cannot cross a C ABI; the C++ front end instantiates the
+ * kernels with them directly. These ids cover the kernel-level sweeps and the kernel-axis
+ * example classifiers (examples/particle_feedback/KernelAxes.hpp:29-42). */
+enum {
+    GF_CLS_KEY_MOD = 0,     /* bin = key % B                                  */
+    GF_CLS_ID_BALANCED = 1, /* bin = id % B                                   */
+    GF_CLS_ID_ONEHOT = 2,   /* bin = 0                                        */
+    GF_CLS_ID_SKEWED = 3,   /* bin = id % 8 == 0 ? id % B : 0                 */
+    GF_CLS_KEY_UNMIX = 4    /* bin = unmix64(key) ^ salt (u64 keys, hash path) */
+};
+
+/* Scatter strategies: core/ScatterMode.hpp (SharedStaging, Direct). */
+enum { GF_SCATTER_SHARED = 0, GF_SCATTER_DIRECT = 1 };
+
+/* Key distributions of the kernel-level sweeps. */
+enum { GF_DIST_UNIFORM = 0, GF_DIST_ZIPF = 1, GF_DIST_ONE_PORT = 2, GF_DIST_ROUND_ROBIN = 3 };
+
+/* ---- host-side planning (no device work) -------------------------------------------------- */
+
+/* core/Reservation.hpp:35-50 outputChunkBound: R = min(n, ceil(n/C) + min(B, n) - 1). */
+gf_status gf_output_chunk_bound(uint64_t n, uint64_t capacity, uint64_t max_bins, uint64_t* h_out);
+
+/* core/Reservation.hpp:61-71 checkedOutputChunkBound (narrowed to 32 bits). */
+gf_status gf_checked_output_chunk_bound(uint64_t n, uint64_t capacity, uint64_t max_bins, uint32_t* h_out);
+
+/* graph/DenseBinTable.hpp:39-77 planDenseBins. h_bin_base[bins], h_fills[fills_cap]. */
+gf_status gf_plan_dense(const uint32_t* h_totals, uint32_t bins, uint32_t capacity, uint32_t* h_bin_base,
+                        uint32_t* h_fills, uint32_t fills_cap, uint32_t* h_num_out);
+
+/* graph/DenseBinTable.hpp:80-91 buildDenseTable: h_table[bins + num_out]. */
+gf_status gf_build_dense_table(const uint32_t* h_bin_base, uint32_t bins, const uint32_t* h_chunk_indices,
+                               uint32_t num_out, uint32_t* h_table);
+
+/* flow/Execution.hpp:113-124 tileCount. */
+gf_status gf_tile_count(uint32_t fill, uint32_t tile_size, uint32_t* h_out);
+
+/* flow/Execution.hpp:2377-2389 flatten loop: one descriptor per <= tile_size slice of every
+ * chunk, in chunk order. Returns GF_ERR_RANGE when `cap` descriptors do not suffice. */
+gf_status gf_flatten_tiles(const uint32_t* h_chunk_index, const uint32_t* h_fills, uint32_t n_chunks,
+                           uint32_t tile_size, gf_tile* h_tiles, uint32_t cap, uint32_t* h_n_tiles);
+
+/* Tile sizes (particles per tile) the partition kernels of this build are compiled for. */
+uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap);
+
+/* ---- dense partition: the reference's two-launch form --------------------------------------- */
+
+/* flow/Execution.hpp:870-954 PartitionClassifyKernel (graph/ClassifyKernel.hpp:33-93) over a u32
+ * key column in the fixed pool layout (slot = chunk_index * capacity + offset).
+ * Writes d_bin_ids[slot] and accumulates d_counts[0..bins) (caller zeroes them);
+ * d_counts[bins] is the status slot (set to 1 on an invalid bin). */
+gf_status gf_classify_dense_u32(void* stream, const uint32_t* d_keys, uint32_t capacity, uint64_t pool_slots,
+                                const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size, uint32_t bins,
+                                int classifier, uint32_t* d_bin_ids, uint32_t* d_counts, uint32_t* d_status);
+
+/* flow/Execution.hpp:985-1189 PartitionScatterKernel (graph/ScatterKernel.hpp:174-289).
+ * d_table = [binBase[bins], chunkIndex[R]] (buildDenseTable layout); d_next[bins] zeroed by the
+ * caller; after the launch d_next[b] == totals[b] (finalise, Execution.hpp:2715-2725).
+ * d_keys_in and d_keys_out may be the same pool column (inputs and outputs are distinct chunks). */
+gf_status gf_scatter_dense_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out, uint32_t capacity,
+                               uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size,
+                               uint32_t bins, const uint32_t* d_bin_ids, const uint32_t* d_table, uint32_t* d_next,
+                               uint32_t* d_counts, int mode, uint32_t* d_status);
+
+/* ---- dense partition: single-pass fused classify -> scan -> scatter -------------------------- */
+
+/* Scratch bytes gf_partition_fused_u32 needs for n_tiles tiles and `bins` ports. */
+gf_status gf_fused_scratch_bytes(uint32_t n_tiles, uint32_t bins, uint64_t* h_bytes);
+
+/* One launch replaces classify + host plan + scatter (flow/Execution.hpp:2363-2642): per tile,
+ * classify, rank stably inside the tile, obtain each port's exclusive prefix across tiles with a
+ * decoupled look-back, take output chunks on first touch from the caller's reservation
+ * d_reserved[n_reserved] (the outputChunkBound credit of GraphRunner.hpp:1014-1037), and write
+ * the payload. Positions inside a port follow the input order (stable partition).
+ * Outputs: d_totals[bins]; d_port_chunks[bins * max_chunks_per_port] (epoch-tagged chunk index
+ * of port b's k-th chunk; read with gf_fused_finish); d_alloc_count[1] (chunks used).
+ * `epoch` must change between launches that share the scratch (any non-zero 30-bit value). */
+gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out, uint32_t capacity,
+                                 uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size,
+                                 uint32_t bins, int classifier, const uint32_t* d_reserved, uint32_t n_reserved,
+                                 uint32_t* d_totals, unsigned long long* d_port_chunks, uint32_t max_chunks_per_port,
+                                 void* d_scratch, uint64_t scratch_bytes, uint32_t epoch, uint32_t* d_status);
+
+/* Builds the reference-layout results of a fused launch on the device: d_table[bins + R]
+ * ([binBase, chunkIndex], DenseBinTable.hpp:80-91), d_descs[R] output descriptors in bin order
+ * with their fills (Execution.hpp:2558-2581), and d_num_out[1] = R. */
+gf_status gf_fused_finish(void* stream, const uint32_t* d_totals, const unsigned long long* d_port_chunks,
+                          uint32_t bins, uint32_t capacity, uint32_t max_chunks_per_port, uint32_t epoch,
+                          uint32_t* d_table, gf_out_desc* d_descs, uint32_t desc_cap, uint32_t* d_num_out,
+                          uint32_t* d_status);
+
+/* ---- synthetic sources ---------------------------------------------------------------------- */
+
+/* Zipf(s) cumulative table over k ranks on the host: cdf[r] = sum_{i<=r} (i+1)^-s / total. */
+gf_status gf_zipf_cdf(double s, uint32_t k, double* h_cdf);
+
+/* Fills d_keys[0..n) with the key distribution `dist` at stream positions
+ * (first_id + i, 0, 0x100 + dist): uniform = first Philox draw, zipf = inverse CDF of that draw
+ * over d_cdf[bins], one_port = 0, round_robin = first_id + i. */
+gf_status gf_generate_keys_u32(void* stream, int dist, uint64_t seed, uint64_t first_id, uint64_t n, uint32_t bins,
+                               const double* d_cdf, uint32_t* d_keys);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,186 @@
+"""GPU parity of the dense partition path against the CPU oracle.
+
+Mirrors the reference's dense-bin and batching tests (tests/integration/test_dense_bins.cpp,
+test_batching.cpp:402-602, test_hash_bins.cpp:286-502 for id % B expectations):
+per-port counts and the exact plan are bit-exact; per-port multisets are bit-exact for the
+two-launch form (whose in-port order is atomic order, ScatterKernel.hpp:255-257) and per-port
+sequences are bit-exact for the fused form (stable partition in input order).
+"""
+import numpy as np
+import pytest
+import torch
+
+from graphflow_b200 import capi
+from graphflow_b200.partition import BatchError, ChunkPool, FusedPartition, PlainPartition
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+DISTS = ["uniform", "zipf", "one_port", "round_robin"]
+
+
+def _device_keys(dist, seed, n, bins, first_id=0):
+    keys = torch.zeros(max(n, 1), dtype=torch.int32, device="cuda")
+    cdf = None
+    if dist == "zipf":
+        cdf = torch.from_numpy(capi.zipf_cdf(1.1, bins)).cuda()
+    capi.check(capi.lib().gf_generate_keys_u32(None, capi.DIST_NAMES[dist], seed, first_id, n, bins,
+                                               cdf.data_ptr() if cdf is not None else None, keys.data_ptr()),
+               "generate")
+    torch.cuda.synchronize()
+    return keys[:n].cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("dist", DISTS)
+@pytest.mark.parametrize("bins", [2, 64])
+def test_key_source_matches_oracle(dist, bins):
+    n = 300_001
+    got = _device_keys(dist, 42, n, bins, first_id=5)
+    exp = O.generate_keys_u32(dist, 42, n, bins, zipf_s=1.1, first_id=5)
+    assert np.array_equal(got, exp)
+
+
+def _fill_pool(pool, chunks, fills, keys):
+    col = pool.column.cpu().numpy().view(np.uint32)
+    off = 0
+    for c, f in zip(chunks, fills):
+        col[c * pool.capacity: c * pool.capacity + f] = keys[off: off + f]
+        off += f
+    pool.column.copy_(torch.from_numpy(col.view(np.int32)))
+
+
+def _batch(n, capacity, rng, shuffle=True, ragged=True):
+    """Chunk list and fills for n particles; ragged fills and shuffled chunk indices."""
+    fills = []
+    left = n
+    while left > 0:
+        f = capacity if not ragged else int(rng.integers(1, capacity + 1))
+        f = min(f, left)
+        fills.append(f)
+        left -= f
+    chunks = list(range(len(fills)))
+    if shuffle:
+        rng.shuffle(chunks)
+    return chunks, fills
+
+
+def _outputs(pool, table, descs, bins):
+    col = pool.column.cpu().numpy().view(np.uint32)
+    per_port = [[] for _ in range(bins)]
+    for chunk, fill, b in descs:
+        per_port[int(b)].append(col[int(chunk) * pool.capacity: int(chunk) * pool.capacity + int(fill)])
+    return [np.concatenate(p) if p else np.zeros(0, np.uint32) for p in per_port]
+
+
+def _check(pool, chunks, fills, keys, bins, result, exact_order, in_snapshot):
+    totals, table, descs = result
+    counts, order = O.partition_stable_u32(keys, bins)
+    assert np.array_equal(totals, counts)
+    base, ofills, r = O.plan_dense(counts, pool.capacity)
+    assert np.array_equal(table[:bins], base)
+    assert len(descs) == r
+    assert np.array_equal(descs[:, 1], ofills)
+    assert np.array_equal(descs[:, 2], np.repeat(np.arange(bins), (counts + pool.capacity - 1) // pool.capacity))
+    assert np.array_equal(table[bins:], descs[:, 0])
+    used = descs[:, 0].astype(np.int64)
+    assert len(set(used.tolist())) == len(used)
+    assert not (set(used.tolist()) & set(chunks))
+    got = _outputs(pool, table, descs, bins)
+    start = 0
+    for b in range(bins):
+        exp = keys[order[start:start + counts[b]]]
+        start += counts[b]
+        if exact_order:
+            assert np.array_equal(got[b], exp), f"port {b}"
+        else:
+            assert np.array_equal(np.sort(got[b]), np.sort(exp)), f"port {b}"
+    # inputs untouched
+    col = pool.column.cpu().numpy().view(np.uint32)
+    for c in chunks:
+        assert np.array_equal(col[c * pool.capacity:(c + 1) * pool.capacity], in_snapshot[c])
+
+
+def _run_case(kind, n, capacity, bins, dist, tile_size, seed=42, mode=capi.SCATTER_SHARED, ragged=True):
+    rng = np.random.default_rng(seed + n + bins)
+    chunks, fills = _batch(n, capacity, rng, ragged=ragged)
+    n_in = len(chunks)
+    bound = capi.output_chunk_bound(n, capacity, bins)
+    pool = ChunkPool(n_in + bound + 3, capacity)
+    keys = O.generate_keys_u32(dist, seed, n, bins, zipf_s=1.1)
+    _fill_pool(pool, chunks, fills, keys)
+    for c in chunks:
+        pool.free.remove(c)
+    col = pool.column.cpu().numpy().view(np.uint32)
+    snap = {c: col[c * capacity:(c + 1) * capacity].copy() for c in chunks}
+    # the batch is the concatenation of the chunks in list order (tile order)
+    if kind == "plain":
+        part = PlainPartition(pool, bins, tile_size=tile_size, mode=mode)
+    else:
+        part = FusedPartition(pool, bins, tile_size=tile_size, max_batch_particles=max(n, 1))
+    result = part.run(chunks, fills)
+    _check(pool, chunks, fills, keys, bins, result, exact_order=(kind == "fused"), in_snapshot=snap)
+    return part
+
+
+@pytest.mark.parametrize("kind", ["plain", "fused"])
+@pytest.mark.parametrize("dist", DISTS)
+@pytest.mark.parametrize("bins", [2, 8, 32, 64])
+def test_partition_matches_oracle(kind, dist, bins):
+    _run_case(kind, 200_003, 8192, bins, dist, 4096)
+
+
+@pytest.mark.parametrize("kind", ["plain", "fused"])
+@pytest.mark.parametrize("n", [0, 1, 17, 4097])
+@pytest.mark.parametrize("capacity", [127, 1024])
+def test_partition_small_and_ragged(kind, n, capacity):
+    _run_case(kind, n, capacity, 8, "uniform", 1024)
+
+
+@pytest.mark.parametrize("tile_size", [1024, 2048, 4096, 8192])
+def test_fused_tile_sizes_many_tiles(tile_size):
+    # ~1000 tiles of look-back at the smallest tile size; full chunks
+    _run_case("fused", 1_000_003, 8192, 32, "zipf", tile_size, ragged=False)
+
+
+def test_plain_direct_mode_matches_oracle():
+    _run_case("plain", 100_000, 1024, 64, "uniform", 2048, mode=capi.SCATTER_DIRECT)
+
+
+def test_plain_counts_one_classify_and_one_scatter_per_batch():
+    # tests/integration/test_batching.cpp:402-450: a batch is two launches regardless of its chunks
+    part = _run_case("plain", 50_000, 1024, 2, "round_robin", 1024)
+    assert part.classify_launches == 1 and part.scatter_launches == 1
+
+
+def test_fused_repeated_batches_share_scratch():
+    rng = np.random.default_rng(3)
+    capacity, bins = 1024, 8
+    pool = ChunkPool(400, capacity)
+    fused = FusedPartition(pool, bins, tile_size=1024, max_batch_particles=60_000)
+    for it in range(4):
+        n = int(rng.integers(1, 60_000))
+        chunks = pool.acquire(-(-n // capacity))
+        fills = [capacity] * (len(chunks) - 1) + [n - capacity * (len(chunks) - 1)]
+        keys = O.generate_keys_u32("uniform", 100 + it, n, bins)
+        _fill_pool(pool, chunks, fills, keys)
+        col = pool.column.cpu().numpy().view(np.uint32)
+        snap = {c: col[c * capacity:(c + 1) * capacity].copy() for c in chunks}
+        res = fused.run(chunks, fills)
+        _check(pool, chunks, fills, keys, bins, res, True, snap)
+        pool.release(chunks)
+        pool.release([int(c) for c in res[2][:, 0]])
+
+
+def test_oversized_tile_sets_status_invalid():
+    pool = ChunkPool(4, 2048)
+    bins = 4
+    counts = torch.zeros(bins + 1, dtype=torch.int32, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    bin_ids = torch.zeros(pool.slots, dtype=torch.int32, device="cuda")
+    tiles = torch.tensor([0, 0, 2048], dtype=torch.int32, device="cuda")  # count 2048 > tile size 1024
+    capi.check(capi.lib().gf_classify_dense_u32(None, pool.ptr(), pool.capacity, pool.slots, tiles.data_ptr(), 1,
+                                                1024, bins, capi.CLS_KEY_MOD, bin_ids.data_ptr(),
+                                                counts.data_ptr(), status.data_ptr()), "classify")
+    torch.cuda.synchronize()
+    assert int(status.item()) == capi.GF_INVALID
+    assert int(counts[:bins].sum().item()) == 0
