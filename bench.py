@@ -298,11 +298,11 @@ def gpu_arm(args):
                     bench.d_tiles.data_ptr(), bench.n_tiles, args.tile, args.bins, capi.CLS_KEY_MOD,
                     bench.fused.reserved.data_ptr(), bench.bound, bench.fused.totals.data_ptr(),
                     bench.fused.port_chunks.data_ptr(), bench.fused.max_k, bench.fused.scratch.data_ptr(),
-                    bench.fused.scratch_bytes, bench.fused.next_epoch(), bench.fused.status.data_ptr()), "fused")
+                    bench.fused.scratch_bytes, bench.fused.status.data_ptr()), "fused")
                 k_end[i].record(stream)
                 capi.check(capi.lib().gf_fused_finish(
                     stream.cuda_stream, bench.fused.totals.data_ptr(), bench.fused.port_chunks.data_ptr(), args.bins,
-                    CAPACITY, bench.fused.max_k, bench.fused.epoch, bench.fused.table.data_ptr(),
+                    CAPACITY, bench.fused.max_k, bench.fused.scratch.data_ptr(), bench.fused.table.data_ptr(),
                     bench.fused.descs.data_ptr(), bench.fused.reserve_cap, bench.fused.num_out.data_ptr(),
                     bench.fused.status.data_ptr()), "finish")
             t_end.record(stream)

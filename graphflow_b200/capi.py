@@ -61,11 +61,22 @@ _SIGS = {
     "gf_scatter_dense_u32": [_VP, _VP, _VP, _U32, _U64, _VP, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _I32, _VP],
     "gf_fused_scratch_bytes": [_U32, _U32, C.POINTER(_U64)],
     "gf_partition_fused_u32": [_VP, _VP, _VP, _U32, _U64, _VP, _U32, _U32, _U32, _I32, _VP, _U32, _VP, _VP, _U32,
-                               _VP, _U64, _U32, _VP],
-    "gf_fused_finish": [_VP, _VP, _VP, _U32, _U32, _U32, _U32, _VP, _VP, _U32, _VP, _VP],
+                               _VP, _U64, _VP],
+    "gf_fused_finish": [_VP, _VP, _VP, _U32, _U32, _U32, _VP, _VP, _VP, _U32, _VP, _VP],
     "gf_zipf_cdf": [C.c_double, _U32, _VP],
     "gf_generate_keys_u32": [_VP, _I32, _U64, _U64, _U64, _U32, _VP, _VP],
+    "gf_classify_hash_r16": [_VP, _VP, _I32, _U32, _U64, _VP, _U32, _U32, _U32, _U64, _VP, _VP, _VP],
+    "gf_scatter_hash_r16": [_VP, _VP, _VP, _I32, _U32, _U64, _VP, _U32, _U32, _U32, _U64, _VP, _VP, _VP, _VP, _VP],
+    "gf_plan_device": [_VP, _VP, _U32, _U32, _VP, _U32, _VP, _VP, _U32, _VP, _VP, _VP],
+    "gf_generate_records16": [_VP, _U64, _U64, _U64, _VP, _U32, _U64, _VP, _I32],
 }
+
+LAYOUT_SOA, LAYOUT_AOS = 0, 1
+
+
+class Rec16Columns(C.Structure):
+    """gf_rec16_columns: device pointers of the 16-byte record columns (SoA) or records (AoS)."""
+    _fields_ = [("key", C.c_void_p), ("weight", C.c_void_p), ("tag", C.c_void_p), ("records", C.c_void_p)]
 
 
 def lib():
@@ -79,8 +90,9 @@ def lib():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = C.c_int
-        L.gf_supported_tile_sizes.argtypes = [_VP, _U32]
-        L.gf_supported_tile_sizes.restype = _U32
+        for name in ("gf_supported_tile_sizes", "gf_supported_hash_tile_sizes"):
+            getattr(L, name).argtypes = [_VP, _U32]
+            getattr(L, name).restype = _U32
         _lib = L
     return _lib
 
@@ -114,7 +126,7 @@ def plan_dense(totals, capacity):
     import numpy as np
     totals = np.ascontiguousarray(totals, np.uint32)
     base = np.zeros(max(totals.size, 1), np.uint32)
-    cap = int(sum(-(-int(t) // capacity) for t in totals)) if capacity else 0
+    cap = int(((totals.astype(np.int64) + capacity - 1) // capacity).sum()) if capacity else 0
     fills = np.zeros(max(cap, 1), np.uint32)
     num = _U32()
     check(lib().gf_plan_dense(totals.ctypes.data, totals.size, capacity, base.ctypes.data, fills.ctypes.data, cap,

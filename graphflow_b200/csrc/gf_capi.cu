@@ -55,13 +55,13 @@ gf_status with_shape(uint32_t tile_size, F&& f)
 {
     switch (tile_size) {
     case 1024u:
-        return f.template operator()<TileShape<kThreads, 4>>();
+        return f.template operator()<TileShape<kThreads, 4, 4>>();
     case 2048u:
-        return f.template operator()<TileShape<kThreads, 8>>();
+        return f.template operator()<TileShape<kThreads, 8, 3>>();
     case 4096u:
-        return f.template operator()<TileShape<kThreads, 16>>();
+        return f.template operator()<TileShape<kThreads, 16, 3>>();
     case 8192u:
-        return f.template operator()<TileShape<kThreads, 32>>();
+        return f.template operator()<TileShape<kThreads, 32, 1>>();
     default:
         return GF_ERR_ARGUMENT;
     }
@@ -177,14 +177,14 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
                                  uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size,
                                  uint32_t bins, int classifier, const uint32_t* d_reserved, uint32_t n_reserved,
                                  uint32_t* d_totals, unsigned long long* d_port_chunks, uint32_t max_chunks_per_port,
-                                 void* d_scratch, uint64_t scratch_bytes, uint32_t epoch, uint32_t* d_status)
+                                 void* d_scratch, uint64_t scratch_bytes, uint32_t* d_status)
 {
     uint64_t need = 0;
     if (gf_fused_scratch_bytes(n_tiles, bins, &need) != GF_OK || scratch_bytes < need || d_scratch == nullptr ||
         (reinterpret_cast<uintptr_t>(d_scratch) & 15u) != 0u)
         return GF_ERR_ARGUMENT;
     if (capacity == 0u || bins > kMaxDenseBins || !valid_tile_size(tile_size) || !valid_classifier(classifier) ||
-        epoch == 0u || (epoch & 0x3FFFFFFFu) == 0u || d_totals == nullptr || d_status == nullptr ||
+        d_totals == nullptr || d_status == nullptr ||
         (n_tiles != 0u && (d_keys_in == nullptr || d_keys_out == nullptr || d_tiles == nullptr ||
                            d_port_chunks == nullptr || max_chunks_per_port == 0u)))
         return GF_ERR_ARGUMENT;
@@ -192,13 +192,13 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
         return cuda_status(cudaMemsetAsync(d_totals, 0, sizeof(uint32_t) * bins, as_stream(stream)));
     FusedCtl* ctl = static_cast<FusedCtl*>(d_scratch);
     unsigned long long* desc = reinterpret_cast<unsigned long long*>(ctl + 1);
-    cudaError_t e = cudaMemsetAsync(ctl, 0, sizeof(FusedCtl), as_stream(stream));
+    cudaError_t e = cudaMemsetAsync(ctl, 0, kFusedCtlResetBytes, as_stream(stream));
     if (e != cudaSuccess)
         return cuda_status(e);
     return with_shape(tile_size, [&]<typename Shape>() -> gf_status {
         using Acc = U32Column;
         auto kernel = fused_partition_kernel<Shape, Acc, KeyClassify<Acc>, NoUpdate>;
-        const size_t smem = staged_smem<Shape, uint32_t>(bins, 6u) + sizeof(uint32_t) * 2;
+        const size_t smem = staged_smem<Shape, uint32_t>(bins, 6u) + sizeof(uint32_t) * (4 + 2 * Shape::kThreads);
         cudaError_t err = allow_smem(kernel, smem);
         if (err != cudaSuccess)
             return cuda_status(err);
@@ -206,17 +206,18 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
         KeyClassify<Acc> cls{key_classifier(classifier, bins)};
         kernel<<<n_tiles, Shape::kThreads, smem, as_stream(stream)>>>(
             acc, cls, NoUpdate{}, 0u, capacity, FastDiv(capacity), pool_slots, d_tiles, n_tiles, bins, d_reserved,
-            n_reserved, d_totals, d_port_chunks, max_chunks_per_port, ctl, desc, epoch, d_status);
+            n_reserved, d_totals, d_port_chunks, max_chunks_per_port, ctl, desc, d_status);
         return cuda_status(cudaGetLastError());
     });
 }
 
 gf_status gf_fused_finish(void* stream, const uint32_t* d_totals, const unsigned long long* d_port_chunks,
-                          uint32_t bins, uint32_t capacity, uint32_t max_chunks_per_port, uint32_t epoch,
+                          uint32_t bins, uint32_t capacity, uint32_t max_chunks_per_port, const void* d_scratch,
                           uint32_t* d_table, gf_out_desc* d_descs, uint32_t desc_cap, uint32_t* d_num_out,
                           uint32_t* d_status)
 {
     if (bins == 0u || capacity == 0u || d_totals == nullptr || d_table == nullptr || d_num_out == nullptr ||
+        d_scratch == nullptr ||
         (desc_cap != 0u && (d_descs == nullptr || d_port_chunks == nullptr)))
         return GF_ERR_ARGUMENT;
     constexpr int T = 1024;
@@ -225,7 +226,8 @@ gf_status gf_fused_finish(void* stream, const uint32_t* d_totals, const unsigned
     if (e != cudaSuccess)
         return cuda_status(e);
     fused_finish_kernel<T><<<1, T, smem, as_stream(stream)>>>(d_totals, d_port_chunks, bins, capacity,
-                                                              FastDiv(capacity), max_chunks_per_port, epoch, d_table,
+                                                              FastDiv(capacity), max_chunks_per_port,
+                                                              static_cast<const FusedCtl*>(d_scratch), d_table,
                                                               d_descs, desc_cap, d_num_out, d_status);
     return cuda_status(cudaGetLastError());
 }

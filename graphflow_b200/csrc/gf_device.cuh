@@ -163,24 +163,10 @@ GF_D void set_status(uint32_t* status, uint32_t code)
         atomicCAS(status, 0u, code);
 }
 
-// Every wait in this library is bounded. `ready()` is polled until it returns true, at most
-// kSpinLimit times (about 50 ms with the back-off); the wait also gives up as soon as the
-// batch's status word reports a failure, so one failed tile cannot make the others spin.
-// Returns false when the wait gave up; the caller then records GF_ERR_TIMEOUT.
+// Every wait in this library is bounded: at most kSpinLimit polls (about 50 ms with the
+// back-off), and a wait also gives up as soon as the batch's status word reports a failure, so
+// one failed tile cannot make the others spin. A wait that gives up records GF_ERR_TIMEOUT.
 constexpr uint32_t kSpinLimit = 1u << 20;
-
-template <typename Ready>
-GF_D bool bounded_wait(Ready ready, const uint32_t* status)
-{
-    for (uint32_t polls = 0; polls < kSpinLimit; ++polls) {
-        if (ready())
-            return true;
-        if ((polls & 255u) == 255u && status != nullptr && ld_relaxed_u32(status) != 0u)
-            return false;
-        __nanosleep(polls < 64u ? 20u : 40u);
-    }
-    return false;
-}
 
 // ---------------------------------------------------------------------------------------------
 // Built-in classifiers of the kernel-level sweeps and the kernel-axis examples

@@ -43,14 +43,23 @@ struct KeyClassify {
     GF_D uint32_t operator()(const typename Access::Payload& p) const { return cls(Access::key(p)); }
 };
 
-template <int THREADS, int IPT>
+// THREADS threads, IPT items per thread, MINB resident CTAs per SM requested from the register
+// allocator (__launch_bounds__ minBlocks).
+template <int THREADS, int IPT, int MINB = 1>
 struct TileShape {
     static constexpr int kThreads = THREADS;
     static constexpr int kIpt = IPT;
+    static constexpr int kMinBlocks = MINB;
     static constexpr int kWarps = THREADS / 32;
     static constexpr int kTile = THREADS * IPT;
     GF_D static uint32_t item(int w, int r, int lane) { return (uint32_t)(w * 32 * IPT + r * 32 + lane); }
 };
+
+// An item's bin and its rank inside its warp's slice share one register: bin in bits 0..15
+// (0xFFFF = no bin), rank in bits 16..31. Dense partitions therefore take at most 65535 bins.
+constexpr uint32_t kNoBin16 = 0xFFFFu;
+GF_HD uint32_t bp_bin(uint32_t bp) { return bp & 0xFFFFu; }
+GF_HD uint32_t bp_pos(uint32_t bp) { return bp >> 16; }
 
 constexpr uint32_t kNoBin = 0xFFFFFFFFu;
 constexpr uint32_t kNoChunk = 0xFFFFFFFFu;
@@ -98,12 +107,11 @@ GF_D uint32_t block_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n
     return total;
 }
 
-// Stable in-tile ranking. bins[r] is the bin of item (w, r, lane) or kNoBin. On return pos[r] is
-// the item's rank among the items of its bin inside its warp's slice, and warp_cnt[w*B + b] holds
-// the number of items of bin b in warp w's slice.
+// Stable in-tile ranking. bp[r] holds the bin of item (w, r, lane) in its low half (kNoBin16 for
+// none). On return its high half holds the item's rank among the items of its bin inside its
+// warp's slice, and warp_cnt[w*B + b] holds the number of items of bin b in warp w's slice.
 template <typename Shape>
-GF_D void warp_rank(const uint32_t (&bins)[Shape::kIpt], uint32_t (&pos)[Shape::kIpt], uint32_t* warp_cnt,
-                    uint32_t B)
+GF_D void warp_rank(uint32_t (&bp)[Shape::kIpt], uint32_t* warp_cnt, uint32_t B)
 {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     uint32_t* cnt = warp_cnt + (size_t)w * B;
@@ -113,14 +121,14 @@ GF_D void warp_rank(const uint32_t (&bins)[Shape::kIpt], uint32_t (&pos)[Shape::
     const uint32_t lt = lanemask_lt();
 #pragma unroll
     for (int r = 0; r < Shape::kIpt; ++r) {
-        const uint32_t bin = bins[r];
+        const uint32_t bin = bp_bin(bp[r]);
         const uint32_t peers = __match_any_sync(0xFFFFFFFFu, bin);
         uint32_t base = 0;
-        if (bin != kNoBin)
+        if (bin != kNoBin16)
             base = cnt[bin];
         __syncwarp();
-        if (bin != kNoBin) {
-            pos[r] = base + __popc(peers & lt);
+        if (bin != kNoBin16) {
+            bp[r] = bin | ((base + __popc(peers & lt)) << 16);
             if (lane == 31 - __clz(peers))
                 cnt[bin] = base + __popc(peers);
         }
@@ -150,7 +158,7 @@ GF_D void warp_offsets(uint32_t* warp_cnt, uint32_t* bin_tot, uint32_t B)
 // counts[B] is the status slot.
 // ---------------------------------------------------------------------------------------------
 template <typename Shape, typename Access, typename Classify>
-__global__ void __launch_bounds__(Shape::kThreads) classify_kernel(Access acc, Classify classify, uint32_t capacity,
+__global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) classify_kernel(Access acc, Classify classify, uint32_t capacity,
                                                                    uint64_t pool_slots, const gf_tile* tiles,
                                                                    uint32_t n_tiles, uint32_t B, uint32_t* bin_ids,
                                                                    uint32_t* counts, uint32_t* status)
@@ -211,7 +219,7 @@ __global__ void __launch_bounds__(Shape::kThreads) classify_kernel(Access acc, C
 // out slot = table[B + table[bin] + j / C] * C + j % C.
 // ---------------------------------------------------------------------------------------------
 template <typename Shape, typename Access, typename Update>
-__global__ void __launch_bounds__(Shape::kThreads) scatter_kernel(Access acc, Update update, uint64_t seed_mixed,
+__global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) scatter_kernel(Access acc, Update update, uint64_t seed_mixed,
                                                                   uint32_t capacity, FastDiv fdc, uint64_t pool_slots,
                                                                   const gf_tile* tiles, uint32_t n_tiles, uint32_t B,
                                                                   const uint32_t* bin_ids, const uint32_t* table,
@@ -233,25 +241,26 @@ __global__ void __launch_bounds__(Shape::kThreads) scatter_kernel(Access acc, Up
         const uint64_t base = (uint64_t)tile.chunk_index * capacity + tile.tile_offset;
         const bool tile_ok = tile.count <= (uint32_t)Shape::kTile && base + tile.count <= pool_slots &&
                              tile.tile_offset + tile.count <= capacity;
-        uint32_t bins[Shape::kIpt], pos[Shape::kIpt];
+        uint32_t bp[Shape::kIpt];
         P p[Shape::kIpt];
 #pragma unroll
         for (int r = 0; r < Shape::kIpt; ++r) {
             const uint32_t i = Shape::item(w, r, lane);
-            bins[r] = kNoBin;
+            bp[r] = kNoBin16;
             if (tile_ok && i < tile.count) {
-                bins[r] = __ldg(bin_ids + base + i);
+                const uint32_t b = __ldg(bin_ids + base + i);
                 p[r] = acc.load(base + i);
-                if (bins[r] >= B) {
+                if (b >= B) {
                     counts[B] = 1u;
                     set_status(status, GF_INVALID);
-                    bins[r] = kNoBin;
+                } else {
+                    bp[r] = b;
                 }
             }
         }
         if (!tile_ok && threadIdx.x == 0)
             set_status(status, GF_INVALID);
-        warp_rank<Shape>(bins, pos, warp_cnt, B);
+        warp_rank<Shape>(bp, warp_cnt, B);
         __syncthreads();
         warp_offsets<Shape>(warp_cnt, bin_tot, B);
         __syncthreads();
@@ -261,16 +270,17 @@ __global__ void __launch_bounds__(Shape::kThreads) scatter_kernel(Access acc, Up
                 gbase[b] = atomicAdd(&next[b], bin_tot[b]) - bin_excl[b];
 #pragma unroll
         for (int r = 0; r < Shape::kIpt; ++r) {
-            if (bins[r] == kNoBin)
-                continue;
-            const uint32_t q = bin_excl[bins[r]] + warp_cnt[(size_t)w * B + bins[r]] + pos[r];
-            const uint32_t res = update(bins[r], p[r], seed_mixed);
-            if (res != kUpdateSuccess) {
-                counts[B] = 1u;
-                set_status(status, res == kUpdateOverflow ? GF_OVERFLOW : GF_INVALID);
+            const uint32_t b = bp_bin(bp[r]);
+            if (b != kNoBin16) {
+                const uint32_t q = bin_excl[b] + warp_cnt[(size_t)w * B + b] + bp_pos(bp[r]);
+                const uint32_t res = update(b, p[r], seed_mixed);
+                if (res != kUpdateSuccess) {
+                    counts[B] = 1u;
+                    set_status(status, res == kUpdateOverflow ? GF_OVERFLOW : GF_INVALID);
+                }
+                stage[q] = p[r];
+                stage_bin[q] = b;
             }
-            stage[q] = p[r];
-            stage_bin[q] = bins[r];
         }
         __syncthreads();
         for (uint32_t q = threadIdx.x; q < n_valid; q += Shape::kThreads) {
@@ -290,7 +300,7 @@ __global__ void __launch_bounds__(Shape::kThreads) scatter_kernel(Access acc, Up
 
 // Scatter (Direct): flow/Execution.hpp:1034-1095, one device atomic per particle.
 template <typename Shape, typename Access, typename Update>
-__global__ void __launch_bounds__(Shape::kThreads) scatter_direct_kernel(Access acc, Update update,
+__global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) scatter_direct_kernel(Access acc, Update update,
                                                                          uint64_t seed_mixed, uint32_t capacity,
                                                                          FastDiv fdc, uint64_t pool_slots,
                                                                          const gf_tile* tiles, uint32_t n_tiles,
@@ -348,22 +358,155 @@ __global__ void __launch_bounds__(Shape::kThreads) scatter_direct_kernel(Access 
 // CTA waits on belongs to a CTA that is already running; every wait is still bounded.
 // ---------------------------------------------------------------------------------------------
 struct FusedCtl {
-    uint32_t tile_counter;
-    uint32_t alloc_cursor;
-    uint32_t pad[14];
+    uint32_t tile_counter; // reset by the host before every launch
+    uint32_t alloc_cursor; // reset by the host before every launch
+    uint32_t done;         // reset by the host before every launch
+    uint32_t epoch;        // persistent: epoch of the last completed launch (0 = none yet)
+    uint32_t pad[12];
 };
+constexpr uint32_t kFusedCtlResetBytes = 3u * sizeof(uint32_t);
+
+GF_HD uint32_t next_epoch(uint32_t e) { return (e % 0x3FFFFFFFu) + 1u; } // 30-bit, never 0
 
 GF_HD unsigned long long make_desc(uint32_t epoch, uint32_t flag, uint32_t value)
 {
     return ((unsigned long long)((epoch << 2) | flag) << 32) | value;
 }
 
+constexpr uint32_t kClaimed = 0xFFFFFFFEu;
+
+// Back-off step of a bounded wait: false when the wait must give up (poll budget spent, or the
+// batch's status word already reports a failure).
+GF_D bool poll_again(uint32_t& polls, const uint32_t* status)
+{
+    if (++polls >= kSpinLimit)
+        return false;
+    if ((polls & 255u) == 0u && ld_relaxed_u32(status) != 0u)
+        return false;
+    __nanosleep(polls < 64u ? 20u : 40u);
+    return true;
+}
+
+// Chunk k of a port's output range, taken on first touch: whichever tile touches it first claims
+// the slot with a CAS (tagging it with this launch's epoch), takes the next reserved chunk and
+// publishes it; later touchers read it, waiting (bounded) only while a claim is in flight.
+// Because any toucher may claim, no tile waits for the look-back of the tile that owns the
+// chunk's first position.
+GF_D uint32_t claim_chunk(unsigned long long* slot, uint32_t epoch, FusedCtl* ctl, const uint32_t* reserved,
+                          uint32_t n_reserved, uint32_t* status)
+{
+    const unsigned long long tag = (unsigned long long)epoch << 32;
+    unsigned long long v = ld_relaxed_u64(slot);
+    if ((uint32_t)(v >> 32) != epoch) {
+        const unsigned long long old = atomicCAS(slot, v, tag | kClaimed);
+        if (old == v) {
+            const uint32_t idx = atomicAdd(&ctl->alloc_cursor, 1u);
+            uint32_t chunk = kNoChunk;
+            if (idx < n_reserved)
+                chunk = __ldg(reserved + idx);
+            else
+                set_status(status, GF_OVERFLOW);
+            st_relaxed_u64(slot, tag | chunk);
+            return chunk;
+        }
+        v = old;
+    }
+    uint32_t polls = 0;
+    while ((uint32_t)(v >> 32) != epoch || (uint32_t)v == kClaimed) {
+        if (!poll_again(polls, status)) {
+            set_status(status, GF_ERR_TIMEOUT);
+            return kNoChunk;
+        }
+        v = ld_relaxed_u64(slot);
+    }
+    return (uint32_t)v;
+}
+
+// Block-wide decoupled look-back over the per-(tile, bin) descriptors of tile t > 0.
+// Pass p covers bins [p*P, p*P + P) with P = min(B, THREADS); each of the W = THREADS / P thread
+// groups reads one predecessor, so one round reads a window of W predecessors for P bins at once.
+// Per bin, the window is reduced up to the nearest inclusive prefix; bins without one move the
+// window further back. On return acc[b] holds bin b's exclusive prefix over tiles 0..t-1.
+template <int THREADS>
+GF_D void block_lookback(const unsigned long long* desc, uint32_t t, uint32_t B, uint32_t epoch_hi, uint32_t* acc,
+                         uint32_t* done, uint32_t* lb_flag, uint32_t* lb_val, uint32_t* status)
+{
+    const uint32_t P = B < (uint32_t)THREADS ? B : (uint32_t)THREADS;
+    const uint32_t W = (uint32_t)THREADS / P;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane_bin = tid % P, woff = tid / P;
+    for (uint32_t pass = 0; pass < B; pass += P) {
+        const uint32_t b = pass + lane_bin;
+        const bool owner = tid < P && b < B;
+        if (owner) {
+            acc[b] = 0u;
+            done[b] = 0u;
+        }
+        __syncthreads();
+        int64_t pred_base = (int64_t)t - 1;
+        for (;;) {
+            uint32_t flag = 2u, val = 0u;
+            if (woff < W && b < B && done[b] == 0u) {
+                const int64_t pred = pred_base - (int64_t)woff;
+                if (pred >= 0) {
+                    const unsigned long long* d = desc + (size_t)pred * B + b;
+                    unsigned long long v = ld_relaxed_u64(d);
+                    uint32_t polls = 0;
+                    bool ok = true;
+                    while ((uint32_t)(v >> 34) != epoch_hi || ((v >> 32) & 3u) == 0u) {
+                        if (!poll_again(polls, status)) {
+                            ok = false;
+                            break;
+                        }
+                        v = ld_relaxed_u64(d);
+                    }
+                    if (ok) {
+                        flag = (uint32_t)(v >> 32) & 3u;
+                        val = (uint32_t)v;
+                    } else {
+                        set_status(status, GF_ERR_TIMEOUT);
+                    }
+                }
+            }
+            lb_flag[tid] = flag;
+            lb_val[tid] = val;
+            __syncthreads();
+            if (owner && done[b] == 0u) {
+                uint32_t a = acc[b];
+                for (uint32_t j = 0; j < W; ++j) {
+                    a += lb_val[j * P + lane_bin];
+                    if (lb_flag[j * P + lane_bin] == 2u) {
+                        done[b] = 1u;
+                        break;
+                    }
+                }
+                acc[b] = a;
+            }
+            if (__syncthreads_and(!owner || done[b] != 0u))
+                break;
+            pred_base -= (int64_t)W;
+        }
+    }
+}
+
+// Called once per CTA by thread 0's block after its last global access: the last CTA of the
+// launch publishes the launch epoch as completed.
+GF_D void fused_retire(FusedCtl* ctl, uint32_t epoch)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ctl->done, 1u) + 1u == gridDim.x)
+            atomicExch(&ctl->epoch, epoch);
+    }
+}
+
 template <typename Shape, typename Access, typename Classify, typename Update>
-__global__ void __launch_bounds__(Shape::kThreads) fused_partition_kernel(
+__global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_partition_kernel(
     Access acc, Classify classify, Update update, uint64_t seed_mixed, uint32_t capacity, FastDiv fdc,
     uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B, const uint32_t* reserved,
     uint32_t n_reserved, uint32_t* totals, unsigned long long* port_chunks, uint32_t max_k, FusedCtl* ctl,
-    unsigned long long* desc, uint32_t epoch, uint32_t* status)
+    unsigned long long* desc, uint32_t* status)
 {
     using P = typename Access::Payload;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -376,17 +519,26 @@ __global__ void __launch_bounds__(Shape::kThreads) fused_partition_kernel(
     uint32_t* k0 = gbase + B;                                 // [B]
     uint32_t* chunk_lo = k0 + B;                              // [B]
     uint32_t* chunk_hi = chunk_lo + B;                        // [B]
-    uint32_t* scan_tmp = chunk_hi + B;                        // [W+1]
-    uint32_t* s_tile = scan_tmp + Shape::kWarps + 1;          // [1]
+    uint32_t* lb_flag = chunk_hi + B;                         // [THREADS]
+    uint32_t* lb_val = lb_flag + Shape::kThreads;             // [THREADS]
+    uint32_t* scan_tmp = lb_val + Shape::kThreads;            // [W+1]
+    uint32_t* s_tile = scan_tmp + Shape::kWarps + 1;          // [3]
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const uint32_t epoch_hi = epoch & 0x3FFFFFFFu;
 
-    if (threadIdx.x == 0)
-        *s_tile = atomicAdd(&ctl->tile_counter, 1u);
+    // The launch epoch is the successor of the last completed launch's epoch; the last CTA to
+    // finish publishes it, so CUDA-graph replays of this launch get a fresh epoch each time.
+    if (threadIdx.x == 0) {
+        s_tile[0] = atomicAdd(&ctl->tile_counter, 1u);
+        s_tile[1] = next_epoch(ld_relaxed_u32(&ctl->epoch));
+    }
     __syncthreads();
-    const uint32_t t = *s_tile;
-    if (t >= n_tiles)
+    const uint32_t t = s_tile[0];
+    const uint32_t epoch = s_tile[1];
+    const uint32_t epoch_hi = epoch;
+    if (t >= n_tiles) {
+        fused_retire(ctl, epoch);
         return;
+    }
 
     const gf_tile tile = tiles[t];
     const uint64_t base = (uint64_t)tile.chunk_index * capacity + tile.tile_offset;
@@ -396,12 +548,12 @@ __global__ void __launch_bounds__(Shape::kThreads) fused_partition_kernel(
         set_status(status, GF_INVALID);
 
     // 1. load and classify
-    uint32_t bins[Shape::kIpt], pos[Shape::kIpt];
+    uint32_t bp[Shape::kIpt];
     P p[Shape::kIpt];
 #pragma unroll
     for (int r = 0; r < Shape::kIpt; ++r) {
         const uint32_t i = Shape::item(w, r, lane);
-        bins[r] = kNoBin;
+        bp[r] = kNoBin16;
         if (tile_ok && i < tile.count)
             p[r] = acc.load(base + i);
     }
@@ -409,16 +561,15 @@ __global__ void __launch_bounds__(Shape::kThreads) fused_partition_kernel(
     for (int r = 0; r < Shape::kIpt; ++r) {
         const uint32_t i = Shape::item(w, r, lane);
         if (tile_ok && i < tile.count) {
-            uint32_t b = classify(p[r]);
-            if (b >= B) {
+            const uint32_t b = classify(p[r]);
+            if (b >= B)
                 set_status(status, GF_INVALID);
-                b = kNoBin;
-            }
-            bins[r] = b;
+            else
+                bp[r] = b;
         }
     }
     // 2. stable rank inside the tile, per-bin tile totals
-    warp_rank<Shape>(bins, pos, warp_cnt, B);
+    warp_rank<Shape>(bp, warp_cnt, B);
     __syncthreads();
     warp_offsets<Shape>(warp_cnt, bin_tot, B);
     __syncthreads();
@@ -428,96 +579,63 @@ __global__ void __launch_bounds__(Shape::kThreads) fused_partition_kernel(
     for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads)
         st_relaxed_u64(my_desc + b, make_desc(epoch_hi, t == 0 ? 2u : 1u, bin_tot[b]));
     const uint32_t n_valid = block_exclusive_scan<Shape::kThreads>(bin_tot, bin_excl, B, scan_tmp);
-    for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads) {
-        uint32_t excl = 0;
-        bool ok = true;
-        for (int64_t pred = (int64_t)t - 1; pred >= 0; --pred) {
-            const unsigned long long* d = desc + (size_t)pred * B + b;
-            unsigned long long v = 0;
-            ok = bounded_wait(
-                [&] {
-                    v = ld_relaxed_u64(d);
-                    return (uint32_t)(v >> 34) == epoch_hi && ((v >> 32) & 3u) != 0u;
-                },
-                status);
-            if (!ok)
-                break;
-            excl += (uint32_t)v;
-            if (((v >> 32) & 3u) == 2u)
-                break;
-        }
-        if (!ok) {
-            set_status(status, GF_ERR_TIMEOUT);
-            __threadfence();
-            excl = 0xFFFFFFFFu;
-        }
-        if (t != 0)
-            st_relaxed_u64(my_desc + b, make_desc(epoch_hi, 2u, excl + bin_tot[b]));
-        if (t + 1 == n_tiles)
-            totals[b] = excl + bin_tot[b];
-        gbase[b] = excl - bin_excl[b];
 
-        // 4. output chunks of this bin's range [excl, excl + tot): take on first touch
+    // 4. apply the updater and stage the tile in bin order (tile-local positions only)
+#pragma unroll
+    for (int r = 0; r < Shape::kIpt; ++r) {
+        const uint32_t b = bp_bin(bp[r]);
+        if (b != kNoBin16) {
+            const uint32_t q = bin_excl[b] + warp_cnt[(size_t)w * B + b] + bp_pos(bp[r]);
+            const uint32_t res = update(b, p[r], seed_mixed);
+            if (res != kUpdateSuccess)
+                set_status(status, res == kUpdateOverflow ? GF_OVERFLOW : GF_INVALID);
+            stage[q] = p[r];
+            stage_bin[q] = b;
+        }
+    }
+
+    // 5. block-wide windowed look-back: every pass covers P bins x W predecessors with all
+    //    threads loading in parallel; excl[b] accumulates in gbase[b], done flags in chunk_lo[b]
+    if (t != 0u)
+        block_lookback<Shape::kThreads>(desc, t, B, epoch_hi, gbase, chunk_lo, lb_flag, lb_val, status);
+    else
+        for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads)
+            gbase[b] = 0u;
+    __syncthreads();
+
+    // 6. publish the inclusive prefixes, then take this range's output chunks by first-touch claim
+    for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads) {
+        const uint32_t excl = gbase[b], tot = bin_tot[b];
+        if (t != 0u)
+            st_relaxed_u64(my_desc + b, make_desc(epoch_hi, 2u, excl + tot));
+        if (t + 1u == n_tiles)
+            totals[b] = excl + tot;
+        gbase[b] = excl - bin_excl[b];
         uint32_t lo = kNoChunk, hi = kNoChunk;
-        const uint32_t tot = bin_tot[b];
-        if (tot != 0u && ok) {
+        if (tot != 0u) {
             const uint32_t ka = fdc.div(excl), kb = fdc.div(excl + tot - 1u);
             k0[b] = ka;
-            for (uint32_t k = ka; k <= kb; ++k) {
-                uint32_t chunk = kNoChunk;
-                if (k >= max_k) {
-                    set_status(status, GF_OVERFLOW);
-                } else if ((uint64_t)k * capacity >= excl) {
-                    const uint32_t idx = atomicAdd(&ctl->alloc_cursor, 1u);
-                    if (idx < n_reserved) {
-                        chunk = __ldg(reserved + idx);
-                        st_relaxed_u64(port_chunks + (size_t)b * max_k + k,
-                                       ((unsigned long long)epoch << 32) | chunk);
-                    } else {
-                        set_status(status, GF_OVERFLOW);
-                    }
-                } else {
-                    const unsigned long long* src = port_chunks + (size_t)b * max_k + k;
-                    unsigned long long v = 0;
-                    if (bounded_wait(
-                            [&] {
-                                v = ld_relaxed_u64(src);
-                                return (uint32_t)(v >> 32) == epoch;
-                            },
-                            status))
-                        chunk = (uint32_t)v;
-                    else
-                        set_status(status, GF_ERR_TIMEOUT);
-                }
-                if (k == ka)
-                    lo = chunk;
-                else
-                    hi = chunk;
+            if (kb >= max_k) {
+                set_status(status, GF_OVERFLOW);
+            } else {
+                lo = claim_chunk(port_chunks + (size_t)b * max_k + ka, epoch, ctl, reserved, n_reserved, status);
+                if (kb != ka)
+                    hi = claim_chunk(port_chunks + (size_t)b * max_k + kb, epoch, ctl, reserved, n_reserved,
+                                     status);
             }
         }
         chunk_lo[b] = lo;
         chunk_hi[b] = hi;
     }
-
-    // 5. apply the updater and stage the tile in bin order
-#pragma unroll
-    for (int r = 0; r < Shape::kIpt; ++r) {
-        if (bins[r] == kNoBin)
-            continue;
-        const uint32_t q = bin_excl[bins[r]] + warp_cnt[(size_t)w * B + bins[r]] + pos[r];
-        const uint32_t res = update(bins[r], p[r], seed_mixed);
-        if (res != kUpdateSuccess)
-            set_status(status, res == kUpdateOverflow ? GF_OVERFLOW : GF_INVALID);
-        stage[q] = p[r];
-        stage_bin[q] = bins[r];
-    }
     if (threadIdx.x == 0)
-        *s_tile = ld_relaxed_u32(status);
+        s_tile[2] = ld_relaxed_u32(status);
     __syncthreads();
-    if (*s_tile != 0u)
-        return; // the batch failed somewhere: write nothing, the host discards it
+    if (s_tile[2] != 0u) {
+        fused_retire(ctl, epoch); // the batch failed somewhere: write nothing, the host discards it
+        return;
+    }
 
-    // 6. coalesced write-out
+    // 7. coalesced write-out
     for (uint32_t q = threadIdx.x; q < n_valid; q += Shape::kThreads) {
         const uint32_t b = stage_bin[q];
         const uint32_t j = gbase[b] + q;
@@ -531,6 +649,7 @@ __global__ void __launch_bounds__(Shape::kThreads) fused_partition_kernel(
         else
             set_status(status, GF_OVERFLOW);
     }
+    fused_retire(ctl, epoch);
 }
 
 // Device form of planDenseBins + buildDenseTable + the output-descriptor loop
@@ -539,10 +658,11 @@ template <int THREADS>
 __global__ void __launch_bounds__(THREADS) fused_finish_kernel(const uint32_t* totals,
                                                                const unsigned long long* port_chunks, uint32_t B,
                                                                uint32_t capacity, FastDiv fdc, uint32_t max_k,
-                                                               uint32_t epoch, uint32_t* table, gf_out_desc* descs,
+                                                               const FusedCtl* ctl, uint32_t* table, gf_out_desc* descs,
                                                                uint32_t desc_cap, uint32_t* num_out, uint32_t* status)
 {
     extern __shared__ uint32_t smem[];
+    const uint32_t epoch = ctl->epoch;
     uint32_t* nck = smem;      // [seg]
     uint32_t* base = nck + 4096; // [seg]
     uint32_t* tmp = base + 4096;  // [W+1]
@@ -583,7 +703,7 @@ __global__ void __launch_bounds__(THREADS) fused_finish_kernel(const uint32_t* t
 
 // Synthetic key source (uniform / Zipf / one port / round robin) at stream positions
 // (first_id + i, 0, 0x100 + dist).
-__global__ void generate_keys_kernel(int dist, uint64_t seed_mixed, uint64_t first_id, uint64_t n, uint32_t bins,
+static __global__ void generate_keys_kernel(int dist, uint64_t seed_mixed, uint64_t first_id, uint64_t n, uint32_t bins,
                                      const double* cdf, uint32_t* keys)
 {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {

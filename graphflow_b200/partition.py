@@ -91,7 +91,12 @@ class PlainPartition(_Common):
         self.scatter_launches = 0
 
     def run(self, chunks, fills, stream=None):
-        """One batch. Returns (totals, table, output descriptors (chunk, fill, bin))."""
+        """One batch. Returns (totals, table, output descriptors (chunk, fill, bin)). Every
+        device operation of the batch, readbacks included, is ordered on `stream`."""
+        with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
+            return self._run(chunks, fills, stream)
+
+    def _run(self, chunks, fills, stream):
         n = int(np.sum(np.asarray(fills, np.uint64)))
         tiles, d_tiles = self._tiles(chunks, fills)
         s = _stream_ptr(stream)
@@ -161,31 +166,30 @@ class FusedPartition(_Common):
         self.table = torch.zeros(bins + max(self.reserve_cap, 1), dtype=torch.int32, device=self.dev)
         self.descs = torch.zeros(3 * max(self.reserve_cap, 1), dtype=torch.int32, device=self.dev)
         self.num_out = torch.zeros(1, dtype=torch.int32, device=self.dev)
-        self.epoch = 0
         self.launches = 0
-
-    def next_epoch(self):
-        self.epoch = (self.epoch % 0x3FFFFFFF) + 1
-        return self.epoch
 
     def enqueue(self, d_tiles, n_tiles, n_reserved, stream=None):
         """Enqueue the fused launch and the finish (no host synchronisation)."""
         s = _stream_ptr(stream)
         L = capi.lib()
-        epoch = self.next_epoch()
         capi.check(L.gf_partition_fused_u32(s, self.pool.ptr(), self.pool.ptr(), self.pool.capacity, self.pool.slots,
                                             d_tiles.data_ptr() if n_tiles else None, n_tiles, self.tile_size,
                                             self.bins, self.cls, self.reserved.data_ptr(), n_reserved,
                                             self.totals.data_ptr(), self.port_chunks.data_ptr(), self.max_k,
-                                            self.scratch.data_ptr(), self.scratch_bytes, epoch,
+                                            self.scratch.data_ptr(), self.scratch_bytes,
                                             self.status.data_ptr()), "fused partition")
         capi.check(L.gf_fused_finish(s, self.totals.data_ptr(), self.port_chunks.data_ptr(), self.bins,
-                                     self.pool.capacity, self.max_k, epoch, self.table.data_ptr(),
+                                     self.pool.capacity, self.max_k, self.scratch.data_ptr(), self.table.data_ptr(),
                                      self.descs.data_ptr(), self.reserve_cap, self.num_out.data_ptr(),
                                      self.status.data_ptr()), "fused finish")
         self.launches += 1
 
     def run(self, chunks, fills, stream=None):
+        """One batch on `stream`; returns (totals, table, output descriptors)."""
+        with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
+            return self._run(chunks, fills, stream)
+
+    def _run(self, chunks, fills, stream):
         n = int(np.sum(np.asarray(fills, np.uint64)))
         if n > self.max_batch:
             raise BatchError("fused partition: batch exceeds the configured maximum")

@@ -123,22 +123,67 @@ gf_status gf_fused_scratch_bytes(uint32_t n_tiles, uint32_t bins, uint64_t* h_by
  * decoupled look-back, take output chunks on first touch from the caller's reservation
  * d_reserved[n_reserved] (the outputChunkBound credit of GraphRunner.hpp:1014-1037), and write
  * the payload. Positions inside a port follow the input order (stable partition).
- * Outputs: d_totals[bins]; d_port_chunks[bins * max_chunks_per_port] (epoch-tagged chunk index
- * of port b's k-th chunk; read with gf_fused_finish); d_alloc_count[1] (chunks used).
- * `epoch` must change between launches that share the scratch (any non-zero 30-bit value). */
+ * Outputs: d_totals[bins] and d_port_chunks[bins * max_chunks_per_port] (epoch-tagged chunk
+ * index of port b's k-th chunk; gf_fused_finish turns them into the reference's table).
+ * d_scratch (gf_fused_scratch_bytes, 16-byte aligned) must be zero-filled before its first use
+ * and then stays owned by this call site: it carries the launch epoch from one launch to the
+ * next, which lets the launch be replayed from a CUDA graph. Launches sharing one scratch must
+ * not overlap on the GPU. */
 gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out, uint32_t capacity,
                                  uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size,
                                  uint32_t bins, int classifier, const uint32_t* d_reserved, uint32_t n_reserved,
                                  uint32_t* d_totals, unsigned long long* d_port_chunks, uint32_t max_chunks_per_port,
-                                 void* d_scratch, uint64_t scratch_bytes, uint32_t epoch, uint32_t* d_status);
+                                 void* d_scratch, uint64_t scratch_bytes, uint32_t* d_status);
 
-/* Builds the reference-layout results of a fused launch on the device: d_table[bins + R]
- * ([binBase, chunkIndex], DenseBinTable.hpp:80-91), d_descs[R] output descriptors in bin order
- * with their fills (Execution.hpp:2558-2581), and d_num_out[1] = R. */
+/* Builds the reference-layout results of the last fused launch on `d_scratch` on the device:
+ * d_table[bins + R] ([binBase, chunkIndex], DenseBinTable.hpp:80-91), d_descs[R] output
+ * descriptors in bin order with their fills (Execution.hpp:2558-2581), and d_num_out[1] = R. */
 gf_status gf_fused_finish(void* stream, const uint32_t* d_totals, const unsigned long long* d_port_chunks,
-                          uint32_t bins, uint32_t capacity, uint32_t max_chunks_per_port, uint32_t epoch,
+                          uint32_t bins, uint32_t capacity, uint32_t max_chunks_per_port, const void* d_scratch,
                           uint32_t* d_table, gf_out_desc* d_descs, uint32_t desc_cap, uint32_t* d_num_out,
                           uint32_t* d_status);
+
+/* ---- hash partition of 16-byte records (large port counts) ---------------------------------- */
+
+/* Columns of the 16-byte record {u64 key, f32 weight, u32 tag}: SoA uses key/weight/tag, AoS
+ * uses `records` (16-byte aligned, 16 bytes per slot). Pointers are device pointers; the struct
+ * itself is passed from host memory. */
+typedef struct gf_rec16_columns {
+    uint64_t* key;
+    float* weight;
+    uint32_t* tag;
+    void* records;
+} gf_rec16_columns;
+enum { GF_LAYOUT_SOA = 0, GF_LAYOUT_AOS = 1 };
+
+/* Tile sizes the hash kernels are compiled for (the shared table has 2 x tile entries). */
+uint32_t gf_supported_hash_tile_sizes(uint32_t* h_sizes, uint32_t cap);
+
+/* flow/Execution.hpp:1208-1307 PartitionHashClassifyKernel (graph/HashClassifyKernel.hpp:35-117).
+ * bin = unmix64(key) ^ salt (< bins, else the status slot d_counts[bins] is set). A shared-memory
+ * open-addressing table aggregates the tile (graph/BinTable.hpp:29-137). d_bin_ids may be NULL
+ * (nothing stored: the scatter then recomputes the bin from the key). */
+gf_status gf_classify_hash_r16(void* stream, const gf_rec16_columns* h_cols, int layout, uint32_t capacity,
+                               uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size,
+                               uint32_t bins, uint64_t salt, uint32_t* d_bin_ids, uint32_t* d_counts,
+                               uint32_t* d_status);
+
+/* flow/Execution.hpp:1336-1502 PartitionHashScatterKernel (graph/HashScatterKernel.hpp:34-183):
+ * rebuild the tile table from d_bin_ids (or recompute bins when NULL), reserve one range per
+ * occupied entry on d_next[bin], write through d_table = [binBase[bins], chunkIndex[R]]. */
+gf_status gf_scatter_hash_r16(void* stream, const gf_rec16_columns* h_in, const gf_rec16_columns* h_out, int layout,
+                              uint32_t capacity, uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles,
+                              uint32_t tile_size, uint32_t bins, uint64_t salt, const uint32_t* d_bin_ids,
+                              const uint32_t* d_table, uint32_t* d_next, uint32_t* d_counts, uint32_t* d_status);
+
+/* Device form of the exact plan (graph/DenseBinTable.hpp:39-91 + the acquisition loop of
+ * flow/Execution.hpp:2558-2590) so that classify -> plan -> scatter needs no host round trip:
+ * from d_counts[bins + 1] (classify output; a set status slot aborts the plan) and a
+ * reservation d_reserved[n_reserved], writes d_table[bins + R], d_descs[R] (bin order, chunk
+ * (b, k) = d_reserved[binBase[b] + k]), d_num_out[1] = R, and zeroes d_next[bins]. */
+gf_status gf_plan_device(void* stream, const uint32_t* d_counts, uint32_t bins, uint32_t capacity,
+                         const uint32_t* d_reserved, uint32_t n_reserved, uint32_t* d_table, gf_out_desc* d_descs,
+                         uint32_t desc_cap, uint32_t* d_num_out, uint32_t* d_next, uint32_t* d_status);
 
 /* ---- synthetic sources ---------------------------------------------------------------------- */
 
@@ -150,6 +195,11 @@ gf_status gf_zipf_cdf(double s, uint32_t k, double* h_cdf);
  * over d_cdf[bins], one_port = 0, round_robin = first_id + i. */
 gf_status gf_generate_keys_u32(void* stream, int dist, uint64_t seed, uint64_t first_id, uint64_t n, uint32_t bins,
                                const double* d_cdf, uint32_t* d_keys);
+
+/* Fills slots [0, n) of the record columns: rank r ~ Zipf over d_cdf[k], key = mix64(r ^ salt),
+ * weight = U(0,1] (f32), tag = first_id + i; stream position (first_id + i, 0, 0x110). */
+gf_status gf_generate_records16(void* stream, uint64_t seed, uint64_t first_id, uint64_t n, const double* d_cdf,
+                                uint32_t k, uint64_t salt, const gf_rec16_columns* h_cols, int layout);
 
 #ifdef __cplusplus
 }

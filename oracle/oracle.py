@@ -170,7 +170,7 @@ def plan_dense(totals, capacity):
     totals = np.ascontiguousarray(totals, np.uint32)
     bins = totals.size
     base = np.zeros(max(bins, 1), np.uint32)
-    cap = int(sum(-(-int(t) // capacity) for t in totals)) if capacity else 0
+    cap = int(((totals.astype(np.int64) + capacity - 1) // capacity).sum()) if capacity else 0
     fills = np.zeros(max(cap, 1), np.uint32)
     num = C.c_uint32()
     _check(lib().gfo_plan_dense(totals if bins else np.zeros(1, np.uint32), bins, capacity, base, fills, cap,

@@ -73,4 +73,4 @@ def test_argument_errors_are_reported_not_thrown():
     cnt = (C.c_uint32 * 5)()
     assert L.gf_classify_dense_u32(None, None, 16, 0, None, 0, 1024, 4, 0, None, C.addressof(cnt), None) == capi.GF_OK
     assert L.gf_partition_fused_u32(None, None, None, 16, 0, None, 0, 1024, 4, 0, None, 0, None, None, 0, None, 0,
-                                    0, None) == capi.GF_ERR_ARGUMENT
+                                    None) == capi.GF_ERR_ARGUMENT
