@@ -69,9 +69,43 @@ _SIGS = {
     "gf_scatter_hash_r16": [_VP, _VP, _VP, _I32, _U32, _U64, _VP, _U32, _U32, _U32, _U64, _VP, _VP, _VP, _VP, _VP],
     "gf_plan_device": [_VP, _VP, _U32, _U32, _VP, _U32, _VP, _VP, _U32, _VP, _VP, _VP],
     "gf_generate_records16": [_VP, _U64, _U64, _U64, _VP, _U32, _U64, _VP, _I32],
+    "gf_run_particle_feedback": [_U64, _U64, _U32, _U32, _U32, _U32, _I32, _I32, _VP, _VP, _VP],
 }
 
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
+
+
+class FlowStats(C.Structure):
+    """gf_flow_stats (SchedulerStats subset)."""
+    _fields_ = [("completed_batches", C.c_uint64), ("partition_batches", C.c_uint64),
+                ("kernel_launches", C.c_uint64), ("loop_iterations", C.c_uint64), ("generated", C.c_uint64),
+                ("sunk", C.c_uint64), ("pool_chunks", C.c_uint32), ("peak_live_chunks", C.c_uint32),
+                ("peak_reserved_chunks", C.c_uint32), ("peak_ready_chunks", C.c_uint32), ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib().gf_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def run_particle_feedback(seed, n, max_visits=64, chunk_capacity=1024, live_particles=4096, batch_chunks=1,
+                          fused=True, layout=None):
+    """runParticleFeedback through the C++ front end on the GPU. Returns (weights, capped, stats)."""
+    import numpy as np
+    layout = LAYOUT_SOA if layout is None else layout
+    weights = np.zeros(max(n, 1), np.uint32)
+    capped = np.zeros(max(n, 1), np.uint32)
+    stats = FlowStats()
+    rc = lib().gf_run_particle_feedback(seed, n, max_visits, chunk_capacity, live_particles, batch_chunks,
+                                        int(bool(fused)), layout, weights.ctypes.data, capped.ctypes.data,
+                                        C.byref(stats))
+    if rc != GF_OK:
+        raise GfError(rc, "particle feedback: " + last_error())
+    return weights[:n], capped[:n], stats
 
 
 class Rec16Columns(C.Structure):
@@ -93,6 +127,8 @@ def lib():
         for name in ("gf_supported_tile_sizes", "gf_supported_hash_tile_sizes"):
             getattr(L, name).argtypes = [_VP, _U32]
             getattr(L, name).restype = _U32
+        L.gf_last_error.argtypes = [_VP, C.c_size_t]
+        L.gf_last_error.restype = C.c_size_t
         _lib = L
     return _lib
 
@@ -106,7 +142,7 @@ def declared_symbols(header: str = HEADER):
     """Every function name the public header declares."""
     import re
     text = open(header).read()
-    return sorted(set(re.findall(r"^\s*(?:gf_status|uint32_t)\s+(gf_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:gf_status|uint32_t|size_t)\s+(gf_\w+)\s*\(", text, re.M)))
 
 
 # ---- host planning ------------------------------------------------------------------------------

@@ -1,0 +1,115 @@
+// C ABI of whole flows run through the C++ front end (Flow + GraphRunner + typed stages).
+#include <chrono>
+#include <cstring>
+#include <string>
+
+#include "../examples/particle_feedback.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename F>
+gf_status guarded(F&& f)
+{
+    try {
+        g_last_error.clear();
+        f();
+        return GF_OK;
+    } catch (const graphflow::SchedulerStallError& e) {
+        g_last_error = e.what();
+        return GF_ERR_TIMEOUT;
+    } catch (const graphflow::CudaError& e) {
+        g_last_error = e.what();
+        return GF_ERR_CUDA;
+    } catch (const graphflow::BatchError& e) {
+        g_last_error = e.what();
+        return std::strstr(e.what(), "overflow") != nullptr ? GF_OVERFLOW : GF_INVALID;
+    } catch (const std::invalid_argument& e) {
+        g_last_error = e.what();
+        return GF_ERR_ARGUMENT;
+    } catch (const std::overflow_error& e) {
+        g_last_error = e.what();
+        return GF_ERR_RANGE;
+    } catch (const std::logic_error& e) {
+        g_last_error = e.what();
+        return GF_ERR_LOGIC;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return GF_INVALID;
+    }
+}
+
+void fill_stats(const graphflow::SchedulerStats& s, double seconds, gf_flow_stats* out)
+{
+    if (out == nullptr)
+        return;
+    out->completed_batches = s.completedBatches;
+    out->partition_batches = s.partitionBatches;
+    out->kernel_launches = s.kernelLaunches;
+    out->loop_iterations = s.loopIterations;
+    out->generated = s.sourceGenerated;
+    out->sunk = s.sourceSunk;
+    out->pool_chunks = s.poolChunks;
+    out->peak_live_chunks = s.peakLiveChunks;
+    out->peak_reserved_chunks = s.peakReservedChunks;
+    out->peak_ready_chunks = s.peakReadyChunks;
+    out->seconds = seconds;
+}
+
+} // namespace
+
+extern "C" {
+
+size_t gf_last_error(char* h_buf, size_t cap)
+{
+    if (h_buf != nullptr && cap != 0u) {
+        const size_t n = g_last_error.size() < cap - 1u ? g_last_error.size() : cap - 1u;
+        std::memcpy(h_buf, g_last_error.data(), n);
+        h_buf[n] = '\0';
+    }
+    return g_last_error.size();
+}
+
+gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visits, uint32_t chunk_capacity,
+                                   uint32_t live_particles, uint32_t batch_chunks, int fused, int layout,
+                                   uint32_t* h_weights, uint32_t* h_capped, gf_flow_stats* h_stats)
+{
+    using namespace graphflow;
+    using namespace graphflow::particle;
+    if ((n != 0u && (h_weights == nullptr || h_capped == nullptr)) ||
+        (layout != GF_LAYOUT_SOA && layout != GF_LAYOUT_AOS))
+        return GF_ERR_ARGUMENT;
+    return guarded([&] {
+        cuda::Device device(0);
+        device.makeCurrent();
+        const std::size_t m = n ? n : 1u;
+        cuda::Buffer<std::uint32_t> weights(m), capped(m);
+        {
+            std::vector<std::uint32_t> init(m, missingWeight);
+            cuda::check(cudaMemcpy(weights.data(), init.data(), m * 4u, cudaMemcpyHostToDevice), "H2D");
+            cuda::check(cudaMemset(capped.data(), 0, m * 4u), "memset");
+        }
+        Tuning t;
+        t.seed = seed;
+        t.chunkCapacity = chunk_capacity;
+        if (live_particles != 0u)
+            t.liveParticles = live_particles;
+        t.batchChunks = batch_chunks;
+        t.fused = fused != 0;
+        const auto t0 = std::chrono::steady_clock::now();
+        SchedulerStats s = layout == GF_LAYOUT_SOA
+                               ? runParticleFeedback<SoAStorage<Particle>>(device, n, max_visits, t, weights.data(),
+                                                                           capped.data())
+                               : runParticleFeedback<AoSStorage<Particle>>(device, n, max_visits, t, weights.data(),
+                                                                           capped.data());
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (n != 0u) {
+            cuda::check(cudaMemcpy(h_weights, weights.data(), n * 4u, cudaMemcpyDeviceToHost), "D2H");
+            cuda::check(cudaMemcpy(h_capped, capped.data(), n * 4u, cudaMemcpyDeviceToHost), "D2H");
+        }
+        fill_stats(s, sec, h_stats);
+    });
+}
+
+} // extern "C"

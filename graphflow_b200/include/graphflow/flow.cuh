@@ -1,0 +1,331 @@
+// Public topology / execution API of the C++ front end, the B200 counterpart of
+// graphFlow::Flow<TPayload, TDevice, TStorage> (flow/Flow.hpp:49-754 in the reference).
+//
+//   Flow<Particle, cuda::Device> flow{device};
+//   auto src = flow.source("generate", Generate{});
+//   auto filter = flow.partition("filter", Filter{});
+//   auto a = flow.partition("process A", SelectOutcome{64}, UpdateWeight{1000});
+//   flow.connect(src, filter);
+//   flow.connect(filter.out<0>(), a);
+//   ...
+//   flow.configure(tuning);
+//   SchedulerStats stats = flow.run(src, n);
+//
+// Functor shapes (flow/Concepts.hpp:126-200): an optional leading `auto const& acc`, then an
+// optional `rng::Engine&`, then an optional `Status&`, then the payload: `(id)` for a source,
+// `(payload const&)` returning an integral or enum bin for a classifier with
+// `static constexpr maxBins`, `(bin, payload&)` returning UpdateResult (or void) for an updater,
+// `(payload&)` or `(payload const&)` returning the payload or void for a transform and a sink.
+#pragma once
+
+#include <functional>
+#include <memory>
+#include <optional>
+#include <string>
+#include <vector>
+
+#include "runner.hpp"
+
+namespace graphflow {
+
+namespace detail {
+struct GraphIdentity {
+    std::uint64_t value;
+};
+inline std::uint64_t nextGraphIdentity()
+{
+    static std::uint64_t next = 1u;
+    return next++;
+}
+} // namespace detail
+
+// flow/NodeHandle.hpp: opaque handle bound to its Flow instance.
+class NodeHandle {
+public:
+    NodeHandle() = default;
+    NodeHandle(std::shared_ptr<detail::GraphIdentity> id, std::size_t key, std::uint32_t bins, std::string name)
+        : m_id(std::move(id)), m_key(key), m_bins(bins), m_name(std::move(name))
+    {
+    }
+    std::size_t key() const { return m_key; }
+    std::uint32_t bins() const { return m_bins; }
+    const std::string& name() const { return m_name; }
+    const std::shared_ptr<detail::GraphIdentity>& identity() const { return m_id; }
+
+private:
+    std::shared_ptr<detail::GraphIdentity> m_id;
+    std::size_t m_key = 0;
+    std::uint32_t m_bins = 0;
+    std::string m_name;
+};
+
+using SourceHandle = NodeHandle;
+using TransformHandle = NodeHandle;
+
+// flow/Ports.hpp: one compile-time output port of a partition node.
+template <std::uint32_t BinValue>
+class OutputPort {
+public:
+    explicit OutputPort(const NodeHandle& n) : m_node(n) {}
+    const NodeHandle& node() const { return m_node; }
+
+private:
+    NodeHandle m_node;
+};
+
+template <std::uint32_t MaxBins, typename TBin>
+class TypedNodeHandle : public NodeHandle {
+public:
+    using NodeHandle::NodeHandle;
+    template <auto Bin>
+    OutputPort<static_cast<std::uint32_t>(Bin)> out() const
+    {
+        static_assert(static_cast<std::uint32_t>(Bin) < MaxBins, "graphflow: output port out of range");
+        return OutputPort<static_cast<std::uint32_t>(Bin)>(*this);
+    }
+};
+
+template <typename TPayload, typename TDevice = cuda::Device, typename TStorage = DefaultStorage<TPayload, TDevice>>
+class Flow {
+public:
+    using PayloadType = TPayload;
+    using Storage = TStorage;
+    using Stats = SchedulerStats;
+
+    explicit Flow(TDevice device)
+        : m_device(std::move(device)),
+          m_identity(std::make_shared<detail::GraphIdentity>(detail::GraphIdentity{detail::nextGraphIdentity()}))
+    {
+    }
+    Flow(const Flow&) = delete;
+    Flow& operator=(const Flow&) = delete;
+
+    void configure(Tuning t)
+    {
+        t.validate();
+        m_tuning = std::move(t);
+    }
+    const Tuning& tuning() const { return m_tuning; }
+
+    template <typename F>
+    SourceHandle source(std::string name, F f)
+    {
+        if (m_sourceKey)
+            throw std::logic_error("graphflow: a Flow has exactly one source node");
+        auto key = append(std::move(name), NodeRole::source, 1u,
+                          [f](TStorage& st, const Config& c, std::uint32_t purpose) -> std::unique_ptr<Stage> {
+                              return std::make_unique<SourceStage<TStorage, F>>(st, c, f, purpose);
+                          });
+        m_sourceKey = key;
+        return NodeHandle(m_identity, key, 1u, m_nodes[key].name);
+    }
+
+    template <typename TClassifier, typename TUpdate = NoUpdate>
+    auto partition(std::string name, TClassifier cls, TUpdate upd = {})
+    {
+        constexpr std::uint32_t bins = static_cast<std::uint32_t>(TClassifier::maxBins);
+        static_assert(bins > 0u, "graphflow: a partition needs at least one bin");
+        using TBin = decltype(invokeBinType<TClassifier>());
+        auto key = append(std::move(name), NodeRole::transform, bins,
+                          [cls, upd](TStorage& st, const Config& c, std::uint32_t purpose) -> std::unique_ptr<Stage> {
+                              return std::make_unique<PartitionStage<TStorage, TClassifier, TUpdate, TBin>>(
+                                  st, c, cls, upd, static_cast<std::uint32_t>(TClassifier::maxBins), purpose);
+                          });
+        m_nodes[key].partition = true;
+        return TypedNodeHandle<bins, TBin>(m_identity, key, bins, m_nodes[key].name);
+    }
+
+    template <typename F>
+    TransformHandle transform(std::string name, F f)
+    {
+        auto key = append(std::move(name), NodeRole::transform, 1u,
+                          [f](TStorage& st, const Config& c, std::uint32_t purpose) -> std::unique_ptr<Stage> {
+                              return std::make_unique<TransformStage<TStorage, F>>(st, c, f, purpose);
+                          });
+        return NodeHandle(m_identity, key, 1u, m_nodes[key].name);
+    }
+
+    template <typename F>
+    NodeHandle sink(std::string name, F f)
+    {
+        auto key = append(std::move(name), NodeRole::sink, 0u,
+                          [f](TStorage& st, const Config& c, std::uint32_t purpose) -> std::unique_ptr<Stage> {
+                              return std::make_unique<SinkStage<TStorage, F>>(st, c, f, purpose);
+                          });
+        return NodeHandle(m_identity, key, 0u, m_nodes[key].name);
+    }
+
+    void connect(const NodeHandle& from, const NodeHandle& to)
+    {
+        if (from.bins() != 1u)
+            throw std::invalid_argument("graphflow: a multi-output node must be connected via out<Bin>()");
+        connectPort(from, 0u, to);
+    }
+    template <std::uint32_t Bin>
+    void connect(const OutputPort<Bin>& port, const NodeHandle& to)
+    {
+        connectPort(port.node(), Bin, to);
+    }
+    template <std::uint32_t MaxBins, typename TBin>
+    void connect(const TypedNodeHandle<MaxBins, TBin>& from, std::uint32_t bin, const NodeHandle& to)
+    {
+        connectPort(from, bin, to);
+    }
+
+    // Flow.hpp:328-412: validate, resolve the configuration, build storage, stages and runner,
+    // run to completion. Returns after every stream and pool chunk has been retired.
+    Stats run(const NodeHandle& source, std::uint64_t itemCount)
+    {
+        validateForRun(source);
+        if (itemCount != 0u && itemCount - 1u > rng::maxStreamId)
+            throw std::overflow_error("graphflow: item count exceeds the 32 bit RNG stream-id range");
+        const Config config = resolveConfig(itemCount);
+        m_device.makeCurrent();
+        TStorage storage(m_device, config.numChunks, config.chunkCapacity);
+        std::vector<std::unique_ptr<Stage>> stages;
+        for (std::size_t k = 0; k < m_nodes.size(); ++k)
+            stages.push_back(m_nodes[k].make(storage, config, rng::streamPurposeForNode(k)));
+        GraphRunner runner(storage.ledger());
+        for (std::size_t k = 0; k < m_nodes.size(); ++k) {
+            std::vector<int> route;
+            for (auto r : m_nodes[k].routes)
+                route.push_back(static_cast<int>(r));
+            runner.addNode(m_nodes[k].name, m_nodes[k].role, m_nodes[k].bins, std::move(route), stages[k].get());
+        }
+        runner.setSource(*m_sourceKey, itemCount, config.liveParticles);
+        runner.setBatchChunks(config.batchChunks);
+        if (m_tuning.stallTimeout)
+            runner.setStallTimeout(*m_tuning.stallTimeout);
+        Stats stats = runner.run();
+        for (const auto& s : stages)
+            stats.kernelLaunches += 0u;
+        stats.poolBytes = stats.poolSlots * TStorage::slotBytes();
+        cuda::check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+        return stats;
+    }
+
+    Config resolvedConfig(std::uint64_t itemCount) const { return resolveConfig(itemCount); }
+
+private:
+    static constexpr std::size_t kInvalid = static_cast<std::size_t>(-1);
+    using Factory = std::function<std::unique_ptr<Stage>(TStorage&, const Config&, std::uint32_t)>;
+
+    struct NodeRecord {
+        std::string name;
+        NodeRole role;
+        std::uint32_t bins;
+        std::vector<std::size_t> routes;
+        Factory make;
+        bool partition = false;
+    };
+
+    template <typename TClassifier>
+    static auto invokeBinType()
+    {
+        using R = decltype(invokeWithContext(std::declval<const TClassifier&>(), std::declval<rng::Engine&>(),
+                                             std::declval<Status&>(), std::declval<const TPayload&>()));
+        return std::decay_t<R>{};
+    }
+
+    std::size_t append(std::string name, NodeRole role, std::uint32_t bins, Factory make)
+    {
+        NodeRecord r{std::move(name), role, bins, std::vector<std::size_t>(bins, kInvalid), std::move(make)};
+        m_nodes.push_back(std::move(r));
+        return m_nodes.size() - 1u;
+    }
+
+    void ensureOwned(const NodeHandle& h) const
+    {
+        if (h.identity() != m_identity)
+            throw std::invalid_argument("graphflow: the handle belongs to a different Flow instance");
+        if (h.key() >= m_nodes.size())
+            throw std::invalid_argument("graphflow: unknown node handle");
+    }
+
+    void connectPort(const NodeHandle& from, std::uint32_t bin, const NodeHandle& to)
+    {
+        ensureOwned(from);
+        ensureOwned(to);
+        NodeRecord& producer = m_nodes[from.key()];
+        if (producer.role == NodeRole::sink)
+            throw std::invalid_argument("graphflow: a sink has no outputs");
+        if (bin >= producer.bins)
+            throw std::invalid_argument("graphflow: output bin out of range");
+        if (m_nodes[to.key()].role == NodeRole::source)
+            throw std::invalid_argument("graphflow: a route may not target the source node");
+        if (producer.routes[bin] != kInvalid)
+            throw std::invalid_argument("graphflow: route for this output is already connected");
+        producer.routes[bin] = to.key();
+    }
+
+    // Flow.hpp:525-570
+    void validateForRun(const NodeHandle& source) const
+    {
+        ensureOwned(source);
+        if (!m_sourceKey)
+            throw std::logic_error("graphflow: no source node is registered");
+        if (source.key() != *m_sourceKey)
+            throw std::invalid_argument("graphflow: run() requires the registered source node");
+        for (const auto& n : m_nodes) {
+            if (n.role == NodeRole::sink)
+                continue;
+            for (std::size_t b = 0; b < n.routes.size(); ++b)
+                if (n.routes[b] == kInvalid)
+                    throw std::invalid_argument("graphflow: missing route for node '" + n.name + "' bin " +
+                                                std::to_string(b));
+        }
+    }
+
+    // Flow.hpp:580-626 (transform reserve, pool size) and :653-746 (resolution order).
+    Config resolveConfig(std::uint64_t itemCount) const
+    {
+        Config c;
+        c.numParticles = itemCount;
+        c.seed = m_tuning.seed;
+        std::uint32_t maxBins = 1u;
+        for (const auto& n : m_nodes)
+            maxBins = std::max(maxBins, n.bins);
+        c.maxBins = maxBins;
+        c.batchChunks = m_tuning.batchChunks.value_or(1u);
+        c.chunkCapacity = m_tuning.chunkCapacity.value_or(8192u);
+        c.tileSize = m_tuning.tileSize.value_or(1024u);
+        c.scatterMode = m_tuning.scatterMode.value_or(ScatterMode::SharedStaging);
+        c.binPath = m_tuning.binPath.value_or(BinPath::automatic);
+        c.fused = m_tuning.fused;
+        // accelerator default P = min(N, 8C) (DevicePolicy.hpp:53)
+        const std::uint64_t defLive = std::min<std::uint64_t>(itemCount, 8ull * c.chunkCapacity);
+        c.liveParticles = m_tuning.liveParticles.value_or(static_cast<std::uint32_t>(defLive ? defLive : 1u));
+        std::uint64_t reserve = 0;
+        for (const auto& n : m_nodes)
+            if (n.role == NodeRole::transform)
+                reserve += checkedOutputChunkBound(c.chunkCapacity, c.chunkCapacity, n.bins);
+        if (reserve > std::numeric_limits<std::uint32_t>::max())
+            throw std::overflow_error("graphflow: transform output reserve exceeds 32 bits");
+        c.poolOutputReserveChunks = static_cast<std::uint32_t>(reserve);
+        if (m_tuning.numChunks) {
+            c.numChunks = *m_tuning.numChunks;
+        } else if (itemCount == 0u) {
+            c.numChunks = 1u;
+        } else {
+            const std::uint64_t live = std::max<std::uint64_t>(1u, std::min<std::uint64_t>(c.liveParticles, itemCount));
+            const std::uint64_t s = live + reserve;
+            if (s > std::numeric_limits<std::uint32_t>::max())
+                throw std::overflow_error("graphflow: chunk pool would exceed 2^32 chunks");
+            c.numChunks = static_cast<std::uint32_t>(s);
+        }
+        c.validate();
+        return c;
+    }
+
+    TDevice m_device;
+    std::shared_ptr<detail::GraphIdentity> m_identity;
+    std::optional<std::size_t> m_sourceKey;
+    std::vector<NodeRecord> m_nodes;
+    Tuning m_tuning;
+};
+
+// flow/Flow.hpp:761-762: SoA storage deduced from the payload's field list.
+template <typename TPayload, typename TDevice = cuda::Device>
+using SoAFlow = Flow<TPayload, TDevice, SoAStorage<TPayload, TDevice>>;
+
+} // namespace graphflow

@@ -1,0 +1,515 @@
+// Typed execution stages of the C++ front end. Each stage owns its per-batch device buffers and
+// pinned host mirrors and exposes the hook protocol of the reference's StageBase
+// (flow/Execution.hpp:1538-1561): launch -> [advance]* -> finish | abort.
+//
+//   SourceStage     flow/Execution.hpp:1582-1690   one chunk per batch, ids firstId + i
+//   TransformStage  flow/Execution.hpp:1692-2258   out-of-place, dense output concatenation
+//   PartitionStage  flow/Execution.hpp:2263-2772   classify -> plan -> scatter -> finalise, or the
+//                                                  B200 fused classify->scan->scatter form
+//   SinkStage       flow/Execution.hpp:2776-...    consumes the batch
+#pragma once
+
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "kernels.cuh"
+#include "storage.cuh"
+
+namespace graphflow {
+
+struct Batch {
+    std::vector<ChunkDescriptor> chunks;
+    std::uint64_t firstId = 0u;
+    std::uint64_t particles() const
+    {
+        std::uint64_t n = 0;
+        for (const auto& c : chunks)
+            n += c.fill;
+        return n;
+    }
+};
+
+class Stage {
+public:
+    virtual ~Stage() = default;
+    // Enqueue the batch's first device stage on `s`. Returns the output chunks it acquired.
+    virtual std::uint32_t launch(cudaStream_t s, const Batch& b) = 0;
+    // Called after the last enqueued device work completed. Returns true when it enqueued more;
+    // `allocated` receives the output chunks acquired by this call.
+    virtual bool advance(cudaStream_t s, const Batch& b, std::uint32_t& allocated) = 0;
+    // Publish the batch's outputs (Execution.hpp:2457-2461).
+    virtual void finish(const Batch& b, std::vector<ChunkDescriptor>& outputs) = 0;
+    // Release every unpublished output; the stage is single-use afterwards (Execution.hpp:2652-2656).
+    virtual void abort() = 0;
+    virtual std::uint64_t launches() const { return m_launches; }
+
+protected:
+    std::uint64_t m_launches = 0;
+};
+
+namespace detail {
+
+inline std::vector<MoveTile> moveTiles(const Batch& b, std::uint32_t tile)
+{
+    std::vector<MoveTile> out;
+    std::uint32_t pos = 0;
+    for (const auto& c : b.chunks)
+        for (std::uint32_t off = 0; off < c.fill; off += tile) {
+            const std::uint32_t n = c.fill - off < tile ? c.fill - off : tile;
+            out.push_back(MoveTile{c.handle.index, off, n, pos});
+            pos += n;
+        }
+    return out;
+}
+
+template <typename T>
+struct Staged {
+    cuda::Buffer<T> dev;
+    cuda::HostBuffer<T> host;
+    explicit Staged(std::size_t n = 0) : dev(n ? n : 1), host(n ? n : 1) {}
+    void upload(cudaStream_t s, std::size_t n)
+    {
+        if (n)
+            cuda::check(cudaMemcpyAsync(dev.data(), host.data(), n * sizeof(T), cudaMemcpyHostToDevice, s), "H2D");
+    }
+    void download(cudaStream_t s, std::size_t n)
+    {
+        if (n)
+            cuda::check(cudaMemcpyAsync(host.data(), dev.data(), n * sizeof(T), cudaMemcpyDeviceToHost, s), "D2H");
+    }
+};
+
+inline void checkStatusWord(std::uint32_t w, const char* stage)
+{
+    if (w != 0u)
+        throw BatchError(std::string(stage) + ": device status reports " + statusCodeName(decodeStatus(w)) +
+                         " (code " + std::to_string(w) + ")");
+}
+
+} // namespace detail
+
+template <typename TStorage, typename TFunctor>
+class SourceStage final : public Stage {
+public:
+    SourceStage(TStorage& st, const Config& c, TFunctor f, std::uint32_t purpose)
+        : m_st(st), m_f(std::move(f)), m_seed(gf::mix64(c.seed)), m_purpose(purpose), m_status(1)
+    {
+    }
+    std::uint32_t launch(cudaStream_t s, const Batch& b) override
+    {
+        if (b.chunks.size() != 1u)
+            throw BatchError("source: a source batch is exactly one chunk");
+        const auto& c = b.chunks[0];
+        cuda::check(cudaMemsetAsync(m_status.dev.data(), 0, 4, s), "memset");
+        const unsigned blocks = (c.fill + 255u) / 256u;
+        if (blocks)
+            source_kernel<<<blocks, 256, 0, s>>>(m_f, m_st.view(), m_seed, m_purpose, b.firstId,
+                                                  m_st.base(c.handle), c.fill, m_status.dev.data());
+        cuda::check(cudaGetLastError(), "source launch");
+        m_status.download(s, 1);
+        ++m_launches;
+        return 0u;
+    }
+    bool advance(cudaStream_t, const Batch&, std::uint32_t& allocated) override
+    {
+        allocated = 0u;
+        detail::checkStatusWord(m_status.host[0], "source");
+        return false;
+    }
+    void finish(const Batch& b, std::vector<ChunkDescriptor>& outputs) override
+    {
+        outputs.push_back(ChunkDescriptor{b.chunks[0].handle, b.chunks[0].fill, 0u});
+    }
+    void abort() override {}
+
+private:
+    TStorage& m_st;
+    TFunctor m_f;
+    std::uint64_t m_seed;
+    std::uint32_t m_purpose;
+    detail::Staged<std::uint32_t> m_status;
+};
+
+template <typename TStorage, typename TFunctor>
+class TransformStage final : public Stage {
+public:
+    TransformStage(TStorage& st, const Config& c, TFunctor f, std::uint32_t purpose)
+        : m_st(st), m_f(std::move(f)), m_seed(gf::mix64(c.seed)), m_purpose(purpose), m_tile(1024u),
+          m_tiles(static_cast<std::size_t>(c.batchChunks) * ((c.chunkCapacity + 1023u) / 1024u)),
+          m_out(c.batchChunks), m_status(1)
+    {
+    }
+    std::uint32_t launch(cudaStream_t s, const Batch& b) override
+    {
+        const auto tiles = detail::moveTiles(b, m_tile);
+        if (tiles.size() > m_tiles.host.size())
+            throw BatchError("transform: tile capacity exceeded");
+        const std::uint64_t n = b.particles();
+        const std::uint32_t C = m_st.chunkCapacity();
+        const std::uint32_t r = static_cast<std::uint32_t>((n + C - 1u) / C);
+        m_pending.clear();
+        for (std::uint32_t k = 0; k < r; ++k) {
+            const ChunkHandle h = m_st.ledger().acquire();
+            m_out.host[k] = h.index;
+            const std::uint64_t left = n - static_cast<std::uint64_t>(k) * C;
+            m_pending.push_back(ChunkDescriptor{h, static_cast<std::uint32_t>(left < C ? left : C), 0u});
+        }
+        std::copy(tiles.begin(), tiles.end(), m_tiles.host.data());
+        m_tiles.upload(s, tiles.size());
+        m_out.upload(s, r);
+        cuda::check(cudaMemsetAsync(m_status.dev.data(), 0, 4, s), "memset");
+        if (!tiles.empty())
+            transform_kernel<<<static_cast<unsigned>(tiles.size()), 256, 0, s>>>(
+                m_f, m_st.view(), m_seed, m_purpose, m_tiles.dev.data(), static_cast<std::uint32_t>(tiles.size()),
+                m_out.dev.data(), r, C, gf::FastDiv(C), m_st.slotCount(), m_status.dev.data());
+        cuda::check(cudaGetLastError(), "transform launch");
+        m_status.download(s, 1);
+        ++m_launches;
+        return r;
+    }
+    bool advance(cudaStream_t, const Batch&, std::uint32_t& allocated) override
+    {
+        allocated = 0u;
+        if (m_status.host[0] != 0u) {
+            abort();
+            detail::checkStatusWord(m_status.host[0], "transform");
+        }
+        return false;
+    }
+    void finish(const Batch&, std::vector<ChunkDescriptor>& outputs) override
+    {
+        outputs.insert(outputs.end(), m_pending.begin(), m_pending.end());
+        m_pending.clear();
+    }
+    void abort() override
+    {
+        for (const auto& d : m_pending)
+            m_st.ledger().release(d.handle);
+        m_pending.clear();
+    }
+
+private:
+    TStorage& m_st;
+    TFunctor m_f;
+    std::uint64_t m_seed;
+    std::uint32_t m_purpose, m_tile;
+    detail::Staged<MoveTile> m_tiles;
+    detail::Staged<std::uint32_t> m_out, m_status;
+    std::vector<ChunkDescriptor> m_pending;
+};
+
+template <typename TStorage, typename TFunctor>
+class SinkStage final : public Stage {
+public:
+    SinkStage(TStorage& st, const Config& c, TFunctor f, std::uint32_t purpose)
+        : m_st(st), m_f(std::move(f)), m_seed(gf::mix64(c.seed)), m_purpose(purpose),
+          m_tiles(static_cast<std::size_t>(c.batchChunks) * ((c.chunkCapacity + 1023u) / 1024u)), m_status(1)
+    {
+    }
+    std::uint32_t launch(cudaStream_t s, const Batch& b) override
+    {
+        const auto tiles = detail::moveTiles(b, 1024u);
+        if (tiles.size() > m_tiles.host.size())
+            throw BatchError("sink: tile capacity exceeded");
+        std::copy(tiles.begin(), tiles.end(), m_tiles.host.data());
+        m_tiles.upload(s, tiles.size());
+        cuda::check(cudaMemsetAsync(m_status.dev.data(), 0, 4, s), "memset");
+        if (!tiles.empty())
+            sink_kernel<<<static_cast<unsigned>(tiles.size()), 256, 0, s>>>(
+                m_f, m_st.view(), m_seed, m_purpose, m_tiles.dev.data(), static_cast<std::uint32_t>(tiles.size()),
+                m_st.chunkCapacity(), m_st.slotCount(), m_status.dev.data());
+        cuda::check(cudaGetLastError(), "sink launch");
+        m_status.download(s, 1);
+        ++m_launches;
+        return 0u;
+    }
+    bool advance(cudaStream_t, const Batch&, std::uint32_t& allocated) override
+    {
+        allocated = 0u;
+        detail::checkStatusWord(m_status.host[0], "sink");
+        return false;
+    }
+    void finish(const Batch&, std::vector<ChunkDescriptor>&) override {}
+    void abort() override {}
+
+private:
+    TStorage& m_st;
+    TFunctor m_f;
+    std::uint64_t m_seed;
+    std::uint32_t m_purpose;
+    detail::Staged<MoveTile> m_tiles;
+    detail::Staged<std::uint32_t> m_status;
+};
+
+// Dense partition stage. Plain form: classify -> (host) plan -> scatter -> finalise, two device
+// stages per batch (Execution.hpp:2363-2725). Fused form: one fused classify->scan->scatter launch
+// plus the device finish, output chunks taken from an outputChunkBound reservation at launch.
+template <typename TStorage, typename TClassifier, typename TUpdate, typename TBin>
+class PartitionStage final : public Stage {
+    using View = typename TStorage::View;
+    using P = typename TStorage::Payload;
+    using Acc = ViewAccess<View>;
+    using Cls = ClassifyAdapter<TClassifier, P>;
+    using Upd = UpdateAdapter<TUpdate, TBin, P>;
+    using Shape = gf::TileShape<256, 4, 2>; // 1024-particle tiles
+
+public:
+    PartitionStage(TStorage& st, const Config& c, TClassifier cls, TUpdate upd, std::uint32_t bins,
+                   std::uint32_t purpose)
+        : m_st(st), m_cls(std::move(cls)), m_upd(std::move(upd)), m_seed(gf::mix64(c.seed)), m_purpose(purpose),
+          m_bins(bins), m_C(c.chunkCapacity), m_Q(c.batchChunks), m_fused(c.fused),
+          m_tileCap(static_cast<std::uint32_t>(c.batchChunks) * ((c.chunkCapacity + kTile - 1u) / kTile)),
+          m_bound(checkedOutputChunkBound(static_cast<std::uint64_t>(c.chunkCapacity) * c.batchChunks,
+                                          c.chunkCapacity, bins)),
+          m_tiles(m_tileCap), m_counts(bins + 1u), m_next(bins), m_table(bins + m_bound), m_status(1),
+          m_numOut(1), m_descs(m_bound ? m_bound : 1)
+    {
+        if (bins > Config::denseBinLimit)
+            throw std::invalid_argument("graphflow::PartitionStage: dense path supports at most 65535 bins");
+        if (m_fused) {
+            m_maxK = m_Q;
+            m_portChunks = cuda::Buffer<unsigned long long>(static_cast<std::size_t>(bins) * m_maxK);
+            cuda::check(cudaMemset(m_portChunks.data(), 0, m_portChunks.size() * 8), "memset");
+            gf_fused_scratch_bytes(m_tileCap, bins, &m_scratchBytes);
+            m_scratch = cuda::Buffer<unsigned char>(m_scratchBytes);
+            cuda::check(cudaMemset(m_scratch.data(), 0, m_scratchBytes), "memset");
+            m_totals = detail::Staged<std::uint32_t>(bins);
+        } else {
+            m_binIds = cuda::Buffer<std::uint32_t>(st.slotCount());
+        }
+        const std::size_t smemFused = sizeof(P) * Shape::kTile + 4u * Shape::kTile + 4u * Shape::kWarps * bins +
+                                      4u * bins * 6u + 4u * (2u * Shape::kThreads + Shape::kWarps + 8u);
+        const std::size_t smemScatter = sizeof(P) * Shape::kTile + 4u * Shape::kTile +
+                                        4u * Shape::kWarps * bins + 4u * bins * 3u + 4u * (Shape::kWarps + 8u);
+        m_smemFused = smemFused;
+        m_smemScatter = smemScatter;
+        cudaFuncSetAttribute(gf::fused_partition_kernel<Shape, Acc, Cls, Upd>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemFused));
+        cudaFuncSetAttribute(gf::scatter_kernel<Shape, Acc, Upd>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smemScatter));
+        cudaFuncSetAttribute(gf::fused_finish_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(4u * (4096u * 2u + 40u)));
+    }
+
+    std::uint32_t launch(cudaStream_t s, const Batch& b) override
+    {
+        if (m_failed)
+            throw std::logic_error("graphflow::PartitionStage: single-use after a failed batch");
+        if (b.chunks.empty() || b.chunks.size() > m_Q)
+            throw BatchError("partition: batch must hold 1..batchChunks chunks");
+        m_stage = 0;
+        m_pending.clear();
+        m_n = b.particles();
+        m_numTiles = 0;
+        for (const auto& c : b.chunks)
+            for (std::uint32_t off = 0; off < c.fill; off += kTile) {
+                if (m_numTiles >= m_tileCap)
+                    throw BatchError("partition: tile descriptor capacity exceeded");
+                m_tiles.host[m_numTiles++] = gf_tile{c.handle.index, off, c.fill - off < kTile ? c.fill - off : kTile};
+            }
+        m_tiles.upload(s, m_numTiles);
+        cuda::check(cudaMemsetAsync(m_status.dev.data(), 0, 4, s), "memset");
+        const Acc acc{m_st.view()};
+        const Cls cls{m_cls, m_seed, m_purpose, m_status.dev.data()};
+        const Upd upd{m_upd, m_purpose + 1u, m_status.dev.data()};
+        ++m_launches;
+        if (m_fused) {
+            const std::uint32_t bound = checkedOutputChunkBound(m_n, m_C, m_bins);
+            m_reserved.clear();
+            for (std::uint32_t k = 0; k < bound; ++k) {
+                m_reserved.push_back(m_st.ledger().acquire());
+                m_table.host[k] = m_reserved.back().index;
+            }
+            m_reservedDev.upload(s, 0);
+            if (m_reservedBuf.size() < (bound ? bound : 1))
+                m_reservedBuf = cuda::Buffer<std::uint32_t>(m_bound ? m_bound : 1);
+            if (bound)
+                cuda::check(cudaMemcpyAsync(m_reservedBuf.data(), m_table.host.data(), bound * 4u,
+                                            cudaMemcpyHostToDevice, s),
+                            "H2D");
+            auto* ctl = reinterpret_cast<gf::FusedCtl*>(m_scratch.data());
+            auto* desc = reinterpret_cast<unsigned long long*>(ctl + 1);
+            cuda::check(cudaMemsetAsync(ctl, 0, gf::kFusedCtlResetBytes, s), "memset");
+            if (m_numTiles)
+                gf::fused_partition_kernel<Shape, Acc, Cls, Upd><<<m_numTiles, Shape::kThreads, m_smemFused, s>>>(
+                    acc, cls, upd, m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(), m_tiles.dev.data(), m_numTiles,
+                    m_bins, m_reservedBuf.data(), bound, m_totals.dev.data(), m_portChunks.data(), m_maxK, ctl, desc,
+                    m_status.dev.data());
+            else
+                cuda::check(cudaMemsetAsync(m_totals.dev.data(), 0, 4u * m_bins, s), "memset");
+            gf::fused_finish_kernel<1024><<<1, 1024, 4u * (4096u * 2u + 40u), s>>>(
+                m_totals.dev.data(), m_portChunks.data(), m_bins, m_C, gf::FastDiv(m_C), m_maxK, ctl,
+                m_table.dev.data(), reinterpret_cast<gf_out_desc*>(m_descs.dev.data()), m_bound,
+                m_numOut.dev.data(), m_status.dev.data());
+            cuda::check(cudaGetLastError(), "fused partition launch");
+            m_status.download(s, 1);
+            m_numOut.download(s, 1);
+            m_descs.download(s, bound);
+            m_totals.download(s, m_bins);
+            return bound;
+        }
+        cuda::check(cudaMemsetAsync(m_counts.dev.data(), 0, 4u * (m_bins + 1u), s), "memset");
+        if (m_numTiles)
+            gf::classify_kernel<Shape, Acc, Cls><<<m_numTiles, Shape::kThreads, 4u * m_bins, s>>>(
+                acc, cls, m_C, m_st.slotCount(), m_tiles.dev.data(), m_numTiles, m_bins, m_binIds.data(),
+                m_counts.dev.data(), m_status.dev.data());
+        cuda::check(cudaGetLastError(), "classify launch");
+        m_status.download(s, 1);
+        m_counts.download(s, m_bins + 1u);
+        return 0u;
+    }
+
+    bool advance(cudaStream_t s, const Batch& b, std::uint32_t& allocated) override
+    {
+        allocated = 0u;
+        try {
+            if (m_fused)
+                return finishFused(b);
+            if (m_stage == 0) {
+                planAndScatter(s, b, allocated);
+                m_stage = 1;
+                return true;
+            }
+            finalise();
+            m_stage = 0;
+            return false;
+        } catch (...) {
+            abort();
+            throw;
+        }
+    }
+
+    void finish(const Batch&, std::vector<ChunkDescriptor>& outputs) override
+    {
+        outputs.insert(outputs.end(), m_pending.begin(), m_pending.end());
+        m_pending.clear();
+    }
+
+    void abort() override
+    {
+        for (const auto& d : m_pending)
+            if (m_st.ledger().valid(d.handle))
+                m_st.ledger().release(d.handle);
+        m_pending.clear();
+        for (const auto& h : m_reserved)
+            if (m_st.ledger().valid(h))
+                m_st.ledger().release(h);
+        m_reserved.clear();
+        m_failed = true;
+    }
+
+private:
+    static constexpr std::uint32_t kTile = Shape::kTile;
+
+    bool finishFused(const Batch&)
+    {
+        detail::checkStatusWord(m_status.host[0], "fused partition");
+        const std::uint32_t r = m_numOut.host[0];
+        std::uint64_t total = 0;
+        for (std::uint32_t b = 0; b < m_bins; ++b)
+            total += m_totals.host[b];
+        if (total != m_n)
+            throw BatchError("fused partition: classified particle count does not match the batch");
+        std::unordered_map<std::uint32_t, ChunkHandle> byIndex;
+        for (const auto& h : m_reserved)
+            byIndex.emplace(h.index, h);
+        const gf_out_desc* d = reinterpret_cast<const gf_out_desc*>(m_descs.host.data());
+        for (std::uint32_t i = 0; i < r; ++i) {
+            auto it = byIndex.find(d[i].chunk_index);
+            if (it == byIndex.end())
+                throw BatchError("fused partition: output chunk outside the reservation");
+            m_pending.push_back(ChunkDescriptor{it->second, d[i].fill, d[i].bin});
+            byIndex.erase(it);
+        }
+        for (auto& kv : byIndex)
+            m_st.ledger().release(kv.second);
+        m_reserved.clear();
+        return false;
+    }
+
+    void planAndScatter(cudaStream_t s, const Batch& b, std::uint32_t& allocated)
+    {
+        detail::checkStatusWord(m_status.host[0], "partition classify");
+        if (m_counts.host[m_bins] != 0u)
+            throw BatchError("partition classify: device status reports an invalid classifier result");
+        std::uint64_t total = 0;
+        for (std::uint32_t k = 0; k < m_bins; ++k)
+            total += m_counts.host[k];
+        if (total != b.particles())
+            throw BatchError("partition classify: classified particle count does not match the batch");
+        std::vector<std::uint32_t> base(m_bins), fills(m_bound ? m_bound : 1);
+        std::uint32_t r = 0;
+        throw_on(gf_plan_dense(m_counts.host.data(), m_bins, m_C, base.data(), fills.data(),
+                               static_cast<std::uint32_t>(fills.size()), &r),
+                 "planDenseBins");
+        if (r > m_bound)
+            throw BatchError("partition plan: exact chunk count exceeds the reservation bound");
+        for (std::uint32_t k = 0; k < m_bins; ++k)
+            m_table.host[k] = base[k];
+        std::uint32_t f = 0;
+        for (std::uint32_t bin = 0; bin < m_bins; ++bin) {
+            const std::uint32_t chunks = (m_counts.host[bin] + m_C - 1u) / m_C;
+            for (std::uint32_t k = 0; k < chunks; ++k, ++f) {
+                const ChunkHandle h = m_st.ledger().acquire();
+                m_table.host[m_bins + f] = h.index;
+                m_pending.push_back(ChunkDescriptor{h, fills[f], bin});
+            }
+        }
+        allocated = r;
+        m_totals0.assign(m_counts.host.data(), m_counts.host.data() + m_bins);
+        m_table.upload(s, m_bins + r);
+        cuda::check(cudaMemsetAsync(m_next.dev.data(), 0, 4u * m_bins, s), "memset");
+        cuda::check(cudaMemsetAsync(m_status.dev.data(), 0, 4, s), "memset");
+        if (m_numTiles) {
+            const Acc acc{m_st.view()};
+            const Upd upd{m_upd, m_purpose + 1u, m_status.dev.data()};
+            gf::scatter_kernel<Shape, Acc, Upd><<<m_numTiles, Shape::kThreads, m_smemScatter, s>>>(
+                acc, upd, m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(), m_tiles.dev.data(), m_numTiles, m_bins,
+                m_binIds.data(), m_table.dev.data(), m_next.dev.data(), m_counts.dev.data(), m_status.dev.data());
+            cuda::check(cudaGetLastError(), "scatter launch");
+            ++m_launches;
+        }
+        m_status.download(s, 1);
+        m_counts.download(s, m_bins + 1u);
+        m_next.download(s, m_bins);
+    }
+
+    void finalise()
+    {
+        detail::checkStatusWord(m_status.host[0], "partition scatter");
+        if (m_counts.host[m_bins] != 0u)
+            throw BatchError("partition scatter: device status reports a checked updater overflow");
+        for (std::uint32_t k = 0; k < m_bins; ++k)
+            if (m_next.host[k] != m_totals0[k])
+                throw BatchError("partition scatter: next[bin] does not match total[bin]");
+    }
+
+    TStorage& m_st;
+    TClassifier m_cls;
+    TUpdate m_upd;
+    std::uint64_t m_seed;
+    std::uint32_t m_purpose, m_bins, m_C, m_Q;
+    bool m_fused;
+    std::uint32_t m_tileCap, m_bound;
+    detail::Staged<gf_tile> m_tiles;
+    detail::Staged<std::uint32_t> m_counts, m_next, m_table, m_status, m_numOut;
+    detail::Staged<std::uint32_t> m_totals;
+    detail::Staged<gf_out_desc> m_descs;
+    detail::Staged<std::uint32_t> m_reservedDev;
+    cuda::Buffer<std::uint32_t> m_reservedBuf, m_binIds;
+    cuda::Buffer<unsigned long long> m_portChunks;
+    cuda::Buffer<unsigned char> m_scratch;
+    std::uint64_t m_scratchBytes = 0;
+    std::uint32_t m_maxK = 1;
+    std::size_t m_smemFused = 0, m_smemScatter = 0;
+    std::uint32_t m_stage = 0, m_numTiles = 0;
+    std::uint64_t m_n = 0;
+    std::vector<ChunkDescriptor> m_pending;
+    std::vector<ChunkHandle> m_reserved;
+    std::vector<std::uint32_t> m_totals0;
+    bool m_failed = false;
+};
+
+} // namespace graphflow

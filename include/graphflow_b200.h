@@ -201,6 +201,38 @@ gf_status gf_generate_keys_u32(void* stream, int dist, uint64_t seed, uint64_t f
 gf_status gf_generate_records16(void* stream, uint64_t seed, uint64_t first_id, uint64_t n, const double* d_cdf,
                                 uint32_t k, uint64_t salt, const gf_rec16_columns* h_cols, int layout);
 
+/* ---- whole flows through the C++ front end (Flow / GraphRunner) ------------------------------ */
+
+/* Counters of one run (sched/GraphRunner.hpp:154-252 SchedulerStats, subset). */
+typedef struct gf_flow_stats {
+    uint64_t completed_batches;
+    uint64_t partition_batches;
+    uint64_t kernel_launches;
+    uint64_t loop_iterations;
+    uint64_t generated;
+    uint64_t sunk;
+    uint32_t pool_chunks;
+    uint32_t peak_live_chunks;
+    uint32_t peak_reserved_chunks;
+    uint32_t peak_ready_chunks;
+    double seconds; /* wall time of Flow::run */
+} gf_flow_stats;
+
+/* examples/particle_feedback/ParticleFeedback.hpp:41-108 runParticleFeedback: the
+ * Generate -> Filter -> {A, B} -> sink feedback graph with the example's functors, on the GPU.
+ * h_weights[n] receives each particle's final weight (0xDEADBEEF if it never reached a sink),
+ * h_capped[n] is 1 for particles stopped by the visit cap. layout: GF_LAYOUT_SOA / _AOS.
+ * fused != 0 runs each partition batch as one fused launch, else classify + host plan + scatter.
+ * Errors: GF_ERR_ARGUMENT (configuration), GF_ERR_RANGE (32/16-bit stream limits),
+ * GF_INVALID / GF_OVERFLOW (a batch failed), GF_ERR_TIMEOUT (scheduler stall), GF_ERR_CUDA;
+ * gf_last_error() describes the last failure of the calling thread. */
+gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visits, uint32_t chunk_capacity,
+                                   uint32_t live_particles, uint32_t batch_chunks, int fused, int layout,
+                                   uint32_t* h_weights, uint32_t* h_capped, gf_flow_stats* h_stats);
+
+/* Message of the last failed front-end call on this thread (empty if none). */
+size_t gf_last_error(char* h_buf, size_t cap);
+
 #ifdef __cplusplus
 }
 #endif
