@@ -35,7 +35,7 @@ BYTES_PER_PARTICLE = 8  # read the 4-byte key once, write it once (algorithmic)
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--tile", type=int, default=4096)
@@ -70,7 +70,7 @@ class ClockSampler:
             self.path = f"/tmp/gf_clocks_{os.getpid()}.csv"
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -314,6 +314,21 @@ def gpu_arm(args):
     correct &= bench.check_fused()
     value = world * args.n / (ms / 1e3)
 
+    # -------- the per-tile fused kernel (no bulk-copy pipeline) on the same data, for comparison --------
+    capi.check(capi.lib().gf_set_tuning(b"fused_tma", 0), "tuning")
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            bench.fused_step(stream)
+        v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        v0.record(stream)
+        for _ in range(20):
+            bench.fused_step(stream)
+        v1.record(stream)
+    stream.synchronize()
+    capi.check(capi.lib().gf_set_tuning(b"fused_tma", 1), "tuning")
+    per_tile_ms = v0.elapsed_time(v1) / 20
+    correct &= bench.check_fused()
+
     # -------- plain (reference's two-launch form) --------
     plain_ms = None
     if rank == 0 or True:
@@ -321,7 +336,7 @@ def gpu_arm(args):
             bench.plain_step(stream)
         stream.synchronize()
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = max(3, args.steps // 4)
+        reps = max(3, min(args.steps // 4, 100))
         p0.record(stream)
         for _ in range(reps):
             bench.plain_step(stream)
@@ -350,7 +365,7 @@ def gpu_arm(args):
         for _ in range(2):
             e2e_step()
         stream.synchronize()
-        e_reps = max(3, args.steps // 4)
+        e_reps = max(3, min(args.steps // 4, 50))
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -417,6 +432,7 @@ def gpu_arm(args):
                 "d2h_bytes_per_step": out_slots * 4 + 3 * 4 * bench_reserve_cap(args) + 8},
         "clocks": clocks.summary(),
         "gpu_launches": 2 * args.steps,
+        "fused_per_tile_kernel": {"value": world * args.n / (per_tile_ms / 1e3), "ms_per_step": per_tile_ms},
         "plain": {"value": world * args.n / (plain_ms / 1e3), "ms_per_step": plain_ms,
                   "form": "classify kernel + host plan + scatter kernel (reference structure)"},
         "correct": bool(correct),

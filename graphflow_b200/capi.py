@@ -70,6 +70,8 @@ _SIGS = {
     "gf_plan_device": [_VP, _VP, _U32, _U32, _VP, _U32, _VP, _VP, _U32, _VP, _VP, _VP],
     "gf_generate_records16": [_VP, _U64, _U64, _U64, _VP, _U32, _U64, _VP, _I32],
     "gf_run_particle_feedback": [_U64, _U64, _U32, _U32, _U32, _U32, _I32, _I32, _VP, _VP, _VP],
+    "gf_set_tuning": [C.c_char_p, _I32],
+    "gf_run_photon": [_U64, _U64, _U64, _VP, _I32, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP],
 }
 
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
@@ -84,6 +86,56 @@ class FlowStats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+PHOTON_ANALOG, PHOTON_WEIGHTED = 0, 1
+EXEC_FLOW, EXEC_FUSED = 0, 1
+
+
+class PhotonParams(C.Structure):
+    """gf_photon_params."""
+    _fields_ = [("thickness", C.c_double), ("sigma_s", C.c_double), ("sigma_a", C.c_double), ("g", C.c_double),
+                ("roulette_threshold", C.c_double), ("roulette_survival", C.c_double),
+                ("max_scatters", C.c_uint32), ("hist_bins", C.c_uint32), ("model", C.c_int), ("isotropic", C.c_int),
+                ("fp64", C.c_int)]
+
+
+def photon_params(model=PHOTON_WEIGHTED, thickness=1.0, sigma_s=10.0, sigma_a=0.1, g=0.9, roulette_threshold=1e-4,
+                  roulette_survival=0.1, max_scatters=65535, hist_bins=256, isotropic=True, fp64=False):
+    return PhotonParams(thickness, sigma_s, sigma_a, g, roulette_threshold, roulette_survival, max_scatters, hist_bins,
+                        model, int(isotropic), int(fp64))
+
+
+def run_photon(seed, n, params, exec_mode=EXEC_FUSED, first_id=0, chunk_capacity=8192, live_particles=0,
+               batch_chunks=8, records=True):
+    """photon_scattering transform bodies on the GPU. Returns a dict of numpy arrays."""
+    import numpy as np
+    m = max(n, 1)
+    out = {}
+    if records:
+        out["event"] = np.zeros(m, np.uint32)
+        out["scatter_count"] = np.zeros(m, np.uint32)
+        out["weight"] = np.zeros(m, np.float64)
+        out["cos_exit"] = np.zeros(m, np.float64)
+        out["position"] = np.zeros(3 * m, np.float64)
+    hb = max(params.hist_bins, 1)
+    out["refl"] = np.zeros(hb, np.float64)
+    out["trans"] = np.zeros(hb, np.float64)
+    out["event_counts"] = np.zeros(5, np.uint64)
+    stats = FlowStats()
+    ptr = (lambda k: out[k].ctypes.data) if records else (lambda k: None)
+    rc = lib().gf_run_photon(seed, first_id, n, C.byref(params), exec_mode, chunk_capacity, live_particles,
+                             batch_chunks, ptr("event"), ptr("scatter_count"), ptr("weight"), ptr("cos_exit"),
+                             ptr("position"), out["refl"].ctypes.data, out["trans"].ctypes.data,
+                             out["event_counts"].ctypes.data, C.byref(stats))
+    if rc != GF_OK:
+        raise GfError(rc, "photon: " + last_error())
+    if records:
+        for k in ("event", "scatter_count", "weight", "cos_exit"):
+            out[k] = out[k][:n]
+        out["position"] = out["position"][:3 * n].reshape(-1, 3)
+    out["stats"] = stats
+    return out
 
 
 def last_error() -> str:

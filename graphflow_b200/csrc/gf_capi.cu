@@ -1,12 +1,17 @@
 // C ABI of the dense partition kernels and the synthetic key source: argument validation on the
 // host, then dispatch to the tile-size instantiations of gf_partition.cuh.
 #include <cstdio>
+#include <algorithm>
 #include <mutex>
+#include <string>
 
-#include "gf_partition.cuh"
+#include "gf_fused_tma.cuh"
 
 namespace gf {
 namespace {
+
+// Tuning knob: 1 = use the persistent bulk-copy fused kernel where it applies (default).
+int g_fused_tma = 1;
 
 constexpr int kThreads = 256;
 constexpr uint32_t kMaxDenseBins = 65535u;
@@ -94,6 +99,17 @@ uint32_t launch_frames(uint32_t n_tiles, size_t smem_bytes)
 using namespace gf;
 
 extern "C" {
+
+gf_status gf_set_tuning(const char* name, int value)
+{
+    if (name == nullptr)
+        return GF_ERR_ARGUMENT;
+    if (std::string(name) == "fused_tma") {
+        g_fused_tma = value != 0;
+        return GF_OK;
+    }
+    return GF_ERR_ARGUMENT;
+}
 
 uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap)
 {
@@ -195,6 +211,36 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
     cudaError_t e = cudaMemsetAsync(ctl, 0, kFusedCtlResetBytes, as_stream(stream));
     if (e != cudaSuccess)
         return cuda_status(e);
+    const bool tma = g_fused_tma != 0 && bins <= 64u && tile_size == 4096u && (capacity & 3u) == 0u &&
+                     (reinterpret_cast<uintptr_t>(d_keys_in) & 15u) == 0u;
+    if (tma) {
+        using S = TmaShape<256, 16>;
+        auto kernel = fused_partition_tma_kernel<S, KeyClassifier>;
+        cudaError_t err = allow_smem(kernel, S::kSmemBytes);
+        if (err != cudaSuccess)
+            return cuda_status(err);
+        uint32_t rows_log2 = 0;
+        while ((1u << rows_log2) < (bins + 1u) / 2u)
+            ++rows_log2;
+        int per_sm = 0;
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, S::kThreads, S::kSmemBytes);
+        if (err != cudaSuccess)
+            return cuda_status(err);
+        if (per_sm < 1)
+            return GF_ERR_CUDA;
+        const uint32_t grid = std::min<uint32_t>(n_tiles, (uint32_t)per_sm * (uint32_t)device_sms());
+        // cooperative launch: all CTAs resident (the static tile schedule relies on it)
+        const uint32_t* a_in = d_keys_in;
+        uint32_t* a_out = d_keys_out;
+        KeyClassifier a_cls = key_classifier(classifier, bins);
+        FastDiv a_fd(capacity);
+        void* args[] = {&a_in,      &a_out,      &a_cls,     &capacity,   &a_fd,
+                        &pool_slots, &d_tiles,    &n_tiles,   &bins,       &rows_log2,
+                        &d_reserved, &n_reserved, &d_totals,  &d_port_chunks, &max_chunks_per_port,
+                        &ctl,        &desc,       &d_status};
+        return cuda_status(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(grid),
+                                                       dim3(S::kThreads), args, S::kSmemBytes, as_stream(stream)));
+    }
     return with_shape(tile_size, [&]<typename Shape>() -> gf_status {
         using Acc = U32Column;
         auto kernel = fused_partition_kernel<Shape, Acc, KeyClassify<Acc>, NoUpdate>;

@@ -1,5 +1,6 @@
 // C ABI of whole flows run through the C++ front end (Flow + GraphRunner + typed stages).
 #include <chrono>
+#include <functional>
 #include <cstring>
 #include <string>
 
@@ -58,6 +59,9 @@ void fill_stats(const graphflow::SchedulerStats& s, double seconds, gf_flow_stat
 }
 
 } // namespace
+
+// Runs a front-end call, mapping its exceptions to gf_status and the last-error message.
+gf_status gf_flows_guard(const std::function<void()>& body) { return guarded(body); }
 
 extern "C" {
 

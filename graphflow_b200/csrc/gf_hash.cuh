@@ -15,6 +15,7 @@
 #include "gf_partition.cuh"
 
 namespace gf {
+namespace { // internal linkage: see gf_partition.cuh
 
 struct alignas(16) Rec16 {
     uint64_t key;
@@ -382,4 +383,5 @@ __global__ void generate_records16_kernel(Access acc, uint64_t seed_mixed, uint6
     }
 }
 
+} // namespace
 } // namespace gf

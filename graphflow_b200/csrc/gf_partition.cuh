@@ -15,6 +15,9 @@
 #include "gf_device.cuh"
 
 namespace gf {
+// Kernels and their helpers have internal linkage: every translation unit that includes this
+// header owns its own instantiations, so one kernel is never registered by two modules.
+namespace {
 
 // UpdateResult of flow/Concepts.hpp (success / overflow / invalid).
 enum : uint32_t { kUpdateSuccess = 0u, kUpdateOverflow = 1u, kUpdateInvalid = 2u };
@@ -734,4 +737,5 @@ static __global__ void generate_keys_kernel(int dist, uint64_t seed_mixed, uint6
     }
 }
 
+} // namespace
 } // namespace gf

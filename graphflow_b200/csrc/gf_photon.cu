@@ -1,0 +1,160 @@
+// C ABI of the photon_scattering transform bodies: the graph through the C++ Flow, or the fused
+// per-photon transport kernel over the same functors.
+#include <chrono>
+#include <functional>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../examples/photon.cuh"
+
+gf_status gf_flows_guard(const std::function<void()>& body); // gf_flows.cu
+
+namespace {
+
+using namespace graphflow;
+using namespace graphflow::photon;
+
+template <typename T>
+void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const gf_photon_params& P, int exec,
+              std::uint32_t C, std::uint32_t live, std::uint32_t Q, uint32_t* hEvent, uint32_t* hSc, double* hW,
+              double* hCos, double* hPos, double* hRefl, double* hTrans, uint64_t* hCounts, gf_flow_stats* hStats)
+{
+    if (exec == GF_EXEC_FLOW && firstId != 0u)
+        throw std::invalid_argument("graphflow::photon: a Flow run starts at id 0");
+    cuda::Device device(0);
+    device.makeCurrent();
+    const std::size_t m = n ? n : 1u;
+    const bool wantRecords = hEvent || hSc || hW || hCos || hPos;
+    cuda::Buffer<TerminalT<T>> records(wantRecords ? m : 1u);
+    cuda::Buffer<std::uint32_t> visits(m);
+    const std::uint32_t hb = P.model == GF_PHOTON_WEIGHTED ? P.hist_bins : 0u;
+    cuda::Buffer<T> refl(hb ? hb : 1u), trans(hb ? hb : 1u);
+    cuda::Buffer<unsigned long long> counts(5);
+    cuda::Buffer<std::uint32_t> status(1);
+    cuda::check(cudaMemset(visits.data(), 0, m * 4u), "memset");
+    cuda::check(cudaMemset(refl.data(), 0, sizeof(T) * (hb ? hb : 1u)), "memset");
+    cuda::check(cudaMemset(trans.data(), 0, sizeof(T) * (hb ? hb : 1u)), "memset");
+    cuda::check(cudaMemset(counts.data(), 0, 40), "memset");
+    cuda::check(cudaMemset(status.data(), 0, 4), "memset");
+    if (wantRecords)
+        cuda::check(cudaMemset(records.data(), 0xFF, sizeof(TerminalT<T>) * m), "memset");
+
+    const SlabT<T> slab{static_cast<T>(P.thickness), static_cast<T>(P.sigma_s), static_cast<T>(P.sigma_a)};
+    RecordTerminalT<T> terminal{wantRecords ? records.data() : nullptr, visits.data(), refl.data(), trans.data(), hb,
+                                counts.data()};
+    SchedulerStats stats;
+    const auto t0 = std::chrono::steady_clock::now();
+    auto run = [&](auto propose, auto scatter) {
+        if (exec == GF_EXEC_FLOW) {
+            Tuning t;
+            t.seed = seed;
+            t.chunkCapacity = C;
+            if (live != 0u)
+                t.liveParticles = live;
+            t.batchChunks = Q;
+            stats = runPhotonFlow<T, SoAStorage<PhotonT<T>>>(device, n, propose, slab, scatter, terminal, t);
+        } else if (n != 0u) {
+            const unsigned blocks = static_cast<unsigned>(std::min<std::uint64_t>((n + 255u) / 256u, 148u * 64u));
+            transport_kernel<T><<<blocks, 256>>>(propose, AdvanceToEventT<T>{slab}, scatter, terminal,
+                                                 gf::mix64(seed), firstId, n, status.data());
+            cuda::check(cudaGetLastError(), "transport launch");
+            cuda::check(cudaDeviceSynchronize(), "transport");
+        }
+    };
+    if (P.model == GF_PHOTON_ANALOG)
+        run(ProposeFlightT<T>{slab, P.max_scatters}, ScatterT<T>{P.isotropic != 0});
+    else
+        run(ProposeWeightedT<T>{slab,
+                                WeightedT<T>{static_cast<T>(P.g), static_cast<T>(P.roulette_threshold),
+                                             static_cast<T>(P.roulette_survival)},
+                                P.max_scatters},
+            ScatterHGT<T>{static_cast<T>(P.g)});
+    const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::uint32_t st = 0;
+    cuda::check(cudaMemcpy(&st, status.data(), 4, cudaMemcpyDeviceToHost), "D2H");
+    if (st != 0u)
+        throw BatchError("photon transport: device status reports " + std::to_string(st));
+    std::vector<std::uint32_t> v(m);
+    cuda::check(cudaMemcpy(v.data(), visits.data(), m * 4u, cudaMemcpyDeviceToHost), "D2H");
+    for (std::uint64_t i = 0; i < n; ++i)
+        if (v[i] != 1u)
+            throw BatchError("photon transport: photon " + std::to_string(firstId + i) +
+                             " did not reach the terminal exactly once");
+    if (wantRecords && n) {
+        std::vector<TerminalT<T>> r(n);
+        cuda::check(cudaMemcpy(r.data(), records.data(), sizeof(TerminalT<T>) * n, cudaMemcpyDeviceToHost), "D2H");
+        for (std::uint64_t i = 0; i < n; ++i) {
+            if (hEvent)
+                hEvent[i] = r[i].event;
+            if (hSc)
+                hSc[i] = r[i].scatterCount;
+            if (hW)
+                hW[i] = static_cast<double>(r[i].weight);
+            if (hCos)
+                hCos[i] = static_cast<double>(r[i].cosExit);
+            if (hPos) {
+                hPos[3 * i] = r[i].position.x;
+                hPos[3 * i + 1] = r[i].position.y;
+                hPos[3 * i + 2] = r[i].position.z;
+            }
+        }
+    }
+    if (hb && (hRefl || hTrans)) {
+        std::vector<T> a(hb), b(hb);
+        cuda::check(cudaMemcpy(a.data(), refl.data(), sizeof(T) * hb, cudaMemcpyDeviceToHost), "D2H");
+        cuda::check(cudaMemcpy(b.data(), trans.data(), sizeof(T) * hb, cudaMemcpyDeviceToHost), "D2H");
+        for (std::uint32_t k = 0; k < hb; ++k) {
+            if (hRefl)
+                hRefl[k] = a[k];
+            if (hTrans)
+                hTrans[k] = b[k];
+        }
+    }
+    if (hCounts)
+        cuda::check(cudaMemcpy(hCounts, counts.data(), 40, cudaMemcpyDeviceToHost), "D2H");
+    if (hStats) {
+        std::memset(hStats, 0, sizeof(*hStats));
+        hStats->completed_batches = stats.completedBatches;
+        hStats->partition_batches = stats.partitionBatches;
+        hStats->kernel_launches = stats.kernelLaunches;
+        hStats->loop_iterations = stats.loopIterations;
+        hStats->generated = exec == GF_EXEC_FLOW ? stats.sourceGenerated : n;
+        hStats->sunk = exec == GF_EXEC_FLOW ? stats.sourceSunk : n;
+        hStats->pool_chunks = stats.poolChunks;
+        hStats->peak_live_chunks = stats.peakLiveChunks;
+        hStats->peak_reserved_chunks = stats.peakReservedChunks;
+        hStats->peak_ready_chunks = stats.peakReadyChunks;
+        hStats->seconds = sec;
+    }
+}
+
+} // namespace
+
+extern "C" gf_status gf_run_photon(uint64_t seed, uint64_t first_id, uint64_t n, const gf_photon_params* h_params,
+                                   int exec, uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks,
+                                   uint32_t* h_event, uint32_t* h_scatter_count, double* h_weight, double* h_cos_exit,
+                                   double* h_position, double* h_refl, double* h_trans, uint64_t* h_event_counts,
+                                   gf_flow_stats* h_stats)
+{
+    if (h_params == nullptr || (exec != GF_EXEC_FLOW && exec != GF_EXEC_FUSED) ||
+        (h_params->model != GF_PHOTON_ANALOG && h_params->model != GF_PHOTON_WEIGHTED))
+        return GF_ERR_ARGUMENT;
+    const gf_photon_params P = *h_params;
+    if (!(P.thickness > 0.0) || P.sigma_s < 0.0 || P.sigma_a < 0.0 || P.max_scatters > 0xFFFFu ||
+        (P.model == GF_PHOTON_WEIGHTED && (!(P.sigma_s + P.sigma_a > 0.0) || P.g <= -1.0 || P.g >= 1.0 ||
+                                           !(P.roulette_survival > 0.0) || P.roulette_survival > 1.0)))
+        return GF_ERR_ARGUMENT;
+    if (n != 0u && first_id + n - 1u > 0xFFFFFFFFull)
+        return GF_ERR_RANGE;
+    return gf_flows_guard([&] {
+        if (P.fp64)
+            runTyped<double>(seed, first_id, n, P, exec, chunk_capacity, live_particles, batch_chunks, h_event,
+                             h_scatter_count, h_weight, h_cos_exit, h_position, h_refl, h_trans, h_event_counts,
+                             h_stats);
+        else
+            runTyped<float>(seed, first_id, n, P, exec, chunk_capacity, live_particles, batch_chunks, h_event,
+                            h_scatter_count, h_weight, h_cos_exit, h_position, h_refl, h_trans, h_event_counts,
+                            h_stats);
+    });
+}

@@ -285,12 +285,12 @@ public:
                                         4u * Shape::kWarps * bins + 4u * bins * 3u + 4u * (Shape::kWarps + 8u);
         m_smemFused = smemFused;
         m_smemScatter = smemScatter;
-        cudaFuncSetAttribute(gf::fused_partition_kernel<Shape, Acc, Cls, Upd>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemFused));
-        cudaFuncSetAttribute(gf::scatter_kernel<Shape, Acc, Upd>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smemScatter));
-        cudaFuncSetAttribute(gf::fused_finish_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(4u * (4096u * 2u + 40u)));
+        cuda::check(cudaFuncSetAttribute(gf::fused_partition_kernel<Shape, Acc, Cls, Upd>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemFused)),
+                    "partition stage: fused kernel attribute");
+        cuda::check(cudaFuncSetAttribute(gf::scatter_kernel<Shape, Acc, Upd>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemScatter)),
+                    "partition stage: scatter kernel attribute");
     }
 
     std::uint32_t launch(cudaStream_t s, const Batch& b) override
@@ -332,18 +332,20 @@ public:
             auto* ctl = reinterpret_cast<gf::FusedCtl*>(m_scratch.data());
             auto* desc = reinterpret_cast<unsigned long long*>(ctl + 1);
             cuda::check(cudaMemsetAsync(ctl, 0, gf::kFusedCtlResetBytes, s), "memset");
-            if (m_numTiles)
+            if (m_numTiles) {
                 gf::fused_partition_kernel<Shape, Acc, Cls, Upd><<<m_numTiles, Shape::kThreads, m_smemFused, s>>>(
                     acc, cls, upd, m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(), m_tiles.dev.data(), m_numTiles,
                     m_bins, m_reservedBuf.data(), bound, m_totals.dev.data(), m_portChunks.data(), m_maxK, ctl, desc,
                     m_status.dev.data());
-            else
+                cuda::check(cudaGetLastError(), "fused partition kernel launch");
+            } else {
                 cuda::check(cudaMemsetAsync(m_totals.dev.data(), 0, 4u * m_bins, s), "memset");
-            gf::fused_finish_kernel<1024><<<1, 1024, 4u * (4096u * 2u + 40u), s>>>(
-                m_totals.dev.data(), m_portChunks.data(), m_bins, m_C, gf::FastDiv(m_C), m_maxK, ctl,
-                m_table.dev.data(), reinterpret_cast<gf_out_desc*>(m_descs.dev.data()), m_bound,
-                m_numOut.dev.data(), m_status.dev.data());
-            cuda::check(cudaGetLastError(), "fused partition launch");
+            }
+            // the finish kernel of the C ABI builds the table and descriptors on the device
+            throw_on(gf_fused_finish(s, m_totals.dev.data(), m_portChunks.data(), m_bins, m_C, m_maxK, ctl,
+                                     m_table.dev.data(), reinterpret_cast<gf_out_desc*>(m_descs.dev.data()), m_bound,
+                                     m_numOut.dev.data(), m_status.dev.data()),
+                     "fused partition finish");
             m_status.download(s, 1);
             m_numOut.download(s, 1);
             m_descs.download(s, bound);

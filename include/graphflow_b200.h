@@ -94,6 +94,12 @@ gf_status gf_flatten_tiles(const uint32_t* h_chunk_index, const uint32_t* h_fill
 /* Tile sizes (particles per tile) the partition kernels of this build are compiled for. */
 uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap);
 
+/* Process-wide tuning knobs (no reference counterpart; used by the autotuner and the benchmark):
+ *   "fused_tma"  1 (default) = gf_partition_fused_u32 uses the persistent bulk-copy kernel where
+ *                it applies (bins <= 64, 4096-particle tiles, capacity % 4 == 0, 16-byte aligned
+ *                keys); 0 = always the per-tile kernel. Results are identical either way. */
+gf_status gf_set_tuning(const char* name, int value);
+
 /* ---- dense partition: the reference's two-launch form --------------------------------------- */
 
 /* flow/Execution.hpp:870-954 PartitionClassifyKernel (graph/ClassifyKernel.hpp:33-93) over a u32
@@ -229,6 +235,32 @@ typedef struct gf_flow_stats {
 gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visits, uint32_t chunk_capacity,
                                    uint32_t live_particles, uint32_t batch_chunks, int fused, int layout,
                                    uint32_t* h_weights, uint32_t* h_capped, gf_flow_stats* h_stats);
+
+/* photon_scattering (examples/photon_scattering/PhotonScattering.hpp:37-181 topology).
+ * model GF_PHOTON_ANALOG: the reference example (absorption terminal, forward or isotropic
+ * scattering). model GF_PHOTON_WEIGHTED: Henyey-Greenstein g, implicit capture, Russian roulette
+ * below roulette_threshold (survival probability roulette_survival), exit-weight histograms over
+ * hist_bins bins of |cos theta| for reflection and transmission. */
+typedef struct gf_photon_params {
+    double thickness, sigma_s, sigma_a, g, roulette_threshold, roulette_survival;
+    uint32_t max_scatters;
+    uint32_t hist_bins;
+    int model;     /* GF_PHOTON_ANALOG or GF_PHOTON_WEIGHTED */
+    int isotropic; /* analog model: isotropic (1) or forward (0) scattering */
+    int fp64;      /* 1: double arithmetic, 0: float */
+} gf_photon_params;
+enum { GF_PHOTON_ANALOG = 0, GF_PHOTON_WEIGHTED = 1 };
+enum { GF_EXEC_FLOW = 0, GF_EXEC_FUSED = 1 };
+
+/* Runs photons first_id .. first_id + n - 1. exec GF_EXEC_FLOW runs the graph through the C++
+ * Flow (partition + transforms + sink); GF_EXEC_FUSED carries each photon through the same
+ * functors in one kernel (identical histories). Optional host outputs (NULL to skip):
+ * h_event[n], h_scatter_count[n], h_weight[n], h_cos_exit[n], h_position[3n] (per id),
+ * h_refl[hist_bins], h_trans[hist_bins] (summed exit weights), h_event_counts[5]. */
+gf_status gf_run_photon(uint64_t seed, uint64_t first_id, uint64_t n, const gf_photon_params* h_params, int exec,
+                        uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks, uint32_t* h_event,
+                        uint32_t* h_scatter_count, double* h_weight, double* h_cos_exit, double* h_position,
+                        double* h_refl, double* h_trans, uint64_t* h_event_counts, gf_flow_stats* h_stats);
 
 /* Message of the last failed front-end call on this thread (empty if none). */
 size_t gf_last_error(char* h_buf, size_t cap);
