@@ -146,6 +146,38 @@ __device__ inline decltype(auto) invokeWithContext(const F& f, rng::Engine& engi
         return f(std::forward<A>(args)...);
 }
 
+// Result type of a functor under the calling rules above, from its declared signature. Host and
+// device compilation must agree on it (it selects kernel instantiations), so it is computed with
+// std::invoke_result on the functor itself, never through a deduced `decltype(auto)` body.
+// Classifiers therefore declare their return type explicitly (as the reference's functors do).
+template <typename F, typename... A>
+constexpr auto contextResultTag()
+{
+    if constexpr (std::is_invocable_v<const F&, const Acc&, rng::Engine&, Status&, A...>)
+        return std::type_identity<std::invoke_result_t<const F&, const Acc&, rng::Engine&, Status&, A...>>{};
+    else if constexpr (std::is_invocable_v<const F&, const Acc&, rng::Engine&, A...>)
+        return std::type_identity<std::invoke_result_t<const F&, const Acc&, rng::Engine&, A...>>{};
+    else if constexpr (std::is_invocable_v<const F&, const Acc&, Status&, A...>)
+        return std::type_identity<std::invoke_result_t<const F&, const Acc&, Status&, A...>>{};
+    else if constexpr (std::is_invocable_v<const F&, const Acc&, A...>)
+        return std::type_identity<std::invoke_result_t<const F&, const Acc&, A...>>{};
+    else if constexpr (std::is_invocable_v<const F&, rng::Engine&, Status&, A...>)
+        return std::type_identity<std::invoke_result_t<const F&, rng::Engine&, Status&, A...>>{};
+    else if constexpr (std::is_invocable_v<const F&, rng::Engine&, A...>)
+        return std::type_identity<std::invoke_result_t<const F&, rng::Engine&, A...>>{};
+    else if constexpr (std::is_invocable_v<const F&, Status&, A...>)
+        return std::type_identity<std::invoke_result_t<const F&, Status&, A...>>{};
+    else
+        return std::type_identity<std::invoke_result_t<const F&, A...>>{};
+}
+
+template <typename F, typename... A>
+using ContextResult = typename decltype(contextResultTag<F, A...>())::type;
+
+// Bin type of a classifier for a payload (flow/Concepts.hpp ClassifierBin).
+template <typename TClassifier, typename TPayload>
+using ClassifierBin = std::decay_t<ContextResult<TClassifier, const TPayload&>>;
+
 // A transform may mutate its payload in place or return a replacement
 // (flow/Execution.hpp:126-140 finishTransform).
 template <typename F, typename P>

@@ -125,7 +125,8 @@ public:
     {
         constexpr std::uint32_t bins = static_cast<std::uint32_t>(TClassifier::maxBins);
         static_assert(bins > 0u, "graphflow: a partition needs at least one bin");
-        using TBin = decltype(invokeBinType<TClassifier>());
+        using TBin = ClassifierBin<TClassifier, TPayload>;
+        static_assert(!std::is_void_v<TBin>, "graphflow: a classifier must return its bin (declared return type)");
         auto key = append(std::move(name), NodeRole::transform, bins,
                           [cls, upd](TStorage& st, const Config& c, std::uint32_t purpose) -> std::unique_ptr<Stage> {
                               return std::make_unique<PartitionStage<TStorage, TClassifier, TUpdate, TBin>>(
@@ -218,14 +219,6 @@ private:
         Factory make;
         bool partition = false;
     };
-
-    template <typename TClassifier>
-    static auto invokeBinType()
-    {
-        using R = decltype(invokeWithContext(std::declval<const TClassifier&>(), std::declval<rng::Engine&>(),
-                                             std::declval<Status&>(), std::declval<const TPayload&>()));
-        return std::decay_t<R>{};
-    }
 
     std::size_t append(std::string name, NodeRole role, std::uint32_t bins, Factory make)
     {
