@@ -294,3 +294,86 @@ gf_status gf_generate_keys_u32(void* stream, int dist, uint64_t seed, uint64_t f
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Fused partition without device allocation.
+//
+// For callers that cannot allocate device memory when they partition: a host runtime that hands
+// all device memory to its own pool at start-up and forbids cudaMalloc afterwards, or a
+// latency-critical path where cudaMalloc/cudaFree (which can synchronise the device) are not
+// acceptable. Their scratch (control block + per-(tile, port) look-back descriptors) lives in the
+// file-scope array below, sized kNoAllocScratchBytes, which every GPU that loads this library
+// holds until the process exits.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+constexpr uint64_t kNoAllocScratchBytes = 8ull << 20; // 8 MiB
+constexpr int kNoAllocMaxDevices = 64;
+
+// Host code must never pass this name to a kernel: on the host it is only a stand-in for the
+// device array. Its device address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::once_flag g_noalloc_once[kNoAllocMaxDevices];
+void* g_noalloc_ptr[kNoAllocMaxDevices];
+cudaError_t g_noalloc_err[kNoAllocMaxDevices];
+
+// Set-up of the current device, done by its first call: take the array's device address and
+// zero the control block (a 64-byte synchronous cudaMemset; it allocates nothing).
+void* noalloc_scratch(gf_status* rc)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+        *rc = e != cudaSuccess ? cuda_status(e) : GF_ERR_RANGE;
+        return nullptr;
+    }
+    std::call_once(g_noalloc_once[dev], [dev] {
+        void* p = nullptr;
+        cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (err == cudaSuccess)
+            err = cudaMemset(p, 0, sizeof(FusedCtl));
+        g_noalloc_ptr[dev] = err == cudaSuccess ? p : nullptr;
+        g_noalloc_err[dev] = err;
+    });
+    if (g_noalloc_err[dev] != cudaSuccess) {
+        *rc = cuda_status(g_noalloc_err[dev]);
+        return nullptr;
+    }
+    *rc = GF_OK;
+    return g_noalloc_ptr[dev];
+}
+
+} // namespace
+
+void gf_set_last_error(const char* message); // gf_flows.cu
+
+extern "C" gf_status gf_partition_fused_u32_noalloc(
+    void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out, uint32_t capacity, uint64_t pool_slots,
+    const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size, uint32_t bins, int classifier,
+    const uint32_t* d_reserved, uint32_t n_reserved, uint32_t* d_totals, unsigned long long* d_port_chunks,
+    uint32_t max_chunks_per_port, uint32_t* d_table, gf_out_desc* d_descs, uint32_t desc_cap, uint32_t* d_num_out,
+    uint32_t* d_status)
+{
+    uint64_t need = 0;
+    if (gf_fused_scratch_bytes(n_tiles, bins, &need) != GF_OK)
+        return GF_ERR_ARGUMENT;
+    if (need > kNoAllocScratchBytes) {
+        gf_set_last_error(("gf_partition_fused_u32_noalloc: the batch needs " + std::to_string(need) +
+                           " scratch bytes (64 + 8 x tiles x ports) but the static scratch holds " +
+                           std::to_string(kNoAllocScratchBytes) + "; use gf_partition_fused_u32 with caller scratch")
+                              .c_str());
+        return GF_ERR_RANGE;
+    }
+    gf_status rc = GF_OK;
+    void* scratch = noalloc_scratch(&rc);
+    if (scratch == nullptr)
+        return rc;
+    rc = gf_partition_fused_u32(stream, d_keys_in, d_keys_out, capacity, pool_slots, d_tiles, n_tiles, tile_size, bins,
+                                classifier, d_reserved, n_reserved, d_totals, d_port_chunks, max_chunks_per_port,
+                                scratch, kNoAllocScratchBytes, d_status);
+    if (rc != GF_OK)
+        return rc;
+    return gf_fused_finish(stream, d_totals, d_port_chunks, bins, capacity, max_chunks_per_port, scratch, d_table,
+                           d_descs, desc_cap, d_num_out, d_status);
+}

@@ -63,6 +63,9 @@ void fill_stats(const graphflow::SchedulerStats& s, double seconds, gf_flow_stat
 // Runs a front-end call, mapping its exceptions to gf_status and the last-error message.
 gf_status gf_flows_guard(const std::function<void()>& body) { return guarded(body); }
 
+// Records the message gf_last_error returns on this thread.
+void gf_set_last_error(const char* message) { g_last_error = message != nullptr ? message : ""; }
+
 extern "C" {
 
 size_t gf_last_error(char* h_buf, size_t cap)

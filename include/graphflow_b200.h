@@ -149,6 +149,27 @@ gf_status gf_fused_finish(void* stream, const uint32_t* d_totals, const unsigned
                           uint32_t* d_table, gf_out_desc* d_descs, uint32_t desc_cap, uint32_t* d_num_out,
                           uint32_t* d_status);
 
+/* No counterpart in the reference. The fused partition plus its device finish for callers that
+ * cannot allocate device memory at this point: a host runtime that gives all device memory to
+ * its own pool at start-up and forbids cudaMalloc afterwards, or a latency-critical path that
+ * cannot afford the device synchronisation cudaMalloc/cudaFree may cause. Arguments and outputs
+ * are those of gf_partition_fused_u32 followed by gf_fused_finish; the caller still provides
+ * every input and output buffer. The scratch is a fixed 8 MiB array inside the library, held by
+ * every GPU that loads it until the process exits, so one batch may use at most
+ * 64 + 8 x tiles x ports <= 8 MiB (e.g. 24,415 tiles of 4096 keys x 32 ports); larger batches
+ * get GF_ERR_RANGE and a message from gf_last_error(). The first call on a device sets the array
+ * up (takes its device address, zeroes its 64-byte control block with a synchronous memset);
+ * make that first call before any stream capture. Every call on a device shares the array and
+ * it keeps the last call's contents: calls that overlap on the GPU race, so order them on one
+ * stream or synchronise between them. No call allocates or frees device memory. */
+gf_status gf_partition_fused_u32_noalloc(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out,
+                                         uint32_t capacity, uint64_t pool_slots, const gf_tile* d_tiles,
+                                         uint32_t n_tiles, uint32_t tile_size, uint32_t bins, int classifier,
+                                         const uint32_t* d_reserved, uint32_t n_reserved, uint32_t* d_totals,
+                                         unsigned long long* d_port_chunks, uint32_t max_chunks_per_port,
+                                         uint32_t* d_table, gf_out_desc* d_descs, uint32_t desc_cap,
+                                         uint32_t* d_num_out, uint32_t* d_status);
+
 /* ---- hash partition of 16-byte records (large port counts) ---------------------------------- */
 
 /* Columns of the 16-byte record {u64 key, f32 weight, u32 tag}: SoA uses key/weight/tag, AoS
