@@ -315,7 +315,7 @@ def gpu_arm(args):
     value = world * args.n / (ms / 1e3)
 
     # -------- the per-tile fused kernel (no bulk-copy pipeline) on the same data, for comparison --------
-    capi.check(capi.lib().gf_set_tuning(b"fused_tma", 0), "tuning")
+    capi.check(capi.lib().gf_set_tuning(b"fused_coop", 0), "tuning")
     with torch.cuda.stream(stream):
         for _ in range(3):
             bench.fused_step(stream)
@@ -325,7 +325,7 @@ def gpu_arm(args):
             bench.fused_step(stream)
         v1.record(stream)
     stream.synchronize()
-    capi.check(capi.lib().gf_set_tuning(b"fused_tma", 1), "tuning")
+    capi.check(capi.lib().gf_set_tuning(b"fused_coop", 1), "tuning")
     per_tile_ms = v0.elapsed_time(v1) / 20
     correct &= bench.check_fused()
 

@@ -5,13 +5,14 @@
 #include <mutex>
 #include <string>
 
-#include "gf_fused_tma.cuh"
+#include "gf_fused_coop.cuh"
 
 namespace gf {
 namespace {
 
-// Tuning knob: 1 = use the persistent bulk-copy fused kernel where it applies (default).
-int g_fused_tma = 1;
+// Tuning knob: 1 = gf_partition_fused_u32 uses the cooperative count/plan/scatter kernel where it
+// applies (default); 0 = always the per-tile look-back kernel.
+int g_fused_coop = 1;
 
 constexpr int kThreads = 256;
 constexpr uint32_t kMaxDenseBins = 65535u;
@@ -104,8 +105,8 @@ gf_status gf_set_tuning(const char* name, int value)
 {
     if (name == nullptr)
         return GF_ERR_ARGUMENT;
-    if (std::string(name) == "fused_tma") {
-        g_fused_tma = value != 0;
+    if (std::string(name) == "fused_coop") {
+        g_fused_coop = value != 0;
         return GF_OK;
     }
     return GF_ERR_ARGUMENT;
@@ -211,35 +212,53 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
     cudaError_t e = cudaMemsetAsync(ctl, 0, kFusedCtlResetBytes, as_stream(stream));
     if (e != cudaSuccess)
         return cuda_status(e);
-    const bool tma = g_fused_tma != 0 && bins <= 64u && tile_size == 4096u && (capacity & 3u) == 0u &&
-                     (reinterpret_cast<uintptr_t>(d_keys_in) & 15u) == 0u;
-    if (tma) {
-        using S = TmaShape<256, 16>;
-        auto kernel = fused_partition_tma_kernel<S, KeyClassifier>;
-        cudaError_t err = allow_smem(kernel, S::kSmemBytes);
-        if (err != cudaSuccess)
-            return cuda_status(err);
-        uint32_t rows_log2 = 0;
-        while ((1u << rows_log2) < (bins + 1u) / 2u)
-            ++rows_log2;
-        int per_sm = 0;
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, S::kThreads, S::kSmemBytes);
-        if (err != cudaSuccess)
-            return cuda_status(err);
-        if (per_sm < 1)
-            return GF_ERR_CUDA;
-        const uint32_t grid = std::min<uint32_t>(n_tiles, (uint32_t)per_sm * (uint32_t)device_sms());
-        // cooperative launch: all CTAs resident (the static tile schedule relies on it)
-        const uint32_t* a_in = d_keys_in;
-        uint32_t* a_out = d_keys_out;
-        KeyClassifier a_cls = key_classifier(classifier, bins);
-        FastDiv a_fd(capacity);
-        void* args[] = {&a_in,      &a_out,      &a_cls,     &capacity,   &a_fd,
-                        &pool_slots, &d_tiles,    &n_tiles,   &bins,       &rows_log2,
-                        &d_reserved, &n_reserved, &d_totals,  &d_port_chunks, &max_chunks_per_port,
-                        &ctl,        &desc,       &d_status};
-        return cuda_status(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(grid),
-                                                       dim3(S::kThreads), args, S::kSmemBytes, as_stream(stream)));
+    const bool coop = g_fused_coop != 0 && bins <= 64u && (capacity & 3u) == 0u && capacity >= 1024u &&
+                      tile_size <= 4096u && (reinterpret_cast<uintptr_t>(d_keys_in) & 15u) == 0u &&
+                      (reinterpret_cast<uintptr_t>(d_keys_out) & 15u) == 0u &&
+                      scratch_bytes >= sizeof(FusedCtl) + 256u;
+    if (coop) {
+        // per-CTA port totals (64 words per CTA) live in the descriptor area of the scratch
+        uint32_t* cta_tot = reinterpret_cast<uint32_t*>(ctl + 1);
+        const uint64_t cap_ctas = (scratch_bytes - sizeof(FusedCtl)) / 256u;
+        auto launch = [&]<typename S, typename Cls>(Cls cls) -> gf_status {
+            auto kernel = fused_partition_coop_kernel<S, Cls>;
+            cudaError_t err = allow_smem(kernel, S::kSmemBytes);
+            if (err != cudaSuccess)
+                return cuda_status(err);
+            int per_sm = 0;
+            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, S::kThreads, S::kSmemBytes);
+            if (err != cudaSuccess)
+                return cuda_status(err);
+            if (per_sm < 1)
+                return GF_ERR_CUDA;
+            uint64_t g = (uint64_t)per_sm * (uint64_t)device_sms();
+            g = std::min<uint64_t>(g, n_tiles);
+            g = std::min<uint64_t>(g, cap_ctas);
+            const uint32_t* a_in = d_keys_in;
+            uint32_t* a_out = d_keys_out;
+            Cls a_cls = cls;
+            FastDiv a_fd(capacity);
+            void* args[] = {&a_in,       &a_out,      &a_cls,         &capacity,           &a_fd,
+                            &pool_slots, &d_tiles,    &n_tiles,       &bins,               &d_reserved,
+                            &n_reserved, &d_totals,   &d_port_chunks, &max_chunks_per_port, &ctl,
+                            &cta_tot,    &d_status};
+            return cuda_status(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3((uint32_t)g),
+                                                           dim3(S::kThreads), args, S::kSmemBytes,
+                                                           as_stream(stream)));
+        };
+        auto with_cls = [&]<typename S>() -> gf_status {
+            if (classifier == GF_CLS_KEY_MOD || classifier == GF_CLS_ID_BALANCED) {
+                if ((bins & (bins - 1u)) == 0u)
+                    return launch.template operator()<S>(MaskClassify{bins - 1u});
+                return launch.template operator()<S>(ModClassify{FastDiv(bins)});
+            }
+            return launch.template operator()<S>(AnyKeyClassify{key_classifier(classifier, bins)});
+        };
+        if (bins <= 4u)
+            return with_cls.template operator()<CoopShape<2>>();
+        if (bins <= 16u)
+            return with_cls.template operator()<CoopShape<8>>();
+        return with_cls.template operator()<CoopShape<32>>();
     }
     return with_shape(tile_size, [&]<typename Shape>() -> gf_status {
         using Acc = U32Column;

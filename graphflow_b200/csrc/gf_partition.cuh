@@ -678,24 +678,31 @@ __global__ void __launch_bounds__(THREADS) fused_finish_kernel(const uint32_t* t
         }
         __syncthreads();
         const uint32_t sum = block_exclusive_scan<THREADS>(nck, base, n, tmp);
-        for (uint32_t i = threadIdx.x; i < n; i += THREADS) {
-            const uint32_t b = seg + i, bb = carry + base[i], tot = totals[b];
-            table[b] = bb;
-            for (uint32_t k = 0; k < nck[i]; ++k) {
-                const uint32_t f = bb + k;
-                if (f >= desc_cap || k >= max_k) {
-                    set_status(status, GF_OVERFLOW);
-                    break;
-                }
-                const unsigned long long v = port_chunks[(size_t)b * max_k + k];
-                const uint32_t chunk = (uint32_t)(v >> 32) == epoch ? (uint32_t)v : kNoChunk;
-                if (chunk == kNoChunk)
-                    set_status(status, GF_INVALID);
-                table[B + f] = chunk;
-                descs[f].chunk_index = chunk;
-                descs[f].fill = min(capacity, tot - k * capacity);
-                descs[f].bin = b;
+        for (uint32_t i = threadIdx.x; i < n; i += THREADS)
+            table[seg + i] = carry + base[i];
+        // one thread per output chunk of the segment (a port may own most of them)
+        for (uint32_t g = threadIdx.x; g < sum; g += THREADS) {
+            uint32_t lo = 0, hi = n - 1u; // the last port of the segment whose chunks start at or before g
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1u) >> 1;
+                if (base[mid] <= g)
+                    lo = mid;
+                else
+                    hi = mid - 1u;
             }
+            const uint32_t b = seg + lo, k = g - base[lo], f = carry + g;
+            if (f >= desc_cap || k >= max_k) {
+                set_status(status, GF_OVERFLOW);
+                continue;
+            }
+            const unsigned long long v = port_chunks[(size_t)b * max_k + k];
+            const uint32_t chunk = (uint32_t)(v >> 32) == epoch ? (uint32_t)v : kNoChunk;
+            if (chunk == kNoChunk)
+                set_status(status, GF_INVALID);
+            table[B + f] = chunk;
+            descs[f].chunk_index = chunk;
+            descs[f].fill = min(capacity, totals[b] - k * capacity);
+            descs[f].bin = b;
         }
         carry += sum;
         __syncthreads();

@@ -95,9 +95,12 @@ gf_status gf_flatten_tiles(const uint32_t* h_chunk_index, const uint32_t* h_fill
 uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap);
 
 /* Process-wide tuning knobs (no reference counterpart; used by the autotuner and the benchmark):
- *   "fused_tma"  1 (default) = gf_partition_fused_u32 uses the persistent bulk-copy kernel where
- *                it applies (bins <= 64, 4096-particle tiles, capacity % 4 == 0, 16-byte aligned
- *                keys); 0 = always the per-tile kernel. Results are identical either way. */
+ *   "fused_coop" 1 (default) = gf_partition_fused_u32 uses the cooperative count/plan/scatter
+ *                kernel where it applies (bins <= 64, tiles of at most 4096 particles,
+ *                capacity % 4 == 0 and >= 1024, 16-byte aligned key columns); 0 = always the
+ *                per-tile look-back kernel. Per-port counts, the plan and every port's sequence are
+ *                identical either way; the cooperative kernel also takes the output chunks in plan
+ *                order (table[B + f] = reserved[f]). */
 gf_status gf_set_tuning(const char* name, int value);
 
 /* ---- dense partition: the reference's two-launch form --------------------------------------- */

@@ -142,6 +142,48 @@ def test_fused_tile_sizes_many_tiles(tile_size):
     _run_case("fused", 1_000_003, 8192, 32, "zipf", tile_size, ragged=False)
 
 
+@pytest.mark.parametrize("coop", [1, 0])
+@pytest.mark.parametrize("bins,capacity,tile_size,dist", [
+    (1, 8192, 4096, "uniform"),        # one port: every tile one run
+    (3, 1024, 4096, "uniform"),        # key mod 3 (division path); a port's tile run spans several chunks
+    (17, 1028, 4096, "zipf"),          # capacity not a power of two, heavy skew
+    (63, 4096, 2048, "round_robin"),   # port runs start at every residue mod 4
+    (64, 8192, 1024, "one_port"),
+    (64, 8192, 8192, "uniform"),       # tiles the cooperative kernel does not take: per-tile kernel
+])
+def test_fused_kernels_match_oracle(coop, bins, capacity, tile_size, dist):
+    """Both fused kernels (the cooperative count/plan/scatter kernel and the per-tile look-back
+    kernel) give the oracle's counts, plan and per-port sequences; the cooperative kernel also
+    takes the output chunks in plan order (table[B + f] = reserved[f])."""
+    capi.check(capi.lib().gf_set_tuning(b"fused_coop", coop), "tuning")
+    try:
+        n = 250_007
+        rng = np.random.default_rng(5)
+        chunks, fills = _batch(n, capacity, rng)
+        bound = capi.output_chunk_bound(n, capacity, bins)
+        pool = ChunkPool(len(chunks) + bound + 3, capacity)
+        keys = O.generate_keys_u32(dist, 11, n, bins, zipf_s=1.1)
+        _fill_pool(pool, chunks, fills, keys)
+        for ch in chunks:
+            pool.free.remove(ch)
+        col = pool.column.cpu().numpy().view(np.uint32)
+        snap = {ch: col[ch * capacity:(ch + 1) * capacity].copy() for ch in chunks}
+        expect_reserved = list(pool.free)[:bound]
+        part = FusedPartition(pool, bins, tile_size=tile_size, max_batch_particles=n)
+        totals, table, descs = part.run(chunks, fills)
+        _check(pool, chunks, fills, keys, bins, (totals, table, descs), exact_order=True, in_snapshot=snap)
+        if coop and tile_size <= 4096:
+            assert np.array_equal(table[bins:], np.asarray(expect_reserved[:len(descs)], np.uint32))
+    finally:
+        capi.check(capi.lib().gf_set_tuning(b"fused_coop", 1), "tuning")
+
+
+def test_fused_many_tiles_per_cta_and_skew():
+    """A batch large enough that every CTA of the cooperative grid owns many tiles, with all keys
+    in one port (one output run per tile, thousands of output chunks in one port)."""
+    _run_case("fused", 12_000_017, 8192, 8, "one_port", 4096, ragged=False)
+
+
 def test_plain_direct_mode_matches_oracle():
     _run_case("plain", 100_000, 1024, 64, "uniform", 2048, mode=capi.SCATTER_DIRECT)
 
