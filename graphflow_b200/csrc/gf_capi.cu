@@ -212,8 +212,8 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
     cudaError_t e = cudaMemsetAsync(ctl, 0, kFusedCtlResetBytes, as_stream(stream));
     if (e != cudaSuccess)
         return cuda_status(e);
-    const bool coop = g_fused_coop != 0 && bins <= 64u && (capacity & 3u) == 0u && capacity >= 1024u &&
-                      tile_size <= 4096u && (reinterpret_cast<uintptr_t>(d_keys_in) & 15u) == 0u &&
+    const bool coop = g_fused_coop != 0 && bins <= 64u && (capacity & 3u) == 0u && capacity >= 4096u &&
+                      tile_size <= 4096u && pool_slots < 0xFFFFFFFFull && (reinterpret_cast<uintptr_t>(d_keys_in) & 15u) == 0u &&
                       (reinterpret_cast<uintptr_t>(d_keys_out) & 15u) == 0u &&
                       scratch_bytes >= sizeof(FusedCtl) + 256u;
     if (coop) {

@@ -7,7 +7,7 @@
 // wait for, and sum, the aggregates of the many tiles still in flight; this kernel takes one grid
 // barrier instead:
 //   phase 1  every CTA counts the keys of its contiguous range of tiles: bulk copies (TMA engine)
-//            keep four tiles in flight per CTA, threads count with packed 16-bit counters;
+//            keep three tiles in flight per CTA, threads count with packed 16-bit counters;
 //   barrier  cooperative launch (all CTAs resident), bounded wait;
 //   plan     every CTA reads all CTAs' per-port totals and derives its own per-port base and the
 //            reference's dense plan, binBase[b] = sum_{b'<b} ceil(total_b' / C)
@@ -17,10 +17,11 @@
 //   phase 2  every CTA walks its tiles again, last tile first (the last tiles it counted are the ones
 //            still in L2). Per tile: a bulk copy two tiles ahead, a stable rank from per-thread packed
 //            counters and one padded raking scan (cost independent of the port distribution),
-//            staging in port order at shared offsets congruent (mod 4) to the output slots, and one
-//            bulk copy shared -> global per port run (heads and tails of up to 3 keys by stores).
+//            staging in port order (each key with its output slot; with capacity >= 4096 a port's
+//            run of one tile touches at most two output chunks), and a write-out in which every
+//            thread stores stage positions tid, tid + 256, ... (coalesced along each run).
 // Requirements (checked by the dispatcher): B <= 64, tiles of at most 4096 keys, capacity % 4 == 0
-// and >= 1024, key columns 16-byte aligned, scratch for 64 words per CTA.
+// and >= 4096, at most 2^32 pool slots, key columns 16-byte aligned, scratch for 64 words per CTA.
 #pragma once
 
 #include "gf_partition.cuh"
@@ -82,23 +83,6 @@ GF_D void bulk_load(void* sdst, const void* gsrc, uint32_t bytes, uint64_t* bar)
                  : "memory");
 }
 
-// 1-D bulk copy shared -> global (multiple of 16 bytes, both addresses 16-byte aligned).
-GF_D void bulk_store(void* gdst, const void* ssrc, uint32_t bytes)
-{
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_u32(ssrc)),
-                 "r"(bytes)
-                 : "memory");
-}
-GF_D void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// Waits until at most N of this thread's bulk groups still read shared memory.
-template <int N>
-GF_D void bulk_wait_read()
-{
-    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
-}
-// Waits until all of this thread's bulk groups have completed.
-GF_D void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-
 GF_D uint32_t ld_acquire_u32(const uint32_t* p)
 {
     uint32_t v;
@@ -134,20 +118,23 @@ struct CoopShape {
     static constexpr uint32_t kLaneShift = LANES == 2 ? 1u : (LANES == 8 ? 3u : 5u);
     static constexpr uint32_t kMaxBins = 2u * LANES;
     static constexpr uint32_t kBM = 64u; // per-port arrays are 64 wide whatever LANES is
-    static constexpr uint32_t kMinCapacity = 1024u;
-    static constexpr uint32_t kMaxPieces = kMaxCount / kMinCapacity + 2u; // chunks one port run can touch
+    static constexpr uint32_t kMinCapacity = kMaxCount; // one tile's run of a port touches <= 2 chunks
     static constexpr uint32_t kSeg = LANES + 1u;                           // raking segment (padded)
-    static constexpr uint32_t kStageWords = kMaxCount + 8u * kBM;
     static constexpr uint32_t kIdCache = 512u; // chunk ids of this CTA's output held in shared memory
-    // shared memory (32-bit words); phase 1's four-tile ring reuses in[0], in[1], stage[0], stage[1]
+    // shared memory (32-bit words). Phase 2 stages a tile in its own input buffer (its keys are in
+    // registers by then); phase 1's three-tile ring is in[0], in[1] and the slot array.
     static constexpr uint32_t kIn = 0;                              // [2][kInWords]
-    static constexpr uint32_t kStage = kIn + 2u * kInWords;         // [2][kStageWords]
-    static constexpr uint32_t kCnt = kStage + 2u * kStageWords;     // [kSeg][kThreads]
+    static constexpr uint32_t kStage = kIn + 2u * kInWords;         // [kMaxCount] output slot per stage position
+    static constexpr uint32_t kRun = kStage + kMaxCount;            // [65] stage start of each port's run
+    static constexpr uint32_t kSplit = kRun + kBM + 4u;             // [64] stage position where the second chunk starts
+    static constexpr uint32_t kSlotA = kSplit + kBM;                // [64] slot - stage position, first chunk
+    static constexpr uint32_t kSlotB = kSlotA + kBM;                // [64] slot - stage position, second chunk
+    static constexpr uint32_t kOff = kSlotB + kBM;                  // [64] running port position
+    static constexpr uint32_t kCnt = kOff + kBM;                    // [kSeg][kThreads]
     static constexpr uint32_t kBase = kCnt + kSeg * kThreads;       // [64] this CTA's first port position
     static constexpr uint32_t kTotal = kBase + kBM;                 // [64] batch totals
     static constexpr uint32_t kBinBase = kTotal + kBM;              // [64] dense plan
-    static constexpr uint32_t kDelta = kBinBase + kBM;              // [64] stage position - tile position
-    static constexpr uint32_t kOwn = kDelta + kBM;                  // [64] this CTA's totals
+    static constexpr uint32_t kOwn = kBinBase + kBM;                // [64] this CTA's totals
     static constexpr uint32_t kKfirst = kOwn + kBM;                 // [64] first output chunk of the range
     static constexpr uint32_t kAcc = kKfirst + kBM;                 // [64] phase-1 flushed counts
     static constexpr uint32_t kIdOff = kAcc + kBM;                  // [65] id cache offsets
@@ -155,13 +142,10 @@ struct CoopShape {
     static constexpr uint32_t kScan = kIds + kIdCache;              // [W]
     static constexpr uint32_t kTiles = kScan + kWarps;              // [6][4] buffered tile descriptors
     static constexpr uint32_t kMisc = kTiles + 24u;                 // [8]
-    static constexpr uint32_t kMbar = (kMisc + 8u + 1u) & ~1u;      // [4] x u64
-    static constexpr uint32_t kWords = kMbar + 8u;
+    static constexpr uint32_t kMbar = (kMisc + 8u + 1u) & ~1u;      // [3] x u64
+    static constexpr uint32_t kWords = kMbar + 6u;
     static constexpr size_t kSmemBytes = sizeof(uint32_t) * kWords;
-    GF_D static uint32_t ring(uint32_t buf)
-    {
-        return buf == 0u ? kIn : buf == 1u ? kIn + kInWords : buf == 2u ? kStage : kStage + kStageWords;
-    }
+    GF_D static uint32_t ring(uint32_t buf) { return buf == 0u ? kIn : buf == 1u ? kIn + kInWords : kStage; }
 };
 
 // Grid-wide barrier of a cooperative launch on a counter reset before the launch. Bounded: a wait
@@ -220,13 +204,18 @@ __global__ void __launch_bounds__(S::kThreads, 2)
                                 uint32_t* status)
 {
     constexpr int T = S::kThreads, IPT = S::kIpt, W = S::kWarps;
-    constexpr uint32_t BM = S::kBM, L = S::kLanes, SEG = S::kSeg, MP = S::kMaxPieces;
+    constexpr uint32_t BM = S::kBM, L = S::kLanes, SEG = S::kSeg;
     extern __shared__ __align__(128) uint32_t sm[];
     uint32_t* cnt = sm + S::kCnt;
     uint32_t* cbase = sm + S::kBase;
     uint32_t* total = sm + S::kTotal;
     uint32_t* bin_base = sm + S::kBinBase;
-    uint32_t* delta = sm + S::kDelta;
+    uint32_t* run_at = sm + S::kRun;
+    uint32_t* split = sm + S::kSplit;
+    uint32_t* slot_a = sm + S::kSlotA;
+    uint32_t* slot_b = sm + S::kSlotB;
+    uint32_t* off = sm + S::kOff;
+    uint32_t* oslot = sm + S::kStage;
     uint32_t* own = sm + S::kOwn;
     uint32_t* kfirst = sm + S::kKfirst;
     uint32_t* acc = sm + S::kAcc;
@@ -246,7 +235,7 @@ __global__ void __launch_bounds__(S::kThreads, 2)
     if (tid == 0) {
         misc[0] = next_epoch(ld_relaxed_u32(&ctl->epoch));
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 3; ++i)
             mbar_init(&mbar[i], 1u);
         mbar_init_fence();
     }
@@ -257,16 +246,16 @@ __global__ void __launch_bounds__(S::kThreads, 2)
     __syncthreads();
     const uint32_t epoch = misc[0];
 
-    // ---------------- phase 1: per-port counts of this CTA's tiles (forward, four in flight) ----------------
+    // ---------------- phase 1: per-port counts of this CTA's tiles (forward, three in flight) ----------------
     if (tid == 0)
-        for (uint32_t q = 0; q < 4u && q < n_mine; ++q)
+        for (uint32_t q = 0; q < 3u && q < n_mine; ++q)
             coop_fetch(tiles, t_lo + q, in, capacity, pool_slots, S::kMaxCount, sm, S::ring(q), &mbar[q],
                        tdesc + 4u * q, status);
     bool bad = false;
     auto count_key = [&](uint32_t key) {
         const uint32_t b = cls(key);
-        if (b < B)
-            cnt[(b & (L - 1u)) * T + tid] += 1u << ((b >> S::kLaneShift) << 4);
+        if (b < B) // own column: no contention; a reduction, so consecutive keys do not wait on each other
+            atomicAdd(cnt + (b & (L - 1u)) * T + tid, 1u << ((b >> S::kLaneShift) << 4));
         else
             bad = true;
     };
@@ -291,9 +280,9 @@ __global__ void __launch_bounds__(S::kThreads, 2)
         __syncthreads();
     };
     for (uint32_t q = 0; q < n_mine; ++q) {
-        const uint32_t buf = q & 3u;
+        const uint32_t buf = q % 3u;
         const uint32_t* d = tdesc + 4u * buf;
-        mbar_wait(&mbar[buf], (q >> 2) & 1u, status);
+        mbar_wait(&mbar[buf], (q / 3u) & 1u, status);
         const uint32_t count = d[2], flags = d[3];
         if (flags & 2u) {
             const uint4* v = reinterpret_cast<const uint4*>(sm + S::ring(buf));
@@ -318,8 +307,8 @@ __global__ void __launch_bounds__(S::kThreads, 2)
         }
         fence_proxy_async_smem(); // this buffer's reads come before the next bulk copy into it
         __syncthreads();
-        if (tid == 0 && q + 4u < n_mine)
-            coop_fetch(tiles, t_lo + q + 4u, in, capacity, pool_slots, S::kMaxCount, sm, S::ring(buf), &mbar[buf],
+        if (tid == 0 && q + 3u < n_mine)
+            coop_fetch(tiles, t_lo + q + 3u, in, capacity, pool_slots, S::kMaxCount, sm, S::ring(buf), &mbar[buf],
                        tdesc + 4u * buf, status);
         if ((q & 2047u) == 2047u)
             flush();
@@ -334,7 +323,7 @@ __global__ void __launch_bounds__(S::kThreads, 2)
     }
     // phase 2 walks the tiles last to first through in[0] and in[1]; its first two tiles are
     // fetched across the barrier. Uses of each buffer so far set the mbarrier parities.
-    const uint32_t use0 = (n_mine + 3u) / 4u, use1 = (n_mine + 2u) / 4u;
+    const uint32_t use0 = (n_mine + 2u) / 3u, use1 = (n_mine + 1u) / 3u;
     if (tid == 0)
         for (uint32_t k = 0; k < 2u && k < n_mine; ++k)
             coop_fetch(tiles, t_hi - 1u - k, in, capacity, pool_slots, S::kMaxCount, sm, S::ring(k), &mbar[k],
@@ -467,22 +456,17 @@ __global__ void __launch_bounds__(S::kThreads, 2)
         return f < R && f < n_reserved ? __ldg(reserved + f) : kNoChunk;
     };
 
-    // running port positions of warp 0's two ports per lane: the end of this CTA's range
-    uint32_t off2[2] = {0u, 0u};
-    if (w == 0) {
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-            const uint32_t b = 2u * lane + (uint32_t)e;
-            off2[e] = cbase[b] + own[b];
-        }
-    }
+    // running port positions: the end of this CTA's range (its tiles are walked last to first)
+    if (tid < BM)
+        off[tid] = cbase[tid] + own[tid];
+    __syncthreads();
 
     // ---------------- phase 2: rank, stage, write (tiles last to first) ----------------
     for (uint32_t k = 0; k < n_mine; ++k) {
         const uint32_t buf = k & 1u;
         const uint32_t* d = tdesc + 16u + 4u * buf;
-        const uint32_t* tin = sm + S::ring(buf);
-        uint32_t* stage = sm + S::kStage + buf * S::kStageWords;
+        uint32_t* tin = sm + S::ring(buf);
+        uint32_t* stage = tin; // the keys are in registers once counted
         mbar_wait(&mbar[buf], ((buf == 0u ? use0 : use1) + (k >> 1)) & 1u, status);
         const uint32_t count = d[2], flags = d[3];
         uint32_t key[IPT];
@@ -518,11 +502,7 @@ __global__ void __launch_bounds__(S::kThreads, 2)
             }
             bp[i] = b | (lr << 16);
         }
-        fence_proxy_async_smem(); // this tile's input buffer is read
         __syncthreads();
-        if (tid == 0 && k + 2u < n_mine)
-            coop_fetch(tiles, t_hi - 1u - (k + 2u), in, capacity, pool_slots, S::kMaxCount, sm, S::ring(buf),
-                       &mbar[buf], tdesc + 16u + 4u * buf, status);
 
         // raking scan over the (lane, thread) counters, padded segments of SEG words
         uint32_t* seg = cnt + tid * SEG;
@@ -556,61 +536,58 @@ __global__ void __launch_bounds__(S::kThreads, 2)
         }
         __syncthreads();
 
-        // per port (warp 0, ports 2 lane and 2 lane + 1): tile start and total, running position,
-        // padded stage base and stage delta
-        uint32_t tt[2] = {0u, 0u}, jj[2] = {0u, 0u}, sb[2] = {0u, 0u};
-        if (w == 0) {
-            uint32_t st[2];
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const uint32_t b = 2u * lane + (uint32_t)e;
-                st[e] = count;
-                if (b < B)
-                    st[e] = (cnt[(b & (L - 1u)) * T] >> ((b >> S::kLaneShift) << 4)) & 0xFFFFu;
+        // per port (one thread each): its run's stage start, the stage position where its second
+        // output chunk starts, and slot - stage position for each of the two chunks
+        if (tid < BM) {
+            const uint32_t b = tid;
+            uint32_t s0 = count, s1 = count;
+            if (b < B)
+                s0 = (cnt[(b & (L - 1u)) * T] >> ((b >> S::kLaneShift) << 4)) & 0xFFFFu;
+            if (b + 1u < B)
+                s1 = (cnt[((b + 1u) & (L - 1u)) * T] >> (((b + 1u) >> S::kLaneShift) << 4)) & 0xFFFFu;
+            const uint32_t len = b < B ? s1 - s0 : 0u;
+            const uint32_t j0 = off[b] - len;
+            off[b] = j0;
+            run_at[b] = s0;
+            uint32_t sp = s0 + len, sa = kNoChunk, sb = kNoChunk;
+            if (len != 0u) {
+                const uint32_t k0 = fdc.div(j0);
+                const uint32_t room = (k0 + 1u) * capacity - j0; // slots left in the first chunk
+                // a chunk id outside the pool writes nothing and fails the batch
+                auto in_pool = [&](uint32_t ch) {
+                    const bool okc = ch != kNoChunk && ((uint64_t)ch + 1u) * capacity <= pool_slots;
+                    if (!okc && ch != kNoChunk)
+                        set_status(status, GF_OVERFLOW);
+                    return okc;
+                };
+                const uint32_t ca = chunk_of(b, k0);
+                if (in_pool(ca))
+                    sa = ca * capacity + (j0 - k0 * capacity) - s0;
+                if (len > room) {
+                    sp = s0 + room;
+                    const uint32_t cb = chunk_of(b, k0 + 1u);
+                    if (in_pool(cb))
+                        sb = cb * capacity - sp;
+                }
             }
-            uint32_t nxt = __shfl_down_sync(0xFFFFFFFFu, st[0], 1);
-            if (lane == 31u)
-                nxt = count;
-            const uint32_t next_of[2] = {st[1], nxt};
-            uint32_t pad[2];
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const uint32_t b = 2u * lane + (uint32_t)e;
-                tt[e] = b < B ? next_of[e] - st[e] : 0u;
-                off2[e] -= tt[e];
-                jj[e] = off2[e];
-                pad[e] = b < B ? ((tt[e] + 3u) & ~3u) + 4u : 0u;
-            }
-            uint32_t in2 = pad[0] + pad[1];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, in2, o);
-                if ((int)lane >= o)
-                    in2 += y;
-            }
-            sb[0] = in2 - pad[0] - pad[1];
-            sb[1] = sb[0] + pad[0];
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const uint32_t b = 2u * lane + (uint32_t)e;
-                if (b < B)
-                    delta[b] = sb[e] + (jj[e] & 3u) - st[e];
-            }
-            bulk_wait_read<1>(); // the stage buffer of tile k - 2 has been read by its bulk copies
+            split[b] = sp;
+            slot_a[b] = sa;
+            slot_b[b] = sb;
         }
         __syncthreads();
 
-        // stage in port order
+        // stage in port order (the stage position is the rank), each key with its output slot
 #pragma unroll
         for (int i = 0; i < IPT; ++i) {
             const uint32_t b = bp[i] & 0xFFFFu;
             if (b != kNoBin16) {
                 const uint32_t word = cnt[(b & (L - 1u)) * T + tid];
-                const uint32_t pos = ((word >> ((b >> S::kLaneShift) << 4)) & 0xFFFFu) + (bp[i] >> 16) + delta[b];
+                const uint32_t pos = ((word >> ((b >> S::kLaneShift) << 4)) & 0xFFFFu) + (bp[i] >> 16);
+                const uint32_t base = pos < split[b] ? slot_a[b] : slot_b[b];
                 stage[pos] = key[i];
+                oslot[pos] = base == kNoChunk ? kNoChunk : base + pos;
             }
         }
-        fence_proxy_async_smem();
         __syncthreads();
 
         // this thread's counter column is reset for the next tile (no other thread reads it now)
@@ -618,51 +595,20 @@ __global__ void __launch_bounds__(S::kThreads, 2)
         for (uint32_t r = 0; r < SEG; ++r)
             cnt[r * T + tid] = 0u;
 
-        // write-out (warp 0): 16-byte-aligned runs by bulk copy, heads and tails by stores
-        if (w == 0) {
-            if (!failed) {
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    if (tt[e] == 0u)
-                        continue;
-                    const uint32_t b = 2u * lane + (uint32_t)e;
-                    const uint32_t j0 = jj[e], j1 = j0 + tt[e];
-                    const uint32_t sstart = sb[e] + (j0 & 3u);
-                    const uint32_t k0 = fdc.div(j0);
-                    for (uint32_t i = 0; i < MP; ++i) {
-                        const uint64_t lo = (uint64_t)(k0 + i) * capacity;
-                        if (lo >= j1)
-                            break;
-                        const uint32_t pj0 = (uint64_t)j0 > lo ? j0 : (uint32_t)lo;
-                        const uint32_t pj1 = (uint64_t)j1 < lo + capacity ? j1 : (uint32_t)(lo + capacity);
-                        const uint32_t chunk = chunk_of(b, k0 + i);
-                        if (chunk == kNoChunk)
-                            continue;
-                        const uint64_t g0 = (uint64_t)chunk * capacity + (pj0 - (uint32_t)lo);
-                        const uint32_t n = pj1 - pj0;
-                        if (g0 + n > pool_slots) {
-                            set_status(status, GF_OVERFLOW);
-                            continue;
-                        }
-                        const uint32_t* src = stage + sstart + (pj0 - j0);
-                        uint32_t* dst = out + g0;
-                        uint32_t h = (4u - (uint32_t)(g0 & 3u)) & 3u;
-                        h = h < n ? h : n;
-                        const uint32_t body = (n - h) & ~3u;
-                        for (uint32_t x = 0; x < h; ++x)
-                            dst[x] = src[x];
-                        if (body != 0u)
-                            bulk_store(dst + h, src + h, body * 4u);
-                        for (uint32_t x = h + body; x < n; ++x)
-                            dst[x] = src[x];
-                    }
-                }
+        // write-out: consecutive threads take consecutive stage positions (coalesced along each run)
+        if (!failed) {
+            for (uint32_t q = tid; q < count; q += T) {
+                const uint32_t sl = oslot[q];
+                if (sl != kNoChunk)
+                    out[sl] = stage[q];
             }
-            bulk_commit(); // one (possibly empty) group per tile
         }
+        fence_proxy_async_smem(); // this buffer's reads come before the next bulk copy into it
+        __syncthreads();
+        if (tid == 0 && k + 2u < n_mine)
+            coop_fetch(tiles, t_hi - 1u - (k + 2u), in, capacity, pool_slots, S::kMaxCount, sm, S::ring(buf),
+                       &mbar[buf], tdesc + 16u + 4u * buf, status);
     }
-    if (w == 0)
-        bulk_wait_all();
 }
 
 } // namespace

@@ -97,7 +97,8 @@ uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap);
 /* Process-wide tuning knobs (no reference counterpart; used by the autotuner and the benchmark):
  *   "fused_coop" 1 (default) = gf_partition_fused_u32 uses the cooperative count/plan/scatter
  *                kernel where it applies (bins <= 64, tiles of at most 4096 particles,
- *                capacity % 4 == 0 and >= 1024, 16-byte aligned key columns); 0 = always the
+ *                capacity % 4 == 0 and >= 4096, fewer than 2^32 pool slots, 16-byte aligned
+ *                key columns); 0 = always the
  *                per-tile look-back kernel. Per-port counts, the plan and every port's sequence are
  *                identical either way; the cooperative kernel also takes the output chunks in plan
  *                order (table[B + f] = reserved[f]). */

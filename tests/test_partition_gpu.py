@@ -145,11 +145,12 @@ def test_fused_tile_sizes_many_tiles(tile_size):
 @pytest.mark.parametrize("coop", [1, 0])
 @pytest.mark.parametrize("bins,capacity,tile_size,dist", [
     (1, 8192, 4096, "uniform"),        # one port: every tile one run
-    (3, 1024, 4096, "uniform"),        # key mod 3 (division path); a port's tile run spans several chunks
-    (17, 1028, 4096, "zipf"),          # capacity not a power of two, heavy skew
-    (63, 4096, 2048, "round_robin"),   # port runs start at every residue mod 4
+    (3, 4096, 4096, "uniform"),        # key mod 3 (division path); runs cross chunk boundaries often
+    (17, 4100, 4096, "zipf"),          # capacity not a power of two, heavy skew
+    (63, 4096, 2048, "round_robin"),   # a run in every port of every tile
     (64, 8192, 1024, "one_port"),
-    (64, 8192, 8192, "uniform"),       # tiles the cooperative kernel does not take: per-tile kernel
+    (3, 1024, 4096, "uniform"),        # capacity below 4096: per-tile kernel
+    (64, 8192, 8192, "uniform"),       # tiles above 4096: per-tile kernel
 ])
 def test_fused_kernels_match_oracle(coop, bins, capacity, tile_size, dist):
     """Both fused kernels (the cooperative count/plan/scatter kernel and the per-tile look-back
@@ -172,7 +173,7 @@ def test_fused_kernels_match_oracle(coop, bins, capacity, tile_size, dist):
         part = FusedPartition(pool, bins, tile_size=tile_size, max_batch_particles=n)
         totals, table, descs = part.run(chunks, fills)
         _check(pool, chunks, fills, keys, bins, (totals, table, descs), exact_order=True, in_snapshot=snap)
-        if coop and tile_size <= 4096:
+        if coop and tile_size <= 4096 and capacity >= 4096:
             assert np.array_equal(table[bins:], np.asarray(expect_reserved[:len(descs)], np.uint32))
     finally:
         capi.check(capi.lib().gf_set_tuning(b"fused_coop", 1), "tuning")
