@@ -126,10 +126,10 @@ struct CoopShape {
     static constexpr uint32_t kIn = 0;                              // [2][kInWords]
     static constexpr uint32_t kStage = kIn + 2u * kInWords;         // [kMaxCount] output slot per stage position
     static constexpr uint32_t kRun = kStage + kMaxCount;            // [65] stage start of each port's run
-    static constexpr uint32_t kSplit = kRun + kBM + 4u;             // [64] stage position where the second chunk starts
-    static constexpr uint32_t kSlotA = kSplit + kBM;                // [64] slot - stage position, first chunk
-    static constexpr uint32_t kSlotB = kSlotA + kBM;                // [64] slot - stage position, second chunk
-    static constexpr uint32_t kOff = kSlotB + kBM;                  // [64] running port position
+    // [64] x {stage position where the second chunk starts, slot - stage position in the first
+    // chunk, the same in the second chunk, unused}: one 16-byte load per staged key
+    static constexpr uint32_t kPort = (kRun + kBM + 4u + 3u) & ~3u;
+    static constexpr uint32_t kOff = kPort + 4u * kBM;              // [64] running port position
     static constexpr uint32_t kCnt = kOff + kBM;                    // [kSeg][kThreads]
     static constexpr uint32_t kBase = kCnt + kSeg * kThreads;       // [64] this CTA's first port position
     static constexpr uint32_t kTotal = kBase + kBM;                 // [64] batch totals
@@ -211,9 +211,7 @@ __global__ void __launch_bounds__(S::kThreads, 2)
     uint32_t* total = sm + S::kTotal;
     uint32_t* bin_base = sm + S::kBinBase;
     uint32_t* run_at = sm + S::kRun;
-    uint32_t* split = sm + S::kSplit;
-    uint32_t* slot_a = sm + S::kSlotA;
-    uint32_t* slot_b = sm + S::kSlotB;
+    uint4* port4 = reinterpret_cast<uint4*>(sm + S::kPort);
     uint32_t* off = sm + S::kOff;
     uint32_t* oslot = sm + S::kStage;
     uint32_t* own = sm + S::kOwn;
@@ -570,9 +568,7 @@ __global__ void __launch_bounds__(S::kThreads, 2)
                         sb = cb * capacity - sp;
                 }
             }
-            split[b] = sp;
-            slot_a[b] = sa;
-            slot_b[b] = sb;
+            port4[b] = make_uint4(sp, sa, sb, 0u);
         }
         __syncthreads();
 
@@ -583,7 +579,8 @@ __global__ void __launch_bounds__(S::kThreads, 2)
             if (b != kNoBin16) {
                 const uint32_t word = cnt[(b & (L - 1u)) * T + tid];
                 const uint32_t pos = ((word >> ((b >> S::kLaneShift) << 4)) & 0xFFFFu) + (bp[i] >> 16);
-                const uint32_t base = pos < split[b] ? slot_a[b] : slot_b[b];
+                const uint4 pp = port4[b];
+                const uint32_t base = pos < pp.x ? pp.y : pp.z;
                 stage[pos] = key[i];
                 oslot[pos] = base == kNoChunk ? kNoChunk : base + pos;
             }
@@ -597,6 +594,7 @@ __global__ void __launch_bounds__(S::kThreads, 2)
 
         // write-out: consecutive threads take consecutive stage positions (coalesced along each run)
         if (!failed) {
+#pragma unroll 4
             for (uint32_t q = tid; q < count; q += T) {
                 const uint32_t sl = oslot[q];
                 if (sl != kNoChunk)
