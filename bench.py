@@ -30,6 +30,10 @@ SEED = 42
 HEADLINE_BINS = 64
 HEADLINE_DIST = "uniform"
 BYTES_PER_PARTICLE = 8  # read the 4-byte key once, write it once (algorithmic)
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per key of one launch of the
+# cooperative kernel, from an ncu capture of the 5e7-key case with B = 64 uniform keys (traffic
+# grows in proportion to the keys, so it scales to a full launch); None for other workloads.
+MEASURED_TRAFFIC_PER_KEY = {(64, "uniform"): 10.06}
 
 
 def parse():
@@ -423,7 +427,10 @@ def gpu_arm(args):
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Philox keys)",
         "config": workload_config(args),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_source": peak_kind, "kernel": "fused_partition_kernel",
+                     "traffic": (MEASURED_TRAFFIC_PER_KEY[(args.bins, args.dist)] * args.n
+                                 if (args.bins, args.dist) in MEASURED_TRAFFIC_PER_KEY and args.tile <= 4096 else None),
+                     "traffic_source": "ncu capture of the 5e7-key case, scaled by keys per launch",
+                     "peak_source": peak_kind, "kernel": "fused_partition_coop_kernel",
                      "kernel_ms": kernel_ms,
                      "algorithmic_bytes": f"{BYTES_PER_PARTICLE} B/particle x {args.n} particles per launch"},
         "cpu_baseline": cpu,
