@@ -71,6 +71,7 @@ _SIGS = {
     "gf_generate_records16": [_VP, _U64, _U64, _U64, _VP, _U32, _U64, _VP, _I32],
     "gf_run_particle_feedback": [_U64, _U64, _U32, _U32, _U32, _U32, _I32, _I32, _VP, _VP, _VP],
     "gf_set_tuning": [C.c_char_p, _I32],
+    "gf_run_dense_chain": [_U64, _U64, _U32, _U32, _I32, C.c_double, _U32, _U32, _U32, _I32, _I32, _VP, _VP],
     "gf_run_photon": [_U64, _U64, _U64, _VP, _I32, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP],
 }
 
@@ -158,6 +159,22 @@ def run_particle_feedback(seed, n, max_visits=64, chunk_capacity=1024, live_part
     if rc != GF_OK:
         raise GfError(rc, "particle feedback: " + last_error())
     return weights[:n], capped[:n], stats
+
+
+def run_dense_chain(seed, n, bins, nodes=1, dist="uniform", zipf_s=1.1, chunk_capacity=8192, live_particles=16384,
+                    batch_chunks=8, fused=True, layout=None, want_ports=True):
+    """The dense sweep through the C++ Flow (1 to 4 chained partition nodes). Returns
+    (port_of, stats): each particle's final port by id (None unless want_ports)."""
+    import numpy as np
+    layout = LAYOUT_SOA if layout is None else layout
+    port_of = np.zeros(max(n, 1), np.uint32) if want_ports else None
+    stats = FlowStats()
+    rc = lib().gf_run_dense_chain(seed, n, bins, nodes, DIST_NAMES[dist], zipf_s, chunk_capacity, live_particles,
+                                  batch_chunks, int(bool(fused)), layout,
+                                  port_of.ctypes.data if want_ports else None, C.byref(stats))
+    if rc != GF_OK:
+        raise GfError(rc, "dense chain: " + last_error())
+    return (port_of[:n] if want_ports else None), stats
 
 
 class Rec16Columns(C.Structure):

@@ -169,6 +169,33 @@ GF_D void set_status(uint32_t* status, uint32_t code)
 constexpr uint32_t kSpinLimit = 1u << 20;
 
 // ---------------------------------------------------------------------------------------------
+// Synthetic key of stream position (id, 0, 0x100 + dist): uniform (the position's first draw),
+// Zipf over `bins` ports (inverse CDF of a uniform double; cdf[b] = P(rank <= b)), all in port 0,
+// or round robin (key = id).
+// ---------------------------------------------------------------------------------------------
+GF_HD uint32_t synthetic_key(int dist, uint64_t seed_mixed, uint64_t id, uint32_t bins, const double* cdf)
+{
+    if (dist == GF_DIST_UNIFORM || dist == GF_DIST_ZIPF) {
+        const uint32_t d = first_draws(stream_key(seed_mixed, id, 0u, 0x100u + (uint32_t)dist)).v[0];
+        if (dist == GF_DIST_UNIFORM)
+            return d;
+        const double u = uniform_f64(d);
+        uint32_t lo = 0, hi = bins - 1u;
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2u;
+            if (u < cdf[mid])
+                hi = mid;
+            else
+                lo = mid + 1u;
+        }
+        return lo;
+    }
+    if (dist == GF_DIST_ONE_PORT)
+        return 0u;
+    return (uint32_t)id;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Built-in classifiers of the kernel-level sweeps and the kernel-axis examples
 // (examples/particle_feedback/KernelAxes.hpp:29-42). A result >= bins is invalid.
 // ---------------------------------------------------------------------------------------------

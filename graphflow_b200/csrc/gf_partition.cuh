@@ -716,32 +716,8 @@ __global__ void __launch_bounds__(THREADS) fused_finish_kernel(const uint32_t* t
 static __global__ void generate_keys_kernel(int dist, uint64_t seed_mixed, uint64_t first_id, uint64_t n, uint32_t bins,
                                      const double* cdf, uint32_t* keys)
 {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t id = first_id + i;
-        uint32_t k;
-        if (dist == GF_DIST_UNIFORM || dist == GF_DIST_ZIPF) {
-            const uint32_t d = first_draws(stream_key(seed_mixed, id, 0u, 0x100u + (uint32_t)dist)).v[0];
-            if (dist == GF_DIST_UNIFORM) {
-                k = d;
-            } else {
-                const double u = uniform_f64(d);
-                uint32_t lo = 0, hi = bins - 1u;
-                while (lo < hi) {
-                    const uint32_t mid = lo + (hi - lo) / 2u;
-                    if (u < cdf[mid])
-                        hi = mid;
-                    else
-                        lo = mid + 1u;
-                }
-                k = lo;
-            }
-        } else if (dist == GF_DIST_ONE_PORT) {
-            k = 0u;
-        } else {
-            k = (uint32_t)id;
-        }
-        keys[i] = k;
-    }
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        keys[i] = synthetic_key(dist, seed_mixed, first_id + i, bins, cdf);
 }
 
 } // namespace

@@ -249,6 +249,19 @@ typedef struct gf_flow_stats {
     double seconds; /* wall time of Flow::run */
 } gf_flow_stats;
 
+/* The kernel-level dense sweep through the public Flow (flow/Flow.hpp:49-754 with the
+ * reference's runner semantics, sched/GraphRunner.hpp): Generate -> `nodes` (1..4) chained
+ * partition nodes -> sink. Records are {u32 id, u32 key}; keys are gf_generate_keys_u32's for the
+ * same seed and distribution (zipf_s is the Zipf exponent); node i sends a key to port
+ * (key >> 8 i) mod bins, bins in {2, 8, 32, 64}; every port of a node feeds the next node and the
+ * last node feeds the sink. h_port_of[n] (optional) receives each particle's final port
+ * (0xFFFFFFFF if it never reached the sink). chunk_capacity = C, live_particles = P (0: default),
+ * batch_chunks = Q, fused != 0: one fused launch per partition batch, layout GF_LAYOUT_SOA/_AOS.
+ * Errors as gf_run_particle_feedback. */
+gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins, uint32_t nodes, int dist, double zipf_s,
+                             uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks, int fused,
+                             int layout, uint32_t* h_port_of, gf_flow_stats* h_stats);
+
 /* examples/particle_feedback/ParticleFeedback.hpp:41-108 runParticleFeedback: the
  * Generate -> Filter -> {A, B} -> sink feedback graph with the example's functors, on the GPU.
  * h_weights[n] receives each particle's final weight (0xDEADBEEF if it never reached a sink),
