@@ -13,6 +13,10 @@ namespace {
 // Tuning knob: 1 = gf_partition_fused_u32 uses the cooperative count/plan/scatter kernel where it
 // applies (default); 0 = always the per-tile look-back kernel.
 int g_fused_coop = 1;
+// Tuning knob: 1 = the flow entry points run the B200 runner options (sinks take up to Q chunks,
+// every idle node is dispatched per loop iteration); 0 = the reference's one-chunk sinks and one
+// dispatch per iteration.
+int g_runner_batched = 1;
 
 constexpr int kThreads = 256;
 constexpr uint32_t kMaxDenseBins = 65535u;
@@ -107,6 +111,10 @@ gf_status gf_set_tuning(const char* name, int value)
         return GF_ERR_ARGUMENT;
     if (std::string(name) == "fused_coop") {
         g_fused_coop = value != 0;
+        return GF_OK;
+    }
+    if (std::string(name) == "runner_batched") {
+        g_runner_batched = value != 0;
         return GF_OK;
     }
     return GF_ERR_ARGUMENT;
@@ -396,3 +404,6 @@ extern "C" gf_status gf_partition_fused_u32_noalloc(
     return gf_fused_finish(stream, d_totals, d_port_chunks, bins, capacity, max_chunks_per_port, scratch, d_table,
                            d_descs, desc_cap, d_num_out, d_status);
 }
+
+// Read by the flow entry points (gf_flows.cu, gf_dense_flow.cu, gf_photon.cu).
+bool gf_runner_batched() { return gf::g_runner_batched != 0; }

@@ -7,6 +7,7 @@
 #include "../examples/dense_chain.cuh"
 
 gf_status gf_flows_guard(const std::function<void()>& body); // gf_flows.cu
+bool gf_runner_batched();                                       // gf_capi.cu
 
 namespace {
 
@@ -60,6 +61,10 @@ extern "C" gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins
             t.liveParticles = live_particles;
         t.batchChunks = batch_chunks;
         t.fused = fused != 0;
+        if (gf_runner_batched()) {
+            t.sinkBatchChunks = batch_chunks;
+            t.multiDispatch = true;
+        }
         const auto t0 = std::chrono::steady_clock::now();
         const SchedulerStats s =
             layout == GF_LAYOUT_SOA

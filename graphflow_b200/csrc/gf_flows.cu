@@ -60,6 +60,8 @@ void fill_stats(const graphflow::SchedulerStats& s, double seconds, gf_flow_stat
 
 } // namespace
 
+bool gf_runner_batched(); // gf_capi.cu
+
 // Runs a front-end call, mapping its exceptions to gf_status and the last-error message.
 gf_status gf_flows_guard(const std::function<void()>& body) { return guarded(body); }
 
@@ -104,6 +106,10 @@ gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visit
             t.liveParticles = live_particles;
         t.batchChunks = batch_chunks;
         t.fused = fused != 0;
+        if (gf_runner_batched()) {
+            t.sinkBatchChunks = batch_chunks;
+            t.multiDispatch = true;
+        }
         const auto t0 = std::chrono::steady_clock::now();
         SchedulerStats s = layout == GF_LAYOUT_SOA
                                ? runParticleFeedback<SoAStorage<Particle>>(device, n, max_visits, t, weights.data(),

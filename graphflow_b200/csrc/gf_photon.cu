@@ -9,6 +9,7 @@
 #include "../examples/photon.cuh"
 
 gf_status gf_flows_guard(const std::function<void()>& body); // gf_flows.cu
+bool gf_runner_batched();                                       // gf_capi.cu
 
 namespace {
 
@@ -53,6 +54,10 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
             if (live != 0u)
                 t.liveParticles = live;
             t.batchChunks = Q;
+            if (gf_runner_batched()) {
+                t.sinkBatchChunks = Q;
+                t.multiDispatch = true;
+            }
             stats = runPhotonFlow<T, SoAStorage<PhotonT<T>>>(device, n, propose, slab, scatter, terminal, t);
         } else if (n != 0u) {
             const unsigned blocks = static_cast<unsigned>(std::min<std::uint64_t>((n + 255u) / 256u, 148u * 64u));

@@ -85,6 +85,12 @@ struct Tuning {
     // B200: one fused classify->scan->scatter launch per partition batch instead of
     // classify + host plan + scatter.
     bool fused = true;
+    // B200 runner options (results are identical either way). sinkBatchChunks: a sink may take up
+    // to this many ready chunks per launch (the reference's runner takes one, GraphRunner.hpp:600;
+    // capped at batchChunks). multiDispatch: every idle node with ready input is dispatched in the
+    // same loop iteration (the reference dispatches one node per iteration, GraphRunner.hpp:985).
+    std::uint32_t sinkBatchChunks = 1u;
+    bool multiDispatch = false;
 
     void validate() const
     {

@@ -195,6 +195,8 @@ public:
         }
         runner.setSource(*m_sourceKey, itemCount, config.liveParticles);
         runner.setBatchChunks(config.batchChunks);
+        runner.setSinkBatchChunks(std::min(std::max(m_tuning.sinkBatchChunks, 1u), config.batchChunks));
+        runner.setMultiDispatch(m_tuning.multiDispatch);
         if (m_tuning.stallTimeout)
             runner.setStallTimeout(*m_tuning.stallTimeout);
         Stats stats = runner.run();

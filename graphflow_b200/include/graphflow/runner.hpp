@@ -77,6 +77,8 @@ public:
         m_Q = q;
     }
     void setStallTimeout(std::chrono::milliseconds t) { m_stallTimeout = t; }
+    void setSinkBatchChunks(std::uint32_t q) { m_sinkQ = q == 0u ? 1u : q; }
+    void setMultiDispatch(bool on) { m_multiDispatch = on; }
 
     SchedulerStats run()
     {
@@ -163,16 +165,17 @@ public:
                     progress = true;
                 }
 
-                // 3) dispatch: sinks first, then round-robin
+                // 3) dispatch: sinks first, then round-robin (one node per iteration, or every
+                //    node that can take a batch with multiDispatch)
                 bool dispatched = false;
-                for (std::size_t k = 0; k < m_nodes.size() && !dispatched; ++k)
+                for (std::size_t k = 0; k < m_nodes.size() && (m_multiDispatch || !dispatched); ++k)
                     if (m_nodes[k].role == NodeRole::sink)
-                        dispatched = tryDispatch(k, reservedTotal, available, stats);
-                if (!dispatched)
-                    for (std::size_t j = 0; j < m_nodes.size() && !dispatched; ++j) {
+                        dispatched = tryDispatch(k, reservedTotal, available, stats) || dispatched;
+                if (m_multiDispatch || !dispatched)
+                    for (std::size_t j = 0; j < m_nodes.size() && (m_multiDispatch || !dispatched); ++j) {
                         const std::size_t k = (m_roundRobin + j) % m_nodes.size();
                         if (m_nodes[k].role != NodeRole::sink)
-                            dispatched = tryDispatch(k, reservedTotal, available, stats);
+                            dispatched = tryDispatch(k, reservedTotal, available, stats) || dispatched;
                     }
                 ++m_roundRobin;
                 progress = progress || dispatched;
@@ -253,7 +256,11 @@ private:
         Node& node = m_nodes[k];
         if (node.ready.empty() || node.inflight)
             return false;
-        std::size_t wanted = node.role == NodeRole::transform ? std::min<std::size_t>(m_Q, node.ready.size()) : 1u;
+        std::size_t wanted = 1u;
+        if (node.role == NodeRole::transform)
+            wanted = std::min<std::size_t>(m_Q, node.ready.size());
+        else if (node.role == NodeRole::sink)
+            wanted = std::min<std::size_t>(m_sinkQ, node.ready.size());
         std::uint32_t reserve = 0u;
         if (node.role == NodeRole::transform) {
             std::uint64_t n = 0;
@@ -336,6 +343,8 @@ private:
     std::uint64_t m_sourceParticles = 0;
     std::uint32_t m_live = 0;
     std::uint32_t m_Q = 1;
+    std::uint32_t m_sinkQ = 1;
+    bool m_multiDispatch = false;
     std::size_t m_roundRobin = 0;
     std::chrono::milliseconds m_stallTimeout{60000};
 };

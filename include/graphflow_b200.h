@@ -101,7 +101,11 @@ uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap);
  *                key columns); 0 = always the
  *                per-tile look-back kernel. Per-port counts, the plan and every port's sequence are
  *                identical either way; the cooperative kernel also takes the output chunks in plan
- *                order (table[B + f] = reserved[f]). */
+ *                order (table[B + f] = reserved[f]).
+ *   "runner_batched" 1 (default) = the flow entry points (gf_run_particle_feedback,
+ *                gf_run_dense_chain, gf_run_photon) let a sink take up to Q ready chunks per launch
+ *                and dispatch every idle node in one scheduler iteration; 0 = the reference
+ *                runner's one-chunk sinks and one dispatch per iteration. Results are identical. */
 gf_status gf_set_tuning(const char* name, int value);
 
 /* ---- dense partition: the reference's two-launch form --------------------------------------- */
