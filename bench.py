@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--n", type=int, default=N_KEYS)
     p.add_argument("--no-sweep", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-extra", action="store_true", help="skip the other configurations' measurements")
     return p.parse_args()
 
 
@@ -417,6 +418,9 @@ def gpu_arm(args):
         cpu = {"value": v, "unit": "particles/s", "cores": threads, "kind": "port",
                "sample": f"{sample_n} u32 keys (same B, distribution, C; T=128 tiles), median of 3 passes of "
                          f"classify->plan->scatter over a chunk pool ({t:.3f} s each)"}
+    extra = None
+    if rank == 0 and world == 1 and not args.no_extra:
+        extra = other_configs(peak)
     if world > 1:
         dist_mod.destroy_process_group()
     if rank != 0:
@@ -444,8 +448,161 @@ def gpu_arm(args):
                   "form": "classify kernel + host plan + scatter kernel (reference structure)"},
         "correct": bool(correct),
         "sweep": sweep,
+        "configs": extra,
     }
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------
+# The other configurations (bounded samples; each entry states its size)
+# ------------------------------------------------------------------------------------------------
+def _timed(f):
+    import torch
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    r = f()
+    torch.cuda.synchronize()
+    return r, time.perf_counter() - t
+
+
+def _cfg_particle_feedback():
+    """particle_feedback: N = 1e6, seed 42, C = 1024, P = 4096, Q = 1, 64 visits; the sorted weight
+    histogram must match the oracle's scalar model row for row and sum to N."""
+    import numpy as np
+    from graphflow_b200 import capi
+    from oracle import oracle as O
+    n = 1_000_000
+    out = {"workload": "particle_feedback N=1e6 seed 42 C=1024 P=4096 Q=1 maxVisits=64"}
+    (w, c, st), _ = _timed(lambda: capi.run_particle_feedback(42, n, chunk_capacity=1024, live_particles=4096,
+                                                             batch_chunks=1, fused=True))
+    out["flow_fused"] = {"seconds": st.seconds, "particles_per_s": n / st.seconds,
+                         "partition_batches": st.partition_batches, "kernel_launches": st.kernel_launches}
+    capi.check(capi.lib().gf_set_tuning(b"runner_batched", 0), "tuning")
+    try:
+        (w0, c0, st0), _ = _timed(lambda: capi.run_particle_feedback(42, n, chunk_capacity=1024, live_particles=4096,
+                                                                    batch_chunks=1, fused=False))
+    finally:
+        capi.check(capi.lib().gf_set_tuning(b"runner_batched", 1), "tuning")
+    out["flow_plain_reference_runner"] = {"seconds": st0.seconds, "particles_per_s": n / st0.seconds}
+    threads = O.cpu_threads()
+    ref, cpu_s = _timed(lambda: O.particle_scalar(42, n, 64, threads=threads))
+    vals, counts = np.unique(w, return_counts=True)
+    exp_vals, exp_counts = O.histogram_u32(ref[0])
+    out["histogram_rows"] = int(len(vals))
+    out["histogram_sum"] = int(counts.sum())
+    out["histogram_matches_oracle"] = bool(np.array_equal(vals, exp_vals) and np.array_equal(counts, exp_counts))
+    out["forms_identical"] = bool(np.array_equal(w, w0) and np.array_equal(c, c0))
+    out["cpu_scalar_model"] = {"seconds": cpu_s, "particles_per_s": n / cpu_s, "cores": threads,
+                               "kind": "port (tests/reference/ScalarModel.hpp restated: per-particle loop, no runner)"}
+    return out
+
+
+def _cfg_dense_flow():
+    """The dense sweep through the public Flow: B = 64 uniform keys, C = 8192, P = 16384, Q = 8."""
+    from graphflow_b200 import capi
+    out = {"workload": "dense chain through Flow, B=64 uniform, C=8192 P=16384 Q=8 (records {u32 id, u32 key})"}
+
+    def run(nodes, n, fused, batched):
+        capi.check(capi.lib().gf_set_tuning(b"runner_batched", int(batched)), "tuning")
+        try:
+            _, st = capi.run_dense_chain(42, n, 64, nodes=nodes, dist="uniform", chunk_capacity=8192,
+                                         live_particles=16384, batch_chunks=8, fused=fused, want_ports=False)
+        finally:
+            capi.check(capi.lib().gf_set_tuning(b"runner_batched", 1), "tuning")
+        return {"n": n, "seconds": st.seconds, "particles_per_s": n / st.seconds,
+                "partition_batches": st.partition_batches, "kernel_launches": st.kernel_launches}
+    out["nodes1_fused_b200_runner"] = run(1, 100_000_000, True, True)
+    out["nodes1_plain_reference_runner"] = run(1, 10_000_000, False, False)
+    out["nodes4_fused_b200_runner"] = run(4, 1_000_000, True, True)
+    out["nodes4_plain_reference_runner"] = run(4, 200_000, False, False)
+    return out
+
+
+def _cfg_hash(peak):
+    """Hash partition of N = 1e8 16-byte records {u64 key, f32 weight, u32 tag}, keys over K values
+    with Zipf(1.2) popularity; device-planned form (classify -> device plan -> scatter) vs the plain
+    form (classify -> host plan -> scatter). Chunk capacity per K keeps the exact plan's chunk
+    count (one partial chunk per non-empty port) within memory."""
+    import ctypes
+    import numpy as np
+    import torch
+    from graphflow_b200 import capi
+    from graphflow_b200.hashpart import HashPartition, RecordPool
+    n, salt, out = 100_000_000, 0x5EED, {}
+    for k, cap in ((1 << 10, 8192), (1 << 16, 2048), (1 << 20, 512)):
+        for layout in (capi.LAYOUT_SOA, capi.LAYOUT_AOS):
+            if layout == capi.LAYOUT_AOS and k != (1 << 16):
+                continue
+            n_in = -(-n // cap)
+            bound = capi.output_chunk_bound(n, cap, k)
+            pool = RecordPool(n_in + bound, cap, layout=layout)
+            cdf = torch.from_numpy(capi.zipf_cdf(1.2, k)).cuda()
+            capi.check(capi.lib().gf_generate_records16(None, 42, 0, n, cdf.data_ptr(), k, salt,
+                                                        ctypes.byref(pool.cols), layout), "generate")
+            fills = np.full(n_in, cap, np.uint32)
+            fills[-1] = n - cap * (n_in - 1)
+            chunks = np.arange(n_in, dtype=np.uint32)
+            for _ in range(n_in):
+                pool.free.popleft()
+            part = HashPartition(pool, k, salt, tile_size=1024, form="device", max_batch_particles=n)
+            tiles, d_tiles = part._tiles(chunks, fills)
+            part.reserved[:bound].copy_(torch.from_numpy(np.arange(n_in, n_in + bound, dtype=np.uint32).view(np.int32)))
+            for _ in range(2):
+                part.enqueue_device(d_tiles.data_ptr(), len(tiles), bound)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(5):
+                part.enqueue_device(d_tiles.data_ptr(), len(tiles), bound)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 5
+            name = f"K{k}_{'soa' if layout == capi.LAYOUT_SOA else 'aos'}_C{cap}"
+            entry = {"device_form_ms": ms, "records_per_s": n / (ms / 1e3),
+                     "hbm_frac": n * 32 / (ms / 1e3) / 1e9 / peak, "status": int(part.status.item())}
+            if layout == capi.LAYOUT_SOA:
+                plain = HashPartition(pool, k, salt, tile_size=1024, form="plain")
+                descs = plain.run(list(chunks), list(fills))[2]
+                pool.release([int(x) for x in descs[:, 0]])
+                (_, _, descs), sec = _timed(lambda: plain.run(list(chunks), list(fills)))
+                pool.release([int(x) for x in descs[:, 0]])
+                entry["plain_form_ms_wall"] = sec * 1e3
+                del plain
+            out[name] = entry
+            del pool, part
+            torch.cuda.empty_cache()
+    out["workload"] = "hash partition, N=1e8 16-byte records, Zipf 1.2 over K keys, tiles of 1024"
+    return out
+
+
+def _cfg_photon():
+    """photon_scattering (weighted Henyey-Greenstein slab, FP32): the one-kernel transport at N = 1e8,
+    the Flow graph at N = 1e6, and the FP64 CPU restatement at N = 1e5 (photons/s)."""
+    from graphflow_b200 import capi
+    from oracle import oracle as O
+    p = capi.photon_params()
+    out = {"workload": "slab L=1, mu_s=10, mu_a=0.1, g=0.9, roulette below 1e-4, 256-bin exit histograms, FP32"}
+    capi.run_photon(42, 1_000_000, p, exec_mode=capi.EXEC_FUSED, records=False)
+    r = capi.run_photon(42, 100_000_000, p, exec_mode=capi.EXEC_FUSED, records=False)
+    out["transport_kernel_n1e8"] = {"seconds": r["stats"].seconds, "photons_per_s": 1e8 / r["stats"].seconds,
+                                    "event_counts": [int(x) for x in r["event_counts"]]}
+    r = capi.run_photon(42, 1_000_000, p, exec_mode=capi.EXEC_FLOW, records=False)
+    out["flow_n1e6"] = {"seconds": r["stats"].seconds, "photons_per_s": 1e6 / r["stats"].seconds}
+    threads = O.cpu_threads()
+    _, sec = _timed(lambda: O.photon_hg(42, 100_000, threads=threads))
+    out["cpu_fp64_n1e5"] = {"seconds": sec, "photons_per_s": 1e5 / sec, "cores": threads, "kind": "port"}
+    return out
+
+
+def other_configs(peak):
+    out = {}
+    for name, f in (("particle_feedback", _cfg_particle_feedback), ("dense_flow", _cfg_dense_flow),
+                    ("hash", lambda: _cfg_hash(peak)), ("photon", _cfg_photon)):
+        try:
+            out[name] = f()
+        except Exception as e:  # reported, never silent
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+    return out
 
 
 def bench_reserve_cap(args):
