@@ -71,6 +71,7 @@ _SIGS = {
     "gf_generate_records16": [_VP, _U64, _U64, _U64, _VP, _U32, _U64, _VP, _I32],
     "gf_run_particle_feedback": [_U64, _U64, _U32, _U32, _U32, _U32, _I32, _I32, _VP, _VP, _VP],
     "gf_set_tuning": [C.c_char_p, _I32],
+    "gf_run_particle_feedback_kernel": [_U64, _U64, _U32, _VP, _VP, _VP],
     "gf_run_dense_chain": [_U64, _U64, _U32, _U32, _I32, C.c_double, _U32, _U32, _U32, _I32, _I32, _VP, _VP],
     "gf_run_photon": [_U64, _U64, _U64, _VP, _I32, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP],
 }
@@ -158,6 +159,19 @@ def run_particle_feedback(seed, n, max_visits=64, chunk_capacity=1024, live_part
                                         C.byref(stats))
     if rc != GF_OK:
         raise GfError(rc, "particle feedback: " + last_error())
+    return weights[:n], capped[:n], stats
+
+
+def run_particle_feedback_kernel(seed, n, max_visits=64):
+    """The feedback graph as one per-particle kernel. Returns (weights, capped, stats)."""
+    import numpy as np
+    weights = np.zeros(max(n, 1), np.uint32)
+    capped = np.zeros(max(n, 1), np.uint32)
+    stats = FlowStats()
+    rc = lib().gf_run_particle_feedback_kernel(seed, n, max_visits, weights.ctypes.data, capped.ctypes.data,
+                                               C.byref(stats))
+    if rc != GF_OK:
+        raise GfError(rc, "particle feedback kernel: " + last_error())
     return weights[:n], capped[:n], stats
 
 

@@ -125,4 +125,46 @@ gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visit
     });
 }
 
+gf_status gf_run_particle_feedback_kernel(uint64_t seed, uint64_t n, uint32_t max_visits, uint32_t* h_weights,
+                                          uint32_t* h_capped, gf_flow_stats* h_stats)
+{
+    using namespace graphflow;
+    using namespace graphflow::particle;
+    if (n != 0u && (h_weights == nullptr || h_capped == nullptr))
+        return GF_ERR_ARGUMENT;
+    return guarded([&] {
+        if (n != 0u && n - 1u > rng::maxStreamId)
+            throw std::overflow_error("graphflow::particle: particle ids exceed the RNG stream-id range");
+        if (max_visits > rng::maxStreamEvent)
+            throw std::overflow_error("graphflow::particle: max visits exceeds the RNG stream-event range");
+        cuda::Device device(0);
+        device.makeCurrent();
+        const std::size_t m = n ? n : 1u;
+        cuda::Buffer<std::uint32_t> weights(m), capped(m), status(1);
+        std::vector<std::uint32_t> init(m, missingWeight);
+        cuda::check(cudaMemcpy(weights.data(), init.data(), m * 4u, cudaMemcpyHostToDevice), "H2D");
+        cuda::check(cudaMemset(capped.data(), 0, m * 4u), "memset");
+        cuda::check(cudaMemset(status.data(), 0, 4u), "memset");
+        const auto t0 = std::chrono::steady_clock::now();
+        launchParticleTransport(nullptr, seed, 0u, n, max_visits, weights.data(), capped.data(), status.data(),
+                                device.multiProcessorCount());
+        cuda::check(cudaDeviceSynchronize(), "particle transport");
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::uint32_t st = 0;
+        cuda::check(cudaMemcpy(&st, status.data(), 4u, cudaMemcpyDeviceToHost), "D2H");
+        if (st != 0u)
+            throw BatchError(std::string("particle transport: device status reports ") +
+                             (st == GF_OVERFLOW ? "overflow" : "invalid"));
+        if (n != 0u) {
+            cuda::check(cudaMemcpy(h_weights, weights.data(), n * 4u, cudaMemcpyDeviceToHost), "D2H");
+            cuda::check(cudaMemcpy(h_capped, capped.data(), n * 4u, cudaMemcpyDeviceToHost), "D2H");
+        }
+        SchedulerStats s;
+        s.sourceGenerated = n;
+        s.sourceSunk = n;
+        s.kernelLaunches = n != 0u ? 1u : 0u;
+        fill_stats(s, sec, h_stats);
+    });
+}
+
 } // extern "C"

@@ -102,6 +102,68 @@ struct RecordCapped {
     }
 };
 
+// The whole feedback graph as one per-particle kernel. Each thread carries one particle from the
+// source through Filter and A/B (feedback back into Filter) to its sink, calling the graph's own
+// functors with the engines the Flow's stages use: node k (source 0, filter 1, A 2, B 3, sinks 4
+// and 5, in the order runParticleFeedback adds them) draws from purpose 2k at the payload's
+// (id, visit), its updater from 2k + 1, and the updater runs on every payload a partition emits.
+// Per particle the results are therefore those of the Flow run, with no batches and no host round
+// trips. Status word as the stages': overflow or invalid fail the run.
+__global__ void __launch_bounds__(256)
+    particle_transport_kernel(std::uint64_t seedMixed, std::uint64_t firstId, std::uint64_t n, std::uint32_t maxVisits,
+                              std::uint32_t* weights, std::uint32_t* capped, std::uint32_t* status)
+{
+    const GenerateParticles gen{};
+    const FilterByProperty filter{};
+    const SelectOutcome select{maxVisits};
+    const UpdateWeight upd[2] = {UpdateWeight{1000u}, UpdateWeight{1u}};
+    const RecordWeight sink{weights};
+    const RecordCapped cappedSink{weights, capped};
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
+        const std::uint64_t id = firstId + i;
+        Status st(status);
+        rng::Engine e0 = rng::makeEngine(seedMixed, id, 0u, rng::streamPurposeForNode(0u));
+        Particle p = invokeWithContext(gen, e0, st, id);
+        for (;;) {
+            rng::Engine ef = rng::engineFor(seedMixed, p, rng::streamPurposeForNode(1u));
+            const std::uint32_t side = static_cast<std::uint32_t>(invokeWithContext(filter, ef, st, p));
+            const std::uint32_t node = 2u + side; // A for bin 0, B for bin 1
+            rng::Engine es = rng::engineFor(seedMixed, p, rng::streamPurposeForNode(node));
+            const Outcome out = invokeWithContext(select, es, st, p);
+            rng::Engine eu = rng::engineFor(seedMixed, p, rng::streamPurposeForNode(node, 1u));
+            const std::uint32_t res = updateCode(invokeWithContext(upd[side], eu, st, out, p));
+            if (res != 0u) {
+                gf::set_status(status, res == 1u ? GF_OVERFLOW : GF_INVALID);
+                break;
+            }
+            const Acc acc{};
+            if (out == Outcome::sink) {
+                sink(acc, p);
+                break;
+            }
+            if (out == Outcome::capped) {
+                cappedSink(acc, p);
+                break;
+            }
+        }
+    }
+}
+
+// Enqueues the per-particle kernel for ids [firstId, firstId + n) on `stream`.
+inline void launchParticleTransport(cudaStream_t stream, std::uint64_t seed, std::uint64_t firstId, std::uint64_t n,
+                                    std::uint32_t maxVisits, std::uint32_t* weights, std::uint32_t* capped,
+                                    std::uint32_t* status, std::uint32_t sms)
+{
+    if (n == 0u)
+        return;
+    const std::uint64_t want = (n + 255u) / 256u;
+    const unsigned blocks = static_cast<unsigned>(std::min<std::uint64_t>(want, static_cast<std::uint64_t>(sms) * 16u));
+    particle_transport_kernel<<<blocks, 256, 0, stream>>>(gf::mix64(seed), firstId, n, maxVisits, weights, capped,
+                                                          status);
+    cuda::check(cudaGetLastError(), "particle transport launch");
+}
+
 // Builds and runs the feedback graph; weights/capped are device buffers of n entries that the
 // caller initialised (weights to missingWeight, capped to 0).
 template <typename TStorage>

@@ -253,6 +253,13 @@ typedef struct gf_flow_stats {
     double seconds; /* wall time of Flow::run */
 } gf_flow_stats;
 
+/* The same feedback graph with the same functors and RNG streams, run as one per-particle kernel
+ * (every particle carried from the source to its sink by one thread, no batches): h_weights and
+ * h_capped as gf_run_particle_feedback, identical values. No reference counterpart as an entry
+ * point; it is the fused execution of runParticleFeedback's graph. */
+gf_status gf_run_particle_feedback_kernel(uint64_t seed, uint64_t n, uint32_t max_visits, uint32_t* h_weights,
+                                          uint32_t* h_capped, gf_flow_stats* h_stats);
+
 /* The kernel-level dense sweep through the public Flow (flow/Flow.hpp:49-754 with the
  * reference's runner semantics, sched/GraphRunner.hpp): Generate -> `nodes` (1..4) chained
  * partition nodes -> sink. Records are {u32 id, u32 key}; keys are gf_generate_keys_u32's for the

@@ -62,3 +62,16 @@ def test_feedback_invalid_configuration_is_reported():
     with pytest.raises(capi.GfError) as e:
         capi.run_particle_feedback(42, 100, 64, chunk_capacity=0)
     assert e.value.code == capi.GF_ERR_ARGUMENT
+
+
+@pytest.mark.parametrize("n,seed,max_visits", [(1, 42, 64), (300_007, 42, 64), (100_000, 9, 0), (50_000, 3, 5)])
+def test_per_particle_kernel_matches_flow_and_oracle(n, seed, max_visits):
+    """The graph as one per-particle kernel gives the Flow run's weights and capped flags id for id."""
+    w, capped, stats = capi.run_particle_feedback_kernel(seed, n, max_visits)
+    ew, ecapped, _ = O.particle_scalar(seed, n, max_visits)
+    assert np.array_equal(w, ew)
+    assert np.array_equal(capped.astype(np.uint8), ecapped)
+    fw, fcapped, _ = capi.run_particle_feedback(seed, n, max_visits, chunk_capacity=1024, live_particles=8192,
+                                                batch_chunks=4)
+    assert np.array_equal(w, fw) and np.array_equal(capped, fcapped)
+    assert stats.sunk == n
