@@ -72,6 +72,7 @@ _SIGS = {
     "gf_run_particle_feedback": [_U64, _U64, _U32, _U32, _U32, _U32, _I32, _I32, _VP, _VP, _VP],
     "gf_set_tuning": [C.c_char_p, _I32],
     "gf_run_particle_feedback_kernel": [_U64, _U64, _U32, _VP, _VP, _VP],
+    "gf_serve": [_VP, _U32, _I32, _U64, _U32, _VP, _VP],
     "gf_run_dense_chain": [_U64, _U64, _U32, _U32, _I32, C.c_double, _U32, _U32, _U32, _I32, _I32, _VP, _VP],
     "gf_run_photon": [_U64, _U64, _U64, _VP, _I32, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP],
 }
@@ -173,6 +174,62 @@ def run_particle_feedback_kernel(seed, n, max_visits=64):
     if rc != GF_OK:
         raise GfError(rc, "particle feedback kernel: " + last_error())
     return weights[:n], capped[:n], stats
+
+
+# ---- request server ----
+REQ_PARTICLE_FEEDBACK, REQ_PHOTON, REQ_DENSE_CHAIN = 0, 1, 2
+SERVE_PLAIN, SERVE_BATCHED = 0, 1
+REQUEST_DTYPE = None
+RESULT_DTYPE = None
+
+
+def _serve_dtypes():
+    import numpy as np
+    global REQUEST_DTYPE, RESULT_DTYPE
+    if REQUEST_DTYPE is None:
+        REQUEST_DTYPE = np.dtype([("kind", "<u4"), ("bins", "<u4"), ("n", "<u8"), ("seed", "<u8"),
+                                  ("arrival_s", "<f8")])
+        RESULT_DTYPE = np.dtype([("admit_s", "<f8"), ("done_s", "<f8"), ("digest", "<u8"), ("status", "<u4"),
+                                 ("pad", "<u4")])
+    return REQUEST_DTYPE, RESULT_DTYPE
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("peak_bytes", C.c_uint64), ("peak_inflight", C.c_uint32),
+                ("pad", C.c_uint32)]
+
+
+def make_requests(count, seed=1, n_min=1_000, n_max=10_000_000, rate_per_s=None, photon_scale=100,
+                  chain_bins=(2, 8, 32)):
+    """A mixed request stream: Poisson arrivals at rate_per_s (all at t=0 if None), N log-uniform in
+    [n_min, n_max], topology uniform over particle_feedback / photon (N / photon_scale photons) /
+    dense chain (bins uniform over chain_bins), and a seed per request."""
+    import numpy as np
+    req_t, _ = _serve_dtypes()
+    rng = np.random.default_rng(seed)
+    r = np.zeros(count, req_t)
+    r["kind"] = rng.integers(0, 3, count)
+    n = np.exp(rng.uniform(np.log(n_min), np.log(n_max), count)).astype(np.uint64)
+    n = np.where(r["kind"] == REQ_PHOTON, np.maximum(n // photon_scale, 1), n)
+    r["n"] = n
+    r["bins"] = np.where(r["kind"] == REQ_DENSE_CHAIN, rng.choice(np.asarray(chain_bins), count), 0)
+    r["seed"] = rng.integers(1, 2**62, count, dtype=np.uint64)
+    r["arrival_s"] = 0.0 if rate_per_s is None else np.cumsum(rng.exponential(1.0 / rate_per_s, count))
+    return r
+
+
+def serve(requests, mode=SERVE_BATCHED, memory_cap_bytes=40 << 30, max_inflight=32):
+    """Serves a request array (make_requests' dtype). Returns (results array, ServeStats)."""
+    import numpy as np
+    req_t, res_t = _serve_dtypes()
+    req = np.ascontiguousarray(requests, dtype=req_t)
+    res = np.zeros(max(len(req), 1), res_t)
+    stats = ServeStats()
+    rc = lib().gf_serve(req.ctypes.data if len(req) else None, len(req), mode, memory_cap_bytes, max_inflight,
+                        res.ctypes.data, C.byref(stats))
+    if rc != GF_OK:
+        raise GfError(rc, "serve: " + last_error())
+    return res[:len(req)], stats
 
 
 def run_dense_chain(seed, n, bins, nodes=1, dist="uniform", zipf_s=1.1, chunk_capacity=8192, live_particles=16384,

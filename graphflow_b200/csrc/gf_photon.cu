@@ -163,3 +163,33 @@ extern "C" gf_status gf_run_photon(uint64_t seed, uint64_t first_id, uint64_t n,
                             h_stats);
     });
 }
+
+// Enqueues the FP32 transport of photons [0, n) with the parameters' model on `stream`, writing one
+// terminal record per photon to d_records (TerminalT<float>[n]) and counting deliveries in
+// d_visits (zeroed by the caller); failures go to d_status. Used by the request server.
+void gf_photon_enqueue_f32(cudaStream_t stream, const gf_photon_params& P, std::uint64_t seed, std::uint64_t n,
+                           void* d_records, std::uint32_t* d_visits, std::uint32_t* d_status, std::uint32_t sms)
+{
+    if (n == 0u)
+        return;
+    const SlabT<float> slab{static_cast<float>(P.thickness), static_cast<float>(P.sigma_s),
+                            static_cast<float>(P.sigma_a)};
+    RecordTerminalT<float> terminal{static_cast<TerminalT<float>*>(d_records), d_visits, nullptr, nullptr, 0u, nullptr};
+    const unsigned blocks = static_cast<unsigned>(std::min<std::uint64_t>((n + 255u) / 256u, sms * 64u));
+    if (P.model == GF_PHOTON_ANALOG)
+        transport_kernel<float><<<blocks, 256, 0, stream>>>(ProposeFlightT<float>{slab, P.max_scatters},
+                                                            AdvanceToEventT<float>{slab}, ScatterT<float>{P.isotropic != 0},
+                                                            terminal, gf::mix64(seed), 0u, n, d_status);
+    else
+        transport_kernel<float><<<blocks, 256, 0, stream>>>(
+            ProposeWeightedT<float>{slab,
+                                    WeightedT<float>{static_cast<float>(P.g), static_cast<float>(P.roulette_threshold),
+                                                     static_cast<float>(P.roulette_survival)},
+                                    P.max_scatters},
+            AdvanceToEventT<float>{slab}, ScatterHGT<float>{static_cast<float>(P.g)}, terminal, gf::mix64(seed), 0u, n,
+            d_status);
+    cuda::check(cudaGetLastError(), "photon transport launch");
+}
+
+// Size of one FP32 terminal record (the request server sizes its buffers with it).
+std::size_t gf_photon_record_bytes_f32() { return sizeof(TerminalT<float>); }

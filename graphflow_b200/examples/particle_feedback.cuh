@@ -109,7 +109,7 @@ struct RecordCapped {
 // (id, visit), its updater from 2k + 1, and the updater runs on every payload a partition emits.
 // Per particle the results are therefore those of the Flow run, with no batches and no host round
 // trips. Status word as the stages': overflow or invalid fail the run.
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
     particle_transport_kernel(std::uint64_t seedMixed, std::uint64_t firstId, std::uint64_t n, std::uint32_t maxVisits,
                               std::uint32_t* weights, std::uint32_t* capped, std::uint32_t* status)
 {

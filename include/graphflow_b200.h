@@ -260,6 +260,47 @@ typedef struct gf_flow_stats {
 gf_status gf_run_particle_feedback_kernel(uint64_t seed, uint64_t n, uint32_t max_visits, uint32_t* h_weights,
                                           uint32_t* h_capped, gf_flow_stats* h_stats);
 
+/* ---- request server (continuous batching; no reference counterpart) -------------------------- */
+
+/* Whole-flow request kinds: the particle_feedback graph (64 visits), the weighted FP32 photon slab
+ * (L=1, mu_s=10, mu_a=0.1, g=0.9, roulette below 1e-4), and a two-node dense classify chain over
+ * uniform u32 keys (bins in {2, 8, 32}, C=8192). */
+enum { GF_REQ_PARTICLE_FEEDBACK = 0, GF_REQ_PHOTON = 1, GF_REQ_DENSE_CHAIN = 2 };
+/* GF_SERVE_PLAIN: one request at a time in arrival order through the C++ Flow with plain partitions
+ * and the reference runner. GF_SERVE_BATCHED: continuous batching, every admitted request's whole
+ * flow on the device on its own stream, admitted while others run as stream slots and device
+ * memory (an arena capped at memory_cap_bytes) free up. */
+enum { GF_SERVE_PLAIN = 0, GF_SERVE_BATCHED = 1 };
+
+typedef struct gf_request {
+    uint32_t kind;    /* GF_REQ_* */
+    uint32_t bins;    /* dense chain: 2, 8 or 32; ignored otherwise */
+    uint64_t n;       /* particles (photons) of the request, < 2^32 */
+    uint64_t seed;
+    double arrival_s; /* arrival, seconds after the stream starts; non-decreasing */
+} gf_request;
+
+typedef struct gf_request_result {
+    double admit_s;  /* when the request was admitted (plain form: when it started) */
+    double done_s;   /* when its result was on the host; latency = done_s - arrival_s */
+    uint64_t digest; /* order-independent 64-bit digest of the per-particle result */
+    uint32_t status; /* gf_status of the request (GF_ERR_RANGE: larger than the memory cap) */
+    uint32_t pad;
+} gf_request_result;
+
+typedef struct gf_serve_stats {
+    double seconds;         /* stream start to the last completion */
+    uint64_t peak_bytes;    /* most device memory granted to requests at once */
+    uint32_t peak_inflight; /* most requests on the device at once */
+    uint32_t pad;
+} gf_serve_stats;
+
+/* Serves n_requests requests (sorted by arrival) and fills h_results[n_requests]. A request's
+ * digest is the same in either mode and alone or in a mix. max_inflight: 1..256 streams.
+ * Errors: GF_ERR_ARGUMENT before any work; per-request failures in h_results[i].status. */
+gf_status gf_serve(const gf_request* h_requests, uint32_t n_requests, int mode, uint64_t memory_cap_bytes,
+                   uint32_t max_inflight, gf_request_result* h_results, gf_serve_stats* h_stats);
+
 /* The kernel-level dense sweep through the public Flow (flow/Flow.hpp:49-754 with the
  * reference's runner semantics, sched/GraphRunner.hpp): Generate -> `nodes` (1..4) chained
  * partition nodes -> sink. Records are {u32 id, u32 key}; keys are gf_generate_keys_u32's for the
