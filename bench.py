@@ -594,10 +594,44 @@ def _cfg_photon():
     return out
 
 
+def _cfg_serving():
+    """Served mixed stream: whole-flow requests (particle_feedback; photon at 1/100 size; two-node
+    dense chain, B in {2, 8, 32}), N log-uniform, Poisson arrivals, device memory cap 40 GB, 32
+    streams. Both forms run a 256-request stream (N in [1e3, 1e5]); the served form also runs the
+    full 4096-request stream (N in [1e3, 1e7]), at 2000 arrivals/s and with every request arriving
+    at once (capacity). The plain form on the full stream would take tens of minutes."""
+    import numpy as np
+    from graphflow_b200 import capi
+
+    def summary(req, res, st):
+        lat = res["done_s"] - req["arrival_s"]
+        return {"requests": int(len(req)), "seconds": st.seconds, "flows_per_s": len(req) / st.seconds,
+                "p50_latency_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_latency_ms": float(np.percentile(lat, 99) * 1e3),
+                "peak_inflight": int(st.peak_inflight), "peak_bytes": int(st.peak_bytes),
+                "all_ok": bool(np.all(res["status"] == 0))}
+    out = {"workload": "mixed flow requests, Poisson arrivals, memory cap 40 GB, 32 streams"}
+    small = capi.make_requests(256, seed=7, n_min=1_000, n_max=100_000, rate_per_s=2000.0)
+    served, st_s = capi.serve(small, capi.SERVE_BATCHED, max_inflight=32)
+    plain, st_p = capi.serve(small, capi.SERVE_PLAIN)
+    out["stream256_n1e3_1e5_rate2000"] = {"served": summary(small, served, st_s), "plain": summary(small, plain, st_p),
+                                          "results_identical": bool(np.array_equal(served["digest"],
+                                                                                   plain["digest"]))}
+    full = capi.make_requests(4096, seed=8, n_min=1_000, n_max=10_000_000, rate_per_s=2000.0)
+    res, st = capi.serve(full, capi.SERVE_BATCHED, max_inflight=32)
+    out["stream4096_n1e3_1e7_rate2000_served"] = summary(full, res, st)
+    burst = full.copy()
+    burst["arrival_s"] = 0.0
+    res2, st2 = capi.serve(burst, capi.SERVE_BATCHED, max_inflight=32)
+    out["stream4096_n1e3_1e7_all_at_once_served"] = summary(burst, res2, st2)
+    out["stream4096_results_identical_across_arrivals"] = bool(np.array_equal(res["digest"], res2["digest"]))
+    return out
+
+
 def other_configs(peak):
     out = {}
     for name, f in (("particle_feedback", _cfg_particle_feedback), ("dense_flow", _cfg_dense_flow),
-                    ("hash", lambda: _cfg_hash(peak)), ("photon", _cfg_photon)):
+                    ("hash", lambda: _cfg_hash(peak)), ("photon", _cfg_photon), ("serving", _cfg_serving)):
         try:
             out[name] = f()
         except Exception as e:  # reported, never silent
