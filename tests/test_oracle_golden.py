@@ -150,3 +150,25 @@ def test_particle_scalar_max_visits_zero_caps_or_sinks():
     w, capped, ncap = O.particle_scalar(7, 5000, 0)
     assert np.all(w == 0)
     assert ncap == int(capped.sum()) and ncap > 0
+
+
+# ---- published full-size result: docs/benchmarks.md:32-34 and :72-77 of the reference ----
+# The reference's benchmark run at N=1e8, C=8192, P=16384, seed 42 (maxVisits 64) printed 260
+# histogram rows summing to exactly 1e8 whose sorted `weight,count` lines (tools/bench_matrix.sh:719,
+# 723: the rows after "# weight,count", `sort -t, -k1,1n -k2,2n`) hash to this SHA-256, identically
+# for every Q, C and P. A particle's weight does not depend on C, P or Q, so the scalar model
+# reproduces the text exactly.
+PUBLISHED_FEEDBACK_1E8_SHA256 = "21ab0aeb9ec72d380af2ce6e9631f8fa7b9111d24ff7831f272aa9f6a7be9dab"
+
+
+def histogram_text(weights):
+    vals, counts = O.histogram_u32(weights)
+    return "".join(f"{int(v)},{int(c)}\n" for v, c in zip(vals, counts)), len(vals), int(counts.sum())
+
+
+def test_particle_scalar_reproduces_the_published_1e8_histogram():
+    import hashlib
+    w, _, _ = O.particle_scalar(42, 100_000_000, 64)
+    text, rows, total = histogram_text(w)
+    assert rows == 260 and total == 100_000_000
+    assert hashlib.sha256(text.encode()).hexdigest() == PUBLISHED_FEEDBACK_1E8_SHA256

@@ -75,3 +75,15 @@ def test_per_particle_kernel_matches_flow_and_oracle(n, seed, max_visits):
                                                 batch_chunks=4)
     assert np.array_equal(w, fw) and np.array_equal(capped, fcapped)
     assert stats.sunk == n
+
+
+def test_per_particle_kernel_reproduces_the_published_1e8_histogram():
+    """N=1e8, seed 42, 64 visits on the GPU: the sorted weight,count rows hash to the SHA-256 the
+    reference published for its own benchmark run (docs/benchmarks.md:32-34)."""
+    import hashlib
+    w, capped, stats = capi.run_particle_feedback_kernel(42, 100_000_000, 64)
+    vals, counts = O.histogram_u32(w)
+    text = "".join(f"{int(v)},{int(c)}\n" for v, c in zip(vals, counts))
+    assert len(vals) == 260 and int(counts.sum()) == 100_000_000
+    assert hashlib.sha256(text.encode()).hexdigest() == (
+        "21ab0aeb9ec72d380af2ce6e9631f8fa7b9111d24ff7831f272aa9f6a7be9dab")
