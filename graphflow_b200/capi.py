@@ -73,6 +73,8 @@ _SIGS = {
     "gf_set_tuning": [C.c_char_p, _I32],
     "gf_run_particle_feedback_kernel": [_U64, _U64, _U32, _VP, _VP, _VP],
     "gf_serve": [_VP, _U32, _I32, _U64, _U32, _VP, _VP],
+    "gf_histogram_scratch_bytes": [_U64, _VP],
+    "gf_histogram_u32": [_VP, _VP, _U64, _VP, _U64, _VP, _VP, _VP, _VP],
     "gf_run_dense_chain": [_U64, _U64, _U32, _U32, _I32, C.c_double, _U32, _U32, _U32, _I32, _I32, _VP, _VP],
     "gf_run_photon": [_U64, _U64, _U64, _VP, _I32, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP],
 }
@@ -174,6 +176,30 @@ def run_particle_feedback_kernel(seed, n, max_visits=64):
     if rc != GF_OK:
         raise GfError(rc, "particle feedback kernel: " + last_error())
     return weights[:n], capped[:n], stats
+
+
+def histogram_u32(values, stream=None):
+    """Device histogram of a u32 CUDA tensor (int32 storage): sorted (values, counts) numpy arrays."""
+    import numpy as np
+    import torch
+    n = int(values.numel())
+    dev = values.device
+    need = C.c_uint64()
+    check(lib().gf_histogram_scratch_bytes(n, C.byref(need)), "histogram scratch")
+    scratch = torch.empty((need.value + 255) // 8 + 32, dtype=torch.int64, device=dev)
+    base = (scratch.data_ptr() + 255) & ~255
+    rows_v = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    rows_c = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    num = torch.zeros(1, dtype=torch.int32, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    check(lib().gf_histogram_u32(s, values.data_ptr() if n else None, n, base, need.value, rows_v.data_ptr(),
+                                 rows_c.data_ptr(), num.data_ptr(), status.data_ptr()), "histogram")
+    torch.cuda.synchronize()
+    if int(status.item()) != 0:
+        raise GfError(int(status.item()), "histogram: device status")
+    r = int(num.item())
+    return rows_v[:r].cpu().numpy().view(np.uint32), rows_c[:r].cpu().numpy().astype(np.uint64)
 
 
 # ---- request server ----

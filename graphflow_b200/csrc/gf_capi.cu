@@ -226,33 +226,11 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
                       scratch_bytes >= sizeof(FusedCtl) + 256u;
     if (coop) {
         // per-CTA port totals (64 words per CTA) live in the descriptor area of the scratch
-        uint32_t* cta_tot = reinterpret_cast<uint32_t*>(ctl + 1);
-        const uint64_t cap_ctas = (scratch_bytes - sizeof(FusedCtl)) / 256u;
         auto launch = [&]<typename S, typename Cls>(Cls cls) -> gf_status {
-            auto kernel = fused_partition_coop_kernel<S, Cls>;
-            cudaError_t err = allow_smem(kernel, S::kSmemBytes);
-            if (err != cudaSuccess)
-                return cuda_status(err);
-            int per_sm = 0;
-            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, S::kThreads, S::kSmemBytes);
-            if (err != cudaSuccess)
-                return cuda_status(err);
-            if (per_sm < 1)
-                return GF_ERR_CUDA;
-            uint64_t g = (uint64_t)per_sm * (uint64_t)device_sms();
-            g = std::min<uint64_t>(g, n_tiles);
-            g = std::min<uint64_t>(g, cap_ctas);
-            const uint32_t* a_in = d_keys_in;
-            uint32_t* a_out = d_keys_out;
-            Cls a_cls = cls;
-            FastDiv a_fd(capacity);
-            void* args[] = {&a_in,       &a_out,      &a_cls,         &capacity,           &a_fd,
-                            &pool_slots, &d_tiles,    &n_tiles,       &bins,               &d_reserved,
-                            &n_reserved, &d_totals,   &d_port_chunks, &max_chunks_per_port, &ctl,
-                            &cta_tot,    &d_status};
-            return cuda_status(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3((uint32_t)g),
-                                                           dim3(S::kThreads), args, S::kSmemBytes,
-                                                           as_stream(stream)));
+            return cuda_status(launch_fused_coop<S>(as_stream(stream), cls, d_keys_in, d_keys_out, capacity,
+                                                    pool_slots, d_tiles, n_tiles, bins, d_reserved, n_reserved,
+                                                    d_totals, d_port_chunks, max_chunks_per_port, ctl, scratch_bytes,
+                                                    d_status, device_sms()));
         };
         auto with_cls = [&]<typename S>() -> gf_status {
             if (classifier == GF_CLS_KEY_MOD || classifier == GF_CLS_ID_BALANCED) {

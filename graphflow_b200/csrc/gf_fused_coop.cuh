@@ -609,5 +609,43 @@ __global__ void __launch_bounds__(S::kThreads, 2)
     }
 }
 
+// Host side: one cooperative launch of the kernel with classifier `cls`; the grid is as many CTAs
+// as fit on the device at once, capped by the tiles and by the scratch (64 words per CTA after the
+// control block, whose reset words the caller zeroed on the stream).
+template <typename S, typename Cls>
+cudaError_t launch_fused_coop(cudaStream_t stream, Cls cls, const uint32_t* in, uint32_t* out, uint32_t capacity,
+                              uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t bins,
+                              const uint32_t* reserved, uint32_t n_reserved, uint32_t* totals,
+                              unsigned long long* port_chunks, uint32_t max_k, FusedCtl* ctl, uint64_t scratch_bytes,
+                              uint32_t* status, int sms)
+{
+    auto kernel = fused_partition_coop_kernel<S, Cls>;
+    cudaError_t err = cudaSuccess;
+    if (S::kSmemBytes > 48u * 1024u) {
+        err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmemBytes);
+        if (err != cudaSuccess)
+            return err;
+    }
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, S::kThreads, S::kSmemBytes);
+    if (err != cudaSuccess)
+        return err;
+    if (per_sm < 1)
+        return cudaErrorInvalidConfiguration;
+    uint64_t g = (uint64_t)per_sm * (uint64_t)sms;
+    g = g < n_tiles ? g : n_tiles;
+    const uint64_t cap_ctas = (scratch_bytes - sizeof(FusedCtl)) / 256u;
+    g = g < cap_ctas ? g : cap_ctas;
+    if (g == 0u)
+        return cudaErrorInvalidConfiguration;
+    uint32_t* cta_tot = reinterpret_cast<uint32_t*>(ctl + 1);
+    FastDiv fd(capacity);
+    void* args[] = {&in,       &out,        &cls,    &capacity, &fd,          &pool_slots,  &tiles,
+                    &n_tiles,  &bins,       &reserved, &n_reserved, &totals, &port_chunks, &max_k,
+                    &ctl,      &cta_tot,    &status};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3((uint32_t)g), dim3(S::kThreads),
+                                       args, S::kSmemBytes, stream);
+}
+
 } // namespace
 } // namespace gf

@@ -260,6 +260,20 @@ typedef struct gf_flow_stats {
 gf_status gf_run_particle_feedback_kernel(uint64_t seed, uint64_t n, uint32_t max_visits, uint32_t* h_weights,
                                           uint32_t* h_capped, gf_flow_stats* h_stats);
 
+/* ---- device histogram ---------------------------------------------------------------------- */
+
+/* examples/particle_feedback/ParticleTypes.hpp:206-219 histogramOf (sort + run-length encoding) on
+ * the GPU: the sorted (value, count) rows of d_values[n], n <= 2^31. The sort is a radix sort whose
+ * passes are the stable cooperative partition (6-bit digits; digits equal for every value are
+ * skipped). d_row_values / d_row_counts need room for n rows; *d_num_rows receives the row count,
+ * failures go to the caller-zeroed *d_status. The call waits once on `stream` (after one reduction
+ * that selects the passes); everything else is enqueued. Scratch: gf_histogram_scratch_bytes,
+ * 256-byte aligned. */
+gf_status gf_histogram_scratch_bytes(uint64_t n, uint64_t* h_bytes);
+gf_status gf_histogram_u32(void* stream, const uint32_t* d_values, uint64_t n, void* d_scratch,
+                           uint64_t scratch_bytes, uint32_t* d_row_values, unsigned long long* d_row_counts,
+                           uint32_t* d_num_rows, uint32_t* d_status);
+
 /* ---- request server (continuous batching; no reference counterpart) -------------------------- */
 
 /* Whole-flow request kinds: the particle_feedback graph (64 visits), the weighted FP32 photon slab
