@@ -138,6 +138,50 @@ def cpu_pool_pass(n, bins, dist, threads=0, reps=3):
     return n / statistics.median(times), statistics.median(times)
 
 
+class Ranks:
+    """One process per device, as torchrun starts them: rank and world from the environment, a
+    barrier and the max over ranks (NCCL on GPUs; gloo works the same way on CPU)."""
+
+    def __init__(self, backend="nccl", device=None, timeout_s=120):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.device = device
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            kw = {"device_id": device} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, x):
+        if self.dist is None:
+            return float(x)
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def whole_job_value(n_per_rank, world, ms):
+    """Particles per second of the whole job: every rank partitions its own n_per_rank keys and the
+    step takes the slowest rank's ms (weak scaling)."""
+    return world * n_per_rank / (ms / 1e3)
+
+
+REFERENCE_ARM_SECONDS = 90.0  # the reference arm's whole --steps/--warmup run stays near this
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -145,7 +189,24 @@ def reference_arm(args):
     from oracle import oracle as O
     threads = O.cpu_threads()
     import numpy as np
-    n = args.n
+    # each step is a bounded sample of the workload: size it from one probe step so that the whole
+    # run of warmup + steps takes about REFERENCE_ARM_SECONDS
+    probe = min(args.n, 1_000_000)
+    pk = O.generate_keys_u32(args.dist, SEED, probe, args.bins, zipf_s=1.1, threads=threads)
+    pn_in = -(-probe // CAPACITY)
+    pbound = O.output_chunk_bound(probe, CAPACITY, args.bins)
+    ppool = np.zeros((pn_in + pbound) * CAPACITY, np.uint32)
+    ppool[:probe] = pk
+    pfills = np.full(pn_in, CAPACITY, np.uint32)
+    pfills[-1] = probe - CAPACITY * (pn_in - 1)
+    ptiles = O.flatten_tiles(np.arange(pn_in, dtype=np.uint32), pfills, 128)
+    pfree = np.arange(pn_in, pn_in + pbound, dtype=np.uint32)
+    O.partition_pool_u32(ppool, CAPACITY, ptiles, args.bins, pfree, threads=threads, pool_out=ppool.copy())
+    t0 = time.perf_counter()
+    O.partition_pool_u32(ppool, CAPACITY, ptiles, args.bins, pfree, threads=threads, pool_out=ppool.copy())
+    per_key = max((time.perf_counter() - t0) / probe, 1e-10)
+    budget = REFERENCE_ARM_SECONDS / max(args.steps + args.warmup, 1)
+    n = int(min(args.n, max(100_000, budget / per_key)))
     keys = O.generate_keys_u32(args.dist, SEED, n, args.bins, zipf_s=1.1, threads=threads)
     n_in = -(-n // CAPACITY)
     bound = O.output_chunk_bound(n, CAPACITY, args.bins)
@@ -166,8 +227,9 @@ def reference_arm(args):
                              bin_ids=bin_ids)
     dt = (time.perf_counter() - t0) / max(args.steps, 1)
     value = n / dt
-    sample = (f"full workload: {n} u32 keys, B={args.bins} {args.dist}, C={CAPACITY}, T=128 tiles, "
-              f"classify->plan->scatter over a chunk pool, per step")
+    sample = (f"{n} of the workload's {args.n} u32 keys per step (B={args.bins} {args.dist}, C={CAPACITY}, "
+              f"T=128 tiles; classify->plan->scatter over a chunk pool), sized so the run takes about "
+              f"{REFERENCE_ARM_SECONDS:.0f} s")
     print(json.dumps({
         "impl": "reference", "metric": "particles/s", "value": value, "unit": "particles/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
@@ -257,27 +319,14 @@ class DenseBench:
 def gpu_arm(args):
     import numpy as np
     import torch
-    import torch.distributed as dist_mod
     from graphflow_b200 import capi
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        dist_mod.init_process_group("nccl", device_id=dev, timeout=__import__("datetime").timedelta(seconds=120))
-
-    def barrier():
-        if world > 1:
-            dist_mod.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist_mod.all_reduce(t, op=dist_mod.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks("nccl", dev)
+    world, rank = ranks.world, ranks.rank
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     stream = torch.cuda.Stream(device=dev)
     bench = DenseBench(args.n, args.bins, args.dist, args.tile, dev)
@@ -317,7 +366,7 @@ def gpu_arm(args):
     ms = max_over_ranks(t_start.elapsed_time(t_end) / args.steps)
     kernel_ms = statistics.mean(a.elapsed_time(b) for a, b in zip(k_start, k_end))
     correct &= bench.check_fused()
-    value = world * args.n / (ms / 1e3)
+    value = whole_job_value(args.n, world, ms)
 
     # -------- the per-tile fused kernel (no bulk-copy pipeline) on the same data, for comparison --------
     capi.check(capi.lib().gf_set_tuning(b"fused_coop", 0), "tuning")
@@ -421,8 +470,7 @@ def gpu_arm(args):
     extra = None
     if rank == 0 and world == 1 and not args.no_extra:
         extra = other_configs(peak)
-    if world > 1:
-        dist_mod.destroy_process_group()
+    ranks.close()
     if rank != 0:
         return
     line = {
