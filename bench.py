@@ -676,10 +676,44 @@ def _cfg_serving():
     return out
 
 
+def _cfg_tuning_and_graphs():
+    """The autotuner's choice of kernel and tile size for the headline batch (N = 1e8, B = 64
+    uniform) and for a small batch (N = 1e6), and the step time of a CUDA-graph replay of the fused
+    step (reset, partition, finish) against direct launches at both sizes."""
+    import numpy as np
+    import torch
+    from graphflow_b200 import autotune, capi
+    from graphflow_b200.partition import ChunkPool, FusedPartition
+    out = {}
+    for n in (100_000_000, 1_000_000):
+        best, table = autotune.tune_fused_partition(n, 64, tiles=(2048, 4096, 8192), reps=5)
+        out[f"fused_n{n}"] = {"best": best, "candidates": table}
+        cap = 8192
+        n_in = -(-n // cap)
+        bound = capi.output_chunk_bound(n, cap, 64)
+        pool = ChunkPool(n_in + bound, cap)
+        capi.check(capi.lib().gf_generate_keys_u32(None, capi.DIST_UNIFORM, SEED, 0, n, 64, None, pool.ptr()), "gen")
+        fills = np.full(n_in, cap, np.uint32)
+        fills[-1] = n - cap * (n_in - 1)
+        part = FusedPartition(pool, 64, tile_size=4096, max_batch_particles=n)
+        tl, d_tiles = part._tiles(np.arange(n_in, dtype=np.uint32), fills)
+        part.reserved[:bound].copy_(torch.from_numpy(np.arange(n_in, n_in + bound, dtype=np.uint32).view(np.int32)))
+        reps = 50
+        direct = autotune._events_ms(lambda: [part.enqueue(d_tiles, len(tl), bound) for _ in range(reps)], 3) / reps
+        graph = part.capture(d_tiles, len(tl), bound)
+        replay = autotune._events_ms(lambda: [graph.replay() for _ in range(reps)], 3) / reps
+        out[f"graph_n{n}"] = {"direct_step_ms": direct, "graph_replay_step_ms": replay,
+                              "status": int(part.status.item())}
+        del graph, part, pool
+        torch.cuda.empty_cache()
+    return out
+
+
 def other_configs(peak):
     out = {}
     for name, f in (("particle_feedback", _cfg_particle_feedback), ("dense_flow", _cfg_dense_flow),
-                    ("hash", lambda: _cfg_hash(peak)), ("photon", _cfg_photon), ("serving", _cfg_serving)):
+                    ("hash", lambda: _cfg_hash(peak)), ("photon", _cfg_photon), ("serving", _cfg_serving),
+                    ("tuning_and_graphs", _cfg_tuning_and_graphs)):
         try:
             out[name] = f()
         except Exception as e:  # reported, never silent

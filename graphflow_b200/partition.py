@@ -184,6 +184,22 @@ class FusedPartition(_Common):
                                      self.status.data_ptr()), "fused finish")
         self.launches += 1
 
+    def capture(self, d_tiles, n_tiles, n_reserved):
+        """Captures one batch step (control-block reset, fused launch, device finish) into a CUDA
+        graph for repeated replay on the same tiles, reservation and buffers. The launch epoch lives
+        in device memory and advances on every replay, so a replay equals a direct launch."""
+        graph = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(device=self.dev)
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            self.enqueue(d_tiles, n_tiles, n_reserved, side)  # warm-up: kernel attributes, lazy loading
+        torch.cuda.current_stream().wait_stream(side)
+        torch.cuda.synchronize()
+        with torch.cuda.graph(graph, stream=side):
+            self.enqueue(d_tiles, n_tiles, n_reserved, side)
+        torch.cuda.synchronize()
+        return graph
+
     def run(self, chunks, fills, stream=None):
         """One batch on `stream`; returns (totals, table, output descriptors)."""
         with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
