@@ -217,15 +217,13 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
         return cuda_status(cudaMemsetAsync(d_totals, 0, sizeof(uint32_t) * bins, as_stream(stream)));
     FusedCtl* ctl = static_cast<FusedCtl*>(d_scratch);
     unsigned long long* desc = reinterpret_cast<unsigned long long*>(ctl + 1);
-    cudaError_t e = cudaMemsetAsync(ctl, 0, kFusedCtlResetBytes, as_stream(stream));
-    if (e != cudaSuccess)
-        return cuda_status(e);
     const bool coop = g_fused_coop != 0 && bins <= 64u && (capacity & 3u) == 0u && capacity >= 4096u &&
                       tile_size <= 4096u && pool_slots < 0xFFFFFFFFull && (reinterpret_cast<uintptr_t>(d_keys_in) & 15u) == 0u &&
                       (reinterpret_cast<uintptr_t>(d_keys_out) & 15u) == 0u &&
-                      scratch_bytes >= sizeof(FusedCtl) + 256u;
+                      scratch_bytes >= sizeof(FusedCtl) + sizeof(CoopHdr) + 256u;
     if (coop) {
-        // per-CTA port totals (64 words per CTA) live in the descriptor area of the scratch
+        // the cooperative control block and the per-CTA port totals live in the descriptor area of
+        // the scratch; the launcher zeroes the control block's reset words
         auto launch = [&]<typename S, typename Cls>(Cls cls) -> gf_status {
             return cuda_status(launch_fused_coop<S>(as_stream(stream), cls, d_keys_in, d_keys_out, capacity,
                                                     pool_slots, d_tiles, n_tiles, bins, d_reserved, n_reserved,
@@ -246,6 +244,9 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
             return with_cls.template operator()<CoopShape<8>>();
         return with_cls.template operator()<CoopShape<32>>();
     }
+    cudaError_t e = cudaMemsetAsync(ctl, 0, kFusedCtlResetBytes, as_stream(stream));
+    if (e != cudaSuccess)
+        return cuda_status(e);
     return with_shape(tile_size, [&]<typename Shape>() -> gf_status {
         using Acc = U32Column;
         auto kernel = fused_partition_kernel<Shape, Acc, KeyClassify<Acc>, NoUpdate>;

@@ -7,21 +7,25 @@
 // wait for, and sum, the aggregates of the many tiles still in flight; this kernel takes one grid
 // barrier instead:
 //   phase 1  every CTA counts the keys of its contiguous range of tiles: bulk copies (TMA engine)
-//            keep three tiles in flight per CTA, threads count with packed 16-bit counters;
+//            keep the next tile in flight while threads count with packed 16-bit counters; the
+//            CTA's per-port totals go to its row of the scratch and are added to the batch totals;
 //   barrier  cooperative launch (all CTAs resident), bounded wait;
-//   plan     every CTA reads all CTAs' per-port totals and derives its own per-port base and the
-//            reference's dense plan, binBase[b] = sum_{b'<b} ceil(total_b' / C)
-//            (graph/DenseBinTable.hpp:39-91); port b's k-th output chunk is reserved[binBase[b] + k],
-//            so the chunk table equals the host plan's; the chunk ids this CTA will write to are
-//            fetched once into shared memory;
+//   plan     every CTA derives its own per-port base (the sum of the rows before it, or the batch
+//            total minus the rows after it, whichever is fewer rows) and the reference's dense
+//            plan, binBase[b] = sum_{b'<b} ceil(total_b' / C) (graph/DenseBinTable.hpp:39-91); port
+//            b's k-th output chunk is reserved[binBase[b] + k], so the chunk table equals the host
+//            plan's; the chunk ids this CTA will write to are fetched once into shared memory;
 //   phase 2  every CTA walks its tiles again, last tile first (the last tiles it counted are the ones
-//            still in L2). Per tile: a bulk copy two tiles ahead, a stable rank from per-thread packed
-//            counters and one padded raking scan (cost independent of the port distribution),
-//            staging in port order (each key with its output slot; with capacity >= 4096 a port's
-//            run of one tile touches at most two output chunks), and a write-out in which every
-//            thread stores stage positions tid, tid + 256, ... (coalesced along each run).
+//            still in L2). Per tile: a stable rank from per-thread 16-bit counters (thread t owns 33
+//            consecutive keys; shared-memory atomics return the local rank) and one padded raking
+//            scan with 128-bit accesses; staging in port order in the tile's own buffer; warp 0 cuts
+//            each port's run at its output-chunk boundary (at most two pieces) and marks where each
+//            piece starts in a bitmap of stage positions; in the write-out warp w copies stage
+//            positions [1024 w, 1024 w + 1024) in order, each lane finding its piece by a popcount
+//            of the bitmap, so every store of a warp is a coalesced run of slots.
 // Requirements (checked by the dispatcher): B <= 64, tiles of at most 4096 keys, capacity % 4 == 0
-// and >= 4096, at most 2^32 pool slots, key columns 16-byte aligned, scratch for 64 words per CTA.
+// and >= 4096, at most 2^32 pool slots, key columns 16-byte aligned, scratch for the control block
+// and 4 * B_max bytes per CTA.
 #pragma once
 
 #include "gf_partition.cuh"
@@ -104,14 +108,25 @@ struct AnyKeyClassify { // every other built-in rule
     GF_D uint32_t operator()(uint32_t k) const { return c((uint64_t)k); }
 };
 
-// 256 threads; LANES counter rows with two ports per row (up to 2 * LANES ports).
+// Control block of the cooperative kernel, right after the FusedCtl in the scratch; the launcher
+// zeroes its first kCoopHdrResetBytes on the stream before every launch. The per-CTA port totals
+// follow it.
+struct CoopHdr {
+    uint32_t total[64]; // batch per-port totals: atomic sums of the CTAs' counts
+    uint32_t done;      // grid-barrier arrivals
+    uint32_t pad[63];
+};
+constexpr uint32_t kCoopHdrResetBytes = 65u * sizeof(uint32_t);
+
+// 128 threads; LANES counter rows with two 16-bit port counters per word (up to 2 * LANES ports).
 template <int LANES>
 struct CoopShape {
-    static constexpr int kThreads = 256;
+    static constexpr int kThreads = 128;
     static constexpr int kWarps = kThreads / 32;
-    // Phase 2: thread t owns the 17 consecutive keys [17 t, 17 t + 17). An odd count makes the 32
-    // stage stores of a warp that all belong to one port run land in 32 different banks.
-    static constexpr int kIpt = 17;
+    // Phase 2: thread t owns the 33 consecutive keys [33 t, 33 t + 33). An odd count makes the key
+    // loads of a warp, and the stage stores of a warp whose keys all belong to one port run, land
+    // in 32 different banks.
+    static constexpr int kIpt = 33;
     static constexpr uint32_t kMaxCount = 4096u; // keys per tile
     static constexpr uint32_t kInWords = (uint32_t)kThreads * kIpt;
     static constexpr uint32_t kLanes = LANES;
@@ -119,19 +134,19 @@ struct CoopShape {
     static constexpr uint32_t kMaxBins = 2u * LANES;
     static constexpr uint32_t kBM = 64u; // per-port arrays are 64 wide whatever LANES is
     static constexpr uint32_t kMinCapacity = kMaxCount; // one tile's run of a port touches <= 2 chunks
-    static constexpr uint32_t kSeg = LANES + 1u;                           // raking segment (padded)
-    static constexpr uint32_t kIdCache = 512u; // chunk ids of this CTA's output held in shared memory
-    // shared memory (32-bit words). Phase 2 stages a tile in its own input buffer (its keys are in
-    // registers by then); phase 1's three-tile ring is in[0], in[1] and the slot array.
-    static constexpr uint32_t kIn = 0;                              // [2][kInWords]
-    static constexpr uint32_t kStage = kIn + 2u * kInWords;         // [kMaxCount] output slot per stage position
-    static constexpr uint32_t kRun = kStage + kMaxCount;            // [65] stage start of each port's run
-    // [64] x {stage position where the second chunk starts, slot - stage position in the first
-    // chunk, the same in the second chunk, unused}: one 16-byte load per staged key
-    static constexpr uint32_t kPort = (kRun + kBM + 4u + 3u) & ~3u;
-    static constexpr uint32_t kOff = kPort + 4u * kBM;              // [64] running port position
-    static constexpr uint32_t kCnt = kOff + kBM;                    // [kSeg][kThreads]
-    static constexpr uint32_t kBase = kCnt + kSeg * kThreads;       // [64] this CTA's first port position
+    // Raking segment: a multiple of 4 words so that it is read and written with 128-bit accesses;
+    // thread r's segment starts at word r * kSeg, which puts the eight threads of each quarter warp
+    // on eight disjoint groups of four banks.
+    static constexpr uint32_t kSeg = LANES == 2 ? 4u : LANES + 4u;
+    static constexpr uint32_t kIdCache = 128u; // chunk ids of this CTA's output held in shared memory
+    static constexpr uint32_t kMaxPieces = 2u * kMaxBins; // a port's run of one tile is cut at most once
+    static constexpr uint32_t kBmWords = kMaxCount / 32u;  // one bit per stage position
+    // shared memory (32-bit words)
+    static constexpr uint32_t kIn = 0;                              // [2][kInWords] tiles, staged in place
+    static constexpr uint32_t kCnt = kIn + 2u * kInWords;           // [kSeg * kThreads] counters
+    static constexpr uint32_t kPieces = kCnt + kSeg * kThreads;     // [kMaxPieces] {slot - stage position, ok}
+    static constexpr uint32_t kBm = kPieces + 2u * kMaxPieces;      // [kBmWords] stage positions where pieces start
+    static constexpr uint32_t kBase = kBm + kBmWords;               // [64] this CTA's first port position
     static constexpr uint32_t kTotal = kBase + kBM;                 // [64] batch totals
     static constexpr uint32_t kBinBase = kTotal + kBM;              // [64] dense plan
     static constexpr uint32_t kOwn = kBinBase + kBM;                // [64] this CTA's totals
@@ -139,13 +154,14 @@ struct CoopShape {
     static constexpr uint32_t kAcc = kKfirst + kBM;                 // [64] phase-1 flushed counts
     static constexpr uint32_t kIdOff = kAcc + kBM;                  // [65] id cache offsets
     static constexpr uint32_t kIds = kIdOff + kBM + 4u;             // [kIdCache]
-    static constexpr uint32_t kScan = kIds + kIdCache;              // [W]
-    static constexpr uint32_t kTiles = kScan + kWarps;              // [6][4] buffered tile descriptors
-    static constexpr uint32_t kMisc = kTiles + 24u;                 // [8]
-    static constexpr uint32_t kMbar = (kMisc + 8u + 1u) & ~1u;      // [3] x u64
-    static constexpr uint32_t kWords = kMbar + 6u;
+    static constexpr uint32_t kScan = kIds + kIdCache;              // [kWarps]
+    static constexpr uint32_t kTiles = kScan + 4u;                  // [4][4] tile descriptors (phase 1, phase 2)
+    static constexpr uint32_t kMisc = kTiles + 16u;                 // [8]
+    static constexpr uint32_t kMbar = kMisc + 8u;                   // [2] x u64
+    static constexpr uint32_t kWords = kMbar + 4u;
     static constexpr size_t kSmemBytes = sizeof(uint32_t) * kWords;
-    GF_D static uint32_t ring(uint32_t buf) { return buf == 0u ? kIn : buf == 1u ? kIn + kInWords : kStage; }
+    static_assert(kCnt % 4u == 0u && kPieces % 2u == 0u && kMbar % 2u == 0u, "alignment");
+    static_assert(kWarps == 4 && kMaxCount == (uint32_t)kWarps * 1024u, "write-out: one 1024-position quarter per warp");
 };
 
 // Grid-wide barrier of a cooperative launch on a counter reset before the launch. Bounded: a wait
@@ -196,24 +212,23 @@ GF_D void coop_fetch(const gf_tile* tiles, uint32_t t, const uint32_t* in, uint3
 }
 
 template <typename S, typename Classify>
-__global__ void __launch_bounds__(S::kThreads, 2)
+__global__ void __launch_bounds__(S::kThreads, 4)
     fused_partition_coop_kernel(const uint32_t* __restrict__ in, uint32_t* out, Classify cls, uint32_t capacity,
                                 FastDiv fdc, uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B,
                                 const uint32_t* reserved, uint32_t n_reserved, uint32_t* totals,
-                                unsigned long long* port_chunks, uint32_t max_k, FusedCtl* ctl, uint32_t* cta_tot,
-                                uint32_t* status)
+                                unsigned long long* port_chunks, uint32_t max_k, FusedCtl* ctl, CoopHdr* hdr,
+                                uint32_t* cta_tot, uint32_t* status)
 {
     constexpr int T = S::kThreads, IPT = S::kIpt, W = S::kWarps;
-    constexpr uint32_t BM = S::kBM, L = S::kLanes, SEG = S::kSeg;
+    constexpr uint32_t BM = S::kBM, L = S::kLanes, SEG = S::kSeg, MB = S::kMaxBins;
     extern __shared__ __align__(128) uint32_t sm[];
     uint32_t* cnt = sm + S::kCnt;
+    uint16_t* cnt16 = reinterpret_cast<uint16_t*>(cnt);
+    uint2* pieces = reinterpret_cast<uint2*>(sm + S::kPieces);
+    uint32_t* bm = sm + S::kBm;
     uint32_t* cbase = sm + S::kBase;
     uint32_t* total = sm + S::kTotal;
     uint32_t* bin_base = sm + S::kBinBase;
-    uint32_t* run_at = sm + S::kRun;
-    uint4* port4 = reinterpret_cast<uint4*>(sm + S::kPort);
-    uint32_t* off = sm + S::kOff;
-    uint32_t* oslot = sm + S::kStage;
     uint32_t* own = sm + S::kOwn;
     uint32_t* kfirst = sm + S::kKfirst;
     uint32_t* acc = sm + S::kAcc;
@@ -225,6 +240,7 @@ __global__ void __launch_bounds__(S::kThreads, 2)
     uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + S::kMbar);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, w = tid >> 5;
     const uint32_t G = gridDim.x, c = blockIdx.x;
+    auto buffer = [](uint32_t buf) { return S::kIn + buf * S::kInWords; };
 
     // this CTA's tiles: [t_lo, t_hi) of an even split
     const uint32_t t_lo = (uint32_t)((uint64_t)n_tiles * c / G);
@@ -232,9 +248,8 @@ __global__ void __launch_bounds__(S::kThreads, 2)
     const uint32_t n_mine = t_hi - t_lo;
     if (tid == 0) {
         misc[0] = next_epoch(ld_relaxed_u32(&ctl->epoch));
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-            mbar_init(&mbar[i], 1u);
+        mbar_init(&mbar[0], 1u);
+        mbar_init(&mbar[1], 1u);
         mbar_init_fence();
     }
     for (uint32_t i = tid; i < SEG * T; i += T)
@@ -244,10 +259,10 @@ __global__ void __launch_bounds__(S::kThreads, 2)
     __syncthreads();
     const uint32_t epoch = misc[0];
 
-    // ---------------- phase 1: per-port counts of this CTA's tiles (forward, three in flight) ----------------
+    // ---------------- phase 1: per-port counts of this CTA's tiles (forward, two buffers) ----------------
     if (tid == 0)
-        for (uint32_t q = 0; q < 3u && q < n_mine; ++q)
-            coop_fetch(tiles, t_lo + q, in, capacity, pool_slots, S::kMaxCount, sm, S::ring(q), &mbar[q],
+        for (uint32_t q = 0; q < 2u && q < n_mine; ++q)
+            coop_fetch(tiles, t_lo + q, in, capacity, pool_slots, S::kMaxCount, sm, buffer(q), &mbar[q],
                        tdesc + 4u * q, status);
     bool bad = false;
     auto count_key = [&](uint32_t key) {
@@ -257,8 +272,8 @@ __global__ void __launch_bounds__(S::kThreads, 2)
         else
             bad = true;
     };
-    // adds the packed counters into acc[] and clears them (a thread counts at most 16 keys per tile,
-    // so 2048 tiles between flushes keep every 16-bit counter below 2^15)
+    // adds the packed counters into acc[] and clears them (a thread counts at most 32 keys per tile,
+    // so 1024 tiles between flushes keep every 16-bit counter at or below 2^15)
     auto flush = [&]() {
         for (uint32_t r = w; r < L; r += W) {
             uint32_t lo = 0, hi = 0;
@@ -278,12 +293,12 @@ __global__ void __launch_bounds__(S::kThreads, 2)
         __syncthreads();
     };
     for (uint32_t q = 0; q < n_mine; ++q) {
-        const uint32_t buf = q % 3u;
+        const uint32_t buf = q & 1u;
         const uint32_t* d = tdesc + 4u * buf;
-        mbar_wait(&mbar[buf], (q / 3u) & 1u, status);
+        mbar_wait(&mbar[buf], (q >> 1) & 1u, status);
         const uint32_t count = d[2], flags = d[3];
         if (flags & 2u) {
-            const uint4* v = reinterpret_cast<const uint4*>(sm + S::ring(buf));
+            const uint4* v = reinterpret_cast<const uint4*>(sm + buffer(buf));
 #pragma unroll
             for (uint32_t j = 0; j < S::kMaxCount / 4u / (uint32_t)T; ++j) {
                 const uint32_t vi = tid + j * (uint32_t)T;
@@ -305,10 +320,10 @@ __global__ void __launch_bounds__(S::kThreads, 2)
         }
         fence_proxy_async_smem(); // this buffer's reads come before the next bulk copy into it
         __syncthreads();
-        if (tid == 0 && q + 3u < n_mine)
-            coop_fetch(tiles, t_lo + q + 3u, in, capacity, pool_slots, S::kMaxCount, sm, S::ring(buf), &mbar[buf],
+        if (tid == 0 && q + 2u < n_mine)
+            coop_fetch(tiles, t_lo + q + 2u, in, capacity, pool_slots, S::kMaxCount, sm, buffer(buf), &mbar[buf],
                        tdesc + 4u * buf, status);
-        if ((q & 2047u) == 2047u)
+        if ((q & 1023u) == 1023u)
             flush();
     }
     if (bad)
@@ -317,53 +332,65 @@ __global__ void __launch_bounds__(S::kThreads, 2)
     if (tid < BM) {
         const uint32_t v = tid < B ? acc[tid] : 0u;
         own[tid] = v;
-        cta_tot[(size_t)c * BM + tid] = v;
+        if (tid < MB) {
+            cta_tot[(size_t)c * MB + tid] = v;
+            if (v != 0u)
+                atomicAdd(&hdr->total[tid], v);
+        }
     }
-    // phase 2 walks the tiles last to first through in[0] and in[1]; its first two tiles are
+    // phase 2 walks the tiles last to first through the same two buffers; its first two tiles are
     // fetched across the barrier. Uses of each buffer so far set the mbarrier parities.
-    const uint32_t use0 = (n_mine + 2u) / 3u, use1 = (n_mine + 1u) / 3u;
+    const uint32_t use0 = (n_mine + 1u) / 2u, use1 = n_mine / 2u;
     if (tid == 0)
         for (uint32_t k = 0; k < 2u && k < n_mine; ++k)
-            coop_fetch(tiles, t_hi - 1u - k, in, capacity, pool_slots, S::kMaxCount, sm, S::ring(k), &mbar[k],
-                       tdesc + 16u + 4u * k, status);
+            coop_fetch(tiles, t_hi - 1u - k, in, capacity, pool_slots, S::kMaxCount, sm, buffer(k), &mbar[k],
+                       tdesc + 8u + 4u * k, status);
 
-    coop_grid_barrier(&ctl->done, status);
+    coop_grid_barrier(&hdr->done, status);
 
     // ---------------- plan ----------------
     {
-        // thread tid covers port b = tid % 64 of CTAs c' = tid / 64, + 4, + 8, ...
-        const uint32_t b = tid % BM;
-        constexpr uint32_t kStride = (uint32_t)T / BM;
-        uint32_t below = 0, all = 0;
-        for (uint32_t c0 = tid / BM; c0 < G; c0 += kStride * 8u) {
-            uint32_t v[8];
+        // this CTA's per-port base from the fewer of the rows before it and the rows after it:
+        // thread tid sums ports [4 qd, 4 qd + 4) of rows g, g + NG, ... with 128-bit loads
+        constexpr uint32_t QUADS = MB / 4u, NG = (uint32_t)T / QUADS;
+        const uint32_t qd = tid % QUADS, g = tid / QUADS;
+        const bool before = c <= G - 1u - c;
+        const uint32_t r_lo = before ? 0u : c + 1u, r_hi = before ? c : G;
+        uint4 s = make_uint4(0u, 0u, 0u, 0u);
+        for (uint32_t r0 = r_lo + g; r0 < r_hi; r0 += NG * 8u) {
+            uint4 v[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-                const uint32_t cc = c0 + (uint32_t)u * kStride;
-                v[u] = cc < G ? ld_relaxed_u32(cta_tot + (size_t)cc * BM + b) : 0u;
+                const uint32_t rr = r0 + (uint32_t)u * NG;
+                v[u] = rr < r_hi ? __ldcg(reinterpret_cast<const uint4*>(cta_tot + (size_t)rr * MB) + qd)
+                                 : make_uint4(0u, 0u, 0u, 0u);
             }
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-                const uint32_t cc = c0 + (uint32_t)u * kStride;
-                all += v[u];
-                below += cc < c ? v[u] : 0u;
+                s.x += v[u].x;
+                s.y += v[u].y;
+                s.z += v[u].z;
+                s.w += v[u].w;
             }
         }
-        uint32_t* red = sm + S::kStage; // stage buffer 0 is unused until phase 2
-        red[tid] = all;
-        red[T + tid] = below;
+        uint4* red = reinterpret_cast<uint4*>(cnt); // the counters are zero now and are zeroed again below
+        red[tid] = s;
         __syncthreads();
         if (tid < BM) {
-            uint32_t a = 0, bl = 0;
-#pragma unroll
-            for (uint32_t j = 0; j < kStride; ++j) {
-                a += red[j * BM + tid];
-                bl += red[T + j * BM + tid];
+            uint32_t part = 0;
+            if (tid < MB) {
+                const uint32_t q = tid >> 2, e = tid & 3u;
+                for (uint32_t g2 = 0; g2 < NG; ++g2) {
+                    const uint4 x = red[g2 * QUADS + q];
+                    part += e == 0u ? x.x : e == 1u ? x.y : e == 2u ? x.z : x.w;
+                }
             }
-            total[tid] = tid < B ? a : 0u;
-            cbase[tid] = tid < B ? bl : 0u;
+            const uint32_t tot = tid < B ? ld_relaxed_u32(&hdr->total[tid]) : 0u;
+            total[tid] = tot;
+            cbase[tid] = tid < B ? (before ? part : tot - own[tid] - part) : 0u;
         }
         __syncthreads();
+        red[tid] = make_uint4(0u, 0u, 0u, 0u);
         if (w == 0) {
             // binBase = exclusive scan of ceil(total / C); first chunk and chunk count of this CTA's
             // range per port (two ports per lane)
@@ -442,7 +469,13 @@ __global__ void __launch_bounds__(S::kThreads, 2)
             misc[2] = ld_relaxed_u32(status);
         __syncthreads();
     }
-    const bool failed = misc[2] != 0u;
+    if (misc[2] != 0u) {
+        // a failed batch writes nothing: wait for this CTA's two phase-2 copies, then leave
+        if (tid == 0)
+            for (uint32_t k = 0; k < 2u && k < n_mine; ++k)
+                mbar_wait(&mbar[k], (k == 0u ? use0 : use1) & 1u, status);
+        return;
+    }
     const uint32_t R = misc[1];
 
     // chunk id of port b's k-th output chunk (k inside this CTA's range of the port)
@@ -453,18 +486,27 @@ __global__ void __launch_bounds__(S::kThreads, 2)
         const uint32_t f = bin_base[b] + k;
         return f < R && f < n_reserved ? __ldg(reserved + f) : kNoChunk;
     };
+    // a chunk id outside the pool writes nothing and fails the batch
+    auto in_pool = [&](uint32_t ch) {
+        const bool okc = ch != kNoChunk && ((uint64_t)ch + 1u) * capacity <= pool_slots;
+        if (!okc)
+            set_status(status, GF_OVERFLOW);
+        return okc;
+    };
 
-    // running port positions: the end of this CTA's range (its tiles are walked last to first)
-    if (tid < BM)
-        off[tid] = cbase[tid] + own[tid];
-    __syncthreads();
+    // warp 0 keeps the running port positions (two ports per lane): the end of this CTA's range,
+    // since its tiles are walked last to first
+    uint32_t off0 = 0, off1 = 0;
+    if (w == 0) {
+        off0 = cbase[2u * lane] + own[2u * lane];
+        off1 = cbase[2u * lane + 1u] + own[2u * lane + 1u];
+    }
 
     // ---------------- phase 2: rank, stage, write (tiles last to first) ----------------
     for (uint32_t k = 0; k < n_mine; ++k) {
         const uint32_t buf = k & 1u;
-        const uint32_t* d = tdesc + 16u + 4u * buf;
-        uint32_t* tin = sm + S::ring(buf);
-        uint32_t* stage = tin; // the keys are in registers once counted
+        const uint32_t* d = tdesc + 8u + 4u * buf;
+        uint32_t* tin = sm + buffer(buf);
         mbar_wait(&mbar[buf], ((buf == 0u ? use0 : use1) + (k >> 1)) & 1u, status);
         const uint32_t count = d[2], flags = d[3];
         uint32_t key[IPT];
@@ -480,34 +522,34 @@ __global__ void __launch_bounds__(S::kThreads, 2)
                 key[i] = it < count ? __ldg(in + base + it) : 0u;
             }
         }
-        // count: local rank among this thread's earlier keys of the same port
-        uint32_t bp[IPT];
+        // count: a key's local rank is its 16-bit counter before the increment (the atomics of one
+        // thread are independent instructions, so they issue back to back); a slot past the tile's
+        // count adds 0 (its key is never staged)
+        uint32_t pk[IPT];
 #pragma unroll
         for (int i = 0; i < IPT; ++i) {
-            const uint32_t it = tid * IPT + (uint32_t)i;
-            uint32_t b = kNoBin16, lr = 0;
-            if (it < count) {
-                b = cls(key[i]);
-                if (b >= B)
-                    b = kNoBin16; // reported by phase 1
-            }
-            if (b != kNoBin16) {
-                const uint32_t sh = (b >> S::kLaneShift) << 4;
-                uint32_t* ctr = cnt + (b & (L - 1u)) * T + tid;
-                const uint32_t old = *ctr;
-                *ctr = old + (1u << sh);
-                lr = (old >> sh) & 0xFFFFu;
-            }
-            bp[i] = b | (lr << 16);
+            const uint32_t valid = tid * IPT + (uint32_t)i < count ? 1u : 0u;
+            uint32_t b = cls(key[i]);
+            b = b < B ? b : 0u;
+            const uint32_t wi = (b & (L - 1u)) * T + tid;
+            const uint32_t half = b >> S::kLaneShift;
+            const uint32_t old = atomicAdd(cnt + wi, valid << (half << 4));
+            pk[i] = ((wi << 1) | half) | (((old >> (half << 4)) & 0xFFFFu) << 16);
         }
         __syncthreads();
+        // the other buffer's last reader (the previous tile's write-out) is done: fetch the next tile
+        if (tid == 0 && k >= 1u && k + 1u < n_mine)
+            coop_fetch(tiles, t_hi - 2u - k, in, capacity, pool_slots, S::kMaxCount, sm, buffer(buf ^ 1u),
+                       &mbar[buf ^ 1u], tdesc + 8u + 4u * (buf ^ 1u), status);
 
-        // raking scan over the (lane, thread) counters, padded segments of SEG words
-        uint32_t* seg = cnt + tid * SEG;
+        // raking scan over the (row, thread) counters: segments of SEG words, 128-bit accesses
+        uint4* seg = reinterpret_cast<uint4*>(cnt + tid * SEG);
         uint32_t sum = 0;
 #pragma unroll
-        for (uint32_t i = 0; i < SEG; ++i)
-            sum += seg[i];
+        for (uint32_t j = 0; j < SEG / 4u; ++j) {
+            const uint4 x = seg[j];
+            sum += x.x + x.y + x.z + x.w;
+        }
         uint32_t incl = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -526,92 +568,130 @@ __global__ void __launch_bounds__(S::kThreads, 2)
             gtot += x;
         }
         uint32_t run = wpre + incl - sum + ((gtot & 0xFFFFu) << 16); // high ports follow all low ports
+        // words past the L counter rows stay zero (the per-column reset below clears only L rows)
 #pragma unroll
-        for (uint32_t i = 0; i < SEG; ++i) {
-            const uint32_t x = seg[i];
-            seg[i] = run;
-            run += x;
+        for (uint32_t j = 0; j < SEG / 4u; ++j) {
+            const uint4 x = seg[j];
+            uint4 y;
+            y.x = run;
+            y.y = y.x + x.x;
+            y.z = y.y + x.y;
+            y.w = y.z + x.z;
+            run = y.w + x.w;
+            if (tid * SEG + 4u * j < L * (uint32_t)T)
+                seg[j] = y;
         }
         __syncthreads();
 
-        // per port (one thread each): its run's stage start, the stage position where its second
-        // output chunk starts, and slot - stage position for each of the two chunks
-        if (tid < BM) {
-            const uint32_t b = tid;
-            uint32_t s0 = count, s1 = count;
-            if (b < B)
-                s0 = (cnt[(b & (L - 1u)) * T] >> ((b >> S::kLaneShift) << 4)) & 0xFFFFu;
-            if (b + 1u < B)
-                s1 = (cnt[((b + 1u) & (L - 1u)) * T] >> (((b + 1u) >> S::kLaneShift) << 4)) & 0xFFFFu;
-            const uint32_t len = b < B ? s1 - s0 : 0u;
-            const uint32_t j0 = off[b] - len;
-            off[b] = j0;
-            run_at[b] = s0;
-            uint32_t sp = s0 + len, sa = kNoChunk, sb = kNoChunk;
-            if (len != 0u) {
+        // warp 0: each port's run [s, s + len) in the stage is cut at its output-chunk boundary into
+        // at most two pieces; piece i (in stage order) gets {slot - stage position, ok} and a bit at
+        // its first stage position
+        if (w == 0) {
+#pragma unroll
+            for (uint32_t i = lane; i < S::kBmWords; i += 32u)
+                bm[i] = 0u;
+            const uint32_t b0 = 2u * lane, b1 = b0 + 1u;
+            auto start_of = [&](uint32_t b) -> uint32_t {
+                return b < MB ? (uint32_t)cnt16[(((b & (L - 1u)) * T) << 1) | (b >> S::kLaneShift)] : count;
+            };
+            const uint32_t s0 = start_of(b0), s1 = start_of(b1), s2 = start_of(b1 + 1u);
+            uint32_t ps[4], pl[4], pb[4], pv[4];
+            auto cut = [&](uint32_t b, uint32_t s, uint32_t len, uint32_t& off, int p) {
+                pl[p] = pl[p + 1] = 0u;
+                ps[p] = ps[p + 1] = pb[p] = pb[p + 1] = pv[p] = pv[p + 1] = 0u;
+                if (b >= B || len == 0u)
+                    return;
+                const uint32_t j0 = off - len;
+                off = j0;
                 const uint32_t k0 = fdc.div(j0);
                 const uint32_t room = (k0 + 1u) * capacity - j0; // slots left in the first chunk
-                // a chunk id outside the pool writes nothing and fails the batch
-                auto in_pool = [&](uint32_t ch) {
-                    const bool okc = ch != kNoChunk && ((uint64_t)ch + 1u) * capacity <= pool_slots;
-                    if (!okc && ch != kNoChunk)
-                        set_status(status, GF_OVERFLOW);
-                    return okc;
-                };
+                const uint32_t n1 = len < room ? len : room;
                 const uint32_t ca = chunk_of(b, k0);
-                if (in_pool(ca))
-                    sa = ca * capacity + (j0 - k0 * capacity) - s0;
+                ps[p] = s;
+                pl[p] = n1;
+                pv[p] = in_pool(ca) ? 1u : 0u;
+                pb[p] = ca * capacity + (j0 - k0 * capacity) - s;
                 if (len > room) {
-                    sp = s0 + room;
                     const uint32_t cb = chunk_of(b, k0 + 1u);
-                    if (in_pool(cb))
-                        sb = cb * capacity - sp;
+                    ps[p + 1] = s + n1;
+                    pl[p + 1] = len - n1;
+                    pv[p + 1] = in_pool(cb) ? 1u : 0u;
+                    pb[p + 1] = cb * capacity - (s + n1);
                 }
-            }
-            port4[b] = make_uint4(sp, sa, sb, 0u);
-        }
-        __syncthreads();
-
-        // stage in port order (the stage position is the rank), each key with its output slot
+            };
+            cut(b0, s0, s1 - s0, off0, 0);
+            cut(b1, s1, s2 - s1, off1, 2);
+            const uint32_t n_p = (pl[0] != 0u) + (pl[1] != 0u) + (pl[2] != 0u) + (pl[3] != 0u);
+            uint32_t pincl = n_p;
 #pragma unroll
-        for (int i = 0; i < IPT; ++i) {
-            const uint32_t b = bp[i] & 0xFFFFu;
-            if (b != kNoBin16) {
-                const uint32_t word = cnt[(b & (L - 1u)) * T + tid];
-                const uint32_t pos = ((word >> ((b >> S::kLaneShift) << 4)) & 0xFFFFu) + (bp[i] >> 16);
-                const uint4 pp = port4[b];
-                const uint32_t base = pos < pp.x ? pp.y : pp.z;
-                stage[pos] = key[i];
-                oslot[pos] = base == kNoChunk ? kNoChunk : base + pos;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, pincl, o);
+                if ((int)lane >= o)
+                    pincl += y;
             }
+            uint32_t at = pincl - n_p;
+            __syncwarp();
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+                if (pl[p] != 0u && at < S::kMaxPieces) {
+                    pieces[at++] = make_uint2(pb[p], pv[p]);
+                    atomicOr(&bm[ps[p] >> 5], 1u << (ps[p] & 31u));
+                }
+            __syncwarp();
         }
-        __syncthreads();
 
+        // stage in port order (the stage position is the rank) in this tile's own buffer: its keys
+        // are in registers. All positions are read before any key is stored.
+#pragma unroll
+        for (int i = 0; i < IPT; ++i)
+            pk[i] = cnt16[pk[i] & 0xFFFFu] + (pk[i] >> 16);
+#pragma unroll
+        for (int i = 0; i < IPT; ++i)
+            if (tid * IPT + (uint32_t)i < count)
+                tin[pk[i]] = key[i];
         // this thread's counter column is reset for the next tile (no other thread reads it now)
 #pragma unroll
-        for (uint32_t r = 0; r < SEG; ++r)
+        for (uint32_t r = 0; r < L; ++r)
             cnt[r * T + tid] = 0u;
+        __syncthreads();
 
-        // write-out: consecutive threads take consecutive stage positions (coalesced along each run)
-        if (!failed) {
-#pragma unroll 4
-            for (uint32_t q = tid; q < count; q += T) {
-                const uint32_t sl = oslot[q];
-                if (sl != kNoChunk)
-                    out[sl] = stage[q];
+        // write-out: warp w covers stage positions [1024 w, 1024 w + 1024) in windows of 32, lane =
+        // position within the window; a position's piece is the last piece starting at or before it
+        {
+            uint32_t kb = 0; // pieces starting before this warp's first window
+            for (uint32_t i = lane; i < w * 32u; i += 32u)
+                kb += __popc(bm[i]);
+            kb = __reduce_add_sync(0xFFFFFFFFu, kb);
+            const uint32_t upto = 0xFFFFFFFFu >> (31u - lane);
+#pragma unroll
+            for (uint32_t i0 = 0; i0 < 32u; i0 += 8u) {
+                uint32_t wd[8], v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const uint32_t win = w * 32u + i0 + (uint32_t)u;
+                    wd[u] = bm[win];
+                    v[u] = tin[win * 32u + lane];
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const uint32_t q = (w * 32u + i0 + (uint32_t)u) * 32u + lane;
+                    const uint32_t kk = kb + __popc(wd[u] & upto) - 1u;
+                    kb += __popc(wd[u]);
+                    if (q < count) {
+                        const uint2 pc = pieces[kk];
+                        if (pc.y != 0u)
+                            out[q + pc.x] = v[u]; // 32-bit slot arithmetic: pc.x wraps, the slot does not
+                    }
+                }
             }
         }
         fence_proxy_async_smem(); // this buffer's reads come before the next bulk copy into it
-        __syncthreads();
-        if (tid == 0 && k + 2u < n_mine)
-            coop_fetch(tiles, t_hi - 1u - (k + 2u), in, capacity, pool_slots, S::kMaxCount, sm, S::ring(buf),
-                       &mbar[buf], tdesc + 16u + 4u * buf, status);
     }
 }
 
 // Host side: one cooperative launch of the kernel with classifier `cls`; the grid is as many CTAs
-// as fit on the device at once, capped by the tiles and by the scratch (64 words per CTA after the
-// control block, whose reset words the caller zeroed on the stream).
+// as fit on the device at once, capped by the tiles and by the scratch (the control block, then
+// 4 * 2 * LANES bytes per CTA). The control block's reset words are zeroed here, on the stream.
 template <typename S, typename Cls>
 cudaError_t launch_fused_coop(cudaStream_t stream, Cls cls, const uint32_t* in, uint32_t* out, uint32_t capacity,
                               uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t bins,
@@ -620,6 +700,10 @@ cudaError_t launch_fused_coop(cudaStream_t stream, Cls cls, const uint32_t* in, 
                               uint32_t* status, int sms)
 {
     auto kernel = fused_partition_coop_kernel<S, Cls>;
+    constexpr uint64_t kHead = sizeof(FusedCtl) + sizeof(CoopHdr);
+    constexpr uint64_t kRow = sizeof(uint32_t) * S::kMaxBins;
+    if (scratch_bytes < kHead + kRow)
+        return cudaErrorInvalidValue;
     cudaError_t err = cudaSuccess;
     if (S::kSmemBytes > 48u * 1024u) {
         err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmemBytes);
@@ -634,15 +718,19 @@ cudaError_t launch_fused_coop(cudaStream_t stream, Cls cls, const uint32_t* in, 
         return cudaErrorInvalidConfiguration;
     uint64_t g = (uint64_t)per_sm * (uint64_t)sms;
     g = g < n_tiles ? g : n_tiles;
-    const uint64_t cap_ctas = (scratch_bytes - sizeof(FusedCtl)) / 256u;
+    const uint64_t cap_ctas = (scratch_bytes - kHead) / kRow;
     g = g < cap_ctas ? g : cap_ctas;
     if (g == 0u)
         return cudaErrorInvalidConfiguration;
-    uint32_t* cta_tot = reinterpret_cast<uint32_t*>(ctl + 1);
+    CoopHdr* hdr = reinterpret_cast<CoopHdr*>(ctl + 1);
+    uint32_t* cta_tot = reinterpret_cast<uint32_t*>(hdr + 1);
+    err = cudaMemsetAsync(hdr, 0, kCoopHdrResetBytes, stream);
+    if (err != cudaSuccess)
+        return err;
     FastDiv fd(capacity);
-    void* args[] = {&in,       &out,        &cls,    &capacity, &fd,          &pool_slots,  &tiles,
-                    &n_tiles,  &bins,       &reserved, &n_reserved, &totals, &port_chunks, &max_k,
-                    &ctl,      &cta_tot,    &status};
+    void* args[] = {&in,       &out,      &cls,    &capacity,    &fd,    &pool_slots, &tiles,
+                    &n_tiles,  &bins,     &reserved, &n_reserved, &totals, &port_chunks, &max_k,
+                    &ctl,      &hdr,      &cta_tot, &status};
     return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3((uint32_t)g), dim3(S::kThreads),
                                        args, S::kSmemBytes, stream);
 }

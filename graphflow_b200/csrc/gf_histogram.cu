@@ -18,7 +18,7 @@ constexpr uint32_t kHistC = 8192u;    // chunk capacity of the radix passes
 constexpr uint32_t kHistTile = 4096u; // keys per tile
 constexpr uint32_t kHistBins = 64u;   // 6-bit digits
 constexpr uint32_t kRleBlock = 4096u; // values per run-length block (256 threads x 16)
-constexpr uint64_t kCoopScratch = 64u + (1u << 17);
+constexpr uint64_t kCoopScratch = 64u + 512u + (1u << 18); // control blocks + up to 1024 CTAs x 64 words
 
 struct DigitClassify {
     uint32_t shift;
@@ -351,9 +351,7 @@ gf_status gf_histogram_u32(void* stream, const uint32_t* d_values, uint64_t n, v
         const uint32_t n_chunks = any ? (uint32_t)L.R : (uint32_t)L.n_in;
         hist_tiles_kernel<<<(n_chunks + 255u) / 256u, 256, 0, s>>>(n, n_chunks, any ? descs : nullptr, num_out,
                                                                    tiles);
-        e = cudaMemsetAsync(ctl, 0, kFusedCtlResetBytes, s);
-        if (e == cudaSuccess)
-            e = launch_fused_coop<CoopShape<32>>(s, DigitClassify{shift}, in, out, kHistC, L.region, tiles,
+        e = launch_fused_coop<CoopShape<32>>(s, DigitClassify{shift}, in, out, kHistC, L.region, tiles,
                                                  2u * n_chunks, kHistBins, reserved, (uint32_t)L.R, totals,
                                                  port_chunks, (uint32_t)L.max_k, ctl, kCoopScratch, d_status, sms);
         if (e != cudaSuccess)
