@@ -30,6 +30,8 @@
 
 #include "gf_partition.cuh"
 
+#include <type_traits>
+
 namespace gf {
 namespace { // internal linkage: see gf_partition.cuh
 
@@ -96,10 +98,12 @@ GF_D uint32_t ld_acquire_u32(const uint32_t* p)
 
 // Built-in key classifiers of the specialised kernel (a result >= bins is invalid).
 struct MaskClassify { // key mod B for B a power of two
+    static constexpr bool kAlwaysValid = true;
     uint32_t mask;
     GF_D uint32_t operator()(uint32_t k) const { return k & mask; }
 };
 struct ModClassify { // key mod B
+    static constexpr bool kAlwaysValid = true;
     FastDiv fd;
     GF_D uint32_t operator()(uint32_t k) const { return fd.mod(k); }
 };
@@ -107,6 +111,16 @@ struct AnyKeyClassify { // every other built-in rule
     KeyClassifier c;
     GF_D uint32_t operator()(uint32_t k) const { return c((uint64_t)k); }
 };
+
+// True for classifiers whose result is below the port count for every key.
+template <typename C>
+constexpr bool always_valid()
+{
+    if constexpr (requires { C::kAlwaysValid; })
+        return C::kAlwaysValid;
+    else
+        return false;
+}
 
 // Control block of the cooperative kernel, right after the FusedCtl in the scratch; the launcher
 // zeroes its first kCoopHdrResetBytes on the stream before every launch. The per-CTA port totals
@@ -144,8 +158,8 @@ struct CoopShape {
     // shared memory (32-bit words)
     static constexpr uint32_t kIn = 0;                              // [2][kInWords] tiles, staged in place
     static constexpr uint32_t kCnt = kIn + 2u * kInWords;           // [kSeg * kThreads] counters
-    static constexpr uint32_t kPieces = kCnt + kSeg * kThreads;     // [kMaxPieces] {slot - stage position, ok}
-    static constexpr uint32_t kBm = kPieces + 2u * kMaxPieces;      // [kBmWords] stage positions where pieces start
+    static constexpr uint32_t kPieces = kCnt + kSeg * kThreads;     // [kMaxPieces] slot - stage position
+    static constexpr uint32_t kBm = kPieces + kMaxPieces;           // [kBmWords] stage positions where pieces start
     static constexpr uint32_t kBase = kBm + kBmWords;               // [64] this CTA's first port position
     static constexpr uint32_t kTotal = kBase + kBM;                 // [64] batch totals
     static constexpr uint32_t kBinBase = kTotal + kBM;              // [64] dense plan
@@ -160,7 +174,7 @@ struct CoopShape {
     static constexpr uint32_t kMbar = kMisc + 8u;                   // [2] x u64
     static constexpr uint32_t kWords = kMbar + 4u;
     static constexpr size_t kSmemBytes = sizeof(uint32_t) * kWords;
-    static_assert(kCnt % 4u == 0u && kPieces % 2u == 0u && kMbar % 2u == 0u, "alignment");
+    static_assert(kCnt % 4u == 0u && kMbar % 2u == 0u, "alignment");
     static_assert(kWarps == 4 && kMaxCount == (uint32_t)kWarps * 1024u, "write-out: one 1024-position quarter per warp");
 };
 
@@ -221,10 +235,11 @@ __global__ void __launch_bounds__(S::kThreads, 4)
 {
     constexpr int T = S::kThreads, IPT = S::kIpt, W = S::kWarps;
     constexpr uint32_t BM = S::kBM, L = S::kLanes, SEG = S::kSeg, MB = S::kMaxBins;
+    constexpr bool kValid = always_valid<Classify>();
     extern __shared__ __align__(128) uint32_t sm[];
     uint32_t* cnt = sm + S::kCnt;
     uint16_t* cnt16 = reinterpret_cast<uint16_t*>(cnt);
-    uint2* pieces = reinterpret_cast<uint2*>(sm + S::kPieces);
+    uint32_t* pieces = sm + S::kPieces;
     uint32_t* bm = sm + S::kBm;
     uint32_t* cbase = sm + S::kBase;
     uint32_t* total = sm + S::kTotal;
@@ -267,7 +282,7 @@ __global__ void __launch_bounds__(S::kThreads, 4)
     bool bad = false;
     auto count_key = [&](uint32_t key) {
         const uint32_t b = cls(key);
-        if (b < B) // own column: no contention; a reduction, so consecutive keys do not wait on each other
+        if (kValid || b < B) // own column: no contention; a reduction, so consecutive keys do not wait on each other
             atomicAdd(cnt + (b & (L - 1u)) * T + tid, 1u << ((b >> S::kLaneShift) << 4));
         else
             bad = true;
@@ -297,7 +312,17 @@ __global__ void __launch_bounds__(S::kThreads, 4)
         const uint32_t* d = tdesc + 4u * buf;
         mbar_wait(&mbar[buf], (q >> 1) & 1u, status);
         const uint32_t count = d[2], flags = d[3];
-        if (flags & 2u) {
+        if ((flags & 2u) && count == S::kMaxCount) { // a full tile: no per-key checks
+            const uint4* v = reinterpret_cast<const uint4*>(sm + buffer(buf));
+#pragma unroll
+            for (uint32_t j = 0; j < S::kMaxCount / 4u / (uint32_t)T; ++j) {
+                const uint4 x = v[tid + j * (uint32_t)T];
+                count_key(x.x);
+                count_key(x.y);
+                count_key(x.z);
+                count_key(x.w);
+            }
+        } else if (flags & 2u) {
             const uint4* v = reinterpret_cast<const uint4*>(sm + buffer(buf));
 #pragma unroll
             for (uint32_t j = 0; j < S::kMaxCount / 4u / (uint32_t)T; ++j) {
@@ -525,17 +550,26 @@ __global__ void __launch_bounds__(S::kThreads, 4)
         // count: a key's local rank is its 16-bit counter before the increment (the atomics of one
         // thread are independent instructions, so they issue back to back); a slot past the tile's
         // count adds 0 (its key is never staged)
+        // pk: byte offset of the key's 16-bit counter (low half) and its local rank (high half)
         uint32_t pk[IPT];
+        const bool full = tid * IPT + IPT <= count; // every slot of this thread holds a key
+        auto count_keys = [&](auto all) {
 #pragma unroll
-        for (int i = 0; i < IPT; ++i) {
-            const uint32_t valid = tid * IPT + (uint32_t)i < count ? 1u : 0u;
-            uint32_t b = cls(key[i]);
-            b = b < B ? b : 0u;
-            const uint32_t wi = (b & (L - 1u)) * T + tid;
-            const uint32_t half = b >> S::kLaneShift;
-            const uint32_t old = atomicAdd(cnt + wi, valid << (half << 4));
-            pk[i] = ((wi << 1) | half) | (((old >> (half << 4)) & 0xFFFFu) << 16);
-        }
+            for (int i = 0; i < IPT; ++i) {
+                const uint32_t valid = decltype(all)::value || tid * IPT + (uint32_t)i < count ? 1u : 0u;
+                uint32_t b = cls(key[i]);
+                if constexpr (!kValid)
+                    b = b < B ? b : 0u;
+                const uint32_t wi = (b & (L - 1u)) * T + tid;
+                const uint32_t half = b >> S::kLaneShift;
+                const uint32_t old = atomicAdd(cnt + wi, valid << (half << 4));
+                pk[i] = __byte_perm((wi << 2) | (half << 1), old, half != 0u ? 0x7610u : 0x5410u);
+            }
+        };
+        if (full)
+            count_keys(std::true_type{});
+        else
+            count_keys(std::false_type{});
         __syncthreads();
         // the other buffer's last reader (the previous tile's write-out) is done: fetch the next tile
         if (tid == 0 && k >= 1u && k + 1u < n_mine)
@@ -630,25 +664,39 @@ __global__ void __launch_bounds__(S::kThreads, 4)
                     pincl += y;
             }
             uint32_t at = pincl - n_p;
+            bool ok = true;
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+                ok = ok && (pl[p] == 0u || pv[p] != 0u);
+            ok = __all_sync(0xFFFFFFFFu, ok);
             __syncwarp();
 #pragma unroll
             for (int p = 0; p < 4; ++p)
                 if (pl[p] != 0u && at < S::kMaxPieces) {
-                    pieces[at++] = make_uint2(pb[p], pv[p]);
+                    pieces[at++] = pb[p];
                     atomicOr(&bm[ps[p] >> 5], 1u << (ps[p] & 31u));
                 }
+            if (lane == 0u)
+                misc[4] = ok ? 1u : 0u; // a piece outside the pool has failed the batch: the tile writes nothing
             __syncwarp();
         }
 
         // stage in port order (the stage position is the rank) in this tile's own buffer: its keys
         // are in registers. All positions are read before any key is stored.
+        const char* cbytes = reinterpret_cast<const char*>(cnt);
 #pragma unroll
         for (int i = 0; i < IPT; ++i)
-            pk[i] = cnt16[pk[i] & 0xFFFFu] + (pk[i] >> 16);
+            pk[i] = *reinterpret_cast<const uint16_t*>(cbytes + (pk[i] & 0xFFFFu)) + (pk[i] >> 16);
+        if (full) {
 #pragma unroll
-        for (int i = 0; i < IPT; ++i)
-            if (tid * IPT + (uint32_t)i < count)
+            for (int i = 0; i < IPT; ++i)
                 tin[pk[i]] = key[i];
+        } else {
+#pragma unroll
+            for (int i = 0; i < IPT; ++i)
+                if (tid * IPT + (uint32_t)i < count)
+                    tin[pk[i]] = key[i];
+        }
         // this thread's counter column is reset for the next tile (no other thread reads it now)
 #pragma unroll
         for (uint32_t r = 0; r < L; ++r)
@@ -657,33 +705,37 @@ __global__ void __launch_bounds__(S::kThreads, 4)
 
         // write-out: warp w covers stage positions [1024 w, 1024 w + 1024) in windows of 32, lane =
         // position within the window; a position's piece is the last piece starting at or before it
-        {
+        if (misc[4] != 0u) {
             uint32_t kb = 0; // pieces starting before this warp's first window
             for (uint32_t i = lane; i < w * 32u; i += 32u)
                 kb += __popc(bm[i]);
             kb = __reduce_add_sync(0xFFFFFFFFu, kb);
             const uint32_t upto = 0xFFFFFFFFu >> (31u - lane);
+            const uint32_t* pcs = pieces - 1; // indexed by the number of piece starts at or before q
+            auto write_out = [&](auto all) {
 #pragma unroll
-            for (uint32_t i0 = 0; i0 < 32u; i0 += 8u) {
-                uint32_t wd[8], v[8];
+                for (uint32_t i0 = 0; i0 < 32u; i0 += 8u) {
+                    uint32_t wd[8], v[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const uint32_t win = w * 32u + i0 + (uint32_t)u;
-                    wd[u] = bm[win];
-                    v[u] = tin[win * 32u + lane];
-                }
+                    for (int u = 0; u < 8; ++u) {
+                        const uint32_t win = w * 32u + i0 + (uint32_t)u;
+                        wd[u] = bm[win];
+                        v[u] = tin[win * 32u + lane];
+                    }
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const uint32_t q = (w * 32u + i0 + (uint32_t)u) * 32u + lane;
-                    const uint32_t kk = kb + __popc(wd[u] & upto) - 1u;
-                    kb += __popc(wd[u]);
-                    if (q < count) {
-                        const uint2 pc = pieces[kk];
-                        if (pc.y != 0u)
-                            out[q + pc.x] = v[u]; // 32-bit slot arithmetic: pc.x wraps, the slot does not
+                    for (int u = 0; u < 8; ++u) {
+                        const uint32_t q = (w * 32u + i0 + (uint32_t)u) * 32u + lane;
+                        const uint32_t kk = kb + __popc(wd[u] & upto);
+                        kb += __popc(wd[u]);
+                        if (decltype(all)::value || q < count)
+                            out[q + pcs[kk]] = v[u]; // 32-bit slot arithmetic: the base wraps, the slot does not
                     }
                 }
-            }
+            };
+            if (count == S::kMaxCount)
+                write_out(std::true_type{});
+            else
+                write_out(std::false_type{});
         }
         fence_proxy_async_smem(); // this buffer's reads come before the next bulk copy into it
     }

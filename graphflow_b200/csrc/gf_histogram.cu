@@ -21,6 +21,7 @@ constexpr uint32_t kRleBlock = 4096u; // values per run-length block (256 thread
 constexpr uint64_t kCoopScratch = 64u + 512u + (1u << 18); // control blocks + up to 1024 CTAs x 64 words
 
 struct DigitClassify {
+    static constexpr bool kAlwaysValid = true;
     uint32_t shift;
     GF_D uint32_t operator()(uint32_t k) const { return (k >> shift) & (kHistBins - 1u); }
 };
