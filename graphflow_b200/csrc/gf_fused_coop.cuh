@@ -152,7 +152,6 @@ struct CoopShape {
     // thread r's segment starts at word r * kSeg, which puts the eight threads of each quarter warp
     // on eight disjoint groups of four banks.
     static constexpr uint32_t kSeg = LANES == 2 ? 4u : LANES + 4u;
-    static constexpr uint32_t kIdCache = 128u; // chunk ids of this CTA's output held in shared memory
     static constexpr uint32_t kMaxPieces = 2u * kMaxBins; // a port's run of one tile is cut at most once
     static constexpr uint32_t kBmWords = kMaxCount / 32u;  // one bit per stage position
     // shared memory (32-bit words)
@@ -160,21 +159,20 @@ struct CoopShape {
     static constexpr uint32_t kCnt = kIn + 2u * kInWords;           // [kSeg * kThreads] counters
     static constexpr uint32_t kPieces = kCnt + kSeg * kThreads;     // [kMaxPieces] slot - stage position
     static constexpr uint32_t kBm = kPieces + kMaxPieces;           // [kBmWords] stage positions where pieces start
+    // phase 1 and plan: [64] each; in phase 2 the four arrays hold the per-port chunk cache
     static constexpr uint32_t kBase = kBm + kBmWords;               // [64] this CTA's first port position
     static constexpr uint32_t kTotal = kBase + kBM;                 // [64] batch totals
-    static constexpr uint32_t kBinBase = kTotal + kBM;              // [64] dense plan
-    static constexpr uint32_t kOwn = kBinBase + kBM;                // [64] this CTA's totals
-    static constexpr uint32_t kKfirst = kOwn + kBM;                 // [64] first output chunk of the range
-    static constexpr uint32_t kAcc = kKfirst + kBM;                 // [64] phase-1 flushed counts
-    static constexpr uint32_t kIdOff = kAcc + kBM;                  // [65] id cache offsets
-    static constexpr uint32_t kIds = kIdOff + kBM + 4u;             // [kIdCache]
-    static constexpr uint32_t kScan = kIds + kIdCache;              // [kWarps]
+    static constexpr uint32_t kOwn = kTotal + kBM;                  // [64] this CTA's totals
+    static constexpr uint32_t kAcc = kOwn + kBM;                    // [64] phase-1 flushed counts
+    static constexpr uint32_t kChunkCache = kBase;                  // [64] x uint4 {k, id of chunk k, id of k + 1, -}
+    static constexpr uint32_t kBinBase = kAcc + kBM;                // [64] dense plan
+    static constexpr uint32_t kScan = kBinBase + kBM;               // [kWarps]
     static constexpr uint32_t kTiles = kScan + 4u;                  // [4][4] tile descriptors (phase 1, phase 2)
     static constexpr uint32_t kMisc = kTiles + 16u;                 // [8]
     static constexpr uint32_t kMbar = kMisc + 8u;                   // [2] x u64
     static constexpr uint32_t kWords = kMbar + 4u;
     static constexpr size_t kSmemBytes = sizeof(uint32_t) * kWords;
-    static_assert(kCnt % 4u == 0u && kMbar % 2u == 0u, "alignment");
+    static_assert(kCnt % 4u == 0u && kChunkCache % 4u == 0u && kMbar % 2u == 0u, "alignment");
     static_assert(kWarps == 4 && kMaxCount == (uint32_t)kWarps * 1024u, "write-out: one 1024-position quarter per warp");
 };
 
@@ -199,13 +197,13 @@ GF_D void coop_grid_barrier(uint32_t* counter, uint32_t* status)
     __syncthreads();
 }
 
-// Thread 0: fetch tile `t` into the shared buffer at word offset `dst` (bulk copy completing on
+// Thread 0: fetch `tile` into the shared buffer at word offset `dst` (bulk copy completing on
 // `bar`, or a plain arrival when the tile cannot be bulk copied) and describe it in d[0..3]:
-// chunk, offset, count (0 for an invalid tile), flags (1 = valid, 2 = in shared memory).
-GF_D void coop_fetch(const gf_tile* tiles, uint32_t t, const uint32_t* in, uint32_t capacity, uint64_t pool_slots,
+// chunk, offset, count (0 for an invalid tile), flags (1 = valid, 2 = in shared memory). The
+// caller loads the tile's descriptor ahead of time, so its global-memory latency overlaps work.
+GF_D void coop_fetch(const gf_tile tile, const uint32_t* in, uint32_t capacity, uint64_t pool_slots,
                      uint32_t max_count, uint32_t* sm, uint32_t dst, uint64_t* bar, uint32_t* d, uint32_t* status)
 {
-    const gf_tile tile = tiles[t];
     const uint64_t base = (uint64_t)tile.chunk_index * capacity + tile.tile_offset;
     const bool ok =
         tile.count <= max_count && base + tile.count <= pool_slots && tile.tile_offset + tile.count <= capacity;
@@ -245,10 +243,8 @@ __global__ void __launch_bounds__(S::kThreads, 4)
     uint32_t* total = sm + S::kTotal;
     uint32_t* bin_base = sm + S::kBinBase;
     uint32_t* own = sm + S::kOwn;
-    uint32_t* kfirst = sm + S::kKfirst;
     uint32_t* acc = sm + S::kAcc;
-    uint32_t* idoff = sm + S::kIdOff;
-    uint32_t* ids = sm + S::kIds;
+    uint4* ccache = reinterpret_cast<uint4*>(sm + S::kChunkCache);
     uint32_t* scan = sm + S::kScan;
     uint32_t* tdesc = sm + S::kTiles;
     uint32_t* misc = sm + S::kMisc;
@@ -277,7 +273,7 @@ __global__ void __launch_bounds__(S::kThreads, 4)
     // ---------------- phase 1: per-port counts of this CTA's tiles (forward, two buffers) ----------------
     if (tid == 0)
         for (uint32_t q = 0; q < 2u && q < n_mine; ++q)
-            coop_fetch(tiles, t_lo + q, in, capacity, pool_slots, S::kMaxCount, sm, buffer(q), &mbar[q],
+            coop_fetch(tiles[t_lo + q], in, capacity, pool_slots, S::kMaxCount, sm, buffer(q), &mbar[q],
                        tdesc + 4u * q, status);
     bool bad = false;
     auto count_key = [&](uint32_t key) {
@@ -310,6 +306,9 @@ __global__ void __launch_bounds__(S::kThreads, 4)
     for (uint32_t q = 0; q < n_mine; ++q) {
         const uint32_t buf = q & 1u;
         const uint32_t* d = tdesc + 4u * buf;
+        gf_tile next{};
+        if (tid == 0 && q + 2u < n_mine)
+            next = tiles[t_lo + q + 2u]; // used after this tile's barrier
         mbar_wait(&mbar[buf], (q >> 1) & 1u, status);
         const uint32_t count = d[2], flags = d[3];
         if ((flags & 2u) && count == S::kMaxCount) { // a full tile: no per-key checks
@@ -346,7 +345,7 @@ __global__ void __launch_bounds__(S::kThreads, 4)
         fence_proxy_async_smem(); // this buffer's reads come before the next bulk copy into it
         __syncthreads();
         if (tid == 0 && q + 2u < n_mine)
-            coop_fetch(tiles, t_lo + q + 2u, in, capacity, pool_slots, S::kMaxCount, sm, buffer(buf), &mbar[buf],
+            coop_fetch(next, in, capacity, pool_slots, S::kMaxCount, sm, buffer(buf), &mbar[buf],
                        tdesc + 4u * buf, status);
         if ((q & 1023u) == 1023u)
             flush();
@@ -368,7 +367,7 @@ __global__ void __launch_bounds__(S::kThreads, 4)
     const uint32_t use0 = (n_mine + 1u) / 2u, use1 = n_mine / 2u;
     if (tid == 0)
         for (uint32_t k = 0; k < 2u && k < n_mine; ++k)
-            coop_fetch(tiles, t_hi - 1u - k, in, capacity, pool_slots, S::kMaxCount, sm, buffer(k), &mbar[k],
+            coop_fetch(tiles[t_hi - 1u - k], in, capacity, pool_slots, S::kMaxCount, sm, buffer(k), &mbar[k],
                        tdesc + 8u + 4u * k, status);
 
     coop_grid_barrier(&hdr->done, status);
@@ -417,38 +416,24 @@ __global__ void __launch_bounds__(S::kThreads, 4)
         __syncthreads();
         red[tid] = make_uint4(0u, 0u, 0u, 0u);
         if (w == 0) {
-            // binBase = exclusive scan of ceil(total / C); first chunk and chunk count of this CTA's
-            // range per port (two ports per lane)
+            // binBase = exclusive scan of ceil(total / C) (two ports per lane)
             const uint32_t b0 = 2u * lane, b1 = b0 + 1u;
-            uint32_t n0 = 0, n1 = 0, m0 = 0, m1 = 0;
+            uint32_t n0 = 0, n1 = 0;
             if (b0 < B)
                 n0 = fdc.div(total[b0]) + (fdc.mod(total[b0]) != 0u ? 1u : 0u);
             if (b1 < B)
                 n1 = fdc.div(total[b1]) + (fdc.mod(total[b1]) != 0u ? 1u : 0u);
-            const uint32_t kf0 = fdc.div(cbase[b0]), kf1 = fdc.div(cbase[b1]);
-            if (own[b0] != 0u)
-                m0 = fdc.div(cbase[b0] + own[b0] - 1u) - kf0 + 1u;
-            if (own[b1] != 0u)
-                m1 = fdc.div(cbase[b1] + own[b1] - 1u) - kf1 + 1u;
-            kfirst[b0] = kf0;
-            kfirst[b1] = kf1;
-            uint32_t incl = n0 + n1, mincl = m0 + m1;
+            uint32_t incl = n0 + n1;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-                const uint32_t z = __shfl_up_sync(0xFFFFFFFFu, mincl, o);
-                if ((int)lane >= o) {
+                if ((int)lane >= o)
                     incl += y;
-                    mincl += z;
-                }
             }
-            const uint32_t ex = incl - n0 - n1, mex = mincl - m0 - m1;
+            const uint32_t ex = incl - n0 - n1;
             bin_base[b0] = ex;
             bin_base[b1] = ex + n0;
-            idoff[b0] = mex;
-            idoff[b1] = mex + m0;
             if (lane == 31) {
-                idoff[BM] = mincl;
                 misc[1] = incl; // R = chunks of the plan
                 if (incl > n_reserved)
                     set_status(status, GF_OVERFLOW);
@@ -456,20 +441,6 @@ __global__ void __launch_bounds__(S::kThreads, 4)
         }
         __syncthreads();
         const uint32_t R = misc[1];
-        // chunk ids of this CTA's output runs, once
-        const uint32_t n_ids = idoff[BM] < S::kIdCache ? idoff[BM] : S::kIdCache;
-        for (uint32_t i = tid; i < n_ids; i += T) {
-            uint32_t lo = 0, hi = BM - 1u; // the last port whose run starts at or before i
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1u) >> 1;
-                if (idoff[mid] <= i)
-                    lo = mid;
-                else
-                    hi = mid - 1u;
-            }
-            const uint32_t f = bin_base[lo] + kfirst[lo] + (i - idoff[lo]);
-            ids[i] = f < R && f < n_reserved ? __ldg(reserved + f) : kNoChunk;
-        }
         // port b's chunk list, written by CTA b % G; batch totals and the epoch by CTA 0
         for (uint32_t pb = c; pb < B; pb += G) {
             const uint32_t nck = fdc.div(total[pb]) + (fdc.mod(total[pb]) != 0u ? 1u : 0u);
@@ -503,17 +474,15 @@ __global__ void __launch_bounds__(S::kThreads, 4)
     }
     const uint32_t R = misc[1];
 
-    // chunk id of port b's k-th output chunk (k inside this CTA's range of the port)
+    // chunk id of port b's k-th output chunk
     auto chunk_of = [&](uint32_t b, uint32_t k) -> uint32_t {
-        const uint32_t rel = k - kfirst[b];
-        if (rel < idoff[b + 1u] - idoff[b] && idoff[b] + rel < S::kIdCache)
-            return ids[idoff[b] + rel];
         const uint32_t f = bin_base[b] + k;
         return f < R && f < n_reserved ? __ldg(reserved + f) : kNoChunk;
     };
     // a chunk id outside the pool writes nothing and fails the batch
+    const uint32_t pool_chunks = (uint32_t)(pool_slots / capacity); // < 2^20: pool_slots < 2^32, C >= 4096
     auto in_pool = [&](uint32_t ch) {
-        const bool okc = ch != kNoChunk && ((uint64_t)ch + 1u) * capacity <= pool_slots;
+        const bool okc = ch < pool_chunks; // kNoChunk is never below it
         if (!okc)
             set_status(status, GF_OVERFLOW);
         return okc;
@@ -526,12 +495,20 @@ __global__ void __launch_bounds__(S::kThreads, 4)
         off0 = cbase[2u * lane] + own[2u * lane];
         off1 = cbase[2u * lane + 1u] + own[2u * lane + 1u];
     }
+    __syncthreads(); // the plan's per-port arrays are read; their words become the chunk cache
+    // per port: the two chunks its last run touched (walking backwards, the next run touches the
+    // same pair or the pair below), so a tile's pieces rarely reach for the reservation itself
+    if (tid < BM)
+        ccache[tid] = make_uint4(0xFFFFFFFFu, kNoChunk, kNoChunk, 0u);
 
     // ---------------- phase 2: rank, stage, write (tiles last to first) ----------------
     for (uint32_t k = 0; k < n_mine; ++k) {
         const uint32_t buf = k & 1u;
         const uint32_t* d = tdesc + 8u + 4u * buf;
         uint32_t* tin = sm + buffer(buf);
+        gf_tile next{};
+        if (tid == 0 && k >= 1u && k + 1u < n_mine)
+            next = tiles[t_hi - 2u - k]; // used after this tile's first barrier
         mbar_wait(&mbar[buf], ((buf == 0u ? use0 : use1) + (k >> 1)) & 1u, status);
         const uint32_t count = d[2], flags = d[3];
         uint32_t key[IPT];
@@ -552,7 +529,9 @@ __global__ void __launch_bounds__(S::kThreads, 4)
         // count adds 0 (its key is never staged)
         // pk: byte offset of the key's 16-bit counter (low half) and its local rank (high half)
         uint32_t pk[IPT];
-        const bool full = tid * IPT + IPT <= count; // every slot of this thread holds a key
+        // every slot of every thread of this warp holds a key (uniform per warp: a warp with a few
+        // short threads takes the checked path once instead of both paths)
+        const bool full = __all_sync(0xFFFFFFFFu, tid * IPT + IPT <= count);
         auto count_keys = [&](auto all) {
 #pragma unroll
             for (int i = 0; i < IPT; ++i) {
@@ -573,7 +552,7 @@ __global__ void __launch_bounds__(S::kThreads, 4)
         __syncthreads();
         // the other buffer's last reader (the previous tile's write-out) is done: fetch the next tile
         if (tid == 0 && k >= 1u && k + 1u < n_mine)
-            coop_fetch(tiles, t_hi - 2u - k, in, capacity, pool_slots, S::kMaxCount, sm, buffer(buf ^ 1u),
+            coop_fetch(next, in, capacity, pool_slots, S::kMaxCount, sm, buffer(buf ^ 1u),
                        &mbar[buf ^ 1u], tdesc + 8u + 4u * (buf ^ 1u), status);
 
         // raking scan over the (row, thread) counters: segments of SEG words, 128-bit accesses
@@ -640,13 +619,18 @@ __global__ void __launch_bounds__(S::kThreads, 4)
                 const uint32_t k0 = fdc.div(j0);
                 const uint32_t room = (k0 + 1u) * capacity - j0; // slots left in the first chunk
                 const uint32_t n1 = len < room ? len : room;
-                const uint32_t ca = chunk_of(b, k0);
+                uint4 cc = ccache[b];
+                if (cc.x != k0) {
+                    cc = make_uint4(k0, chunk_of(b, k0), chunk_of(b, k0 + 1u), 0u);
+                    ccache[b] = cc;
+                }
+                const uint32_t ca = cc.y;
                 ps[p] = s;
                 pl[p] = n1;
                 pv[p] = in_pool(ca) ? 1u : 0u;
                 pb[p] = ca * capacity + (j0 - k0 * capacity) - s;
                 if (len > room) {
-                    const uint32_t cb = chunk_of(b, k0 + 1u);
+                    const uint32_t cb = cc.z;
                     ps[p + 1] = s + n1;
                     pl[p + 1] = len - n1;
                     pv[p + 1] = in_pool(cb) ? 1u : 0u;
@@ -656,14 +640,12 @@ __global__ void __launch_bounds__(S::kThreads, 4)
             cut(b0, s0, s1 - s0, off0, 0);
             cut(b1, s1, s2 - s1, off1, 2);
             const uint32_t n_p = (pl[0] != 0u) + (pl[1] != 0u) + (pl[2] != 0u) + (pl[3] != 0u);
-            uint32_t pincl = n_p;
+            // exclusive prefix of the lanes' piece counts (0..4): one ballot per bit
+            const uint32_t below = lanemask_lt();
+            uint32_t at = 0;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, pincl, o);
-                if ((int)lane >= o)
-                    pincl += y;
-            }
-            uint32_t at = pincl - n_p;
+            for (int bit = 0; bit < 3; ++bit)
+                at += (uint32_t)__popc(__ballot_sync(0xFFFFFFFFu, (n_p >> bit) & 1u) & below) << bit;
             bool ok = true;
 #pragma unroll
             for (int p = 0; p < 4; ++p)
