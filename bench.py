@@ -592,7 +592,7 @@ def _cfg_hash(peak):
             chunks = np.arange(n_in, dtype=np.uint32)
             for _ in range(n_in):
                 pool.free.popleft()
-            part = HashPartition(pool, k, salt, tile_size=1024, form="device", max_batch_particles=n)
+            part = HashPartition(pool, k, salt, tile_size=2048, form="device", max_batch_particles=n)
             tiles, d_tiles = part._tiles(chunks, fills)
             part.reserved[:bound].copy_(torch.from_numpy(np.arange(n_in, n_in + bound, dtype=np.uint32).view(np.int32)))
             for _ in range(2):
@@ -609,7 +609,7 @@ def _cfg_hash(peak):
             entry = {"device_form_ms": ms, "records_per_s": n / (ms / 1e3),
                      "hbm_frac": n * 32 / (ms / 1e3) / 1e9 / peak, "status": int(part.status.item())}
             if layout == capi.LAYOUT_SOA:
-                plain = HashPartition(pool, k, salt, tile_size=1024, form="plain")
+                plain = HashPartition(pool, k, salt, tile_size=2048, form="plain")
                 descs = plain.run(list(chunks), list(fills))[2]
                 pool.release([int(x) for x in descs[:, 0]])
                 (_, _, descs), sec = _timed(lambda: plain.run(list(chunks), list(fills)))
@@ -619,7 +619,7 @@ def _cfg_hash(peak):
             out[name] = entry
             del pool, part
             torch.cuda.empty_cache()
-    out["workload"] = "hash partition, N=1e8 16-byte records, Zipf 1.2 over K keys, tiles of 1024"
+    out["workload"] = "hash partition, N=1e8 16-byte records, Zipf 1.2 over K keys, tiles of 2048"
     return out
 
 

@@ -17,6 +17,9 @@ int g_fused_coop = 1;
 // every idle node is dispatched per loop iteration); 0 = the reference's one-chunk sinks and one
 // dispatch per iteration.
 int g_runner_batched = 1;
+// Tuning knob: 1 = the hash classify/scatter entry points use the persistent kernels (one shared
+// counter per port and CTA); 0 = the per-tile open-addressing kernels.
+int g_hash_persistent = 1;
 
 constexpr int kThreads = 256;
 constexpr uint32_t kMaxDenseBins = 65535u;
@@ -115,6 +118,10 @@ gf_status gf_set_tuning(const char* name, int value)
     }
     if (std::string(name) == "runner_batched") {
         g_runner_batched = value != 0;
+        return GF_OK;
+    }
+    if (std::string(name) == "hash_persistent") {
+        g_hash_persistent = value != 0;
         return GF_OK;
     }
     return GF_ERR_ARGUMENT;
@@ -386,3 +393,5 @@ extern "C" gf_status gf_partition_fused_u32_noalloc(
 
 // Read by the flow entry points (gf_flows.cu, gf_dense_flow.cu, gf_photon.cu).
 bool gf_runner_batched() { return gf::g_runner_batched != 0; }
+// Read by the hash entry points (gf_capi_hash.cu).
+bool gf_hash_persistent() { return gf::g_hash_persistent != 0; }

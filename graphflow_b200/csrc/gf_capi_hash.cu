@@ -1,8 +1,11 @@
 // C ABI of the hash partition path (16-byte records, SoA or AoS), the device-side plan and the
 // record source.
+#include <algorithm>
 #include <cstdio>
 
 #include "gf_hash.cuh"
+
+bool gf_hash_persistent(); // gf_capi.cu
 
 namespace gf {
 namespace {
@@ -10,6 +13,17 @@ namespace {
 constexpr int kHashThreads = 256;
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int device_sms()
+{
+    static int sms = [] {
+        int dev = 0, n = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess)
+            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n;
+    }();
+    return sms;
+}
 
 gf_status cuda_status(cudaError_t e)
 {
@@ -25,6 +39,17 @@ cudaError_t allow_smem(Kernel k, size_t bytes)
     if (bytes <= 48u * 1024u)
         return cudaSuccess;
     return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// Grid of a persistent kernel: as many CTAs as fit on the device at once, at most one per tile.
+template <typename Kernel>
+uint32_t persist_grid(Kernel k, size_t smem, uint32_t n_tiles)
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kHashPThreads, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const uint64_t g = (uint64_t)per_sm * (uint64_t)device_sms();
+    return (uint32_t)std::max<uint64_t>(1u, std::min<uint64_t>(g, n_tiles));
 }
 
 template <typename F>
@@ -107,6 +132,20 @@ gf_status gf_classify_hash_r16(void* stream, const gf_rec16_columns* h_cols, int
     if (n_tiles == 0u)
         return GF_OK;
     UnmixClassify cls{salt, bins};
+    if (gf_hash_persistent()) {
+        return with_layout(layout, h_cols, nullptr, [&](auto acc) -> gf_status {
+            using Acc = decltype(acc);
+            auto kernel = hash_count_persist_kernel<Acc>;
+            const size_t smem = sizeof(uint32_t) * std::min(bins, kHashSmemBins);
+            cudaError_t e = allow_smem(kernel, smem);
+            if (e != cudaSuccess)
+                return cuda_status(e);
+            const uint32_t grid = persist_grid(kernel, smem, n_tiles);
+            kernel<<<grid, kHashPThreads, smem, as_stream(stream)>>>(acc, cls, capacity, pool_slots, d_tiles, n_tiles,
+                                                                    bins, d_bin_ids, d_counts, d_status);
+            return cuda_status(cudaGetLastError());
+        });
+    }
     return with_hash_shape(tile_size, [&]<typename Shape>() -> gf_status {
         return with_layout(layout, h_cols, nullptr, [&](auto acc) -> gf_status {
             using Acc = decltype(acc);
@@ -131,6 +170,40 @@ gf_status gf_scatter_hash_r16(void* stream, const gf_rec16_columns* h_in, const 
         return GF_OK;
     UnmixClassify cls{salt, bins};
     const FastDiv fdc(capacity);
+    if (gf_hash_persistent() && bins <= kHashGroupBins) {
+        return with_layout(layout, h_in, h_out, [&](auto acc) -> gf_status {
+            using Acc = decltype(acc);
+            auto kernel = hash_scatter_grouped_kernel<Acc, NoUpdate>;
+            const uint32_t unit = tile_size; // 1024 or 2048
+            const size_t smem = sizeof(Rec16) * unit + 4u * sizeof(uint32_t) * bins + sizeof(uint16_t) * ((unit + 1u) & ~1u) +
+                                sizeof(uint32_t) * (kHashPThreads / 32 + 1);
+            cudaError_t e = allow_smem(kernel, smem);
+            if (e != cudaSuccess)
+                return cuda_status(e);
+            const uint32_t grid = persist_grid(kernel, smem, n_tiles);
+            kernel<<<grid, kHashPThreads, smem, as_stream(stream)>>>(acc, cls, NoUpdate{}, 0u, capacity, fdc,
+                                                                    pool_slots, d_tiles, n_tiles, bins, unit, d_bin_ids,
+                                                                    d_table, d_next, d_counts, d_status);
+            return cuda_status(cudaGetLastError());
+        });
+    }
+    // ports in (kHashGroupBins, 65536]: the per-tile table kernel below measured faster than the
+    // per-record persistent form; above 65536 the persistent form is faster
+    if (gf_hash_persistent() && bins > 65536u) {
+        return with_layout(layout, h_in, h_out, [&](auto acc) -> gf_status {
+            using Acc = decltype(acc);
+            auto kernel = hash_scatter_persist_kernel<Acc, NoUpdate>;
+            const size_t smem = 2u * sizeof(uint32_t) * std::min(bins, kHashSmemBins);
+            cudaError_t e = allow_smem(kernel, smem);
+            if (e != cudaSuccess)
+                return cuda_status(e);
+            const uint32_t grid = persist_grid(kernel, smem, n_tiles);
+            kernel<<<grid, kHashPThreads, smem, as_stream(stream)>>>(acc, cls, NoUpdate{}, 0u, capacity, fdc,
+                                                                    pool_slots, d_tiles, n_tiles, bins, d_bin_ids,
+                                                                    d_table, d_next, d_counts, d_status);
+            return cuda_status(cudaGetLastError());
+        });
+    }
     return with_hash_shape(tile_size, [&]<typename Shape>() -> gf_status {
         return with_layout(layout, h_in, h_out, [&](auto acc) -> gf_status {
             using Acc = decltype(acc);
@@ -157,10 +230,19 @@ gf_status gf_plan_device(void* stream, const uint32_t* d_counts, uint32_t bins, 
     if (bins == 0u || capacity == 0u || d_counts == nullptr || d_table == nullptr || d_num_out == nullptr ||
         d_next == nullptr || (n_reserved != 0u && d_reserved == nullptr) || (desc_cap != 0u && d_descs == nullptr))
         return GF_ERR_ARGUMENT;
-    constexpr int T = 1024;
-    plan_device_kernel<T><<<1, T, 0, as_stream(stream)>>>(d_counts, bins, capacity, FastDiv(capacity), d_reserved,
-                                                         n_reserved, d_table, d_descs, desc_cap, d_num_out, d_next,
-                                                         d_status);
+    const cudaStream_t s = as_stream(stream);
+    const FastDiv fdc(capacity);
+    const uint32_t n_blocks = (uint32_t)(((uint64_t)bins + kPlanBlock - 1u) / kPlanBlock);
+    plan_blocksum_kernel<<<n_blocks, kPlanThreads, 0, s>>>(d_counts, bins, fdc, d_next);
+    plan_scan_kernel<1024><<<1, 1024, 0, s>>>(d_counts, bins, n_blocks, n_reserved, desc_cap, d_next, d_num_out,
+                                              d_status);
+    plan_bins_kernel<<<n_blocks, kPlanThreads, 0, s>>>(d_counts, bins, fdc, n_blocks, d_table, d_next, d_status);
+    // one thread per output chunk (at most min(desc_cap, n_reserved) of them), grid-stride
+    const uint64_t most = std::max<uint64_t>(std::min<uint64_t>(desc_cap, n_reserved), n_blocks);
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((most + kPlanThreads - 1u) / kPlanThreads,
+                                                       (uint64_t)device_sms() * 16u);
+    plan_chunks_kernel<<<std::max(grid, 1u), kPlanThreads, 0, s>>>(d_counts, bins, capacity, d_reserved, n_blocks,
+                                                                   d_table, d_descs, d_num_out, d_next, d_status);
     return cuda_status(cudaGetLastError());
 }
 

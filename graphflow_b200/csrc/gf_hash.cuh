@@ -298,63 +298,445 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) hash_scatt
 }
 
 // ---------------------------------------------------------------------------------------------
+// Persistent form of hash classify and scatter. The ports of this path are dense ranks
+// (unmix64(key) ^ salt < bins), so no per-tile open-addressing table is needed: every CTA owns a
+// contiguous range of tiles and keeps, for the ports below kHashSmemBins, one shared-memory
+// counter per port for its whole range (one device atomic per CTA and port instead of one per
+// tile and port); a record of a port at or above kHashSmemBins goes to a device atomic directly.
+// The scatter counts its range first, reserves one range per (CTA, port) on next[port] (arrival
+// order between CTAs, as the per-tile reservations of graph/HashScatterKernel.hpp:132-150), then
+// places every record with one shared-memory atomic on its port's running position and writes
+// it through the dense table layout out = table[B + table[port] + j / C] * C + j % C.
+// ---------------------------------------------------------------------------------------------
+constexpr uint32_t kHashSmemBins = 8192u;
+constexpr uint32_t kHashGroupBins = 2048u; // up to this many ports the scatter groups each tile by port
+constexpr int kHashPThreads = 256;
+constexpr int kHashPUnroll = 4; // records per thread in flight
+
+GF_D bool hash_tile_range(const gf_tile* tiles, uint32_t t, uint32_t capacity, uint64_t pool_slots, uint64_t& base,
+                          uint32_t& count, uint32_t* status)
+{
+    const gf_tile tile = tiles[t];
+    base = (uint64_t)tile.chunk_index * capacity + tile.tile_offset;
+    const bool ok = base + tile.count <= pool_slots && tile.tile_offset + tile.count <= capacity;
+    if (!ok && threadIdx.x == 0)
+        set_status(status, GF_INVALID);
+    count = ok ? tile.count : 0u;
+    return ok;
+}
+
+// Counts of ports [0, ks) of this CTA's range into hist (zeroed here); ports >= ks go to
+// counts[] directly. With bin_ids, every record's port is stored.
+template <typename Access>
+GF_D void hash_count_range(const Access& acc, const UnmixClassify& cls, uint32_t capacity, uint64_t pool_slots,
+                           const gf_tile* tiles, uint32_t t_lo, uint32_t t_hi, uint32_t B, uint32_t ks,
+                           uint32_t* bin_ids, uint32_t* hist, uint32_t* counts, uint32_t* status)
+{
+    for (uint32_t i = threadIdx.x; i < ks; i += blockDim.x)
+        hist[i] = 0u;
+    __syncthreads();
+    bool bad = false;
+    for (uint32_t t = t_lo; t < t_hi; ++t) {
+        uint64_t base;
+        uint32_t count;
+        hash_tile_range(tiles, t, capacity, pool_slots, base, count, status);
+        for (uint32_t i0 = 0; i0 < count; i0 += kHashPThreads * kHashPUnroll) {
+            uint64_t key[kHashPUnroll];
+#pragma unroll
+            for (int u = 0; u < kHashPUnroll; ++u) {
+                const uint32_t i = i0 + (uint32_t)u * kHashPThreads + threadIdx.x;
+                key[u] = i < count ? acc.load_key(base + i) : 0ull;
+            }
+#pragma unroll
+            for (int u = 0; u < kHashPUnroll; ++u) {
+                const uint32_t i = i0 + (uint32_t)u * kHashPThreads + threadIdx.x;
+                if (i >= count)
+                    continue;
+                const uint32_t b = cls(key[u]);
+                if (b >= B) {
+                    bad = true;
+                    continue;
+                }
+                if (bin_ids != nullptr)
+                    bin_ids[base + i] = b;
+                if (b < ks)
+                    atomicAdd(&hist[b], 1u);
+                else
+                    atomicAdd(&counts[b], 1u);
+            }
+        }
+    }
+    if (bad) {
+        counts[B] = 1u;
+        set_status(status, GF_INVALID);
+    }
+    __syncthreads();
+}
+
+template <typename Access>
+__global__ void __launch_bounds__(kHashPThreads) hash_count_persist_kernel(Access acc, UnmixClassify cls,
+                                                                           uint32_t capacity, uint64_t pool_slots,
+                                                                           const gf_tile* tiles, uint32_t n_tiles,
+                                                                           uint32_t B, uint32_t* bin_ids,
+                                                                           uint32_t* counts, uint32_t* status)
+{
+    extern __shared__ uint32_t hist[]; // [ks]
+    const uint32_t ks = B < kHashSmemBins ? B : kHashSmemBins;
+    const uint32_t G = gridDim.x, c = blockIdx.x;
+    const uint32_t t_lo = (uint32_t)((uint64_t)n_tiles * c / G), t_hi = (uint32_t)((uint64_t)n_tiles * (c + 1u) / G);
+    hash_count_range(acc, cls, capacity, pool_slots, tiles, t_lo, t_hi, B, ks, bin_ids, hist, counts, status);
+    for (uint32_t b = threadIdx.x; b < ks; b += blockDim.x)
+        if (hist[b] != 0u)
+            atomicAdd(&counts[b], hist[b]);
+}
+
+template <typename Access, typename Update>
+__global__ void __launch_bounds__(kHashPThreads) hash_scatter_persist_kernel(
+    Access acc, UnmixClassify cls, Update update, uint64_t seed_mixed, uint32_t capacity, FastDiv fdc,
+    uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B, const uint32_t* bin_ids,
+    const uint32_t* table, uint32_t* next, uint32_t* counts, uint32_t* status)
+{
+    using P = typename Access::Payload;
+    extern __shared__ uint32_t sm[];
+    const uint32_t ks = B < kHashSmemBins ? B : kHashSmemBins;
+    uint32_t* run = sm;        // [ks] this CTA's count, then its next position, per port
+    uint32_t* port_base = sm + ks; // [ks] table[port]
+    const uint32_t G = gridDim.x, c = blockIdx.x;
+    const uint32_t t_lo = (uint32_t)((uint64_t)n_tiles * c / G), t_hi = (uint32_t)((uint64_t)n_tiles * (c + 1u) / G);
+    // 1. count (the ports >= ks are reserved per record below, so they are not counted here)
+    {
+        for (uint32_t i = threadIdx.x; i < ks; i += blockDim.x)
+            run[i] = 0u;
+        __syncthreads();
+        for (uint32_t t = t_lo; t < t_hi; ++t) {
+            uint64_t base;
+            uint32_t count;
+            hash_tile_range(tiles, t, capacity, pool_slots, base, count, status);
+            for (uint32_t i0 = 0; i0 < count; i0 += kHashPThreads * kHashPUnroll) {
+                uint32_t b[kHashPUnroll];
+#pragma unroll
+                for (int u = 0; u < kHashPUnroll; ++u) {
+                    const uint32_t i = i0 + (uint32_t)u * kHashPThreads + threadIdx.x;
+                    b[u] = i >= count ? B : bin_ids != nullptr ? __ldg(bin_ids + base + i) : cls(acc.load_key(base + i));
+                }
+#pragma unroll
+                for (int u = 0; u < kHashPUnroll; ++u)
+                    if (b[u] < ks)
+                        atomicAdd(&run[b[u]], 1u);
+            }
+        }
+        __syncthreads();
+    }
+    // 2. reserve this CTA's range of every port it holds
+    for (uint32_t p = threadIdx.x; p < ks; p += blockDim.x) {
+        const uint32_t n = run[p];
+        if (n != 0u) {
+            run[p] = atomicAdd(&next[p], n);
+            port_base[p] = __ldg(table + p);
+        }
+    }
+    __syncthreads();
+    // 3. place and write every record
+    bool bad = false, overflow = false;
+    uint32_t upd = kUpdateSuccess;
+    for (uint32_t t = t_lo; t < t_hi; ++t) {
+        uint64_t base;
+        uint32_t count;
+        hash_tile_range(tiles, t, capacity, pool_slots, base, count, status);
+        for (uint32_t i0 = 0; i0 < count; i0 += kHashPThreads * kHashPUnroll) {
+            P rec[kHashPUnroll];
+            uint32_t b[kHashPUnroll];
+#pragma unroll
+            for (int u = 0; u < kHashPUnroll; ++u) {
+                const uint32_t i = i0 + (uint32_t)u * kHashPThreads + threadIdx.x;
+                if (i < count) {
+                    rec[u] = acc.load(base + i);
+                    b[u] = bin_ids != nullptr ? __ldg(bin_ids + base + i) : cls(rec[u].key);
+                } else {
+                    b[u] = B + 1u; // no record
+                }
+            }
+            uint32_t j[kHashPUnroll], pb[kHashPUnroll];
+#pragma unroll
+            for (int u = 0; u < kHashPUnroll; ++u) {
+                if (b[u] < ks) {
+                    j[u] = atomicAdd(&run[b[u]], 1u);
+                    pb[u] = port_base[b[u]];
+                } else if (b[u] < B) {
+                    j[u] = atomicAdd(&next[b[u]], 1u);
+                    pb[u] = __ldg(table + b[u]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kHashPUnroll; ++u) {
+                if (b[u] >= B) {
+                    bad = bad || b[u] == B;
+                    continue;
+                }
+                const uint32_t k = fdc.div(j[u]);
+                const uint32_t chunk = __ldg(table + B + pb[u] + k);
+                const uint64_t slot = (uint64_t)chunk * capacity + (j[u] - k * capacity);
+                const uint32_t r = update(b[u], rec[u], seed_mixed);
+                if (r != kUpdateSuccess)
+                    upd = r;
+                if (slot < pool_slots)
+                    acc.store(slot, rec[u]);
+                else
+                    overflow = true;
+            }
+        }
+    }
+    if (bad || upd != kUpdateSuccess) {
+        counts[B] = 1u;
+        set_status(status, bad || upd == kUpdateInvalid ? GF_INVALID : GF_OVERFLOW);
+    }
+    if (overflow)
+        set_status(status, GF_OVERFLOW);
+}
+
+// Grouped scatter for B <= kHashGroupBins: persistent CTAs over contiguous tile ranges; every
+// unit of up to `unit` records of a tile is grouped by port in shared memory (a direct-indexed
+// count per port that also gives each record its rank, an exclusive scan over the ports), each
+// port present in the unit reserves its range with one device atomic on next[port] (arrival order
+// between units, as graph/HashScatterKernel.hpp:132-150 reserves per table entry), and a port's
+// records of the unit go to consecutive slots from consecutive threads.
+template <typename Access, typename Update>
+__global__ void __launch_bounds__(kHashPThreads) hash_scatter_grouped_kernel(
+    Access acc, UnmixClassify cls, Update update, uint64_t seed_mixed, uint32_t capacity, FastDiv fdc,
+    uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B, uint32_t unit, const uint32_t* bin_ids,
+    const uint32_t* table, uint32_t* next, uint32_t* counts, uint32_t* status)
+{
+    using P = typename Access::Payload;
+    constexpr uint32_t T = kHashPThreads, RPT = 2048u / T; // records per thread per unit, units of <= 2048
+    extern __shared__ __align__(16) uint32_t sm[];
+    P* stage = reinterpret_cast<P*>(sm);                                 // [unit]
+    uint32_t* port_base = reinterpret_cast<uint32_t*>(stage + unit);     // [B] table[port]
+    uint32_t* tcnt = port_base + B;                                      // [B] records of the unit per port
+    uint32_t* tpre = tcnt + B;                                           // [B] the unit's stage start per port
+    uint32_t* tpos = tpre + B;                                           // [B] the port's reserved position
+    uint16_t* sport = reinterpret_cast<uint16_t*>(tpos + B);             // [unit] port per stage position
+    uint32_t* scan_tmp = reinterpret_cast<uint32_t*>(sport + ((unit + 1u) & ~1u)); // [T / 32 + 1]
+    const uint32_t G = gridDim.x, c = blockIdx.x;
+    const uint32_t t_lo = (uint32_t)((uint64_t)n_tiles * c / G), t_hi = (uint32_t)((uint64_t)n_tiles * (c + 1u) / G);
+    for (uint32_t i = threadIdx.x; i < B; i += T) {
+        port_base[i] = __ldg(table + i);
+        tcnt[i] = 0u;
+    }
+    __syncthreads();
+    bool bad = false, overflow = false;
+    uint32_t upd = kUpdateSuccess;
+    for (uint32_t t = t_lo; t < t_hi; ++t) {
+        uint64_t base;
+        uint32_t count;
+        hash_tile_range(tiles, t, capacity, pool_slots, base, count, status);
+        for (uint32_t u0 = 0; u0 < count; u0 += unit) {
+            const uint32_t n = count - u0 < unit ? count - u0 : unit;
+            P rec[RPT];
+            uint32_t bp[RPT]; // port | rank << 16 (rank < unit <= 2048), or kNoBin16 in the low half
+#pragma unroll
+            for (uint32_t r = 0; r < RPT; ++r) {
+                const uint32_t i = r * T + threadIdx.x;
+                if (i < n)
+                    rec[r] = acc.load(base + u0 + i);
+            }
+#pragma unroll
+            for (uint32_t r = 0; r < RPT; ++r) {
+                const uint32_t i = r * T + threadIdx.x;
+                bp[r] = kNoBin16;
+                if (i < n) {
+                    const uint32_t b = bin_ids != nullptr ? __ldg(bin_ids + base + u0 + i) : cls(rec[r].key);
+                    if (b < B)
+                        bp[r] = b | (atomicAdd(&tcnt[b], 1u) << 16);
+                    else
+                        bad = true;
+                }
+            }
+            __syncthreads();
+            const uint32_t n_valid = block_exclusive_scan<T>(tcnt, tpre, B, scan_tmp); // records staged
+            __syncthreads();
+            for (uint32_t p = threadIdx.x; p < B; p += T) {
+                const uint32_t m = tcnt[p];
+                if (m != 0u) {
+                    tpos[p] = atomicAdd(&next[p], m);
+                    tcnt[p] = 0u;
+                }
+            }
+#pragma unroll
+            for (uint32_t r = 0; r < RPT; ++r) {
+                const uint32_t b = bp[r] & 0xFFFFu;
+                if (b != kNoBin16) {
+                    const uint32_t q = tpre[b] + (bp[r] >> 16);
+                    const uint32_t res = update(b, rec[r], seed_mixed);
+                    if (res != kUpdateSuccess)
+                        upd = res;
+                    stage[q] = rec[r];
+                    sport[q] = (uint16_t)b;
+                }
+            }
+            __syncthreads();
+            // positions [0, n_valid) are this unit's, in port order; consecutive positions of a port
+            // go to consecutive slots
+            for (uint32_t q = threadIdx.x; q < n_valid; q += T) {
+                const uint32_t b = sport[q];
+                const uint32_t j = tpos[b] + (q - tpre[b]);
+                const uint32_t k = fdc.div(j);
+                const uint32_t chunk = __ldg(table + B + port_base[b] + k);
+                const uint64_t slot = (uint64_t)chunk * capacity + (j - k * capacity);
+                if (slot < pool_slots)
+                    acc.store(slot, stage[q]);
+                else
+                    overflow = true;
+            }
+            __syncthreads();
+        }
+    }
+    if (bad || upd != kUpdateSuccess) {
+        counts[B] = 1u;
+        set_status(status, bad || upd == kUpdateInvalid ? GF_INVALID : GF_OVERFLOW);
+    }
+    if (overflow)
+        set_status(status, GF_OVERFLOW);
+}
+
+// ---------------------------------------------------------------------------------------------
 // Device plan from the per-bin totals and a reservation: binBase = exclusive scan of
 // ceil(total_b / C) (DenseBinTable.hpp:39-77), chunk (b, k) = reserved[binBase[b] + k],
 // table = [binBase[B], chunkIndex[R]] (DenseBinTable.hpp:80-91), descriptors in bin order with
-// their fills (Execution.hpp:2558-2581), next[] zeroed for the scatter. One CTA.
+// their fills (Execution.hpp:2558-2581), next[] zeroed for the scatter.
 // counts[B] (the classify status slot) must be zero; the plan also checks R <= n_reserved.
+// Four grid-wide steps, so that the cost does not grow with B on one CTA:
+//   A  block sums of ceil(total_b / C) over blocks of kPlanBlock bins, into next[block];
+//   B  one CTA: exclusive scan of the block sums in place, R, the checks, num_out;
+//   C  per block: binBase of every bin into table[b], next[b] = 0 for b >= #blocks;
+//   D  one thread per output chunk r < R: its bin by binary search over table[0, B), the chunk id
+//      and the descriptor; next[0, #blocks) = 0.
+// A failed batch (status set) leaves table, descriptors and next untouched after step B.
 // ---------------------------------------------------------------------------------------------
+constexpr uint32_t kPlanThreads = 256u, kPlanPerThread = 8u, kPlanBlock = kPlanThreads * kPlanPerThread;
+
+GF_D uint32_t chunks_of(uint32_t c, FastDiv fdc) { return fdc.div(c) + (fdc.mod(c) != 0u ? 1u : 0u); }
+
+// Sum of v over the CTA, valid in every thread.
+GF_D uint32_t plan_block_sum(uint32_t v, uint32_t* tmp)
+{
+    v = __reduce_add_sync(0xFFFFFFFFu, v);
+    if ((threadIdx.x & 31u) == 0u)
+        tmp[threadIdx.x >> 5] = v;
+    __syncthreads();
+    uint32_t s = 0;
+    for (uint32_t i = 0; i < blockDim.x / 32u; ++i)
+        s += tmp[i];
+    __syncthreads();
+    return s;
+}
+
+__global__ void __launch_bounds__(kPlanThreads) plan_blocksum_kernel(const uint32_t* counts, uint32_t B, FastDiv fdc,
+                                                                      uint32_t* next)
+{
+    __shared__ uint32_t tmp[kPlanThreads / 32];
+    const uint32_t b0 = blockIdx.x * kPlanBlock + threadIdx.x * kPlanPerThread;
+    uint32_t s = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < kPlanPerThread; ++i)
+        if (b0 + i < B)
+            s += chunks_of(counts[b0 + i], fdc);
+    s = plan_block_sum(s, tmp);
+    if (threadIdx.x == 0)
+        next[blockIdx.x] = s;
+}
+
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) plan_device_kernel(const uint32_t* counts, uint32_t B, uint32_t capacity,
-                                                              FastDiv fdc, const uint32_t* reserved,
-                                                              uint32_t n_reserved, uint32_t* table,
-                                                              gf_out_desc* descs, uint32_t desc_cap,
-                                                              uint32_t* num_out, uint32_t* next, uint32_t* status)
+__global__ void __launch_bounds__(THREADS) plan_scan_kernel(const uint32_t* counts, uint32_t B, uint32_t n_blocks,
+                                                            uint32_t n_reserved, uint32_t desc_cap, uint32_t* next,
+                                                            uint32_t* num_out, uint32_t* status)
 {
     __shared__ uint32_t tmp[THREADS / 32 + 1];
-    __shared__ uint32_t s_part[THREADS];
-    if (counts[B] != 0u) {
-        if (threadIdx.x == 0) {
+    const uint32_t total = block_exclusive_scan<THREADS>(next, next, n_blocks, tmp);
+    if (threadIdx.x == 0) {
+        if (counts[B] != 0u) {
             set_status(status, GF_INVALID);
             *num_out = 0u;
-        }
-        return;
-    }
-    // contiguous segment per thread
-    const uint32_t per = (B + THREADS - 1) / THREADS;
-    const uint32_t lo = min(B, threadIdx.x * per), hi = min(B, lo + per);
-    uint32_t sum = 0;
-    for (uint32_t b = lo; b < hi; ++b) {
-        const uint32_t c = counts[b];
-        sum += fdc.div(c) + (fdc.mod(c) != 0u ? 1u : 0u);
-    }
-    s_part[threadIdx.x] = sum;
-    __syncthreads();
-    const uint32_t total = block_exclusive_scan<THREADS>(s_part, s_part, THREADS, tmp);
-    if (total > n_reserved || total > desc_cap) {
-        if (threadIdx.x == 0) {
+        } else if (total > n_reserved || total > desc_cap) {
             set_status(status, GF_OVERFLOW);
             *num_out = 0u;
+        } else {
+            *num_out = total;
         }
+    }
+}
+
+__global__ void __launch_bounds__(kPlanThreads) plan_bins_kernel(const uint32_t* counts, uint32_t B, FastDiv fdc,
+                                                                  uint32_t n_blocks, uint32_t* table, uint32_t* next,
+                                                                  const uint32_t* status)
+{
+    __shared__ uint32_t tmp[kPlanThreads / 32 + 1];
+    if (ld_relaxed_u32(status) != 0u)
         return;
+    const uint32_t b0 = blockIdx.x * kPlanBlock + threadIdx.x * kPlanPerThread;
+    uint32_t nk[kPlanPerThread], s = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < kPlanPerThread; ++i) {
+        nk[i] = b0 + i < B ? chunks_of(counts[b0 + i], fdc) : 0u;
+        s += nk[i];
     }
-    uint32_t run = s_part[threadIdx.x];
-    for (uint32_t b = lo; b < hi; ++b) {
-        const uint32_t c = counts[b];
-        const uint32_t nk = fdc.div(c) + (fdc.mod(c) != 0u ? 1u : 0u);
-        table[b] = run;
-        next[b] = 0u;
-        for (uint32_t k = 0; k < nk; ++k) {
-            const uint32_t chunk = __ldg(reserved + run + k);
-            table[B + run + k] = chunk;
-            descs[run + k].chunk_index = chunk;
-            descs[run + k].fill = min(capacity, c - k * capacity);
-            descs[run + k].bin = b;
+    // exclusive prefix of s over the CTA
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    uint32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if ((int)lane >= o)
+            incl += y;
+    }
+    if (lane == 31u)
+        tmp[w] = incl;
+    __syncthreads();
+    uint32_t run = next[blockIdx.x] + incl - s; // every CTA reads its base before any CTA could reuse the word
+#pragma unroll
+    for (uint32_t i = 0; i < kPlanThreads / 32u; ++i)
+        run += i < w ? tmp[i] : 0u;
+#pragma unroll
+    for (uint32_t i = 0; i < kPlanPerThread; ++i) {
+        const uint32_t b = b0 + i;
+        if (b < B) {
+            table[b] = run;
+            if (b >= n_blocks)
+                next[b] = 0u;
         }
-        run += nk;
+        run += nk[i];
     }
-    if (threadIdx.x == 0)
-        *num_out = total;
+}
+
+__global__ void __launch_bounds__(kPlanThreads) plan_chunks_kernel(const uint32_t* counts, uint32_t B, uint32_t capacity,
+                                                                    const uint32_t* reserved, uint32_t n_blocks,
+                                                                    uint32_t* table, gf_out_desc* descs,
+                                                                    const uint32_t* num_out, uint32_t* next,
+                                                                    const uint32_t* status)
+{
+    if (ld_relaxed_u32(status) != 0u)
+        return;
+    const uint32_t R = *num_out;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < R || r < n_blocks; r += stride) {
+        if (r < n_blocks)
+            next[r] = 0u;
+        if (r >= R)
+            continue;
+        uint32_t lo = 0, hi = B - 1u; // the last bin whose first chunk is at or before r
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1u) >> 1;
+            if (table[mid] <= r)
+                lo = mid;
+            else
+                hi = mid - 1u;
+        }
+        const uint32_t k = r - table[lo];
+        const uint32_t chunk = __ldg(reserved + r);
+        table[B + r] = chunk;
+        descs[r].chunk_index = chunk;
+        descs[r].fill = min(capacity, counts[lo] - k * capacity);
+        descs[r].bin = lo;
+    }
 }
 
 // Synthetic 16-byte records: rank r ~ Zipf(cdf over k), key = mix64(r ^ salt), weight = U(0,1]

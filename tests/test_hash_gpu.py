@@ -96,3 +96,23 @@ def test_hash_partition_small(form, n):
 def test_hash_one_bin_per_particle_sparse():
     # tests/integration/test_hash_bins.cpp: sparse 65536 bins, every particle in its own bin
     _run(capi.LAYOUT_AOS, "device", 60_000, 65536, 0.0, capacity=64, tile=2048)
+
+
+@pytest.mark.parametrize("k", [2048, 2049, 70_000])
+@pytest.mark.parametrize("tile", [1024, 2048])
+def test_hash_kernel_forms_at_their_boundaries(k, tile):
+    """Port counts on both sides of the grouped scatter's limit (2048 ports: direct-indexed
+    per-unit grouping) and of the per-record persistent form (above 65536 ports)."""
+    _run(capi.LAYOUT_SOA, "device", 90_001, k, 1.1, tile=tile)
+
+
+@pytest.mark.parametrize("form", ["plain", "device"])
+@pytest.mark.parametrize("k", [1024, 2**20])
+def test_hash_per_tile_kernels_agree(form, k):
+    """The per-tile open-addressing kernels (tuning knob hash_persistent = 0) give the same
+    counts, plan and per-port multisets as the persistent kernels."""
+    try:
+        capi.check(capi.lib().gf_set_tuning(b"hash_persistent", 0), "tuning")
+        _run(capi.LAYOUT_AOS, form, 80_003, k, 1.2, tile=2048)
+    finally:
+        capi.check(capi.lib().gf_set_tuning(b"hash_persistent", 1), "tuning")
