@@ -170,12 +170,14 @@ gf_status gf_scatter_hash_r16(void* stream, const gf_rec16_columns* h_in, const 
         return GF_OK;
     UnmixClassify cls{salt, bins};
     const FastDiv fdc(capacity);
-    if (gf_hash_persistent() && bins <= kHashGroupBins) {
+    if (gf_hash_persistent()) {
         return with_layout(layout, h_in, h_out, [&](auto acc) -> gf_status {
             using Acc = decltype(acc);
-            auto kernel = hash_scatter_grouped_kernel<Acc, NoUpdate>;
+            auto kernel = bins > kHashGroupBins ? hash_scatter_grouped_kernel<Acc, NoUpdate, true>
+                                                : hash_scatter_grouped_kernel<Acc, NoUpdate, false>;
             const uint32_t unit = tile_size; // 1024 or 2048
-            const size_t smem = sizeof(Rec16) * unit + 4u * sizeof(uint32_t) * bins + sizeof(uint16_t) * ((unit + 1u) & ~1u) +
+            const size_t smem = sizeof(Rec16) * unit + 4u * sizeof(uint32_t) * std::min(bins, kHashGroupBins) +
+                                sizeof(uint16_t) * ((unit + 1u) & ~1u) +
                                 sizeof(uint32_t) * (kHashPThreads / 32 + 1);
             cudaError_t e = allow_smem(kernel, smem);
             if (e != cudaSuccess)
@@ -183,23 +185,6 @@ gf_status gf_scatter_hash_r16(void* stream, const gf_rec16_columns* h_in, const 
             const uint32_t grid = persist_grid(kernel, smem, n_tiles);
             kernel<<<grid, kHashPThreads, smem, as_stream(stream)>>>(acc, cls, NoUpdate{}, 0u, capacity, fdc,
                                                                     pool_slots, d_tiles, n_tiles, bins, unit, d_bin_ids,
-                                                                    d_table, d_next, d_counts, d_status);
-            return cuda_status(cudaGetLastError());
-        });
-    }
-    // ports in (kHashGroupBins, 65536]: the per-tile table kernel below measured faster than the
-    // per-record persistent form; above 65536 the persistent form is faster
-    if (gf_hash_persistent() && bins > 65536u) {
-        return with_layout(layout, h_in, h_out, [&](auto acc) -> gf_status {
-            using Acc = decltype(acc);
-            auto kernel = hash_scatter_persist_kernel<Acc, NoUpdate>;
-            const size_t smem = 2u * sizeof(uint32_t) * std::min(bins, kHashSmemBins);
-            cudaError_t e = allow_smem(kernel, smem);
-            if (e != cudaSuccess)
-                return cuda_status(e);
-            const uint32_t grid = persist_grid(kernel, smem, n_tiles);
-            kernel<<<grid, kHashPThreads, smem, as_stream(stream)>>>(acc, cls, NoUpdate{}, 0u, capacity, fdc,
-                                                                    pool_slots, d_tiles, n_tiles, bins, d_bin_ids,
                                                                     d_table, d_next, d_counts, d_status);
             return cuda_status(cudaGetLastError());
         });

@@ -303,10 +303,8 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) hash_scatt
 // contiguous range of tiles and keeps, for the ports below kHashSmemBins, one shared-memory
 // counter per port for its whole range (one device atomic per CTA and port instead of one per
 // tile and port); a record of a port at or above kHashSmemBins goes to a device atomic directly.
-// The scatter counts its range first, reserves one range per (CTA, port) on next[port] (arrival
-// order between CTAs, as the per-tile reservations of graph/HashScatterKernel.hpp:132-150), then
-// places every record with one shared-memory atomic on its port's running position and writes
-// it through the dense table layout out = table[B + table[port] + j / C] * C + j % C.
+// The scatter (hash_scatter_grouped_kernel below) writes through the dense table layout
+// out = table[B + table[port] + j / C] * C + j % C.
 // ---------------------------------------------------------------------------------------------
 constexpr uint32_t kHashSmemBins = 8192u;
 constexpr uint32_t kHashGroupBins = 2048u; // up to this many ports the scatter groups each tile by port
@@ -390,117 +388,16 @@ __global__ void __launch_bounds__(kHashPThreads) hash_count_persist_kernel(Acces
             atomicAdd(&counts[b], hist[b]);
 }
 
-template <typename Access, typename Update>
-__global__ void __launch_bounds__(kHashPThreads) hash_scatter_persist_kernel(
-    Access acc, UnmixClassify cls, Update update, uint64_t seed_mixed, uint32_t capacity, FastDiv fdc,
-    uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B, const uint32_t* bin_ids,
-    const uint32_t* table, uint32_t* next, uint32_t* counts, uint32_t* status)
-{
-    using P = typename Access::Payload;
-    extern __shared__ uint32_t sm[];
-    const uint32_t ks = B < kHashSmemBins ? B : kHashSmemBins;
-    uint32_t* run = sm;        // [ks] this CTA's count, then its next position, per port
-    uint32_t* port_base = sm + ks; // [ks] table[port]
-    const uint32_t G = gridDim.x, c = blockIdx.x;
-    const uint32_t t_lo = (uint32_t)((uint64_t)n_tiles * c / G), t_hi = (uint32_t)((uint64_t)n_tiles * (c + 1u) / G);
-    // 1. count (the ports >= ks are reserved per record below, so they are not counted here)
-    {
-        for (uint32_t i = threadIdx.x; i < ks; i += blockDim.x)
-            run[i] = 0u;
-        __syncthreads();
-        for (uint32_t t = t_lo; t < t_hi; ++t) {
-            uint64_t base;
-            uint32_t count;
-            hash_tile_range(tiles, t, capacity, pool_slots, base, count, status);
-            for (uint32_t i0 = 0; i0 < count; i0 += kHashPThreads * kHashPUnroll) {
-                uint32_t b[kHashPUnroll];
-#pragma unroll
-                for (int u = 0; u < kHashPUnroll; ++u) {
-                    const uint32_t i = i0 + (uint32_t)u * kHashPThreads + threadIdx.x;
-                    b[u] = i >= count ? B : bin_ids != nullptr ? __ldg(bin_ids + base + i) : cls(acc.load_key(base + i));
-                }
-#pragma unroll
-                for (int u = 0; u < kHashPUnroll; ++u)
-                    if (b[u] < ks)
-                        atomicAdd(&run[b[u]], 1u);
-            }
-        }
-        __syncthreads();
-    }
-    // 2. reserve this CTA's range of every port it holds
-    for (uint32_t p = threadIdx.x; p < ks; p += blockDim.x) {
-        const uint32_t n = run[p];
-        if (n != 0u) {
-            run[p] = atomicAdd(&next[p], n);
-            port_base[p] = __ldg(table + p);
-        }
-    }
-    __syncthreads();
-    // 3. place and write every record
-    bool bad = false, overflow = false;
-    uint32_t upd = kUpdateSuccess;
-    for (uint32_t t = t_lo; t < t_hi; ++t) {
-        uint64_t base;
-        uint32_t count;
-        hash_tile_range(tiles, t, capacity, pool_slots, base, count, status);
-        for (uint32_t i0 = 0; i0 < count; i0 += kHashPThreads * kHashPUnroll) {
-            P rec[kHashPUnroll];
-            uint32_t b[kHashPUnroll];
-#pragma unroll
-            for (int u = 0; u < kHashPUnroll; ++u) {
-                const uint32_t i = i0 + (uint32_t)u * kHashPThreads + threadIdx.x;
-                if (i < count) {
-                    rec[u] = acc.load(base + i);
-                    b[u] = bin_ids != nullptr ? __ldg(bin_ids + base + i) : cls(rec[u].key);
-                } else {
-                    b[u] = B + 1u; // no record
-                }
-            }
-            uint32_t j[kHashPUnroll], pb[kHashPUnroll];
-#pragma unroll
-            for (int u = 0; u < kHashPUnroll; ++u) {
-                if (b[u] < ks) {
-                    j[u] = atomicAdd(&run[b[u]], 1u);
-                    pb[u] = port_base[b[u]];
-                } else if (b[u] < B) {
-                    j[u] = atomicAdd(&next[b[u]], 1u);
-                    pb[u] = __ldg(table + b[u]);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < kHashPUnroll; ++u) {
-                if (b[u] >= B) {
-                    bad = bad || b[u] == B;
-                    continue;
-                }
-                const uint32_t k = fdc.div(j[u]);
-                const uint32_t chunk = __ldg(table + B + pb[u] + k);
-                const uint64_t slot = (uint64_t)chunk * capacity + (j[u] - k * capacity);
-                const uint32_t r = update(b[u], rec[u], seed_mixed);
-                if (r != kUpdateSuccess)
-                    upd = r;
-                if (slot < pool_slots)
-                    acc.store(slot, rec[u]);
-                else
-                    overflow = true;
-            }
-        }
-    }
-    if (bad || upd != kUpdateSuccess) {
-        counts[B] = 1u;
-        set_status(status, bad || upd == kUpdateInvalid ? GF_INVALID : GF_OVERFLOW);
-    }
-    if (overflow)
-        set_status(status, GF_OVERFLOW);
-}
-
-// Grouped scatter for B <= kHashGroupBins: persistent CTAs over contiguous tile ranges; every
-// unit of up to `unit` records of a tile is grouped by port in shared memory (a direct-indexed
-// count per port that also gives each record its rank, an exclusive scan over the ports), each
-// port present in the unit reserves its range with one device atomic on next[port] (arrival order
-// between units, as graph/HashScatterKernel.hpp:132-150 reserves per table entry), and a port's
-// records of the unit go to consecutive slots from consecutive threads.
-template <typename Access, typename Update>
+// Grouped scatter: persistent CTAs over contiguous tile ranges; in every unit of up to `unit`
+// records of a tile, the records of ports below GB = min(B, kHashGroupBins) are grouped by port
+// in shared memory (a direct-indexed count per port that also gives each record its rank, an
+// exclusive scan over the GB ports), each such port present in the unit reserves its range with
+// one device atomic on next[port] (arrival order between units, as
+// graph/HashScatterKernel.hpp:132-150 reserves per table entry), and a port's records of the unit
+// go to consecutive slots from consecutive threads. A record of a port >= GB (the tail of a
+// popularity-ranked key space) reserves its own slot with one device atomic and is written at
+// once; that path is compiled only when B > kHashGroupBins (kTail).
+template <typename Access, typename Update, bool kTail>
 __global__ void __launch_bounds__(kHashPThreads) hash_scatter_grouped_kernel(
     Access acc, UnmixClassify cls, Update update, uint64_t seed_mixed, uint32_t capacity, FastDiv fdc,
     uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B, uint32_t unit, const uint32_t* bin_ids,
@@ -510,20 +407,32 @@ __global__ void __launch_bounds__(kHashPThreads) hash_scatter_grouped_kernel(
     constexpr uint32_t T = kHashPThreads, RPT = 2048u / T; // records per thread per unit, units of <= 2048
     extern __shared__ __align__(16) uint32_t sm[];
     P* stage = reinterpret_cast<P*>(sm);                                 // [unit]
-    uint32_t* port_base = reinterpret_cast<uint32_t*>(stage + unit);     // [B] table[port]
-    uint32_t* tcnt = port_base + B;                                      // [B] records of the unit per port
-    uint32_t* tpre = tcnt + B;                                           // [B] the unit's stage start per port
-    uint32_t* tpos = tpre + B;                                           // [B] the port's reserved position
-    uint16_t* sport = reinterpret_cast<uint16_t*>(tpos + B);             // [unit] port per stage position
+    const uint32_t GB = B < kHashGroupBins ? B : kHashGroupBins;
+    uint32_t* port_base = reinterpret_cast<uint32_t*>(stage + unit);     // [GB] table[port]
+    uint32_t* tcnt = port_base + GB;                                     // [GB] records of the unit per port
+    uint32_t* tpre = tcnt + GB;                                          // [GB] the unit's stage start per port
+    uint32_t* tpos = tpre + GB;                                          // [GB] the port's reserved position
+    uint16_t* sport = reinterpret_cast<uint16_t*>(tpos + GB);            // [unit] port per stage position
     uint32_t* scan_tmp = reinterpret_cast<uint32_t*>(sport + ((unit + 1u) & ~1u)); // [T / 32 + 1]
     const uint32_t G = gridDim.x, c = blockIdx.x;
     const uint32_t t_lo = (uint32_t)((uint64_t)n_tiles * c / G), t_hi = (uint32_t)((uint64_t)n_tiles * (c + 1u) / G);
-    for (uint32_t i = threadIdx.x; i < B; i += T) {
+    for (uint32_t i = threadIdx.x; i < GB; i += T) {
         port_base[i] = __ldg(table + i);
         tcnt[i] = 0u;
     }
     __syncthreads();
     bool bad = false, overflow = false;
+    // a record of a port >= GB: its own slot, written now
+    auto place = [&](uint32_t b, P& r) {
+        const uint32_t j = atomicAdd(&next[b], 1u);
+        const uint32_t k = fdc.div(j);
+        const uint32_t chunk = __ldg(table + B + __ldg(table + b) + k);
+        const uint64_t slot = (uint64_t)chunk * capacity + (j - k * capacity);
+        if (slot < pool_slots)
+            acc.store(slot, r);
+        else
+            overflow = true;
+    };
     uint32_t upd = kUpdateSuccess;
     for (uint32_t t = t_lo; t < t_hi; ++t) {
         uint64_t base;
@@ -545,16 +454,22 @@ __global__ void __launch_bounds__(kHashPThreads) hash_scatter_grouped_kernel(
                 bp[r] = kNoBin16;
                 if (i < n) {
                     const uint32_t b = bin_ids != nullptr ? __ldg(bin_ids + base + u0 + i) : cls(rec[r].key);
-                    if (b < B)
+                    if (b < GB) {
                         bp[r] = b | (atomicAdd(&tcnt[b], 1u) << 16);
-                    else
+                    } else if (kTail && b < B) {
+                        const uint32_t res = update(b, rec[r], seed_mixed);
+                        if (res != kUpdateSuccess)
+                            upd = res;
+                        place(b, rec[r]);
+                    } else {
                         bad = true;
+                    }
                 }
             }
             __syncthreads();
-            const uint32_t n_valid = block_exclusive_scan<T>(tcnt, tpre, B, scan_tmp); // records staged
+            const uint32_t n_valid = block_exclusive_scan<T>(tcnt, tpre, GB, scan_tmp); // records staged
             __syncthreads();
-            for (uint32_t p = threadIdx.x; p < B; p += T) {
+            for (uint32_t p = threadIdx.x; p < GB; p += T) {
                 const uint32_t m = tcnt[p];
                 if (m != 0u) {
                     tpos[p] = atomicAdd(&next[p], m);
