@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--no-sweep", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the other configurations' measurements")
+    p.add_argument("--hash", type=int, default=0, metavar="K",
+                   help="only run the device-planned hash partition of --n records over K keys (Zipf 1.2, "
+                        "tiles of 2048) --steps times after --warmup batches and print its timing; for profiling")
     return p.parse_args()
 
 
@@ -542,6 +545,21 @@ def _cfg_particle_feedback():
     out["forms_identical"] = bool(np.array_equal(w, w0) and np.array_equal(c, c0))
     out["cpu_scalar_model"] = {"seconds": cpu_s, "particles_per_s": n / cpu_s, "cores": threads,
                                "kind": "port (tests/reference/ScalarModel.hpp restated: per-particle loop, no runner)"}
+    # the reference's published configuration (docs/benchmarks.md:24-34: N=1e8, C=8192, P=16384,
+    # Q=8, 1.3e7 particles/s on a V100) through the same Flow; its sorted weight,count rows must
+    # hash to the SHA-256 the reference published
+    import hashlib
+    n8 = 100_000_000
+    w8, _, st8 = capi.run_particle_feedback(42, n8, chunk_capacity=8192, live_particles=16384, batch_chunks=8)
+    v8, c8 = O.histogram_u32(w8)
+    text = "".join(f"{int(v)},{int(c)}\n" for v, c in zip(v8, c8))
+    out["published_config_flow"] = {
+        "workload": "particle_feedback N=1e8 seed 42 C=8192 P=16384 Q=8 maxVisits=64 through the Flow",
+        "seconds": st8.seconds, "particles_per_s": n8 / st8.seconds, "partition_batches": st8.partition_batches,
+        "kernel_launches": st8.kernel_launches, "histogram_rows": int(len(v8)),
+        "histogram_sha256_matches_published": hashlib.sha256(text.encode()).hexdigest()
+        == "21ab0aeb9ec72d380af2ce6e9631f8fa7b9111d24ff7831f272aa9f6a7be9dab",
+        "reference_published_particles_per_s": 1.3e7}
     return out
 
 
@@ -726,8 +744,50 @@ def bench_reserve_cap(args):
     return capi.output_chunk_bound(args.n, CAPACITY, args.bins)
 
 
+def hash_only(args):
+    """One hash-partition workload (16-byte records in three columns, keys over args.hash values
+    with Zipf(1.2) popularity, C = 8192 for K <= 4096, else 2048 (K <= 65536) or 512): warm-up
+    batches, then timed batches of classify -> device plan -> scatter; prints one JSON line."""
+    import ctypes
+    import numpy as np
+    import torch
+    from graphflow_b200 import capi
+    from graphflow_b200.hashpart import HashPartition, RecordPool
+    n, k, salt = args.n, args.hash, 0x5EED
+    cap = 8192 if k <= 4096 else (2048 if k <= 65536 else 512)
+    n_in = -(-n // cap)
+    bound = capi.output_chunk_bound(n, cap, k)
+    pool = RecordPool(n_in + bound, cap, layout=capi.LAYOUT_SOA)
+    cdf = torch.from_numpy(capi.zipf_cdf(1.2, k)).cuda()
+    capi.check(capi.lib().gf_generate_records16(None, SEED, 0, n, cdf.data_ptr(), k, salt, ctypes.byref(pool.cols),
+                                                capi.LAYOUT_SOA), "generate")
+    fills = np.full(n_in, cap, np.uint32)
+    fills[-1] = n - cap * (n_in - 1)
+    for _ in range(n_in):
+        pool.free.popleft()
+    part = HashPartition(pool, k, salt, tile_size=2048, form="device", max_batch_particles=n)
+    tiles, d_tiles = part._tiles(np.arange(n_in, dtype=np.uint32), fills)
+    part.reserved[:bound].copy_(torch.from_numpy(np.arange(n_in, n_in + bound, dtype=np.uint32).view(np.int32)))
+    for _ in range(args.warmup):
+        part.enqueue_device(d_tiles.data_ptr(), len(tiles), bound)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        part.enqueue_device(d_tiles.data_ptr(), len(tiles), bound)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    print(json.dumps({"workload": f"hash partition, N={n} 16-byte records (SoA), Zipf 1.2 over K={k} keys, C={cap}, "
+                                  "tiles of 2048", "ms_per_batch": ms, "records_per_s": n / (ms / 1e3),
+                      "status": int(part.status.item())}))
+
+
 def main():
     args = parse()
+    if args.hash:
+        hash_only(args)
+        return
     if args.impl == "reference":
         reference_arm(args)
         return

@@ -87,3 +87,17 @@ def test_per_particle_kernel_reproduces_the_published_1e8_histogram():
     assert len(vals) == 260 and int(counts.sum()) == 100_000_000
     assert hashlib.sha256(text.encode()).hexdigest() == (
         "21ab0aeb9ec72d380af2ce6e9631f8fa7b9111d24ff7831f272aa9f6a7be9dab")
+
+
+def test_flow_at_the_published_configuration_reproduces_the_published_histogram():
+    """The whole Flow (runner, partition kernels, functors) at the reference's published
+    configuration, N=1e8, C=8192, P=16384, Q=8, seed 42 (docs/benchmarks.md:24-34): the sorted
+    weight,count rows hash to the published SHA-256."""
+    import hashlib
+    w, capped, stats = capi.run_particle_feedback(42, 100_000_000, 64, chunk_capacity=8192, live_particles=16384,
+                                                  batch_chunks=8)
+    vals, counts = O.histogram_u32(w)
+    text = "".join(f"{int(v)},{int(c)}\n" for v, c in zip(vals, counts))
+    assert stats.sunk == 100_000_000 and len(vals) == 260
+    assert hashlib.sha256(text.encode()).hexdigest() == (
+        "21ab0aeb9ec72d380af2ce6e9631f8fa7b9111d24ff7831f272aa9f6a7be9dab")
