@@ -9,6 +9,8 @@
 //   SinkStage       flow/Execution.hpp:2776-...    consumes the batch
 #pragma once
 
+#include <algorithm>
+#include <cstring>
 #include <memory>
 #include <string>
 #include <unordered_map>
@@ -273,9 +275,21 @@ public:
             m_portChunks = cuda::Buffer<unsigned long long>(static_cast<std::size_t>(bins) * m_maxK);
             cuda::check(cudaMemset(m_portChunks.data(), 0, m_portChunks.size() * 8), "memset");
             gf_fused_scratch_bytes(m_tileCap, bins, &m_scratchBytes);
-            m_scratch = cuda::Buffer<unsigned char>(m_scratchBytes);
-            cuda::check(cudaMemset(m_scratch.data(), 0, m_scratchBytes), "memset");
-            m_totals = detail::Staged<std::uint32_t>(bins);
+            // one mirrored buffer per stage (u32 words): [numOut | totals | descs | tiles | reserved |
+            // status | pad | fused scratch (control block, descriptors)]. A batch uploads tiles through
+            // the control block's three reset words (zeroing status and those words; the persistent
+            // epoch after them is not touched) and downloads numOut through status: one copy each way.
+            m_oTotals = 1u;
+            m_oDescs = m_oTotals + bins;
+            m_oTiles = m_oDescs + 3u * (m_bound ? m_bound : 1u);
+            m_oReserved = m_oTiles + 3u * m_tileCap;
+            m_oStatus = m_oReserved + (m_bound ? m_bound : 1u);
+            m_oCtl = (m_oStatus + 1u + 15u) & ~15u; // 64-byte aligned control block
+            static_assert(sizeof(gf_tile) == 12 && sizeof(gf_out_desc) == 12, "packed layout");
+            static_assert(gf::kFusedCtlResetBytes == 12, "three reset words");
+            m_io = detail::Staged<std::uint32_t>(m_oCtl + (m_scratchBytes + 3u) / 4u);
+            cuda::check(cudaMemset(m_io.dev.data(), 0, m_io.dev.size() * 4u), "memset");
+            std::fill(m_io.host.data(), m_io.host.data() + m_io.host.size(), 0u);
         } else {
             m_binIds = cuda::Buffer<std::uint32_t>(st.slotCount());
         }
@@ -309,49 +323,49 @@ public:
                     throw BatchError("partition: tile descriptor capacity exceeded");
                 m_tiles.host[m_numTiles++] = gf_tile{c.handle.index, off, c.fill - off < kTile ? c.fill - off : kTile};
             }
-        m_tiles.upload(s, m_numTiles);
-        cuda::check(cudaMemsetAsync(m_status.dev.data(), 0, 4, s), "memset");
         const Acc acc{m_st.view()};
-        const Cls cls{m_cls, m_seed, m_purpose, m_status.dev.data()};
-        const Upd upd{m_upd, m_purpose + 1u, m_status.dev.data()};
         ++m_launches;
         if (m_fused) {
+            std::uint32_t* io = m_io.dev.data();
+            std::uint32_t* status = io + m_oStatus;
+            const Cls cls{m_cls, m_seed, m_purpose, status};
+            const Upd upd{m_upd, m_purpose + 1u, status};
             const std::uint32_t bound = checkedOutputChunkBound(m_n, m_C, m_bins);
+            std::memcpy(m_io.host.data() + m_oTiles, m_tiles.host.data(), sizeof(gf_tile) * m_numTiles);
             m_reserved.clear();
             for (std::uint32_t k = 0; k < bound; ++k) {
                 m_reserved.push_back(m_st.ledger().acquire());
-                m_table.host[k] = m_reserved.back().index;
+                m_io.host[m_oReserved + k] = m_reserved.back().index;
             }
-            m_reservedDev.upload(s, 0);
-            if (m_reservedBuf.size() < (bound ? bound : 1))
-                m_reservedBuf = cuda::Buffer<std::uint32_t>(m_bound ? m_bound : 1);
-            if (bound)
-                cuda::check(cudaMemcpyAsync(m_reservedBuf.data(), m_table.host.data(), bound * 4u,
-                                            cudaMemcpyHostToDevice, s),
-                            "H2D");
-            auto* ctl = reinterpret_cast<gf::FusedCtl*>(m_scratch.data());
+            m_io.host[m_oStatus] = 0u;
+            for (std::uint32_t i = 0; i < 3u; ++i)
+                m_io.host[m_oCtl + i] = 0u; // FusedCtl tile counter, allocation cursor, done
+            cuda::check(cudaMemcpyAsync(io + m_oTiles, m_io.host.data() + m_oTiles, 4u * (m_oCtl + 3u - m_oTiles),
+                                        cudaMemcpyHostToDevice, s),
+                        "H2D");
+            auto* ctl = reinterpret_cast<gf::FusedCtl*>(io + m_oCtl);
             auto* desc = reinterpret_cast<unsigned long long*>(ctl + 1);
-            cuda::check(cudaMemsetAsync(ctl, 0, gf::kFusedCtlResetBytes, s), "memset");
+            auto* tiles = reinterpret_cast<const gf_tile*>(io + m_oTiles);
             if (m_numTiles) {
                 gf::fused_partition_kernel<Shape, Acc, Cls, Upd><<<m_numTiles, Shape::kThreads, m_smemFused, s>>>(
-                    acc, cls, upd, m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(), m_tiles.dev.data(), m_numTiles,
-                    m_bins, m_reservedBuf.data(), bound, m_totals.dev.data(), m_portChunks.data(), m_maxK, ctl, desc,
-                    m_status.dev.data());
+                    acc, cls, upd, m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(), tiles, m_numTiles, m_bins,
+                    io + m_oReserved, bound, io + m_oTotals, m_portChunks.data(), m_maxK, ctl, desc, status);
                 cuda::check(cudaGetLastError(), "fused partition kernel launch");
             } else {
-                cuda::check(cudaMemsetAsync(m_totals.dev.data(), 0, 4u * m_bins, s), "memset");
+                cuda::check(cudaMemsetAsync(io + m_oTotals, 0, 4u * m_bins, s), "memset");
             }
             // the finish kernel of the C ABI builds the table and descriptors on the device
-            throw_on(gf_fused_finish(s, m_totals.dev.data(), m_portChunks.data(), m_bins, m_C, m_maxK, ctl,
-                                     m_table.dev.data(), reinterpret_cast<gf_out_desc*>(m_descs.dev.data()), m_bound,
-                                     m_numOut.dev.data(), m_status.dev.data()),
+            throw_on(gf_fused_finish(s, io + m_oTotals, m_portChunks.data(), m_bins, m_C, m_maxK, ctl,
+                                     m_table.dev.data(), reinterpret_cast<gf_out_desc*>(io + m_oDescs), m_bound,
+                                     io, status),
                      "fused partition finish");
-            m_status.download(s, 1);
-            m_numOut.download(s, 1);
-            m_descs.download(s, bound);
-            m_totals.download(s, m_bins);
+            cuda::check(cudaMemcpyAsync(m_io.host.data(), io, 4u * (m_oStatus + 1u), cudaMemcpyDeviceToHost, s),
+                        "D2H");
             return bound;
         }
+        m_tiles.upload(s, m_numTiles);
+        cuda::check(cudaMemsetAsync(m_status.dev.data(), 0, 4, s), "memset");
+        const Cls cls{m_cls, m_seed, m_purpose, m_status.dev.data()};
         cuda::check(cudaMemsetAsync(m_counts.dev.data(), 0, 4u * (m_bins + 1u), s), "memset");
         if (m_numTiles)
             gf::classify_kernel<Shape, Acc, Cls><<<m_numTiles, Shape::kThreads, 4u * m_bins, s>>>(
@@ -407,17 +421,19 @@ private:
 
     bool finishFused(const Batch&)
     {
-        detail::checkStatusWord(m_status.host[0], "fused partition");
-        const std::uint32_t r = m_numOut.host[0];
+        detail::checkStatusWord(m_io.host[m_oStatus], "fused partition");
+        const std::uint32_t r = m_io.host[0];
         std::uint64_t total = 0;
         for (std::uint32_t b = 0; b < m_bins; ++b)
-            total += m_totals.host[b];
+            total += m_io.host[m_oTotals + b];
         if (total != m_n)
             throw BatchError("fused partition: classified particle count does not match the batch");
         std::unordered_map<std::uint32_t, ChunkHandle> byIndex;
         for (const auto& h : m_reserved)
             byIndex.emplace(h.index, h);
-        const gf_out_desc* d = reinterpret_cast<const gf_out_desc*>(m_descs.host.data());
+        if (r > m_bound)
+            throw BatchError("fused partition: more output chunks than the reservation bound");
+        const gf_out_desc* d = reinterpret_cast<const gf_out_desc*>(m_io.host.data() + m_oDescs);
         for (std::uint32_t i = 0; i < r; ++i) {
             auto it = byIndex.find(d[i].chunk_index);
             if (it == byIndex.end())
@@ -497,12 +513,11 @@ private:
     std::uint32_t m_tileCap, m_bound;
     detail::Staged<gf_tile> m_tiles;
     detail::Staged<std::uint32_t> m_counts, m_next, m_table, m_status, m_numOut;
-    detail::Staged<std::uint32_t> m_totals;
     detail::Staged<gf_out_desc> m_descs;
-    detail::Staged<std::uint32_t> m_reservedDev;
-    cuda::Buffer<std::uint32_t> m_reservedBuf, m_binIds;
+    detail::Staged<std::uint32_t> m_io; // fused form: the packed per-batch buffer (layout in the constructor)
+    std::uint32_t m_oTotals = 0, m_oDescs = 0, m_oTiles = 0, m_oReserved = 0, m_oStatus = 0, m_oCtl = 0;
+    cuda::Buffer<std::uint32_t> m_binIds;
     cuda::Buffer<unsigned long long> m_portChunks;
-    cuda::Buffer<unsigned char> m_scratch;
     std::uint64_t m_scratchBytes = 0;
     std::uint32_t m_maxK = 1;
     std::size_t m_smemFused = 0, m_smemScatter = 0;
