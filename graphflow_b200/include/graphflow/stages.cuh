@@ -83,6 +83,28 @@ struct Staged {
     }
 };
 
+// A stage's device status word: zeroed once, written by a kernel only on a failure, so it is reset
+// before a launch only after a batch has reported one (a failure normally ends the run).
+struct StatusWord {
+    Staged<std::uint32_t> w{1};
+    bool dirty = false;
+    StatusWord() { cuda::check(cudaMemset(w.dev.data(), 0, 4), "memset"); }
+    std::uint32_t* dev() const { return w.dev.data(); }
+    void prepare(cudaStream_t s)
+    {
+        if (dirty)
+            cuda::check(cudaMemsetAsync(w.dev.data(), 0, 4, s), "memset");
+        dirty = false;
+    }
+    void download(cudaStream_t s) { w.download(s, 1); }
+    std::uint32_t read()
+    {
+        const std::uint32_t v = w.host[0];
+        dirty = dirty || v != 0u;
+        return v;
+    }
+};
+
 inline void checkStatusWord(std::uint32_t w, const char* stage)
 {
     if (w != 0u)
@@ -96,7 +118,7 @@ template <typename TStorage, typename TFunctor>
 class SourceStage final : public Stage {
 public:
     SourceStage(TStorage& st, const Config& c, TFunctor f, std::uint32_t purpose)
-        : m_st(st), m_f(std::move(f)), m_seed(gf::mix64(c.seed)), m_purpose(purpose), m_status(1)
+        : m_st(st), m_f(std::move(f)), m_seed(gf::mix64(c.seed)), m_purpose(purpose)
     {
     }
     std::uint32_t launch(cudaStream_t s, const Batch& b) override
@@ -104,20 +126,20 @@ public:
         if (b.chunks.size() != 1u)
             throw BatchError("source: a source batch is exactly one chunk");
         const auto& c = b.chunks[0];
-        cuda::check(cudaMemsetAsync(m_status.dev.data(), 0, 4, s), "memset");
+        m_status.prepare(s);
         const unsigned blocks = (c.fill + 255u) / 256u;
         if (blocks)
             source_kernel<<<blocks, 256, 0, s>>>(m_f, m_st.view(), m_seed, m_purpose, b.firstId,
-                                                  m_st.base(c.handle), c.fill, m_status.dev.data());
+                                                  m_st.base(c.handle), c.fill, m_status.dev());
         cuda::check(cudaGetLastError(), "source launch");
-        m_status.download(s, 1);
+        m_status.download(s);
         ++m_launches;
         return 0u;
     }
     bool advance(cudaStream_t, const Batch&, std::uint32_t& allocated) override
     {
         allocated = 0u;
-        detail::checkStatusWord(m_status.host[0], "source");
+        detail::checkStatusWord(m_status.read(), "source");
         return false;
     }
     void finish(const Batch& b, std::vector<ChunkDescriptor>& outputs) override
@@ -131,7 +153,7 @@ private:
     TFunctor m_f;
     std::uint64_t m_seed;
     std::uint32_t m_purpose;
-    detail::Staged<std::uint32_t> m_status;
+    detail::StatusWord m_status;
 };
 
 template <typename TStorage, typename TFunctor>
@@ -139,14 +161,15 @@ class TransformStage final : public Stage {
 public:
     TransformStage(TStorage& st, const Config& c, TFunctor f, std::uint32_t purpose)
         : m_st(st), m_f(std::move(f)), m_seed(gf::mix64(c.seed)), m_purpose(purpose), m_tile(1024u),
-          m_tiles(static_cast<std::size_t>(c.batchChunks) * ((c.chunkCapacity + 1023u) / 1024u)),
-          m_out(c.batchChunks), m_status(1)
+          m_tileCap(static_cast<std::uint32_t>(c.batchChunks) * ((c.chunkCapacity + 1023u) / 1024u)),
+          m_io(4u * m_tileCap + c.batchChunks) // [tiles (4 words each) | output chunk indices]
     {
+        static_assert(sizeof(MoveTile) == 16, "packed layout");
     }
     std::uint32_t launch(cudaStream_t s, const Batch& b) override
     {
         const auto tiles = detail::moveTiles(b, m_tile);
-        if (tiles.size() > m_tiles.host.size())
+        if (tiles.size() > m_tileCap)
             throw BatchError("transform: tile capacity exceeded");
         const std::uint64_t n = b.particles();
         const std::uint32_t C = m_st.chunkCapacity();
@@ -154,29 +177,32 @@ public:
         m_pending.clear();
         for (std::uint32_t k = 0; k < r; ++k) {
             const ChunkHandle h = m_st.ledger().acquire();
-            m_out.host[k] = h.index;
+            m_io.host[4u * m_tileCap + k] = h.index;
             const std::uint64_t left = n - static_cast<std::uint64_t>(k) * C;
             m_pending.push_back(ChunkDescriptor{h, static_cast<std::uint32_t>(left < C ? left : C), 0u});
         }
-        std::copy(tiles.begin(), tiles.end(), m_tiles.host.data());
-        m_tiles.upload(s, tiles.size());
-        m_out.upload(s, r);
-        cuda::check(cudaMemsetAsync(m_status.dev.data(), 0, 4, s), "memset");
+        if (!tiles.empty())
+            std::memcpy(m_io.host.data(), tiles.data(), sizeof(MoveTile) * tiles.size());
+        // one upload: the whole tile region and the output chunk indices after it
+        m_io.upload(s, 4u * m_tileCap + r);
+        m_status.prepare(s);
+        auto* dtiles = reinterpret_cast<const MoveTile*>(m_io.dev.data());
         if (!tiles.empty())
             transform_kernel<<<static_cast<unsigned>(tiles.size()), 256, 0, s>>>(
-                m_f, m_st.view(), m_seed, m_purpose, m_tiles.dev.data(), static_cast<std::uint32_t>(tiles.size()),
-                m_out.dev.data(), r, C, gf::FastDiv(C), m_st.slotCount(), m_status.dev.data());
+                m_f, m_st.view(), m_seed, m_purpose, dtiles, static_cast<std::uint32_t>(tiles.size()),
+                m_io.dev.data() + 4u * m_tileCap, r, C, gf::FastDiv(C), m_st.slotCount(), m_status.dev());
         cuda::check(cudaGetLastError(), "transform launch");
-        m_status.download(s, 1);
+        m_status.download(s);
         ++m_launches;
         return r;
     }
     bool advance(cudaStream_t, const Batch&, std::uint32_t& allocated) override
     {
         allocated = 0u;
-        if (m_status.host[0] != 0u) {
+        const std::uint32_t st = m_status.read();
+        if (st != 0u) {
             abort();
-            detail::checkStatusWord(m_status.host[0], "transform");
+            detail::checkStatusWord(st, "transform");
         }
         return false;
     }
@@ -196,9 +222,9 @@ private:
     TStorage& m_st;
     TFunctor m_f;
     std::uint64_t m_seed;
-    std::uint32_t m_purpose, m_tile;
-    detail::Staged<MoveTile> m_tiles;
-    detail::Staged<std::uint32_t> m_out, m_status;
+    std::uint32_t m_purpose, m_tile, m_tileCap;
+    detail::Staged<std::uint32_t> m_io;
+    detail::StatusWord m_status;
     std::vector<ChunkDescriptor> m_pending;
 };
 
@@ -207,7 +233,7 @@ class SinkStage final : public Stage {
 public:
     SinkStage(TStorage& st, const Config& c, TFunctor f, std::uint32_t purpose)
         : m_st(st), m_f(std::move(f)), m_seed(gf::mix64(c.seed)), m_purpose(purpose),
-          m_tiles(static_cast<std::size_t>(c.batchChunks) * ((c.chunkCapacity + 1023u) / 1024u)), m_status(1)
+          m_tiles(static_cast<std::size_t>(c.batchChunks) * ((c.chunkCapacity + 1023u) / 1024u))
     {
     }
     std::uint32_t launch(cudaStream_t s, const Batch& b) override
@@ -217,20 +243,20 @@ public:
             throw BatchError("sink: tile capacity exceeded");
         std::copy(tiles.begin(), tiles.end(), m_tiles.host.data());
         m_tiles.upload(s, tiles.size());
-        cuda::check(cudaMemsetAsync(m_status.dev.data(), 0, 4, s), "memset");
+        m_status.prepare(s);
         if (!tiles.empty())
             sink_kernel<<<static_cast<unsigned>(tiles.size()), 256, 0, s>>>(
                 m_f, m_st.view(), m_seed, m_purpose, m_tiles.dev.data(), static_cast<std::uint32_t>(tiles.size()),
-                m_st.chunkCapacity(), m_st.slotCount(), m_status.dev.data());
+                m_st.chunkCapacity(), m_st.slotCount(), m_status.dev());
         cuda::check(cudaGetLastError(), "sink launch");
-        m_status.download(s, 1);
+        m_status.download(s);
         ++m_launches;
         return 0u;
     }
     bool advance(cudaStream_t, const Batch&, std::uint32_t& allocated) override
     {
         allocated = 0u;
-        detail::checkStatusWord(m_status.host[0], "sink");
+        detail::checkStatusWord(m_status.read(), "sink");
         return false;
     }
     void finish(const Batch&, std::vector<ChunkDescriptor>&) override {}
@@ -242,7 +268,7 @@ private:
     std::uint64_t m_seed;
     std::uint32_t m_purpose;
     detail::Staged<MoveTile> m_tiles;
-    detail::Staged<std::uint32_t> m_status;
+    detail::StatusWord m_status;
 };
 
 // Dense partition stage. Plain form: classify -> (host) plan -> scatter -> finalise, two device
