@@ -454,21 +454,36 @@ private:
             total += m_io.host[m_oTotals + b];
         if (total != m_n)
             throw BatchError("fused partition: classified particle count does not match the batch");
-        std::unordered_map<std::uint32_t, ChunkHandle> byIndex;
-        for (const auto& h : m_reserved)
-            byIndex.emplace(h.index, h);
+        // reservation slot of every reserved chunk index (a flat table over the pool, cleared after use)
+        if (m_slotOf.size() != m_st.ledger().numChunks())
+            m_slotOf.assign(m_st.ledger().numChunks(), -1);
+        for (std::size_t k = 0; k < m_reserved.size(); ++k)
+            m_slotOf[m_reserved[k].index] = static_cast<std::int32_t>(k);
+        struct Clear { // on every exit: the table is all -1 again
+            std::vector<std::int32_t>& t;
+            const std::vector<ChunkHandle>& r;
+            ~Clear()
+            {
+                for (const auto& h : r)
+                    t[h.index] = -1;
+            }
+        } clear{m_slotOf, m_reservedCopy};
+        m_reservedCopy = m_reserved;
         if (r > m_bound)
             throw BatchError("fused partition: more output chunks than the reservation bound");
         const gf_out_desc* d = reinterpret_cast<const gf_out_desc*>(m_io.host.data() + m_oDescs);
+        std::vector<bool>& used = m_usedSlot;
+        used.assign(m_reserved.size(), false);
         for (std::uint32_t i = 0; i < r; ++i) {
-            auto it = byIndex.find(d[i].chunk_index);
-            if (it == byIndex.end())
+            const std::int32_t k = d[i].chunk_index < m_slotOf.size() ? m_slotOf[d[i].chunk_index] : -1;
+            if (k < 0 || used[static_cast<std::size_t>(k)])
                 throw BatchError("fused partition: output chunk outside the reservation");
-            m_pending.push_back(ChunkDescriptor{it->second, d[i].fill, d[i].bin});
-            byIndex.erase(it);
+            used[static_cast<std::size_t>(k)] = true;
+            m_pending.push_back(ChunkDescriptor{m_reserved[static_cast<std::size_t>(k)], d[i].fill, d[i].bin});
         }
-        for (auto& kv : byIndex)
-            m_st.ledger().release(kv.second);
+        for (std::size_t k = 0; k < m_reserved.size(); ++k)
+            if (!used[k])
+                m_st.ledger().release(m_reserved[k]);
         m_reserved.clear();
         return false;
     }
@@ -550,7 +565,9 @@ private:
     std::uint32_t m_stage = 0, m_numTiles = 0;
     std::uint64_t m_n = 0;
     std::vector<ChunkDescriptor> m_pending;
-    std::vector<ChunkHandle> m_reserved;
+    std::vector<ChunkHandle> m_reserved, m_reservedCopy;
+    std::vector<std::int32_t> m_slotOf; // fused form: reservation slot by chunk index, -1 elsewhere
+    std::vector<bool> m_usedSlot;
     std::vector<std::uint32_t> m_totals0;
     bool m_failed = false;
 };
