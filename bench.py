@@ -33,7 +33,7 @@ BYTES_PER_PARTICLE = 8  # read the 4-byte key once, write it once (algorithmic)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per key of one launch of the
 # cooperative kernel, from an ncu capture of the 5e7-key case with B = 64 uniform keys (traffic
 # grows in proportion to the keys, so it scales to a full launch); None for other workloads.
-MEASURED_TRAFFIC_PER_KEY = {(64, "uniform"): 10.15}
+MEASURED_TRAFFIC_PER_KEY = {(64, "uniform"): 10.11}
 
 
 def parse():
