@@ -265,7 +265,7 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
         KeyClassify<Acc> cls{key_classifier(classifier, bins)};
         kernel<<<n_tiles, Shape::kThreads, smem, as_stream(stream)>>>(
             acc, cls, NoUpdate{}, 0u, capacity, FastDiv(capacity), pool_slots, d_tiles, n_tiles, bins, d_reserved,
-            n_reserved, d_totals, d_port_chunks, max_chunks_per_port, ctl, desc, d_status);
+            n_reserved, d_totals, d_port_chunks, max_chunks_per_port, ctl, desc, d_status, InlineFinish{});
         return cuda_status(cudaGetLastError());
     });
 }

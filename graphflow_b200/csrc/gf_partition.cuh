@@ -492,16 +492,67 @@ GF_D void block_lookback(const unsigned long long* desc, uint32_t t, uint32_t B,
     }
 }
 
-// Called once per CTA by thread 0's block after its last global access: the last CTA of the
-// launch publishes the launch epoch as completed.
-GF_D void fused_retire(FusedCtl* ctl, uint32_t epoch)
+// Optional in-kernel finish of a fused launch: when `table` is set, the last CTA of the launch
+// builds the chunk table, the output descriptors and the output count itself (what
+// fused_finish_kernel does), so a caller that would launch the finish right after saves a launch.
+struct InlineFinish {
+    uint32_t* table = nullptr;
+    gf_out_desc* descs = nullptr;
+    uint32_t desc_cap = 0u;
+    uint32_t* num_out = nullptr;
+};
+
+// Device form of planDenseBins + buildDenseTable + the output-descriptor loop
+// (DenseBinTable.hpp:39-91, Execution.hpp:2558-2581) for a fused launch, by one CTA of THREADS
+// threads: bins in segments of `seg` (nck and base hold `seg` words each, tmp THREADS / 32 + 1),
+// one thread per output chunk of a segment. Totals and chunk claims are read from L2, so the last
+// CTA of the fused launch itself can run it after the launch's other CTAs retired.
+template <int THREADS>
+GF_D void finish_plan(const uint32_t* totals, const unsigned long long* port_chunks, uint32_t B, uint32_t capacity,
+                      FastDiv fdc, uint32_t max_k, uint32_t epoch, uint32_t* table, gf_out_desc* descs,
+                      uint32_t desc_cap, uint32_t* num_out, uint32_t* status, uint32_t* nck, uint32_t* base,
+                      uint32_t seg_words, uint32_t* tmp)
 {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        if (atomicAdd(&ctl->done, 1u) + 1u == gridDim.x)
-            atomicExch(&ctl->epoch, epoch);
+    uint32_t carry = 0;
+    for (uint32_t seg = 0; seg < B; seg += seg_words) {
+        const uint32_t n = min(seg_words, B - seg);
+        for (uint32_t i = threadIdx.x; i < n; i += THREADS) {
+            const uint32_t tot = ld_relaxed_u32(totals + seg + i);
+            nck[i] = fdc.div(tot) + (fdc.mod(tot) != 0u ? 1u : 0u);
+        }
+        __syncthreads();
+        const uint32_t sum = block_exclusive_scan<THREADS>(nck, base, n, tmp);
+        for (uint32_t i = threadIdx.x; i < n; i += THREADS)
+            table[seg + i] = carry + base[i];
+        // one thread per output chunk of the segment (a port may own most of them)
+        for (uint32_t g = threadIdx.x; g < sum; g += THREADS) {
+            uint32_t lo = 0, hi = n - 1u; // the last port of the segment whose chunks start at or before g
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1u) >> 1;
+                if (base[mid] <= g)
+                    lo = mid;
+                else
+                    hi = mid - 1u;
+            }
+            const uint32_t b = seg + lo, k = g - base[lo], f = carry + g;
+            if (f >= desc_cap || k >= max_k) {
+                set_status(status, GF_OVERFLOW);
+                continue;
+            }
+            const unsigned long long v = ld_relaxed_u64(port_chunks + (size_t)b * max_k + k);
+            const uint32_t chunk = (uint32_t)(v >> 32) == epoch ? (uint32_t)v : kNoChunk;
+            if (chunk == kNoChunk)
+                set_status(status, GF_INVALID);
+            table[B + f] = chunk;
+            descs[f].chunk_index = chunk;
+            descs[f].fill = min(capacity, ld_relaxed_u32(totals + b) - k * capacity);
+            descs[f].bin = b;
+        }
+        carry += sum;
+        __syncthreads();
     }
+    if (threadIdx.x == 0)
+        *num_out = carry;
 }
 
 template <typename Shape, typename Access, typename Classify, typename Update>
@@ -509,7 +560,7 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
     Access acc, Classify classify, Update update, uint64_t seed_mixed, uint32_t capacity, FastDiv fdc,
     uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B, const uint32_t* reserved,
     uint32_t n_reserved, uint32_t* totals, unsigned long long* port_chunks, uint32_t max_k, FusedCtl* ctl,
-    unsigned long long* desc, uint32_t* status)
+    unsigned long long* desc, uint32_t* status, InlineFinish fin)
 {
     using P = typename Access::Payload;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -538,8 +589,30 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
     const uint32_t t = s_tile[0];
     const uint32_t epoch = s_tile[1];
     const uint32_t epoch_hi = epoch;
+    // retire this CTA; with an inline finish, the last CTA then builds the table and descriptors
+    // (its stage area and look-back words are free by then)
+    auto retire = [&]() {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            const bool last = atomicAdd(&ctl->done, 1u) + 1u == gridDim.x;
+            if (last)
+                atomicExch(&ctl->epoch, epoch);
+            s_tile[2] = last ? 1u : 0u;
+        }
+        if (fin.table == nullptr)
+            return;
+        __syncthreads();
+        if (s_tile[2] == 0u)
+            return;
+        __threadfence(); // every other CTA's totals and chunk claims were published before its arrival
+        constexpr uint32_t kSeg = (uint32_t)(sizeof(P) * Shape::kTile / 8u);
+        uint32_t* scratch = reinterpret_cast<uint32_t*>(smem_raw);
+        finish_plan<Shape::kThreads>(totals, port_chunks, B, capacity, fdc, max_k, epoch, fin.table, fin.descs,
+                                     fin.desc_cap, fin.num_out, status, scratch, scratch + kSeg, kSeg, lb_flag);
+    };
     if (t >= n_tiles) {
-        fused_retire(ctl, epoch);
+        retire();
         return;
     }
 
@@ -634,7 +707,7 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
         s_tile[2] = ld_relaxed_u32(status);
     __syncthreads();
     if (s_tile[2] != 0u) {
-        fused_retire(ctl, epoch); // the batch failed somewhere: write nothing, the host discards it
+        retire(); // the batch failed somewhere: write nothing, the host discards it
         return;
     }
 
@@ -652,7 +725,7 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
         else
             set_status(status, GF_OVERFLOW);
     }
-    fused_retire(ctl, epoch);
+    retire();
 }
 
 // Device form of planDenseBins + buildDenseTable + the output-descriptor loop
@@ -665,50 +738,11 @@ __global__ void __launch_bounds__(THREADS) fused_finish_kernel(const uint32_t* t
                                                                uint32_t desc_cap, uint32_t* num_out, uint32_t* status)
 {
     extern __shared__ uint32_t smem[];
-    const uint32_t epoch = ctl->epoch;
-    uint32_t* nck = smem;      // [seg]
-    uint32_t* base = nck + 4096; // [seg]
+    uint32_t* nck = smem;         // [4096]
+    uint32_t* base = nck + 4096;  // [4096]
     uint32_t* tmp = base + 4096;  // [W+1]
-    uint32_t carry = 0;
-    for (uint32_t seg = 0; seg < B; seg += 4096) {
-        const uint32_t n = min(4096u, B - seg);
-        for (uint32_t i = threadIdx.x; i < n; i += THREADS) {
-            const uint32_t tot = totals[seg + i];
-            nck[i] = fdc.div(tot) + (fdc.mod(tot) != 0u ? 1u : 0u);
-        }
-        __syncthreads();
-        const uint32_t sum = block_exclusive_scan<THREADS>(nck, base, n, tmp);
-        for (uint32_t i = threadIdx.x; i < n; i += THREADS)
-            table[seg + i] = carry + base[i];
-        // one thread per output chunk of the segment (a port may own most of them)
-        for (uint32_t g = threadIdx.x; g < sum; g += THREADS) {
-            uint32_t lo = 0, hi = n - 1u; // the last port of the segment whose chunks start at or before g
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1u) >> 1;
-                if (base[mid] <= g)
-                    lo = mid;
-                else
-                    hi = mid - 1u;
-            }
-            const uint32_t b = seg + lo, k = g - base[lo], f = carry + g;
-            if (f >= desc_cap || k >= max_k) {
-                set_status(status, GF_OVERFLOW);
-                continue;
-            }
-            const unsigned long long v = port_chunks[(size_t)b * max_k + k];
-            const uint32_t chunk = (uint32_t)(v >> 32) == epoch ? (uint32_t)v : kNoChunk;
-            if (chunk == kNoChunk)
-                set_status(status, GF_INVALID);
-            table[B + f] = chunk;
-            descs[f].chunk_index = chunk;
-            descs[f].fill = min(capacity, totals[b] - k * capacity);
-            descs[f].bin = b;
-        }
-        carry += sum;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-        *num_out = carry;
+    finish_plan<THREADS>(totals, port_chunks, B, capacity, fdc, max_k, ctl->epoch, table, descs, desc_cap, num_out,
+                         status, nck, base, 4096u, tmp);
 }
 
 // Synthetic key source (uniform / Zipf / one port / round robin) at stream positions

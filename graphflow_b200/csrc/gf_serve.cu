@@ -261,16 +261,18 @@ void enqueueChain(cudaStream_t s, char* base, const ChainLayout& L, std::uint32_
                                                                         numOut, tiles);
         if (nTiles != 0u) {
             cuda::check(cudaMemsetAsync(ctl, 0, gf::kFusedCtlResetBytes, s), "memset");
+            // the last CTA builds this node's table and descriptors (no separate finish launch)
             kernel<<<nTiles, ChainShape::kThreads, smem, s>>>(
                 acc_cols, ShiftPort{8u * node, gf::FastDiv(bins)}, gf::NoUpdate{}, 0u, kChainCapacity, fdc, L.slots,
                 tiles, nTiles, bins, reserved + node * L.bound, static_cast<std::uint32_t>(L.bound), totals,
-                portChunks, static_cast<std::uint32_t>(L.maxK), ctl, desc, status);
+                portChunks, static_cast<std::uint32_t>(L.maxK), ctl, desc, status,
+                gf::InlineFinish{table, descs, static_cast<std::uint32_t>(L.bound), numOut});
         } else {
             cuda::check(cudaMemsetAsync(totals, 0, bins * 4u, s), "memset");
+            gf::fused_finish_kernel<FT><<<1, FT, fsmem, s>>>(totals, portChunks, bins, kChainCapacity, fdc,
+                                                              static_cast<std::uint32_t>(L.maxK), ctl, table, descs,
+                                                              static_cast<std::uint32_t>(L.bound), numOut, status);
         }
-        gf::fused_finish_kernel<FT><<<1, FT, fsmem, s>>>(totals, portChunks, bins, kChainCapacity, fdc,
-                                                          static_cast<std::uint32_t>(L.maxK), ctl, table, descs,
-                                                          static_cast<std::uint32_t>(L.bound), numOut, status);
     }
     chain_sink_kernel<<<static_cast<unsigned>(std::min<std::uint64_t>(std::max<std::uint64_t>(L.bound, 1u), 4096u)),
                         256, 0, s>>>(descs, numOut, id, portOf, L.n);

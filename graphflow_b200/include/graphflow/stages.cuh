@@ -372,19 +372,21 @@ public:
             auto* ctl = reinterpret_cast<gf::FusedCtl*>(io + m_oCtl);
             auto* desc = reinterpret_cast<unsigned long long*>(ctl + 1);
             auto* tiles = reinterpret_cast<const gf_tile*>(io + m_oTiles);
+            auto* descs = reinterpret_cast<gf_out_desc*>(io + m_oDescs);
             if (m_numTiles) {
+                // the launch's last CTA builds the table and descriptors (no separate finish launch)
                 gf::fused_partition_kernel<Shape, Acc, Cls, Upd><<<m_numTiles, Shape::kThreads, m_smemFused, s>>>(
                     acc, cls, upd, m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(), tiles, m_numTiles, m_bins,
-                    io + m_oReserved, bound, io + m_oTotals, m_portChunks.data(), m_maxK, ctl, desc, status);
+                    io + m_oReserved, bound, io + m_oTotals, m_portChunks.data(), m_maxK, ctl, desc, status,
+                    gf::InlineFinish{m_table.dev.data(), descs, m_bound, io});
                 cuda::check(cudaGetLastError(), "fused partition kernel launch");
             } else {
                 cuda::check(cudaMemsetAsync(io + m_oTotals, 0, 4u * m_bins, s), "memset");
+                // the finish kernel of the C ABI builds the (empty) table and descriptors
+                throw_on(gf_fused_finish(s, io + m_oTotals, m_portChunks.data(), m_bins, m_C, m_maxK, ctl,
+                                         m_table.dev.data(), descs, m_bound, io, status),
+                         "fused partition finish");
             }
-            // the finish kernel of the C ABI builds the table and descriptors on the device
-            throw_on(gf_fused_finish(s, io + m_oTotals, m_portChunks.data(), m_bins, m_C, m_maxK, ctl,
-                                     m_table.dev.data(), reinterpret_cast<gf_out_desc*>(io + m_oDescs), m_bound,
-                                     io, status),
-                     "fused partition finish");
             cuda::check(cudaMemcpyAsync(m_io.host.data(), io, 4u * (m_oStatus + 1u), cudaMemcpyDeviceToHost, s),
                         "D2H");
             return bound;
