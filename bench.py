@@ -6,7 +6,8 @@ N = 1e8 u32 keys into pooled output chunks (C = 8192), one whole-array batch per
           partitions its own 1e8 keys; the path has no exchange step, so no collective).
   plain   the reference's two-launch form (classify, host plan, scatter) on the same data.
   e2e     the same step through the C ABI from pinned host buffers: H2D of the keys, fused
-          partition, D2H of the output chunks and descriptors, inside the timed region.
+          partition, D2H of the output chunks and descriptors, every step inside the timed
+          region; a step's upload overlaps the previous step's download (full-duplex link).
 
 ``--impl reference`` times the reference algorithm's CPU restatement (the oracle's pool path:
 per-tile histogram -> plan -> scatter, OpenMP over all host threads) on the same workload.
@@ -410,26 +411,42 @@ def gpu_arm(args):
     host_small = torch.empty(2, dtype=torch.int32, pin_memory=True)
     out_view = bench.pool.column[bench.n_in * CAPACITY: bench.n_in * CAPACITY + out_slots]
 
-    def e2e_step():
-        bench.pool.column[: args.n].copy_(host_keys, non_blocking=True)
-        bench.fused_step(stream)
-        host_out.copy_(out_view, non_blocking=True)
-        host_descs.copy_(bench.fused.descs, non_blocking=True)
-        host_small[0:1].copy_(bench.fused.num_out, non_blocking=True)
-        host_small[1:2].copy_(bench.fused.status, non_blocking=True)
+    # Every step uploads its keys, runs the fused step and reads back its output, descriptors and
+    # status. Consecutive steps overlap on the full-duplex host link: step k+1's upload (copy
+    # stream) waits only for step k's kernel, which has finished reading the input chunks, and runs
+    # while step k's download (compute stream) drains the output chunks; step k+1's kernel waits
+    # for its upload and, in stream order, for step k's download.
+    copy_stream = torch.cuda.Stream(device=dev)
 
-    with torch.cuda.stream(stream):
-        for _ in range(2):
-            e2e_step()
-        stream.synchronize()
-        e_reps = max(3, min(args.steps // 4, 50))
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(e_reps):
-            e2e_step()
-        e1.record(stream)
-        stream.synchronize()
+    def e2e_steps(count, start):
+        prev = start
+        for _ in range(count):
+            copy_stream.wait_event(prev)
+            with torch.cuda.stream(copy_stream):
+                bench.pool.column[: args.n].copy_(host_keys, non_blocking=True)
+                up = torch.cuda.Event()
+                up.record(copy_stream)
+            stream.wait_event(up)
+            with torch.cuda.stream(stream):
+                bench.fused_step(stream)
+                prev = torch.cuda.Event()
+                prev.record(stream)
+                host_out.copy_(out_view, non_blocking=True)
+                host_descs.copy_(bench.fused.descs, non_blocking=True)
+                host_small[0:1].copy_(bench.fused.num_out, non_blocking=True)
+                host_small[1:2].copy_(bench.fused.status, non_blocking=True)
+
+    warm = torch.cuda.Event()
+    warm.record(stream)
+    e2e_steps(2, warm)
+    stream.synchronize()
+    e_reps = max(3, min(args.steps // 4, 50))
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    e2e_steps(e_reps, e0)
+    e1.record(stream)
+    stream.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e_reps)
     correct &= int(host_small[1].item()) == 0
 
