@@ -105,7 +105,13 @@ uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap);
  *   "runner_batched" 1 (default) = the flow entry points (gf_run_particle_feedback,
  *                gf_run_dense_chain, gf_run_photon) let a sink take up to Q ready chunks per launch
  *                and dispatch every idle node in one scheduler iteration; 0 = the reference
- *                runner's one-chunk sinks and one dispatch per iteration. Results are identical. */
+ *                runner's one-chunk sinks and one dispatch per iteration. Results are identical.
+ *   "hash_persistent" 1 (default) = gf_classify_hash_r16 and gf_scatter_hash_r16 use the
+ *                persistent kernels (one shared-memory counter per port and CTA for the count;
+ *                the scatter groups each tile's records of ports below 2048 by port and places
+ *                rarer ports one record at a time); 0 = the per-tile open-addressing table
+ *                kernels (graph/BinTable.hpp design). Counts, the plan and every port's record
+ *                multiset are identical; the order inside a port is arrival order either way. */
 gf_status gf_set_tuning(const char* name, int value);
 
 /* ---- dense partition: the reference's two-launch form --------------------------------------- */
