@@ -119,33 +119,43 @@ static __global__ void __launch_bounds__(256)
     const UpdateWeight upd[2] = {UpdateWeight{1000u}, UpdateWeight{1u}};
     const RecordWeight sink{weights};
     const RecordCapped cappedSink{weights, capped};
-    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<std::uint64_t>(gridDim.x) * blockDim.x) {
-        const std::uint64_t id = firstId + i;
-        Status st(status);
+    Status st(status);
+    const Acc acc{};
+    const std::uint64_t stride = static_cast<std::uint64_t>(gridDim.x) * blockDim.x;
+    std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    auto generate = [&](std::uint64_t k) {
+        const std::uint64_t id = firstId + k;
         rng::Engine e0 = rng::makeEngine(seedMixed, id, 0u, rng::streamPurposeForNode(0u));
-        Particle p = invokeWithContext(gen, e0, st, id);
-        for (;;) {
-            rng::Engine ef = rng::engineFor(seedMixed, p, rng::streamPurposeForNode(1u));
-            const std::uint32_t side = static_cast<std::uint32_t>(invokeWithContext(filter, ef, st, p));
-            const std::uint32_t node = 2u + side; // A for bin 0, B for bin 1
-            rng::Engine es = rng::engineFor(seedMixed, p, rng::streamPurposeForNode(node));
-            const Outcome out = invokeWithContext(select, es, st, p);
-            rng::Engine eu = rng::engineFor(seedMixed, p, rng::streamPurposeForNode(node, 1u));
-            const std::uint32_t res = updateCode(invokeWithContext(upd[side], eu, st, out, p));
-            if (res != 0u) {
-                gf::set_status(status, res == 1u ? GF_OVERFLOW : GF_INVALID);
+        return invokeWithContext(gen, e0, st, id);
+    };
+    if (i >= n)
+        return;
+    Particle p = generate(i);
+    // One visit per iteration; a lane whose particle ends starts its next particle at once, so a
+    // warp stays full instead of waiting for its longest walk. Every particle's draws are keyed
+    // by its own id and visit counter, so results do not depend on the order.
+    for (;;) {
+        rng::Engine ef = rng::engineFor(seedMixed, p, rng::streamPurposeForNode(1u));
+        const std::uint32_t side = static_cast<std::uint32_t>(invokeWithContext(filter, ef, st, p));
+        const std::uint32_t node = 2u + side; // A for bin 0, B for bin 1
+        rng::Engine es = rng::engineFor(seedMixed, p, rng::streamPurposeForNode(node));
+        const Outcome out = invokeWithContext(select, es, st, p);
+        rng::Engine eu = rng::engineFor(seedMixed, p, rng::streamPurposeForNode(node, 1u));
+        const std::uint32_t res = updateCode(invokeWithContext(upd[side], eu, st, out, p));
+        bool done = true;
+        if (res != 0u)
+            gf::set_status(status, res == 1u ? GF_OVERFLOW : GF_INVALID);
+        else if (out == Outcome::sink)
+            sink(acc, p);
+        else if (out == Outcome::capped)
+            cappedSink(acc, p);
+        else
+            done = false;
+        if (done) {
+            i += stride;
+            if (i >= n)
                 break;
-            }
-            const Acc acc{};
-            if (out == Outcome::sink) {
-                sink(acc, p);
-                break;
-            }
-            if (out == Outcome::capped) {
-                cappedSink(acc, p);
-                break;
-            }
+            p = generate(i);
         }
     }
 }

@@ -330,23 +330,37 @@ __global__ void __launch_bounds__(256) transport_kernel(TPropose propose, Advanc
                                                         std::uint64_t firstId, std::uint64_t n, std::uint32_t* status)
 {
     const Acc acc{};
-    for (std::uint64_t i = (std::uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (std::uint64_t)gridDim.x * blockDim.x) {
-        Status st(status);
-        PhotonT<T> p = GeneratePhotonT<T>{}(acc, firstId + i);
-        for (std::uint32_t guard = 0; guard <= 0x10000u; ++guard) {
-            rng::Engine ef = rng::engineFor(seedMixed, p, rng::streamPurposeForNode(1));
-            propose(acc, ef, st, p);
-            if (advance(acc, p.proposal.event, p) != UpdateResult::success) {
-                st.set(StatusCode::invalid);
-                break;
-            }
-            if (p.proposal.event != Event::scatter) {
-                terminal(acc, st, p);
-                break;
-            }
+    Status st(status);
+    const std::uint64_t stride = (std::uint64_t)gridDim.x * blockDim.x;
+    std::uint64_t i = (std::uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    PhotonT<T> p = GeneratePhotonT<T>{}(acc, firstId + i);
+    std::uint32_t scatters = 0;
+    // One event per iteration; a lane whose photon ends (or reaches 0x10001 scatters) starts its
+    // next photon at once, so a warp stays full instead of waiting for its longest walk. Every
+    // photon's draws are keyed by its own id and counters, so results do not depend on the order.
+    for (;;) {
+        rng::Engine ef = rng::engineFor(seedMixed, p, rng::streamPurposeForNode(1));
+        propose(acc, ef, st, p);
+        bool done;
+        if (advance(acc, p.proposal.event, p) != UpdateResult::success) {
+            st.set(StatusCode::invalid);
+            done = true;
+        } else if (p.proposal.event != Event::scatter) {
+            terminal(acc, st, p);
+            done = true;
+        } else {
             rng::Engine es = rng::engineFor(seedMixed, p, rng::streamPurposeForNode(3));
             scatter(acc, es, st, p);
+            done = ++scatters > 0x10000u;
+        }
+        if (done) {
+            i += stride;
+            if (i >= n)
+                break;
+            p = GeneratePhotonT<T>{}(acc, firstId + i);
+            scatters = 0;
         }
     }
 }
