@@ -321,13 +321,11 @@ struct RecordTerminalT {
     }
 };
 
-// Fused transport: one thread carries one photon through propose -> advance -> scatter until a
-// terminal event, calling the very functors the graph runs at the same stream positions, so a
-// history is identical to the one the Flow produces.
+// The walks of one thread's photons (grid-stride over [0, n)).
 template <typename T, typename TPropose, typename TScatter>
-__global__ void __launch_bounds__(256) transport_kernel(TPropose propose, AdvanceToEventT<T> advance, TScatter scatter,
-                                                        RecordTerminalT<T> terminal, std::uint64_t seedMixed,
-                                                        std::uint64_t firstId, std::uint64_t n, std::uint32_t* status)
+__device__ void transport_walks(const TPropose& propose, const AdvanceToEventT<T>& advance, const TScatter& scatter,
+                                const RecordTerminalT<T>& terminal, std::uint64_t seedMixed, std::uint64_t firstId,
+                                std::uint64_t n, std::uint32_t* status)
 {
     const Acc acc{};
     Status st(status);
@@ -363,6 +361,48 @@ __global__ void __launch_bounds__(256) transport_kernel(TPropose propose, Advanc
             scatters = 0;
         }
     }
+}
+
+// Fused transport: a thread carries photons through propose -> advance -> scatter until their
+// terminal events (transport_walks), calling the very functors the graph runs at the same stream
+// positions, so a history is identical to the one the Flow produces.
+template <typename T, typename TPropose, typename TScatter>
+__global__ void __launch_bounds__(256) transport_kernel(TPropose propose, AdvanceToEventT<T> advance, TScatter scatter,
+                                                        RecordTerminalT<T> terminal, std::uint64_t seedMixed,
+                                                        std::uint64_t firstId, std::uint64_t n, std::uint32_t* status)
+{
+    // The event counts and exit histograms of this CTA's photons accumulate in shared memory
+    // (every photon ends in one of two events, so device atomics per photon would queue on two
+    // words) and are added to the device arrays once at the end.
+    constexpr std::uint32_t kLocalHistBins = 1024u;
+    __shared__ T s_hist[2][kLocalHistBins];
+    __shared__ unsigned long long s_counts[eventBins];
+    const bool localHist = terminal.histBins != 0u && terminal.histBins <= kLocalHistBins &&
+                           terminal.transHist != nullptr && terminal.reflHist != nullptr;
+    for (std::uint32_t k = threadIdx.x; k < 2u * kLocalHistBins; k += blockDim.x)
+        s_hist[k / kLocalHistBins][k % kLocalHistBins] = T(0);
+    for (std::uint32_t k = threadIdx.x; k < eventBins; k += blockDim.x)
+        s_counts[k] = 0ull;
+    __syncthreads();
+    RecordTerminalT<T> local = terminal;
+    if (localHist) {
+        local.transHist = s_hist[0];
+        local.reflHist = s_hist[1];
+    }
+    if (terminal.eventCounts != nullptr)
+        local.eventCounts = s_counts;
+    transport_walks(propose, advance, scatter, local, seedMixed, firstId, n, status);
+    __syncthreads();
+    if (terminal.eventCounts != nullptr)
+        for (std::uint32_t k = threadIdx.x; k < eventBins; k += blockDim.x)
+            if (s_counts[k] != 0ull)
+                atomicAdd(&terminal.eventCounts[k], s_counts[k]);
+    if (localHist)
+        for (std::uint32_t k = threadIdx.x; k < 2u * terminal.histBins; k += blockDim.x) {
+            const std::uint32_t h = k / terminal.histBins, bin = k % terminal.histBins;
+            if (s_hist[h][bin] != T(0))
+                atomicAdd(h == 0u ? &terminal.transHist[bin] : &terminal.reflHist[bin], s_hist[h][bin]);
+        }
 }
 
 } // namespace graphflow::photon
