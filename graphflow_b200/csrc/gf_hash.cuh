@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(kHashPThreads) hash_count_persist_kernel(Acces
 // popularity-ranked key space) reserves its own slot with one device atomic and is written at
 // once; that path is compiled only when B > kHashGroupBins (kTail).
 template <typename Access, typename Update, bool kTail>
-__global__ void __launch_bounds__(kHashPThreads) hash_scatter_grouped_kernel(
+__global__ void __launch_bounds__(kHashPThreads, 4) hash_scatter_grouped_kernel(
     Access acc, UnmixClassify cls, Update update, uint64_t seed_mixed, uint32_t capacity, FastDiv fdc,
     uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B, uint32_t unit, const uint32_t* bin_ids,
     const uint32_t* table, uint32_t* next, uint32_t* counts, uint32_t* status)
