@@ -1,7 +1,8 @@
 """Benchmark of the B200 transform-batch hot path: dense classify + exact plan + scatter of
 N = 1e8 u32 keys into pooled output chunks (C = 8192), one whole-array batch per step.
 
-  value   fused single-pass form (one classify->scan->scatter launch + device finish), inputs
+  value   fused single-pass form (one classify->plan->scatter launch that also writes the chunk
+          table and descriptors: gf_partition_fused_full_u32), inputs
           resident in HBM; particles/s summed over all ranks (weak scaling: every rank
           partitions its own 1e8 keys; the path has no exchange step, so no collective).
   plain   the reference's two-launch form (classify, host plan, scatter) on the same data.
@@ -350,19 +351,17 @@ def gpu_arm(args):
         with torch.cuda.stream(stream):
             t_start.record(stream)
             for i in range(args.steps):
+                # one step: the fused partition and its finish in one launch (+ the control-block reset)
                 k_start[i].record(stream)
-                capi.check(capi.lib().gf_partition_fused_u32(
+                capi.check(capi.lib().gf_partition_fused_full_u32(
                     stream.cuda_stream, bench.pool.ptr(), bench.pool.ptr(), CAPACITY, bench.pool.slots,
                     bench.d_tiles.data_ptr(), bench.n_tiles, args.tile, args.bins, capi.CLS_KEY_MOD,
                     bench.fused.reserved.data_ptr(), bench.bound, bench.fused.totals.data_ptr(),
                     bench.fused.port_chunks.data_ptr(), bench.fused.max_k, bench.fused.scratch.data_ptr(),
-                    bench.fused.scratch_bytes, bench.fused.status.data_ptr()), "fused")
+                    bench.fused.scratch_bytes, bench.fused.table.data_ptr(), bench.fused.descs.data_ptr(),
+                    bench.fused.reserve_cap, bench.fused.num_out.data_ptr(), bench.fused.status.data_ptr()),
+                    "fused")
                 k_end[i].record(stream)
-                capi.check(capi.lib().gf_fused_finish(
-                    stream.cuda_stream, bench.fused.totals.data_ptr(), bench.fused.port_chunks.data_ptr(), args.bins,
-                    CAPACITY, bench.fused.max_k, bench.fused.scratch.data_ptr(), bench.fused.table.data_ptr(),
-                    bench.fused.descs.data_ptr(), bench.fused.reserve_cap, bench.fused.num_out.data_ptr(),
-                    bench.fused.status.data_ptr()), "finish")
             t_end.record(stream)
         stream.synchronize()
     barrier()
@@ -510,7 +509,7 @@ def gpu_arm(args):
                 "h2d_bytes_per_step": args.n * 4,
                 "d2h_bytes_per_step": out_slots * 4 + 3 * 4 * bench_reserve_cap(args) + 8},
         "clocks": clocks.summary(),
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": args.steps,  # one fused_partition_coop_kernel launch per timed step
         "fused_per_tile_kernel": {"value": world * args.n / (per_tile_ms / 1e3), "ms_per_step": per_tile_ms},
         "plain": {"value": world * args.n / (plain_ms / 1e3), "ms_per_step": plain_ms,
                   "form": "classify kernel + host plan + scatter kernel (reference structure)"},

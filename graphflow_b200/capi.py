@@ -63,6 +63,8 @@ _SIGS = {
     "gf_partition_fused_u32": [_VP, _VP, _VP, _U32, _U64, _VP, _U32, _U32, _U32, _I32, _VP, _U32, _VP, _VP, _U32,
                                _VP, _U64, _VP],
     "gf_fused_finish": [_VP, _VP, _VP, _U32, _U32, _U32, _VP, _VP, _VP, _U32, _VP, _VP],
+    "gf_partition_fused_full_u32": [_VP, _VP, _VP, _U32, _U64, _VP, _U32, _U32, _U32, _I32, _VP, _U32, _VP, _VP,
+                                    _U32, _VP, _U64, _VP, _VP, _U32, _VP, _VP],
     "gf_zipf_cdf": [C.c_double, _U32, _VP],
     "gf_generate_keys_u32": [_VP, _I32, _U64, _U64, _U64, _U32, _VP, _VP],
     "gf_classify_hash_r16": [_VP, _VP, _I32, _U32, _U64, _VP, _U32, _U32, _U32, _U64, _VP, _VP, _VP],

@@ -205,12 +205,19 @@ gf_status gf_fused_scratch_bytes(uint32_t n_tiles, uint32_t bins, uint64_t* h_by
     return GF_OK;
 }
 
-gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out, uint32_t capacity,
-                                 uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size,
-                                 uint32_t bins, int classifier, const uint32_t* d_reserved, uint32_t n_reserved,
-                                 uint32_t* d_totals, unsigned long long* d_port_chunks, uint32_t max_chunks_per_port,
-                                 void* d_scratch, uint64_t scratch_bytes, uint32_t* d_status)
+} // extern "C"
+
+namespace {
+// The fused partition; with `fin` set, the same launch also writes gf_fused_finish's outputs (the
+// cooperative kernel during its plan, the per-tile kernel in its last CTA). `finished` reports
+// whether it did (false only for an empty batch).
+gf_status fused_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out, uint32_t capacity,
+                    uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size, uint32_t bins,
+                    int classifier, const uint32_t* d_reserved, uint32_t n_reserved, uint32_t* d_totals,
+                    unsigned long long* d_port_chunks, uint32_t max_chunks_per_port, void* d_scratch,
+                    uint64_t scratch_bytes, uint32_t* d_status, InlineFinish fin, bool* finished)
 {
+    *finished = false;
     uint64_t need = 0;
     if (gf_fused_scratch_bytes(n_tiles, bins, &need) != GF_OK || scratch_bytes < need || d_scratch == nullptr ||
         (reinterpret_cast<uintptr_t>(d_scratch) & 15u) != 0u)
@@ -222,6 +229,7 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
         return GF_ERR_ARGUMENT;
     if (n_tiles == 0u)
         return cuda_status(cudaMemsetAsync(d_totals, 0, sizeof(uint32_t) * bins, as_stream(stream)));
+    *finished = fin.table != nullptr;
     FusedCtl* ctl = static_cast<FusedCtl*>(d_scratch);
     unsigned long long* desc = reinterpret_cast<unsigned long long*>(ctl + 1);
     const bool coop = g_fused_coop != 0 && bins <= 64u && (capacity & 3u) == 0u && capacity >= 4096u &&
@@ -235,7 +243,7 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
             return cuda_status(launch_fused_coop<S>(as_stream(stream), cls, d_keys_in, d_keys_out, capacity,
                                                     pool_slots, d_tiles, n_tiles, bins, d_reserved, n_reserved,
                                                     d_totals, d_port_chunks, max_chunks_per_port, ctl, scratch_bytes,
-                                                    d_status, device_sms()));
+                                                    d_status, device_sms(), fin));
         };
         auto with_cls = [&]<typename S>() -> gf_status {
             if (classifier == GF_CLS_KEY_MOD || classifier == GF_CLS_ID_BALANCED) {
@@ -265,9 +273,45 @@ gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32
         KeyClassify<Acc> cls{key_classifier(classifier, bins)};
         kernel<<<n_tiles, Shape::kThreads, smem, as_stream(stream)>>>(
             acc, cls, NoUpdate{}, 0u, capacity, FastDiv(capacity), pool_slots, d_tiles, n_tiles, bins, d_reserved,
-            n_reserved, d_totals, d_port_chunks, max_chunks_per_port, ctl, desc, d_status, InlineFinish{});
+            n_reserved, d_totals, d_port_chunks, max_chunks_per_port, ctl, desc, d_status, fin);
         return cuda_status(cudaGetLastError());
     });
+}
+} // namespace
+
+extern "C" {
+
+gf_status gf_partition_fused_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out, uint32_t capacity,
+                                 uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size,
+                                 uint32_t bins, int classifier, const uint32_t* d_reserved, uint32_t n_reserved,
+                                 uint32_t* d_totals, unsigned long long* d_port_chunks, uint32_t max_chunks_per_port,
+                                 void* d_scratch, uint64_t scratch_bytes, uint32_t* d_status)
+{
+    bool finished = false;
+    return fused_u32(stream, d_keys_in, d_keys_out, capacity, pool_slots, d_tiles, n_tiles, tile_size, bins,
+                     classifier, d_reserved, n_reserved, d_totals, d_port_chunks, max_chunks_per_port, d_scratch,
+                     scratch_bytes, d_status, InlineFinish{}, &finished);
+}
+
+gf_status gf_partition_fused_full_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out,
+                                      uint32_t capacity, uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles,
+                                      uint32_t tile_size, uint32_t bins, int classifier, const uint32_t* d_reserved,
+                                      uint32_t n_reserved, uint32_t* d_totals, unsigned long long* d_port_chunks,
+                                      uint32_t max_chunks_per_port, void* d_scratch, uint64_t scratch_bytes,
+                                      uint32_t* d_table, gf_out_desc* d_descs, uint32_t desc_cap,
+                                      uint32_t* d_num_out, uint32_t* d_status)
+{
+    if (d_table == nullptr || d_num_out == nullptr || (desc_cap != 0u && d_descs == nullptr))
+        return GF_ERR_ARGUMENT;
+    bool finished = false;
+    const gf_status rc = fused_u32(stream, d_keys_in, d_keys_out, capacity, pool_slots, d_tiles, n_tiles, tile_size,
+                                   bins, classifier, d_reserved, n_reserved, d_totals, d_port_chunks,
+                                   max_chunks_per_port, d_scratch, scratch_bytes, d_status,
+                                   InlineFinish{d_table, d_descs, desc_cap, d_num_out}, &finished);
+    if (rc != GF_OK || finished)
+        return rc;
+    return gf_fused_finish(stream, d_totals, d_port_chunks, bins, capacity, max_chunks_per_port, d_scratch, d_table,
+                           d_descs, desc_cap, d_num_out, d_status);
 }
 
 gf_status gf_fused_finish(void* stream, const uint32_t* d_totals, const unsigned long long* d_port_chunks,

@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(S::kThreads, 4)
                                 FastDiv fdc, uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B,
                                 const uint32_t* reserved, uint32_t n_reserved, uint32_t* totals,
                                 unsigned long long* port_chunks, uint32_t max_k, FusedCtl* ctl, CoopHdr* hdr,
-                                uint32_t* cta_tot, uint32_t* status)
+                                uint32_t* cta_tot, uint32_t* status, InlineFinish fin)
 {
     constexpr int T = S::kThreads, IPT = S::kIpt, W = S::kWarps;
     constexpr uint32_t BM = S::kBM, L = S::kLanes, SEG = S::kSeg, MB = S::kMaxBins;
@@ -453,6 +453,37 @@ __global__ void __launch_bounds__(S::kThreads, 4)
                 const uint32_t f = bin_base[pb] + k;
                 const uint32_t chunk = f < R && f < n_reserved ? __ldg(reserved + f) : kNoChunk;
                 port_chunks[(size_t)pb * max_k + k] = ((unsigned long long)epoch << 32) | chunk;
+            }
+        }
+        if (fin.table != nullptr) {
+            // the finish, spread over the grid: output chunk r of the plan is reserved[r]; its port is
+            // the last one whose chunks start at or before r (table = [binBase, chunkIndex],
+            // DenseBinTable.hpp:80-91; descriptors in bin order with fills, Execution.hpp:2558-2581)
+            for (uint32_t r = c * (uint32_t)T + tid; r < R; r += G * (uint32_t)T) {
+                if (r >= fin.desc_cap) {
+                    set_status(status, GF_OVERFLOW);
+                    continue;
+                }
+                uint32_t lo = 0, hi = B - 1u;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi + 1u) >> 1;
+                    if (bin_base[mid] <= r)
+                        lo = mid;
+                    else
+                        hi = mid - 1u;
+                }
+                const uint32_t k = r - bin_base[lo];
+                const uint32_t chunk = r < n_reserved ? __ldg(reserved + r) : kNoChunk;
+                fin.table[B + r] = chunk;
+                fin.descs[r].chunk_index = chunk;
+                fin.descs[r].fill = min(capacity, total[lo] - k * capacity);
+                fin.descs[r].bin = lo;
+            }
+            if (c == 0) {
+                for (uint32_t b2 = tid; b2 < B; b2 += T)
+                    fin.table[b2] = bin_base[b2];
+                if (tid == 0)
+                    *fin.num_out = R;
             }
         }
         if (c == 0) {
@@ -726,12 +757,13 @@ __global__ void __launch_bounds__(S::kThreads, 4)
 // Host side: one cooperative launch of the kernel with classifier `cls`; the grid is as many CTAs
 // as fit on the device at once, capped by the tiles and by the scratch (the control block, then
 // 4 * 2 * LANES bytes per CTA). The control block's reset words are zeroed here, on the stream.
+// With `fin` set, the launch also writes the chunk table, descriptors and output count.
 template <typename S, typename Cls>
 cudaError_t launch_fused_coop(cudaStream_t stream, Cls cls, const uint32_t* in, uint32_t* out, uint32_t capacity,
                               uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t bins,
                               const uint32_t* reserved, uint32_t n_reserved, uint32_t* totals,
                               unsigned long long* port_chunks, uint32_t max_k, FusedCtl* ctl, uint64_t scratch_bytes,
-                              uint32_t* status, int sms)
+                              uint32_t* status, int sms, InlineFinish fin = {})
 {
     auto kernel = fused_partition_coop_kernel<S, Cls>;
     constexpr uint64_t kHead = sizeof(FusedCtl) + sizeof(CoopHdr);
@@ -764,7 +796,7 @@ cudaError_t launch_fused_coop(cudaStream_t stream, Cls cls, const uint32_t* in, 
     FastDiv fd(capacity);
     void* args[] = {&in,       &out,      &cls,    &capacity,    &fd,    &pool_slots, &tiles,
                     &n_tiles,  &bins,     &reserved, &n_reserved, &totals, &port_chunks, &max_k,
-                    &ctl,      &hdr,      &cta_tot, &status};
+                    &ctl,      &hdr,      &cta_tot, &status, &fin};
     return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3((uint32_t)g), dim3(S::kThreads),
                                        args, S::kSmemBytes, stream);
 }

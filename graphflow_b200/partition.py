@@ -167,11 +167,23 @@ class FusedPartition(_Common):
         self.descs = torch.zeros(3 * max(self.reserve_cap, 1), dtype=torch.int32, device=self.dev)
         self.num_out = torch.zeros(1, dtype=torch.int32, device=self.dev)
         self.launches = 0
+        self.combined = True
 
-    def enqueue(self, d_tiles, n_tiles, n_reserved, stream=None):
-        """Enqueue the fused launch and the finish (no host synchronisation)."""
+    def enqueue(self, d_tiles, n_tiles, n_reserved, stream=None, combined=None):
+        """Enqueue the fused launch and the finish (no host synchronisation): one launch that
+        does both (gf_partition_fused_full_u32), or with combined=False (default: the object's
+        `combined` attribute, True) the two calls gf_partition_fused_u32 + gf_fused_finish."""
         s = _stream_ptr(stream)
         L = capi.lib()
+        if self.combined if combined is None else combined:
+            capi.check(L.gf_partition_fused_full_u32(
+                s, self.pool.ptr(), self.pool.ptr(), self.pool.capacity, self.pool.slots,
+                d_tiles.data_ptr() if n_tiles else None, n_tiles, self.tile_size, self.bins, self.cls,
+                self.reserved.data_ptr(), n_reserved, self.totals.data_ptr(), self.port_chunks.data_ptr(), self.max_k,
+                self.scratch.data_ptr(), self.scratch_bytes, self.table.data_ptr(), self.descs.data_ptr(),
+                self.reserve_cap, self.num_out.data_ptr(), self.status.data_ptr()), "fused partition + finish")
+            self.launches += 1
+            return
         capi.check(L.gf_partition_fused_u32(s, self.pool.ptr(), self.pool.ptr(), self.pool.capacity, self.pool.slots,
                                             d_tiles.data_ptr() if n_tiles else None, n_tiles, self.tile_size,
                                             self.bins, self.cls, self.reserved.data_ptr(), n_reserved,

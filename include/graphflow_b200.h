@@ -163,6 +163,18 @@ gf_status gf_fused_finish(void* stream, const uint32_t* d_totals, const unsigned
                           uint32_t* d_table, gf_out_desc* d_descs, uint32_t desc_cap, uint32_t* d_num_out,
                           uint32_t* d_status);
 
+/* gf_partition_fused_u32 followed by gf_fused_finish, in one launch (no reference counterpart;
+ * the pair above restates flow/Execution.hpp:2363-2642 + 2558-2590): the cooperative kernel writes
+ * d_table, d_descs and d_num_out during its plan, the per-tile kernel in its last CTA. Arguments,
+ * outputs and scratch rules are those of the two calls; results are identical to them. */
+gf_status gf_partition_fused_full_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out,
+                                      uint32_t capacity, uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles,
+                                      uint32_t tile_size, uint32_t bins, int classifier, const uint32_t* d_reserved,
+                                      uint32_t n_reserved, uint32_t* d_totals, unsigned long long* d_port_chunks,
+                                      uint32_t max_chunks_per_port, void* d_scratch, uint64_t scratch_bytes,
+                                      uint32_t* d_table, gf_out_desc* d_descs, uint32_t desc_cap,
+                                      uint32_t* d_num_out, uint32_t* d_status);
+
 /* No counterpart in the reference. The fused partition plus its device finish for callers that
  * cannot allocate device memory at this point: a host runtime that gives all device memory to
  * its own pool at start-up and forbids cudaMalloc afterwards, or a latency-critical path that

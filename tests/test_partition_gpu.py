@@ -142,6 +142,7 @@ def test_fused_tile_sizes_many_tiles(tile_size):
     _run_case("fused", 1_000_003, 8192, 32, "zipf", tile_size, ragged=False)
 
 
+@pytest.mark.parametrize("combined", [True, False])
 @pytest.mark.parametrize("coop", [1, 0])
 @pytest.mark.parametrize("bins,capacity,tile_size,dist", [
     (1, 8192, 4096, "uniform"),        # one port: every tile one run
@@ -152,10 +153,11 @@ def test_fused_tile_sizes_many_tiles(tile_size):
     (3, 1024, 4096, "uniform"),        # capacity below 4096: per-tile kernel
     (64, 8192, 8192, "uniform"),       # tiles above 4096: per-tile kernel
 ])
-def test_fused_kernels_match_oracle(coop, bins, capacity, tile_size, dist):
+def test_fused_kernels_match_oracle(combined, coop, bins, capacity, tile_size, dist):
     """Both fused kernels (the cooperative count/plan/scatter kernel and the per-tile look-back
     kernel) give the oracle's counts, plan and per-port sequences; the cooperative kernel also
-    takes the output chunks in plan order (table[B + f] = reserved[f])."""
+    takes the output chunks in plan order (table[B + f] = reserved[f]). Both forms of the finish:
+    inside the partition launch (gf_partition_fused_full_u32) and as its own launch."""
     capi.check(capi.lib().gf_set_tuning(b"fused_coop", coop), "tuning")
     try:
         n = 250_007
@@ -171,6 +173,7 @@ def test_fused_kernels_match_oracle(coop, bins, capacity, tile_size, dist):
         snap = {ch: col[ch * capacity:(ch + 1) * capacity].copy() for ch in chunks}
         expect_reserved = list(pool.free)[:bound]
         part = FusedPartition(pool, bins, tile_size=tile_size, max_batch_particles=n)
+        part.combined = combined
         totals, table, descs = part.run(chunks, fills)
         _check(pool, chunks, fills, keys, bins, (totals, table, descs), exact_order=True, in_snapshot=snap)
         if coop and tile_size <= 4096 and capacity >= 4096:
