@@ -173,12 +173,11 @@ gf_status gf_scatter_hash_r16(void* stream, const gf_rec16_columns* h_in, const 
     if (gf_hash_persistent()) {
         return with_layout(layout, h_in, h_out, [&](auto acc) -> gf_status {
             using Acc = decltype(acc);
-            auto kernel = bins > kHashGroupBins ? hash_scatter_grouped_kernel<Acc, NoUpdate, true>
-                                                : hash_scatter_grouped_kernel<Acc, NoUpdate, false>;
+            auto kernel = bins > kHashGroupBins     ? hash_scatter_grouped_kernel<Acc, NoUpdate, true, 8u>
+                          : bins > kHashGroupBins / 2u ? hash_scatter_grouped_kernel<Acc, NoUpdate, false, 8u>
+                                                       : hash_scatter_grouped_kernel<Acc, NoUpdate, false, 4u>;
             const uint32_t unit = tile_size; // 1024 or 2048
-            const size_t smem = sizeof(Rec16) * unit + 4u * sizeof(uint32_t) * std::min(bins, kHashGroupBins) +
-                                sizeof(uint16_t) * ((unit + 1u) & ~1u) +
-                                sizeof(uint32_t) * (kHashPThreads / 32 + 1);
+            const size_t smem = hash_grouped_smem(bins, unit);
             cudaError_t e = allow_smem(kernel, smem);
             if (e != cudaSuccess)
                 return cuda_status(e);

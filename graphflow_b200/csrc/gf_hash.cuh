@@ -14,6 +14,8 @@
 
 #include "gf_partition.cuh"
 
+#include <type_traits>
+
 namespace gf {
 namespace { // internal linkage: see gf_partition.cuh
 
@@ -388,122 +390,314 @@ __global__ void __launch_bounds__(kHashPThreads) hash_count_persist_kernel(Acces
             atomicAdd(&counts[b], hist[b]);
 }
 
-// Grouped scatter: persistent CTAs over contiguous tile ranges; in every unit of up to `unit`
-// records of a tile, the records of ports below GB = min(B, kHashGroupBins) are grouped by port
-// in shared memory (a direct-indexed count per port that also gives each record its rank, an
-// exclusive scan over the GB ports), each such port present in the unit reserves its range with
-// one device atomic on next[port] (arrival order between units, as
+// Grouped scatter: persistent CTAs over contiguous tile ranges, processed in units of up to
+// `unit` records (unit / 256 rows; a row is up to 256 consecutive records of one tile, so a unit
+// spans several small tiles). In every unit the records of ports below GB = min(B, kHashGroupBins)
+// are grouped by port in shared memory: a direct-indexed count per port gives each record its
+// rank, an exclusive scan over the GB ports its stage position, each port present in the unit
+// reserves its range with one device atomic on next[port] (arrival order between units, as
 // graph/HashScatterKernel.hpp:132-150 reserves per table entry), and a port's records of the unit
 // go to consecutive slots from consecutive threads. A record of a port >= GB (the tail of a
-// popularity-ranked key space) reserves its own slot with one device atomic and is written at
-// once; that path is compiled only when B > kHashGroupBins (kTail).
-template <typename Access, typename Update, bool kTail>
-__global__ void __launch_bounds__(kHashPThreads, 4) hash_scatter_grouped_kernel(
+// popularity-ranked key space; compiled only when B > kHashGroupBins, kTail) is staged at the end
+// of the unit's stage and reserves its own slot with one device atomic.
+//
+// A record is staged at its input position as soon as it is classified (its registers are free for
+// the scan); the stage step only writes, per port-order position, the record's input position.
+// Thread t owns ports t, t + 256, ... (PPT of them; the popular low ports spread over all warps):
+// it scans their counts and issues their reservations before the stage step, which hides the
+// atomics' latency behind a barrier and the staging. Warp 0 prefetches the next unit's tile
+// descriptors with cp.async while the unit's records are counted, and builds its row table from
+// them. The tail's reservations are issued at the same point and consumed after the grouped
+// write-out.
+constexpr uint32_t kHashRowsEnd = 0xFFFFFFFFu;
+constexpr uint32_t kHashTailEarly = 2u; // tail records per thread reserved ahead of the write-out
+
+GF_D void cp_async4(void* smem_dst, const void* gmem_src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+                 "l"(gmem_src)
+                 : "memory");
+}
+GF_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+GF_D void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Warp 0: copy the descriptors of tiles cur_t .. cur_t + nr_max - 1 (those below t_hi) into tstage.
+GF_D void hash_prefetch_tiles(const gf_tile* tiles, uint32_t t_hi, uint32_t nr_max, uint32_t cur_t, uint32_t* tstage)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    if (cur_t < t_hi && lane < nr_max && lane < t_hi - cur_t) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(tiles + cur_t + lane);
+        cp_async4(tstage + 3u * lane, src);
+        cp_async4(tstage + 3u * lane + 1u, src + 1);
+        cp_async4(tstage + 3u * lane + 2u, src + 2);
+    }
+    cp_async_commit();
+}
+
+// Warp 0 (every lane keeps the same cursor): row table of the unit that starts at tile cur_t,
+// record cur_off, from the descriptors prefetched into tstage. Rows are taken in tile order up to
+// nr_max; the cursor moves past them.
+GF_D void hash_build_rows(uint32_t t_hi, uint32_t capacity, uint64_t pool_slots, uint32_t nr_max, uint32_t& cur_t,
+                          uint32_t& cur_off, const uint32_t* tstage, uint64_t* rbase, uint32_t* rcnt, uint32_t* nrows,
+                          uint32_t* status)
+{
+    constexpr uint32_t T = kHashPThreads;
+    const uint32_t lane = threadIdx.x & 31u;
+    cp_async_wait_all();
+    __syncwarp();
+    if (cur_t >= t_hi) {
+        if (lane == 0u)
+            *nrows = kHashRowsEnd;
+        return;
+    }
+    const uint32_t loaded = t_hi - cur_t < nr_max ? t_hi - cur_t : nr_max;
+    uint64_t base = 0;
+    uint32_t rows = 0, rem = 0, off = 0;
+    if (lane < loaded) {
+        const uint32_t chunk = tstage[3u * lane], toff = tstage[3u * lane + 1u], tcount = tstage[3u * lane + 2u];
+        base = (uint64_t)chunk * capacity + toff;
+        const bool ok = base + tcount <= pool_slots && (uint64_t)toff + tcount <= capacity;
+        if (!ok)
+            set_status(status, GF_INVALID);
+        const uint32_t count = ok ? tcount : 0u;
+        off = lane == 0u ? cur_off : 0u;
+        rem = count > off ? count - off : 0u;
+        rows = (rem + T - 1u) / T;
+    }
+    uint32_t incl = rows;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if ((int)lane >= o)
+            incl += y;
+    }
+    const uint32_t excl = incl - rows;
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    for (uint32_t j = excl; j < incl && j < nr_max; ++j) {
+        const uint32_t k = j - excl;
+        rbase[j] = base + off + (uint64_t)k * T;
+        rcnt[j] = rem - k * T < T ? rem - k * T : T;
+    }
+    if (total <= nr_max) {
+        cur_t += loaded;
+        cur_off = 0u;
+    } else {
+        const uint32_t L = (uint32_t)__ffs(__ballot_sync(0xFFFFFFFFu, incl >= nr_max)) - 1u;
+        const uint32_t ex = __shfl_sync(0xFFFFFFFFu, excl, L), in = __shfl_sync(0xFFFFFFFFu, incl, L);
+        const uint32_t of = __shfl_sync(0xFFFFFFFFu, off, L);
+        if (in == nr_max) {
+            cur_t += L + 1u;
+            cur_off = 0u;
+        } else {
+            cur_t += L;
+            cur_off = of + (nr_max - ex) * T;
+        }
+    }
+    if (lane == 0u)
+        *nrows = total < nr_max ? total : nr_max;
+    __syncwarp(); // tstage is refilled by the next prefetch
+}
+
+// With more than 1024 grouped ports the port arrays take 24 KB: three CTAs per SM, whose register
+// bound then leaves room for the eight owned ports.
+template <typename Access, typename Update, bool kTail, uint32_t PPT>
+__global__ void __launch_bounds__(kHashPThreads, PPT == 8u ? 3 : 4) hash_scatter_grouped_kernel(
     Access acc, UnmixClassify cls, Update update, uint64_t seed_mixed, uint32_t capacity, FastDiv fdc,
     uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B, uint32_t unit, const uint32_t* bin_ids,
     const uint32_t* table, uint32_t* next, uint32_t* counts, uint32_t* status)
 {
     using P = typename Access::Payload;
-    constexpr uint32_t T = kHashPThreads, RPT = 2048u / T; // records per thread per unit, units of <= 2048
+    using SPort = std::conditional_t<kTail, uint32_t, uint16_t>;
+    constexpr uint32_t T = kHashPThreads, W = T / 32u, RPT = 2048u / T; // rows per unit: unit / T <= RPT
+    static_assert((PPT == 4u || PPT == 8u) && PPT * T >= kHashGroupBins / 2u && (!kTail || PPT * T >= kHashGroupBins),
+                  "owned ports: PPT per thread cover the grouped ports");
     extern __shared__ __align__(16) uint32_t sm[];
-    P* stage = reinterpret_cast<P*>(sm);                                 // [unit]
     const uint32_t GB = B < kHashGroupBins ? B : kHashGroupBins;
-    uint32_t* port_base = reinterpret_cast<uint32_t*>(stage + unit);     // [GB] table[port]
-    uint32_t* tcnt = port_base + GB;                                     // [GB] records of the unit per port
-    uint32_t* tpre = tcnt + GB;                                          // [GB] the unit's stage start per port
-    uint32_t* tpos = tpre + GB;                                          // [GB] the port's reserved position
-    uint16_t* sport = reinterpret_cast<uint16_t*>(tpos + GB);            // [unit] port per stage position
-    uint32_t* scan_tmp = reinterpret_cast<uint32_t*>(sport + ((unit + 1u) & ~1u)); // [T / 32 + 1]
+    P* stage = reinterpret_cast<P*>(sm);                              // [unit]
+    uint64_t* rbase = reinterpret_cast<uint64_t*>(stage + unit);      // [2][RPT]
+    uint32_t* tc = reinterpret_cast<uint32_t*>(rbase + 2u * RPT);     // [GB] count | stage start << 16
+    uint32_t* D = tc + GB;                                            // [GB] reserved position - stage start
+    uint32_t* PB = D + GB;                                            // [GB] table[port]
+    uint32_t* rcnt = PB + GB;                                         // [2][RPT]
+    uint32_t* nrows = rcnt + 2u * RPT;                                // [2]
+    uint32_t* ntail = nrows + 2u;                                     // [2]
+    uint32_t* scan_tmp = ntail + 2u;                                  // [PPT][W]
+    uint32_t* tstage = scan_tmp + PPT * W;                            // [3 * RPT] prefetched tile descriptors
+    SPort* sport = reinterpret_cast<SPort*>(tstage + 3u * RPT);       // [unit] port per output position
+    uint16_t* src = reinterpret_cast<uint16_t*>(sport + unit);        // [unit] input position per output position
+    const uint32_t tid = threadIdx.x, w = tid >> 5, lane = tid & 31u;
     const uint32_t G = gridDim.x, c = blockIdx.x;
     const uint32_t t_lo = (uint32_t)((uint64_t)n_tiles * c / G), t_hi = (uint32_t)((uint64_t)n_tiles * (c + 1u) / G);
-    for (uint32_t i = threadIdx.x; i < GB; i += T) {
-        port_base[i] = __ldg(table + i);
-        tcnt[i] = 0u;
+    const uint32_t nr_max = unit / T;
+    for (uint32_t i = tid; i < GB; i += T) {
+        tc[i] = 0u;
+        PB[i] = __ldg(table + i);
     }
+    uint32_t cur_t = t_lo, cur_off = 0u;
+    if (w == 0u) {
+        hash_prefetch_tiles(tiles, t_hi, nr_max, cur_t, tstage);
+        hash_build_rows(t_hi, capacity, pool_slots, nr_max, cur_t, cur_off, tstage, rbase, rcnt, nrows, status);
+    }
+    if (tid == 0u)
+        ntail[0] = ntail[1] = 0u;
     __syncthreads();
     bool bad = false, overflow = false;
-    // a record of a port >= GB: its own slot, written now
-    auto place = [&](uint32_t b, P& r) {
-        const uint32_t j = atomicAdd(&next[b], 1u);
-        const uint32_t k = fdc.div(j);
-        const uint32_t chunk = __ldg(table + B + __ldg(table + b) + k);
-        const uint64_t slot = (uint64_t)chunk * capacity + (j - k * capacity);
-        if (slot < pool_slots)
-            acc.store(slot, r);
-        else
-            overflow = true;
-    };
     uint32_t upd = kUpdateSuccess;
-    for (uint32_t t = t_lo; t < t_hi; ++t) {
-        uint64_t base;
-        uint32_t count;
-        hash_tile_range(tiles, t, capacity, pool_slots, base, count, status);
-        for (uint32_t u0 = 0; u0 < count; u0 += unit) {
-            const uint32_t n = count - u0 < unit ? count - u0 : unit;
-            P rec[RPT];
-            uint32_t bp[RPT]; // port | rank << 16 (rank < unit <= 2048), or kNoBin16 in the low half
+    for (uint32_t it = 0;; ++it) {
+        const uint32_t buf = it & 1u;
+        const uint32_t nr = nrows[buf];
+        if (nr == kHashRowsEnd)
+            break;
+        P rec[RPT];
+        uint32_t bp[RPT];   // port | rank << 16 of a grouped record, else kNoBin16
+        uint32_t valid = 0; // bit r: this thread has a record in row r
 #pragma unroll
-            for (uint32_t r = 0; r < RPT; ++r) {
-                const uint32_t i = r * T + threadIdx.x;
-                if (i < n)
-                    rec[r] = acc.load(base + u0 + i);
+        for (uint32_t r = 0; r < RPT; ++r) {
+            if (r < nr && tid < rcnt[buf * RPT + r]) {
+                valid |= 1u << r;
+                rec[r] = acc.load(rbase[buf * RPT + r] + tid);
             }
+        }
+        // the next unit's tile descriptors arrive while this unit is counted and staged
+        if (w == 0u)
+            hash_prefetch_tiles(tiles, t_hi, nr_max, cur_t, tstage);
+        if (tid == 0u)
+            ntail[buf ^ 1u] = 0u; // its last reader (the previous unit's write-out) is past a barrier
 #pragma unroll
-            for (uint32_t r = 0; r < RPT; ++r) {
-                const uint32_t i = r * T + threadIdx.x;
-                bp[r] = kNoBin16;
-                if (i < n) {
-                    const uint32_t b = bin_ids != nullptr ? __ldg(bin_ids + base + u0 + i) : cls(rec[r].key);
-                    if (b < GB) {
-                        bp[r] = b | (atomicAdd(&tcnt[b], 1u) << 16);
-                    } else if (kTail && b < B) {
-                        const uint32_t res = update(b, rec[r], seed_mixed);
-                        if (res != kUpdateSuccess)
-                            upd = res;
-                        place(b, rec[r]);
-                    } else {
-                        bad = true;
-                    }
+        for (uint32_t r = 0; r < RPT; ++r) {
+            bp[r] = kNoBin16;
+            if (valid & (1u << r)) {
+                const uint32_t b = bin_ids != nullptr ? __ldg(bin_ids + rbase[buf * RPT + r] + tid) : cls(rec[r].key);
+                if (b < GB) {
+                    bp[r] = b | ((atomicAdd(&tc[b], 1u) & 0xFFFFu) << 16);
+                } else if (kTail && b < B) {
+                    const uint32_t q = unit - 1u - atomicAdd(&ntail[buf], 1u);
+                    src[q] = (uint16_t)(r * T + tid);
+                    sport[q] = (SPort)b;
+                } else {
+                    bad = true;
+                    continue;
+                }
+                const uint32_t res = update(b, rec[r], seed_mixed);
+                if (res != kUpdateSuccess)
+                    upd = res;
+                stage[r * T + tid] = rec[r];
+            }
+        }
+        __syncthreads();
+        // exclusive scan over the grouped ports in port order: one warp scan per owned column
+        // (and each owned port's reservation, issued as soon as its count is final)
+        uint32_t cw[PPT], incl[PPT], j0[PPT];
+#pragma unroll
+        for (uint32_t i = 0; i < PPT; ++i) {
+            const uint32_t p = tid + i * T;
+            cw[i] = p < GB ? tc[p] & 0xFFFFu : 0u;
+            incl[i] = cw[i];
+        }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+            for (uint32_t i = 0; i < PPT; ++i) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl[i], o);
+                if ((int)lane >= o)
+                    incl[i] += y;
+            }
+        }
+        if (lane == 31u) {
+#pragma unroll
+            for (uint32_t i = 0; i < PPT; ++i)
+                scan_tmp[i * W + w] = incl[i];
+        }
+        // the tail's reservations: all tail records of the unit are staged by now
+        uint32_t tj[kHashTailEarly], tpb[kHashTailEarly];
+        uint32_t nt = 0;
+        if constexpr (kTail) {
+            nt = ntail[buf];
+#pragma unroll
+            for (uint32_t u = 0; u < kHashTailEarly; ++u) {
+                const uint32_t i = u * T + tid;
+                const uint32_t b = i < nt ? (uint32_t)sport[unit - 1u - i] : 0u;
+                tj[u] = i < nt ? atomicAdd(&next[b], 1u) : 0u;
+                tpb[u] = i < nt ? __ldg(table + b) : 0u;
+            }
+        }
+        __syncthreads();
+        uint32_t n_grouped = 0;
+#pragma unroll
+        for (uint32_t i = 0; i < PPT; ++i) {
+            uint32_t pre = n_grouped; // ports of the columns before, and of the warps before in this column
+#pragma unroll
+            for (uint32_t v = 0; v < W; ++v) {
+                const uint32_t x = scan_tmp[i * W + v];
+                pre += v < w ? x : 0u;
+                n_grouped += x;
+            }
+            const uint32_t start = pre + incl[i] - cw[i];
+            const uint32_t p = tid + i * T;
+            j0[i] = cw[i] != 0u ? atomicAdd(&next[p], cw[i]) : 0u;
+            if (p < GB)
+                tc[p] = start << 16; // the stage start replaces the count
+            cw[i] = cw[i] != 0u ? start : 0xFFFFFFFFu;
+        }
+        __syncthreads();
+        // the grouped records in port order: output position -> input position and port
+#pragma unroll
+        for (uint32_t r = 0; r < RPT; ++r) {
+            const uint32_t b = bp[r] & 0xFFFFu;
+            if (b != kNoBin16) {
+                const uint32_t q = (tc[b] >> 16) + (bp[r] >> 16);
+                src[q] = (uint16_t)(r * T + tid);
+                sport[q] = (SPort)b;
+            }
+        }
+#pragma unroll
+        for (uint32_t i = 0; i < PPT; ++i)
+            if (cw[i] != 0xFFFFFFFFu)
+                D[tid + i * T] = j0[i] - cw[i];
+        // the next unit's rows (the row table this unit read is past two barriers)
+        if (w == 0u)
+            hash_build_rows(t_hi, capacity, pool_slots, nr_max, cur_t, cur_off, tstage, rbase + (buf ^ 1u) * RPT,
+                            rcnt + (buf ^ 1u) * RPT, nrows + (buf ^ 1u), status);
+        __syncthreads();
+        // write-out: grouped positions [0, n_grouped), then the tail [unit - n_tail, unit)
+        constexpr uint32_t kU = 4u;
+        for (uint32_t q0 = 0; q0 < n_grouped; q0 += kU * T) {
+#pragma unroll
+            for (uint32_t u = 0; u < kU; ++u) {
+                const uint32_t q = q0 + u * T + tid;
+                if (q < n_grouped) {
+                    const uint32_t b = sport[q];
+                    const uint32_t j = D[b] + q;
+                    const uint32_t k = fdc.div(j);
+                    const uint32_t chunk = __ldg(table + B + PB[b] + k);
+                    const uint64_t slot = (uint64_t)chunk * capacity + (j - k * capacity);
+                    if (slot < pool_slots)
+                        acc.store(slot, stage[src[q]]);
+                    else
+                        overflow = true;
                 }
             }
-            __syncthreads();
-            const uint32_t n_valid = block_exclusive_scan<T>(tcnt, tpre, GB, scan_tmp); // records staged
-            __syncthreads();
-            for (uint32_t p = threadIdx.x; p < GB; p += T) {
-                const uint32_t m = tcnt[p];
-                if (m != 0u) {
-                    tpos[p] = atomicAdd(&next[p], m);
-                    tcnt[p] = 0u;
-                }
-            }
-#pragma unroll
-            for (uint32_t r = 0; r < RPT; ++r) {
-                const uint32_t b = bp[r] & 0xFFFFu;
-                if (b != kNoBin16) {
-                    const uint32_t q = tpre[b] + (bp[r] >> 16);
-                    const uint32_t res = update(b, rec[r], seed_mixed);
-                    if (res != kUpdateSuccess)
-                        upd = res;
-                    stage[q] = rec[r];
-                    sport[q] = (uint16_t)b;
-                }
-            }
-            __syncthreads();
-            // positions [0, n_valid) are this unit's, in port order; consecutive positions of a port
-            // go to consecutive slots
-            for (uint32_t q = threadIdx.x; q < n_valid; q += T) {
-                const uint32_t b = sport[q];
-                const uint32_t j = tpos[b] + (q - tpre[b]);
+        }
+        if constexpr (kTail) {
+            auto put_tail = [&](uint32_t i, uint32_t j, uint32_t pbase) {
                 const uint32_t k = fdc.div(j);
-                const uint32_t chunk = __ldg(table + B + port_base[b] + k);
+                const uint32_t chunk = __ldg(table + B + pbase + k);
                 const uint64_t slot = (uint64_t)chunk * capacity + (j - k * capacity);
                 if (slot < pool_slots)
-                    acc.store(slot, stage[q]);
+                    acc.store(slot, stage[src[unit - 1u - i]]);
                 else
                     overflow = true;
+            };
+#pragma unroll
+            for (uint32_t u = 0; u < kHashTailEarly; ++u)
+                if (u * T + tid < nt)
+                    put_tail(u * T + tid, tj[u], tpb[u]);
+            for (uint32_t i = kHashTailEarly * T + tid; i < nt; i += T) {
+                const uint32_t b = sport[unit - 1u - i];
+                put_tail(i, atomicAdd(&next[b], 1u), __ldg(table + b));
             }
-            __syncthreads();
         }
+        __syncthreads();
     }
     if (bad || upd != kUpdateSuccess) {
         counts[B] = 1u;
@@ -511,6 +705,17 @@ __global__ void __launch_bounds__(kHashPThreads, 4) hash_scatter_grouped_kernel(
     }
     if (overflow)
         set_status(status, GF_OVERFLOW);
+}
+
+// Shared memory of hash_scatter_grouped_kernel for `bins` ports and units of `unit` records.
+inline size_t hash_grouped_smem(uint32_t bins, uint32_t unit)
+{
+    constexpr size_t rpt = 2048u / kHashPThreads, w = kHashPThreads / 32u;
+    const size_t gb = bins < kHashGroupBins ? bins : kHashGroupBins;
+    const size_t ppt = bins > kHashGroupBins / 2u ? 8u : 4u;
+    const size_t port_bytes = (bins > kHashGroupBins ? sizeof(uint32_t) : sizeof(uint16_t)) + sizeof(uint16_t);
+    return sizeof(Rec16) * unit + sizeof(uint64_t) * 2u * rpt + sizeof(uint32_t) * 3u * gb +
+           sizeof(uint32_t) * (2u * rpt + 4u + ppt * w + 3u * rpt) + port_bytes * unit;
 }
 
 // ---------------------------------------------------------------------------------------------
