@@ -20,6 +20,7 @@ int g_runner_batched = 1;
 // Tuning knob: 1 = the hash classify/scatter entry points use the persistent kernels (one shared
 // counter per port and CTA); 0 = the per-tile open-addressing kernels.
 int g_hash_persistent = 1;
+int g_sink_batch = 256;
 
 constexpr int kThreads = 256;
 constexpr uint32_t kMaxDenseBins = 65535u;
@@ -122,6 +123,12 @@ gf_status gf_set_tuning(const char* name, int value)
     }
     if (std::string(name) == "hash_persistent") {
         g_hash_persistent = value != 0;
+        return GF_OK;
+    }
+    if (std::string(name) == "sink_batch_chunks") {
+        if (value < 1 || value > 256)
+            return GF_ERR_ARGUMENT;
+        g_sink_batch = value;
         return GF_OK;
     }
     return GF_ERR_ARGUMENT;
@@ -437,5 +444,7 @@ extern "C" gf_status gf_partition_fused_u32_noalloc(
 
 // Read by the flow entry points (gf_flows.cu, gf_dense_flow.cu, gf_photon.cu).
 bool gf_runner_batched() { return gf::g_runner_batched != 0; }
+// Chunks a sink takes per launch in the batched runner (gf_flows.cu, gf_dense_flow.cu, gf_photon.cu).
+uint32_t gf_runner_sink_batch() { return (uint32_t)gf::g_sink_batch; }
 // Read by the hash entry points (gf_capi_hash.cu).
 bool gf_hash_persistent() { return gf::g_hash_persistent != 0; }

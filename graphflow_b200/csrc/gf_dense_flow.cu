@@ -8,6 +8,7 @@
 
 gf_status gf_flows_guard(const std::function<void()>& body); // gf_flows.cu
 bool gf_runner_batched();                                       // gf_capi.cu
+uint32_t gf_runner_sink_batch();                                // gf_capi.cu
 
 namespace {
 
@@ -62,7 +63,7 @@ extern "C" gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins
         t.batchChunks = batch_chunks;
         t.fused = fused != 0;
         if (gf_runner_batched()) {
-            t.sinkBatchChunks = batch_chunks;
+            t.sinkBatchChunks = gf_runner_sink_batch();
             t.multiDispatch = true;
         }
         const auto t0 = std::chrono::steady_clock::now();

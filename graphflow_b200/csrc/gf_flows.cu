@@ -60,7 +60,8 @@ void fill_stats(const graphflow::SchedulerStats& s, double seconds, gf_flow_stat
 
 } // namespace
 
-bool gf_runner_batched(); // gf_capi.cu
+bool gf_runner_batched();        // gf_capi.cu
+uint32_t gf_runner_sink_batch(); // gf_capi.cu
 
 // Runs a front-end call, mapping its exceptions to gf_status and the last-error message.
 gf_status gf_flows_guard(const std::function<void()>& body) { return guarded(body); }
@@ -107,7 +108,7 @@ gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visit
         t.batchChunks = batch_chunks;
         t.fused = fused != 0;
         if (gf_runner_batched()) {
-            t.sinkBatchChunks = batch_chunks;
+            t.sinkBatchChunks = gf_runner_sink_batch();
             t.multiDispatch = true;
         }
         const auto t0 = std::chrono::steady_clock::now();

@@ -10,6 +10,7 @@
 
 gf_status gf_flows_guard(const std::function<void()>& body); // gf_flows.cu
 bool gf_runner_batched();                                       // gf_capi.cu
+uint32_t gf_runner_sink_batch();                                // gf_capi.cu
 
 namespace {
 
@@ -55,7 +56,7 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
                 t.liveParticles = live;
             t.batchChunks = Q;
             if (gf_runner_batched()) {
-                t.sinkBatchChunks = Q;
+                t.sinkBatchChunks = gf_runner_sink_batch();
                 t.multiDispatch = true;
             }
             stats = runPhotonFlow<T, SoAStorage<PhotonT<T>>>(device, n, propose, slab, scatter, terminal, t);

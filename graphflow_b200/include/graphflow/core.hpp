@@ -87,10 +87,12 @@ struct Tuning {
     bool fused = true;
     // B200 runner options (results are identical either way). sinkBatchChunks: a sink may take up
     // to this many ready chunks per launch (the reference's runner takes one, GraphRunner.hpp:600;
-    // capped at batchChunks). multiDispatch: every idle node with ready input is dispatched in the
+    // at most kMaxSinkBatchChunks, independent of Q: a sink reserves no output chunks, so a
+    // partition's whole fan-out can drain in one launch). multiDispatch: every idle node with ready input is dispatched in the
     // same loop iteration (the reference dispatches one node per iteration, GraphRunner.hpp:985).
     std::uint32_t sinkBatchChunks = 1u;
     bool multiDispatch = false;
+    static constexpr std::uint32_t kMaxSinkBatchChunks = 256u;
 
     void validate() const
     {
@@ -118,6 +120,7 @@ struct Config {
     std::uint32_t chunkCapacity = 8192u;
     std::uint32_t liveParticles = 0u;
     std::uint32_t batchChunks = 1u;
+    std::uint32_t sinkBatchChunks = 1u; // chunks per sink launch (B200 runner option)
     std::uint32_t tileSize = 4096u;
     std::uint32_t numChunks = 0u;
     std::uint32_t maxBins = 1u;

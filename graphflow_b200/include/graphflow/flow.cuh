@@ -195,7 +195,7 @@ public:
         }
         runner.setSource(*m_sourceKey, itemCount, config.liveParticles);
         runner.setBatchChunks(config.batchChunks);
-        runner.setSinkBatchChunks(std::min(std::max(m_tuning.sinkBatchChunks, 1u), config.batchChunks));
+        runner.setSinkBatchChunks(config.sinkBatchChunks);
         runner.setMultiDispatch(m_tuning.multiDispatch);
         if (m_tuning.stallTimeout)
             runner.setStallTimeout(*m_tuning.stallTimeout);
@@ -282,6 +282,7 @@ private:
             maxBins = std::max(maxBins, n.bins);
         c.maxBins = maxBins;
         c.batchChunks = m_tuning.batchChunks.value_or(1u);
+        c.sinkBatchChunks = std::min(std::max(m_tuning.sinkBatchChunks, 1u), Tuning::kMaxSinkBatchChunks);
         c.chunkCapacity = m_tuning.chunkCapacity.value_or(8192u);
         c.tileSize = m_tuning.tileSize.value_or(1024u);
         c.scatterMode = m_tuning.scatterMode.value_or(ScatterMode::SharedStaging);

@@ -233,7 +233,7 @@ class SinkStage final : public Stage {
 public:
     SinkStage(TStorage& st, const Config& c, TFunctor f, std::uint32_t purpose)
         : m_st(st), m_f(std::move(f)), m_seed(gf::mix64(c.seed)), m_purpose(purpose),
-          m_tiles(static_cast<std::size_t>(c.batchChunks) * ((c.chunkCapacity + 1023u) / 1024u))
+          m_tiles(static_cast<std::size_t>(c.sinkBatchChunks) * ((c.chunkCapacity + 1023u) / 1024u))
     {
     }
     std::uint32_t launch(cudaStream_t s, const Batch& b) override

@@ -103,9 +103,11 @@ uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap);
  *                identical either way; the cooperative kernel also takes the output chunks in plan
  *                order (table[B + f] = reserved[f]).
  *   "runner_batched" 1 (default) = the flow entry points (gf_run_particle_feedback,
- *                gf_run_dense_chain, gf_run_photon) let a sink take up to Q ready chunks per launch
- *                and dispatch every idle node in one scheduler iteration; 0 = the reference
- *                runner's one-chunk sinks and one dispatch per iteration. Results are identical.
+ *                gf_run_dense_chain, gf_run_photon) let a sink take up to "sink_batch_chunks"
+ *                ready chunks per launch and dispatch every idle node in one scheduler iteration;
+ *                0 = the reference runner's one-chunk sinks and one dispatch per iteration.
+ *                Results are identical.
+ *   "sink_batch_chunks" 1..256 (default 256) = chunks per sink launch in the batched runner.
  *   "hash_persistent" 1 (default) = gf_classify_hash_r16 and gf_scatter_hash_r16 use the
  *                persistent kernels (one shared-memory counter per port and CTA for the count;
  *                the scatter groups each tile's records of ports below 2048 by port and places
