@@ -74,3 +74,17 @@ def test_argument_errors_are_reported_not_thrown():
     assert L.gf_classify_dense_u32(None, None, 16, 0, None, 0, 1024, 4, 0, None, C.addressof(cnt), None) == capi.GF_OK
     assert L.gf_partition_fused_u32(None, None, None, 16, 0, None, 0, 1024, 4, 0, None, 0, None, None, 0, None, 0,
                                     None) == capi.GF_ERR_ARGUMENT
+
+
+def test_tuning_knobs():
+    """Host-side knobs: names and ranges are checked; sink_batch_chunks takes 1..256."""
+    L = capi.lib()
+    assert L.gf_set_tuning(None, 1) == capi.GF_ERR_ARGUMENT
+    assert L.gf_set_tuning(b"no_such_knob", 1) == capi.GF_ERR_ARGUMENT
+    for bad in (0, 257, -1):
+        assert L.gf_set_tuning(b"sink_batch_chunks", bad) == capi.GF_ERR_ARGUMENT
+    try:
+        for good in (1, 8, 256):
+            assert L.gf_set_tuning(b"sink_batch_chunks", good) == capi.GF_OK
+    finally:
+        assert L.gf_set_tuning(b"sink_batch_chunks", 256) == capi.GF_OK

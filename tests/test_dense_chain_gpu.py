@@ -52,20 +52,26 @@ def test_chain_empty_and_argument_errors():
 
 
 def test_runner_options_give_identical_results():
-    """The B200 runner options (multi-chunk sinks, every idle node dispatched per iteration) and
-    the reference runner's one-chunk sinks / one dispatch per iteration give the same results."""
+    """The B200 runner options (sinks of up to sink_batch_chunks chunks, every idle node dispatched
+    per iteration) and the reference runner's one-chunk sinks / one dispatch per iteration give the
+    same results."""
     n, seed = 200_003, 3
     out = {}
+    L = capi.lib()
     try:
-        for on in (1, 0):
-            capi.check(capi.lib().gf_set_tuning(b"runner_batched", on), "tuning")
+        for on, sink in ((1, 256), (1, 8), (1, 1), (0, 256)):
+            capi.check(L.gf_set_tuning(b"runner_batched", on), "tuning")
+            capi.check(L.gf_set_tuning(b"sink_batch_chunks", sink), "tuning")
             ports, _ = capi.run_dense_chain(seed, n, 32, nodes=3, chunk_capacity=1024, live_particles=8192,
                                             batch_chunks=4)
             weights, capped, _ = capi.run_particle_feedback(seed, 50_000, chunk_capacity=1024, live_particles=4096,
                                                             batch_chunks=4)
-            out[on] = (ports, weights, capped)
+            out[(on, sink)] = (ports, weights, capped)
     finally:
-        capi.check(capi.lib().gf_set_tuning(b"runner_batched", 1), "tuning")
-    for a, b in zip(out[1], out[0]):
-        assert np.array_equal(a, b)
-    assert np.array_equal(out[1][0], _expect(n, 32, 3, "uniform", seed))
+        capi.check(L.gf_set_tuning(b"runner_batched", 1), "tuning")
+        capi.check(L.gf_set_tuning(b"sink_batch_chunks", 256), "tuning")
+    first = out[(1, 256)]
+    for key, res in out.items():
+        for a, b in zip(first, res):
+            assert np.array_equal(a, b), key
+    assert np.array_equal(first[0], _expect(n, 32, 3, "uniform", seed))
