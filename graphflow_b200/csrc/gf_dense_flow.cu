@@ -43,7 +43,7 @@ extern "C" gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins
         (layout != GF_LAYOUT_SOA && layout != GF_LAYOUT_AOS))
         return GF_ERR_ARGUMENT;
     return gf_flows_guard([&] {
-        cuda::Device device(0);
+        cuda::Device device = cuda::Device::current();
         device.makeCurrent();
         const std::size_t m = n ? n : 1u;
         cuda::Buffer<std::uint32_t> portOf(m);

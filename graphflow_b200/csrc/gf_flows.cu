@@ -91,7 +91,7 @@ gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visit
         (layout != GF_LAYOUT_SOA && layout != GF_LAYOUT_AOS))
         return GF_ERR_ARGUMENT;
     return guarded([&] {
-        cuda::Device device(0);
+        cuda::Device device = cuda::Device::current();
         device.makeCurrent();
         const std::size_t m = n ? n : 1u;
         cuda::Buffer<std::uint32_t> weights(m), capped(m);
@@ -138,7 +138,7 @@ gf_status gf_run_particle_feedback_kernel(uint64_t seed, uint64_t n, uint32_t ma
             throw std::overflow_error("graphflow::particle: particle ids exceed the RNG stream-id range");
         if (max_visits > rng::maxStreamEvent)
             throw std::overflow_error("graphflow::particle: max visits exceeds the RNG stream-event range");
-        cuda::Device device(0);
+        cuda::Device device = cuda::Device::current();
         device.makeCurrent();
         const std::size_t m = n ? n : 1u;
         cuda::Buffer<std::uint32_t> weights(m), capped(m), status(1);

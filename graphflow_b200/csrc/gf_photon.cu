@@ -24,7 +24,7 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
 {
     if (exec == GF_EXEC_FLOW && firstId != 0u)
         throw std::invalid_argument("graphflow::photon: a Flow run starts at id 0");
-    cuda::Device device(0);
+    cuda::Device device = cuda::Device::current();
     device.makeCurrent();
     const std::size_t m = n ? n : 1u;
     const bool wantRecords = hEvent || hSc || hW || hCos || hPos;

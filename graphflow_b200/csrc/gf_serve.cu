@@ -481,7 +481,7 @@ extern "C" gf_status gf_serve(const gf_request* h_requests, uint32_t n_requests,
             return GF_ERR_ARGUMENT;
     }
     return gf_flows_guard([&] {
-        cuda::Device device(0);
+        cuda::Device device = cuda::Device::current();
         device.makeCurrent();
         const std::uint32_t sms = device.multiProcessorCount();
         if (gf_photon_record_bytes_f32() != sizeof(PhotonRecordF32))

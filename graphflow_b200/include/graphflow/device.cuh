@@ -212,6 +212,14 @@ public:
         m_sms = static_cast<std::uint32_t>(p.multiProcessorCount);
         m_smemPerBlock = static_cast<std::uint32_t>(p.sharedMemPerBlockOptin);
     }
+    // The calling thread's current device (cudaSetDevice), as the C entry points use it.
+    static Device current()
+    {
+        int ordinal = 0;
+        if (cudaGetDevice(&ordinal) != cudaSuccess)
+            throw CudaError("graphflow::cuda::Device: no current CUDA device");
+        return Device(ordinal);
+    }
     int ordinal() const { return m_ordinal; }
     std::uint32_t multiProcessorCount() const { return m_sms; }
     std::uint32_t sharedMemPerBlock() const { return m_smemPerBlock; }

@@ -257,6 +257,8 @@ gf_status gf_generate_records16(void* stream, uint64_t seed, uint64_t first_id, 
                                 uint32_t k, uint64_t salt, const gf_rec16_columns* h_cols, int layout);
 
 /* ---- whole flows through the C++ front end (Flow / GraphRunner) ------------------------------ */
+/* The flow entry points (gf_run_particle_feedback*, gf_run_dense_chain, gf_run_photon) and the
+ * request server run on the calling thread's current CUDA device (cudaSetDevice). */
 
 /* Counters of one run (sched/GraphRunner.hpp:154-252 SchedulerStats, subset). */
 typedef struct gf_flow_stats {

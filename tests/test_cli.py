@@ -1,0 +1,100 @@
+"""The command-line drop-in for the reference's example binary graphFlow_particle_feedback
+(examples/particle_feedback/main.cpp, Cli.hpp): flags, exit codes and the printed report.
+
+The report format follows main.cpp:22-33 and 48-58: '# ...' lines, '# weight,count', one
+'weight,count' row per distinct final weight in ascending order, and '# non-terminating K' when the
+visit cap stopped K particles. The GPU tests check the rows against the oracle's scalar model
+(tests/reference/ScalarModel.hpp restated) and, at the reference's published configuration, the
+SHA-256 the reference published for its rows (docs/benchmarks.md:32-34).
+"""
+import hashlib
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from graphflow_b200 import capi
+from oracle import oracle as O
+
+
+def _run(*args, timeout=600):
+    assert os.path.exists(capi.CLI_PATH), "build the library first (graphflow_b200.capi.build())"
+    return subprocess.run([capi.CLI_PATH, *args], capture_output=True, text=True, timeout=timeout)
+
+
+def _rows(stdout):
+    lines = stdout.splitlines()
+    start = lines.index("# weight,count") + 1
+    rows = [ln for ln in lines[start:] if not ln.startswith("#")]
+    capped = [ln for ln in lines[start:] if ln.startswith("# non-terminating ")]
+    w = np.array([int(r.split(",")[0]) for r in rows], np.uint64)
+    c = np.array([int(r.split(",")[1]) for r in rows], np.uint64)
+    ncap = int(capped[0].split()[-1]) if capped else 0
+    return w, c, ncap, "".join(r + "\n" for r in rows)
+
+
+def test_cli_help():
+    r = _run("--help")
+    assert r.returncode == 0 and r.stdout.startswith("usage: graphflow_b200_particle_feedback")
+
+
+@pytest.mark.parametrize("args", [
+    ["--bogus"],
+    ["--particles"],                              # missing value
+    ["--particles", "-5"],
+    ["--particles", "18446744073709551616"],      # 2^64
+    ["--chunk-size", "0"],
+    ["--chunk-size", "4294967296"],               # 2^32
+    ["--backend", "cpu", "--particles", "10"],    # this build runs on CUDA only
+    ["--backend", "cuda", "--workload", "kernel"],
+    ["--backend", "cuda", "--bins", "64"],        # a kernel-workload flag without --workload kernel
+    ["--backend", "cuda", "--pool-mode", "arena"],
+    ["--backend", "cuda", "--workload", "both"],
+])
+def test_cli_rejects_bad_command_lines(args):
+    """Configuration errors exit 2 with the message and the usage text on stderr, before any
+    device work (Cli.hpp: parseOptions / resolveOptions throw std::invalid_argument)."""
+    r = _run(*args)
+    assert r.returncode == 2 and "usage:" in r.stderr and r.stdout == ""
+
+
+@pytest.mark.gpu
+def test_cli_config1_matches_the_scalar_model():
+    """Config 1 (N=1e6, seed 42, C=1024, P=4096, Q=1, 64 visits): the printed rows are the
+    oracle's histogram, they sum to N, and the non-terminating count is the oracle's."""
+    n = 1_000_000
+    r = _run("--backend", "cuda", "--particles", str(n), "--chunk-size", "1024", "--live-particles", "4096",
+             "--batch-chunks", "1", "--seed", "42", "--max-visits", "64")
+    assert r.returncode == 0, r.stderr
+    w, c, ncap, _ = _rows(r.stdout)
+    ew, _, encap = O.particle_scalar(42, n, 64)
+    erw, erc = O.histogram_u32(ew)
+    assert np.array_equal(w, erw.astype(np.uint64)) and np.array_equal(c, erc.astype(np.uint64))
+    assert int(c.sum()) == n and ncap == encap
+    head = r.stdout.splitlines()[0]
+    assert head.startswith("# graphFlow_particle_feedback backend=cuda") and f"particles={n}" in head
+
+
+@pytest.mark.gpu
+def test_cli_inert_flags_are_noted_and_change_nothing():
+    base = ["--backend", "cuda", "--particles", "20000", "--chunk-size", "1024", "--live-particles", "4096",
+            "--seed", "7"]
+    a = _run(*base)
+    b = _run(*base, "--frame-cap", "4", "--pool-mode", "slotArena", "--tile-size", "256")
+    assert a.returncode == 0 and b.returncode == 0
+    assert "--frame-cap has no effect" in b.stderr and "--tile-size has no effect" in b.stderr
+    assert _rows(a.stdout)[3] == _rows(b.stdout)[3]
+
+
+@pytest.mark.gpu
+def test_cli_published_configuration_reproduces_the_published_rows():
+    """N=1e8, C=8192, P=16384, Q=8, seed 42 (docs/benchmarks.md:24-34): the rows the binary prints
+    hash to the SHA-256 the reference published for its own run."""
+    r = _run("--backend", "cuda", "--particles", "100000000", "--chunk-size", "8192", "--live-particles", "16384",
+             "--batch-chunks", "8", "--seed", "42")
+    assert r.returncode == 0, r.stderr
+    w, c, _, text = _rows(r.stdout)
+    assert len(w) == 260 and int(c.sum()) == 100_000_000
+    assert hashlib.sha256(text.encode()).hexdigest() == (
+        "21ab0aeb9ec72d380af2ce6e9631f8fa7b9111d24ff7831f272aa9f6a7be9dab")
