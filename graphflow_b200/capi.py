@@ -36,6 +36,19 @@ class Tile(C.Structure):
     _fields_ = [("chunk_index", C.c_uint32), ("tile_offset", C.c_uint32), ("count", C.c_uint32)]
 
 
+class DeviceProps(C.Structure):
+    """gf_device_props: the device fields the C/P/T policy reads."""
+    _fields_ = [("sms", C.c_uint32), ("warp_size", C.c_uint32), ("max_threads_per_block", C.c_uint32),
+                ("max_blocks_per_grid", C.c_uint32), ("shared_mem_per_block", C.c_uint32),
+                ("global_mem_bytes", C.c_uint64)]
+
+
+class Policy(C.Structure):
+    """gf_policy: C, P, T and the payload budget chosen by gf_device_policy."""
+    _fields_ = [("chunk_capacity", C.c_uint32), ("live_particles", C.c_uint32), ("tile_size", C.c_uint32),
+                ("live_explicit", C.c_uint32), ("budget_bytes", C.c_uint64)]
+
+
 class OutDesc(C.Structure):
     _fields_ = [("chunk_index", C.c_uint32), ("fill", C.c_uint32), ("bin", C.c_uint32)]
 
@@ -75,6 +88,7 @@ _SIGS = {
     "gf_generate_records16": [_VP, _U64, _U64, _U64, _VP, _U32, _U64, _VP, _I32],
     "gf_run_particle_feedback": [_U64, _U64, _U32, _U32, _U32, _U32, _I32, _I32, _VP, _VP, _VP],
     "gf_set_tuning": [C.c_char_p, _I32],
+    "gf_device_policy": [_VP, _U64, _U32, _U32, _U32, _U32, _U64, _U64, _VP],
     "gf_run_particle_feedback_kernel": [_U64, _U64, _U32, _VP, _VP, _VP],
     "gf_serve": [_VP, _U32, _I32, _U64, _U32, _VP, _VP],
     "gf_histogram_scratch_bytes": [_U64, _VP],
@@ -338,6 +352,16 @@ def plan_dense(totals, capacity):
     check(lib().gf_plan_dense(totals.ctypes.data, totals.size, capacity, base.ctypes.data, fills.ctypes.data, cap,
                               C.byref(num)), "planDenseBins")
     return base[:totals.size], fills[:num.value], num.value
+
+
+def device_policy(n, props=None, chunk_capacity=0, live_particles=0, tile_size=0, live_per_chunk=0,
+                  budget_bytes=0, slot_bytes=0):
+    """gf_device_policy: the reference's default C, P, T for n particles on `props` (a DeviceProps,
+    or None for the current CUDA device); 0 means "derive". Raises GfError for impossible requests."""
+    out = Policy()
+    check(lib().gf_device_policy(C.byref(props) if props is not None else None, n, chunk_capacity, live_particles,
+                                 tile_size, live_per_chunk, budget_bytes, slot_bytes, C.byref(out)), "device policy")
+    return out
 
 
 def build_dense_table(bin_base, chunk_indices):

@@ -57,7 +57,8 @@ extern "C" gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins
         }
         Tuning t;
         t.seed = seed;
-        t.chunkCapacity = chunk_capacity;
+        if (chunk_capacity != 0u) // 0: the device policy derives C (and P with it)
+            t.chunkCapacity = chunk_capacity;
         if (live_particles != 0u)
             t.liveParticles = live_particles;
         t.batchChunks = batch_chunks;

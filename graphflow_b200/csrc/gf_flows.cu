@@ -66,6 +66,46 @@ uint32_t gf_runner_sink_batch(); // gf_capi.cu
 // Runs a front-end call, mapping its exceptions to gf_status and the last-error message.
 gf_status gf_flows_guard(const std::function<void()>& body) { return guarded(body); }
 
+gf_status gf_device_policy(const gf_device_props* h_props, uint64_t n, uint32_t chunk_capacity,
+                           uint32_t live_particles, uint32_t tile_size, uint32_t live_per_chunk,
+                           uint64_t budget_bytes, uint64_t slot_bytes, gf_policy* h_out)
+{
+    if (h_out == nullptr)
+        return GF_ERR_ARGUMENT;
+    return guarded([&] {
+        graphflow::DeviceProperties d;
+        if (h_props != nullptr) {
+            d.multiProcessorCount = h_props->sms;
+            d.warpSize = h_props->warp_size;
+            d.maxThreadsPerBlock = h_props->max_threads_per_block;
+            d.maxBlocksPerGrid = h_props->max_blocks_per_grid;
+            d.sharedMemPerBlockBytes = h_props->shared_mem_per_block;
+            d.globalMemBytes = h_props->global_mem_bytes;
+        } else {
+            d = graphflow::cuda::Device::current().getDeviceProperties();
+        }
+        graphflow::DevicePolicyOverrides o;
+        if (chunk_capacity != 0u)
+            o.chunkCapacity = chunk_capacity;
+        if (live_particles != 0u)
+            o.liveParticles = live_particles;
+        if (tile_size != 0u)
+            o.tileSize = tile_size;
+        graphflow::DevicePolicyConfig c;
+        if (live_per_chunk != 0u)
+            c.liveParticlesPerChunk = live_per_chunk;
+        c.memoryBudgetBytes = budget_bytes;
+        if (slot_bytes != 0u)
+            c.slotBytes = slot_bytes;
+        const graphflow::DevicePolicy p = graphflow::makeDevicePolicy(d, n, o, c);
+        h_out->chunk_capacity = p.chunkCapacity;
+        h_out->live_particles = p.liveParticles;
+        h_out->tile_size = p.tileSize;
+        h_out->live_explicit = p.liveParticlesExplicit ? 1u : 0u;
+        h_out->budget_bytes = p.memoryBudgetBytes;
+    });
+}
+
 // Records the message gf_last_error returns on this thread.
 void gf_set_last_error(const char* message) { g_last_error = message != nullptr ? message : ""; }
 
@@ -102,7 +142,8 @@ gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visit
         }
         Tuning t;
         t.seed = seed;
-        t.chunkCapacity = chunk_capacity;
+        if (chunk_capacity != 0u) // 0: the device policy derives C (and P with it)
+            t.chunkCapacity = chunk_capacity;
         if (live_particles != 0u)
             t.liveParticles = live_particles;
         t.batchChunks = batch_chunks;

@@ -51,7 +51,8 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
         if (exec == GF_EXEC_FLOW) {
             Tuning t;
             t.seed = seed;
-            t.chunkCapacity = C;
+            if (C != 0u) // 0: the device policy derives C (and P with it)
+                t.chunkCapacity = C;
             if (live != 0u)
                 t.liveParticles = live;
             t.batchChunks = Q;

@@ -6,13 +6,17 @@
 // the Flow (gf_run_particle_feedback) on the current CUDA device, then the sorted histogram on the
 // device (gf_histogram_u32) instead of the reference's host sort.
 //
-// Differences, by design: only --backend cuda runs (there is no CPU or other backend); C, P and T
-// default to C = 8192 and P = 8 C (the reference's accelerator P/C ratio, Cli.hpp resolveOptions)
-// instead of a device-policy derivation; the partition stages use 1024-particle tiles whatever
-// --tile-size says. Flags that configure parts of the reference this build does not have (frame
-// cap, occupancy target, pool budget and mode, per-chunk transform schedule) are parsed and
-// checked as the reference does and reported as inert on stderr. The kernel workload
-// (--workload kernel) is not part of this build.
+// C, P and T the command line leaves out come from the device policy (gf_device_policy, the
+// reference's makeDevicePolicy rules) with the accelerator ratio P/C = 8 unless an explicit C is
+// below the logical tile width, as Cli.hpp resolveOptions does; an explicit P above the run size or
+// the payload budget is a command-line error there and here.
+//
+// Differences, by design: only --backend cuda runs (there is no CPU or other backend); T shapes
+// the policy's C (a multiple of T) but the partition kernels keep their own 1024-particle tiles.
+// Flags that configure parts of the reference this build does not have (frame cap, occupancy
+// target, pool budget and mode, per-chunk transform schedule) are parsed and checked as the
+// reference does and reported as inert on stderr. The kernel workload (--workload kernel) is not
+// part of this build.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -30,9 +34,8 @@
 namespace {
 
 constexpr const char* kName = "graphflow_b200_particle_feedback";
-constexpr std::uint32_t kDefaultChunk = 8192u;
-constexpr std::uint32_t kLivePerChunk = 8u;
-constexpr std::uint32_t kTile = 1024u;
+constexpr std::uint32_t kAcceleratorLivePerChunk = 8u; // DevicePolicy.hpp:53
+constexpr std::uint32_t kLogicalTileWidth = 128u;      // DevicePolicyConfig::logicalTileWidth
 
 struct Options {
     bool help = false;
@@ -59,7 +62,8 @@ void usage(std::ostream& out)
            "       [--pool-mode fixed|slotArena] [--slot-arena-budget BYTES]\n"
            "       [--chunk-kernel-schedule off|perChunk] [--chunk-queue-depth D]\n"
            "       [--chunk-latency-cap-us U]\n"
-           "       defaults: C = 8192, P = 8 C, Q = 1, seed 0, 64 visits; tiles are 1024 particles.\n"
+           "       defaults: C, P and T from the device policy (the reference's rules), Q = 1,\n"
+           "       seed 0, 64 visits.\n"
            "       Output: '# ...' lines, '# weight,count', then one 'weight,count' row per distinct\n"
            "       final weight in ascending order, and '# non-terminating K' if K particles hit the cap.\n";
 }
@@ -230,17 +234,16 @@ int run(const Options& o)
         throw std::invalid_argument("--backend: this build runs on CUDA (sm_100a) only, got '" + o.backend + "'");
     if (o.workload == "kernel")
         throw std::invalid_argument("--workload kernel: the kernel workload is not part of this build");
-    const std::uint32_t C = o.chunkSize.value_or(kDefaultChunk);
-    if (!o.liveParticles && static_cast<std::uint64_t>(C) * kLivePerChunk > std::numeric_limits<std::uint32_t>::max())
-        throw std::invalid_argument("--chunk-size: the default P = 8 C exceeds 32 bits; give --live-particles");
-    const std::uint32_t P = o.liveParticles.value_or(C * kLivePerChunk);
     for (const auto& f : o.inert)
         std::cerr << kName << ": note: " << f << " has no effect in this build\n";
-    if (o.tileSize && *o.tileSize != kTile)
-        std::cerr << kName << ": note: --tile-size has no effect in this build (tiles are " << kTile
-                  << " particles)\n";
 
     cudaOrThrow(cudaSetDevice(static_cast<int>(o.device)), "cudaSetDevice");
+    const bool wideChunk = !o.chunkSize || *o.chunkSize >= kLogicalTileWidth;
+    gf_policy pol{};
+    if (gf_device_policy(nullptr, o.particles, o.chunkSize.value_or(0u), o.liveParticles.value_or(0u),
+                         o.tileSize.value_or(0u), wideChunk ? kAcceleratorLivePerChunk : 0u, 0u, 0u, &pol) != GF_OK)
+        throw std::invalid_argument(lastError());
+    const std::uint32_t C = pol.chunk_capacity, P = pol.live_particles, T = pol.tile_size;
     cudaDeviceProp prop{};
     cudaOrThrow(cudaGetDeviceProperties(&prop, static_cast<int>(o.device)), "cudaGetDeviceProperties");
 
@@ -258,7 +261,7 @@ int run(const Options& o)
 
     std::cout << "# graphFlow_particle_feedback backend=cuda device=" << o.device << " device-name=" << prop.name
               << " particles=" << o.particles << " chunk-size=" << C << " live-particles=" << P
-              << " tile-size=" << kTile << " batch-chunks=" << o.batchChunks << " seed=" << o.seed
+              << " tile-size=" << T << " batch-chunks=" << o.batchChunks << " seed=" << o.seed
               << " max-visits=" << o.maxVisits << '\n';
     std::cout << "# pool-chunks=" << st.pool_chunks << " peak-live-chunks=" << st.peak_live_chunks
               << " peak-reserved-chunks=" << st.peak_reserved_chunks << '\n';

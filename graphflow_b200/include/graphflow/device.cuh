@@ -14,6 +14,7 @@
 
 #include "core.hpp"
 #include "gf_device.cuh"
+#include "policy.hpp"
 
 namespace graphflow {
 
@@ -211,6 +212,12 @@ public:
             throw CudaError("graphflow::cuda::Device: no CUDA device " + std::to_string(ordinal));
         m_sms = static_cast<std::uint32_t>(p.multiProcessorCount);
         m_smemPerBlock = static_cast<std::uint32_t>(p.sharedMemPerBlockOptin);
+        m_props.multiProcessorCount = m_sms;
+        m_props.warpSize = static_cast<std::uint32_t>(p.warpSize);
+        m_props.maxThreadsPerBlock = static_cast<std::uint32_t>(p.maxThreadsPerBlock);
+        m_props.maxBlocksPerGrid = static_cast<std::uint32_t>(p.maxGridSize[0]);
+        m_props.sharedMemPerBlockBytes = static_cast<std::uint32_t>(p.sharedMemPerBlock);
+        m_props.globalMemBytes = static_cast<std::uint64_t>(p.totalGlobalMem);
     }
     // The calling thread's current device (cudaSetDevice), as the C entry points use it.
     static Device current()
@@ -223,11 +230,14 @@ public:
     int ordinal() const { return m_ordinal; }
     std::uint32_t multiProcessorCount() const { return m_sms; }
     std::uint32_t sharedMemPerBlock() const { return m_smemPerBlock; }
+    // The fields the device policy reads (alpaka's getDeviceProperties).
+    const DeviceProperties& getDeviceProperties() const { return m_props; }
     void makeCurrent() const { cudaSetDevice(m_ordinal); }
 
 private:
     int m_ordinal;
     std::uint32_t m_sms = 0u, m_smemPerBlock = 0u;
+    DeviceProperties m_props{};
 };
 
 inline void check(cudaError_t e, const char* what)

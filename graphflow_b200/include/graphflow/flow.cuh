@@ -283,14 +283,27 @@ private:
         c.maxBins = maxBins;
         c.batchChunks = m_tuning.batchChunks.value_or(1u);
         c.sinkBatchChunks = std::min(std::max(m_tuning.sinkBatchChunks, 1u), Tuning::kMaxSinkBatchChunks);
-        c.chunkCapacity = m_tuning.chunkCapacity.value_or(8192u);
+        // C and P the caller left out come from the device policy (core/DevicePolicy.hpp:344-614)
+        // with the accelerator P/C ratio of 8 and this storage's slot size, as Flow does there
+        std::optional<DevicePolicy> policy;
+        if (!m_tuning.chunkCapacity || !m_tuning.liveParticles) {
+            DevicePolicyConfig pc;
+            pc.liveParticlesPerChunk = DevicePolicyConfig::kAcceleratorLiveParticlesPerChunk;
+            pc.slotBytes = TStorage::slotBytes();
+            DevicePolicyOverrides ov;
+            ov.chunkCapacity = m_tuning.chunkCapacity;
+            if (ov.chunkCapacity)
+                pc.maxChunkCapacity = std::max(pc.maxChunkCapacity, *ov.chunkCapacity);
+            if (m_tuning.liveParticles && *m_tuning.liveParticles <= itemCount)
+                ov.liveParticles = m_tuning.liveParticles;
+            policy = makeDevicePolicy(m_device.getDeviceProperties(), itemCount, ov, pc);
+        }
+        c.chunkCapacity = m_tuning.chunkCapacity.value_or(policy ? policy->chunkCapacity : 8192u);
         c.tileSize = m_tuning.tileSize.value_or(1024u);
         c.scatterMode = m_tuning.scatterMode.value_or(ScatterMode::SharedStaging);
         c.binPath = m_tuning.binPath.value_or(BinPath::automatic);
         c.fused = m_tuning.fused;
-        // accelerator default P = min(N, 8C) (DevicePolicy.hpp:53)
-        const std::uint64_t defLive = std::min<std::uint64_t>(itemCount, 8ull * c.chunkCapacity);
-        c.liveParticles = m_tuning.liveParticles.value_or(static_cast<std::uint32_t>(defLive ? defLive : 1u));
+        c.liveParticles = m_tuning.liveParticles.value_or(policy && policy->liveParticles ? policy->liveParticles : 1u);
         std::uint64_t reserve = 0;
         for (const auto& n : m_nodes)
             if (n.role == NodeRole::transform)

@@ -256,9 +256,44 @@ gf_status gf_generate_keys_u32(void* stream, int dist, uint64_t seed, uint64_t f
 gf_status gf_generate_records16(void* stream, uint64_t seed, uint64_t first_id, uint64_t n, const double* d_cdf,
                                 uint32_t k, uint64_t salt, const gf_rec16_columns* h_cols, int layout);
 
+/* ---- device policy: default C, P and T (core/DevicePolicy.hpp:344-614 makeDevicePolicy) ------- */
+
+/* The fields of a device the policy reads (alpaka DeviceProperties subset). */
+typedef struct gf_device_props {
+    uint32_t sms;
+    uint32_t warp_size;
+    uint32_t max_threads_per_block;
+    uint32_t max_blocks_per_grid;
+    uint32_t shared_mem_per_block; /* bytes, default per-block limit */
+    uint64_t global_mem_bytes;
+} gf_device_props;
+
+typedef struct gf_policy {
+    uint32_t chunk_capacity; /* C */
+    uint32_t live_particles; /* P */
+    uint32_t tile_size;      /* T */
+    uint32_t live_explicit;  /* P came from the caller */
+    uint64_t budget_bytes;   /* payload budget the clamps used */
+} gf_policy;
+
+/* C, P and T for a run of n particles on h_props (NULL: the current CUDA device), with the
+ * reference's rules: T = 128 rounded to the warp and capped by a 2T-entry hash table in shared
+ * memory; C = waves x SMs x 4 x T capped by 8192 (or the explicit C), the grid, n and the payload
+ * budget, rounded to T; P = min(n, ratio x C) clamped so P x C x slot_bytes fits the budget, the
+ * budget being min(global memory / 8, 3 GiB) unless budget_bytes is given. 0 in chunk_capacity,
+ * live_particles, tile_size or budget_bytes means "derive"; live_per_chunk 0 means the
+ * reference's direct-call ratio 2 (the Flow uses 8); slot_bytes 0 means 24. An impossible request
+ * (explicit P above n or beyond the budget, explicit C above the maximum or the grid) returns
+ * GF_ERR_ARGUMENT with the reason in gf_last_error(). */
+gf_status gf_device_policy(const gf_device_props* h_props, uint64_t n, uint32_t chunk_capacity,
+                           uint32_t live_particles, uint32_t tile_size, uint32_t live_per_chunk,
+                           uint64_t budget_bytes, uint64_t slot_bytes, gf_policy* h_out);
+
 /* ---- whole flows through the C++ front end (Flow / GraphRunner) ------------------------------ */
 /* The flow entry points (gf_run_particle_feedback*, gf_run_dense_chain, gf_run_photon) and the
- * request server run on the calling thread's current CUDA device (cudaSetDevice). */
+ * request server run on the calling thread's current CUDA device (cudaSetDevice). A chunk_capacity
+ * or live_particles of 0 takes the device policy's C or P (gf_device_policy on that device with the
+ * Flow's ratio P/C = 8 and the flow's slot size). */
 
 /* Counters of one run (sched/GraphRunner.hpp:154-252 SchedulerStats, subset). */
 typedef struct gf_flow_stats {

@@ -83,8 +83,32 @@ def test_cli_inert_flags_are_noted_and_change_nothing():
     a = _run(*base)
     b = _run(*base, "--frame-cap", "4", "--pool-mode", "slotArena", "--tile-size", "256")
     assert a.returncode == 0 and b.returncode == 0
-    assert "--frame-cap has no effect" in b.stderr and "--tile-size has no effect" in b.stderr
+    assert "--frame-cap has no effect" in b.stderr and "--pool-mode has no effect" in b.stderr
     assert _rows(a.stdout)[3] == _rows(b.stdout)[3]
+
+
+@pytest.mark.gpu
+def test_cli_defaults_come_from_the_device_policy():
+    """Without --chunk-size / --live-particles the run takes the device policy's C and P (the
+    accelerator ratio 8 under the 3 GiB budget cap: C = 4096, P = 32768 on a B200), and the rows are
+    the oracle's whatever C and P are."""
+    n = 200_000
+    r = _run("--backend", "cuda", "--particles", str(n), "--seed", "5")
+    assert r.returncode == 0, r.stderr
+    pol = capi.device_policy(n, live_per_chunk=8)
+    head = r.stdout.splitlines()[0]
+    assert f"chunk-size={pol.chunk_capacity} " in head and f"live-particles={pol.live_particles} " in head
+    assert f"tile-size={pol.tile_size} " in head
+    w, c, ncap, _ = _rows(r.stdout)
+    ew, _, encap = O.particle_scalar(5, n, 64)
+    erw, erc = O.histogram_u32(ew)
+    assert np.array_equal(w, erw.astype(np.uint64)) and np.array_equal(c, erc.astype(np.uint64)) and ncap == encap
+
+
+@pytest.mark.gpu
+def test_cli_rejects_a_live_particle_count_above_the_run():
+    r = _run("--backend", "cuda", "--particles", "1000", "--live-particles", "2000")
+    assert r.returncode == 2 and "liveParticles" in r.stderr
 
 
 @pytest.mark.gpu

@@ -59,9 +59,18 @@ def test_feedback_config1_full():
 
 
 def test_feedback_invalid_configuration_is_reported():
-    with pytest.raises(capi.GfError) as e:
-        capi.run_particle_feedback(42, 100, 64, chunk_capacity=0)
-    assert e.value.code == capi.GF_ERR_ARGUMENT
+    """Configuration errors come back as GF_ERR_ARGUMENT before any device work (Config.hpp:233-349):
+    Q = 0, and a pool of 2^32 or more slots."""
+    for kw in (dict(batch_chunks=0), dict(chunk_capacity=1 << 20, live_particles=1 << 13)):
+        with pytest.raises(capi.GfError) as e:
+            capi.run_particle_feedback(42, 100_000, 64, **kw)
+        assert e.value.code == capi.GF_ERR_ARGUMENT, kw
+
+
+def test_feedback_default_chunk_and_live_counts_come_from_the_device_policy():
+    """chunk_capacity = 0 and live_particles = 0 take the device policy's C and P (Flow's ratio 8);
+    the results do not depend on them."""
+    _check(11, 300_000, 64, chunk_capacity=0, live_particles=0, batch_chunks=4)
 
 
 @pytest.mark.parametrize("n,seed,max_visits", [(1, 42, 64), (300_007, 42, 64), (100_000, 9, 0), (50_000, 3, 5)])
