@@ -13,6 +13,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_build", "libgraphflow_b200.so")
 # command-line drop-in for the reference's graphFlow_particle_feedback binary (built with the library)
 CLI_PATH = os.path.join(_HERE, "_build", "graphflow_b200_particle_feedback")
+PHOTON_CLI_PATH = os.path.join(_HERE, "_build", "graphflow_b200_photon_scattering")
 HEADER = os.path.join(os.path.dirname(_HERE), "include", "graphflow_b200.h")
 
 GF_OK, GF_INVALID, GF_OVERFLOW, GF_ERR_ARGUMENT, GF_ERR_RANGE, GF_ERR_LOGIC, GF_ERR_CUDA, GF_ERR_TIMEOUT, \

@@ -29,9 +29,16 @@
 #include <string_view>
 #include <vector>
 
+#include "cli_common.hpp"
 #include "graphflow_b200.h"
 
 namespace {
+
+using gfcli::cudaOrThrow;
+using gfcli::expectOneOf;
+using gfcli::lastError;
+using gfcli::parseU32;
+using gfcli::parseU64;
 
 constexpr const char* kName = "graphflow_b200_particle_feedback";
 constexpr std::uint32_t kAcceleratorLivePerChunk = 8u; // DevicePolicy.hpp:53
@@ -66,41 +73,6 @@ void usage(std::ostream& out)
            "       seed 0, 64 visits.\n"
            "       Output: '# ...' lines, '# weight,count', then one 'weight,count' row per distinct\n"
            "       final weight in ascending order, and '# non-terminating K' if K particles hit the cap.\n";
-}
-
-std::uint64_t parseU64(std::string_view flag, const std::string& value)
-{
-    if (value.empty() || value.find_first_not_of("0123456789") != std::string::npos)
-        throw std::invalid_argument(std::string(flag) + ": expected an unsigned integer, got '" + value + "'");
-    std::uint64_t v = 0u;
-    for (const char ch : value) {
-        const std::uint64_t d = static_cast<std::uint64_t>(ch - '0');
-        if (v > (std::numeric_limits<std::uint64_t>::max() - d) / 10u)
-            throw std::invalid_argument(std::string(flag) + ": value '" + value + "' exceeds 64 bits");
-        v = v * 10u + d;
-    }
-    return v;
-}
-
-std::uint32_t parseU32(std::string_view flag, const std::string& value, bool allowZero = false)
-{
-    const std::uint64_t v = parseU64(flag, value);
-    if (v > std::numeric_limits<std::uint32_t>::max())
-        throw std::invalid_argument(std::string(flag) + ": value '" + value + "' exceeds 32 bits");
-    if (!allowZero && v == 0u)
-        throw std::invalid_argument(std::string(flag) + ": value must be non-zero");
-    return static_cast<std::uint32_t>(v);
-}
-
-void expectOneOf(std::string_view flag, const std::string& value, std::initializer_list<std::string_view> allowed)
-{
-    for (const auto a : allowed)
-        if (value == a)
-            return;
-    std::string list;
-    for (const auto a : allowed)
-        list += (list.empty() ? "" : " or ") + std::string(a);
-    throw std::invalid_argument(std::string(flag) + ": expected " + list + ", got '" + value + "'");
 }
 
 Options parse(int argc, char** argv)
@@ -163,19 +135,6 @@ Options parse(int argc, char** argv)
     if (!o.kernelOnly.empty() && o.workload != "kernel")
         throw std::invalid_argument("--scatter, --bin-path, --bins and --distribution require --workload kernel");
     return o;
-}
-
-std::string lastError()
-{
-    char buf[512] = {0};
-    gf_last_error(buf, sizeof(buf));
-    return buf;
-}
-
-void cudaOrThrow(cudaError_t e, const char* what)
-{
-    if (e != cudaSuccess)
-        throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
 // Sorted (weight, count) rows of w on the device; the caller's stream is the default stream.

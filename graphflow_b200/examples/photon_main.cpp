@@ -1,0 +1,265 @@
+// graphflow_b200_photon_scattering: a command-line drop-in for the reference example binary
+// graphFlow_photon_scattering (examples/photon_scattering/main.cpp and PhotonCli.hpp). It takes the
+// same flags (with their short aliases --N, --L, --sigmaS, --sigmaA, --cap, --C, --P, --T, --Q) and
+// prints the same report: "# ..." provenance lines, "# event,count" with the transmitted,
+// reflected, absorbed and capped counts, "# outcome,scatter-count,count" rows in (outcome,
+// scatter count) order, "# terminal-sum,N" and "# inconsistent,K" (main.cpp:52-68 and
+// PhotonScattering.hpp:132-156: a photon is consistent when it reached exactly one terminal
+// event). The run is the reference example's analog model (absorption terminal, forward or
+// isotropic scattering) in FP64, the reference's CUDA precision, through gf_run_photon on the
+// current CUDA device; C, P and T the command line leaves out come from the device policy as in
+// PhotonCli.hpp resolveOptions.
+//
+// Differences, by design: only --backend cuda runs. --exec fused (default) carries each photon
+// through the same functors in one kernel and --exec flow runs the graph through the Flow; both
+// give identical histories. The output directory (--output-dir) and path traces (--trace-photons,
+// --trace-vertices) are not part of this build (its terminal records keep the exit cosine, not the
+// full direction, and no path vertices). Pool, frame-cap, occupancy and per-chunk-schedule flags
+// are checked as the reference does and reported inert on stderr. At most 65535 scatters per
+// photon (16-bit counter).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdlib>
+#include <iostream>
+#include <map>
+#include <optional>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "cli_common.hpp"
+#include "graphflow_b200.h"
+
+namespace {
+
+using gfcli::cudaOrThrow;
+using gfcli::expectOneOf;
+using gfcli::lastError;
+using gfcli::parseDouble;
+using gfcli::parseU32;
+using gfcli::parseU64;
+
+constexpr const char* kName = "graphflow_b200_photon_scattering";
+constexpr std::uint32_t kAcceleratorLivePerChunk = 8u; // DevicePolicy.hpp:53
+constexpr std::uint32_t kLogicalTileWidth = 128u;
+constexpr std::uint32_t kMaxScatters = 0xFFFFu;
+const char* const kEventName[5] = {"scatter", "transmitted", "reflected", "absorbed", "capped"};
+
+struct Options {
+    bool help = false;
+    std::string backend = "cpu";
+    std::uint64_t photons = 0u;
+    double thickness = 1.0, sigmaS = 0.0, sigmaA = 0.0;
+    std::string mode = "forward";
+    std::uint32_t maxScatters = 64u;
+    std::uint64_t seed = 0u;
+    std::optional<std::uint32_t> chunkSize, liveParticles, tileSize;
+    std::uint32_t batchChunks = 1u;
+    std::uint32_t device = 0u;
+    std::string exec = "fused";
+    std::vector<std::string> inert, unsupported;
+};
+
+void usage(std::ostream& out)
+{
+    out << "usage: " << kName << " --backend cuda [--device D]\n"
+           "                                        [--photons N] [--thickness L]\n"
+           "                                        [--sigma-s S] [--sigma-a A]\n"
+           "                                        [--mode forward|isotropic]\n"
+           "                                        [--max-scatters M] [--seed S]\n"
+           "                                        [--chunk-size C] [--live-particles P]\n"
+           "                                        [--tile-size T] [--batch-chunks Q]\n"
+           "                                        [--exec fused|flow]\n"
+           "       accepted for parity with graphFlow_photon_scattering, no effect here:\n"
+           "       [--occupancy-target D] [--frame-cap F] [--pool-budget-bytes B]\n"
+           "       [--pool-mode fixed|slotArena] [--slot-arena-budget BYTES]\n"
+           "       [--chunk-kernel-schedule off|perChunk] [--chunk-queue-depth D]\n"
+           "       [--chunk-latency-cap-us U]\n"
+           "       not part of this build: [--output-dir DIR] [--trace-photons M] [--trace-vertices V]\n"
+           "       defaults: L = 1, sigma-s = sigma-a = 0, forward, 64 scatters, seed 0; C, P and T from\n"
+           "       the device policy; --exec fused (the Flow and the fused kernel give identical results).\n";
+}
+
+Options parse(int argc, char** argv)
+{
+    Options o;
+    for (int i = 1; i < argc; ++i) {
+        const std::string flag = argv[i];
+        auto next = [&]() -> std::string {
+            if (i + 1 >= argc)
+                throw std::invalid_argument(flag + ": missing value");
+            return argv[++i];
+        };
+        if (flag == "--help" || flag == "-h") {
+            o.help = true;
+            return o;
+        } else if (flag == "--backend") {
+            o.backend = next();
+        } else if (flag == "--photons" || flag == "--N") {
+            o.photons = parseU64(flag, next());
+        } else if (flag == "--thickness" || flag == "--L") {
+            o.thickness = parseDouble(flag, next());
+        } else if (flag == "--sigma-s" || flag == "--sigmaS") {
+            o.sigmaS = parseDouble(flag, next());
+        } else if (flag == "--sigma-a" || flag == "--sigmaA") {
+            o.sigmaA = parseDouble(flag, next());
+        } else if (flag == "--mode") {
+            o.mode = next();
+            expectOneOf(flag, o.mode, {"forward", "isotropic"});
+        } else if (flag == "--max-scatters" || flag == "--cap") {
+            o.maxScatters = parseU32(flag, next(), true);
+        } else if (flag == "--seed") {
+            o.seed = parseU64(flag, next());
+        } else if (flag == "--chunk-size" || flag == "--C") {
+            o.chunkSize = parseU32(flag, next());
+        } else if (flag == "--live-particles" || flag == "--P") {
+            o.liveParticles = parseU32(flag, next());
+        } else if (flag == "--tile-size" || flag == "--T") {
+            o.tileSize = parseU32(flag, next());
+        } else if (flag == "--batch-chunks" || flag == "--Q") {
+            o.batchChunks = parseU32(flag, next());
+        } else if (flag == "--device") {
+            o.device = parseU32(flag, next(), true);
+        } else if (flag == "--exec") {
+            o.exec = next();
+            expectOneOf(flag, o.exec, {"fused", "flow"});
+        } else if (flag == "--frame-cap" || flag == "--chunk-queue-depth") {
+            parseU32(flag, next());
+            o.inert.push_back(flag);
+        } else if (flag == "--occupancy-target" || flag == "--chunk-latency-cap-us") {
+            parseU32(flag, next(), true);
+            o.inert.push_back(flag);
+        } else if (flag == "--pool-budget-bytes") {
+            if (parseU64(flag, next()) == 0u)
+                throw std::invalid_argument(flag + ": value must be non-zero");
+            o.inert.push_back(flag);
+        } else if (flag == "--slot-arena-budget") {
+            parseU64(flag, next());
+            o.inert.push_back(flag);
+        } else if (flag == "--pool-mode") {
+            expectOneOf(flag, next(), {"fixed", "slotArena"});
+            o.inert.push_back(flag);
+        } else if (flag == "--chunk-kernel-schedule") {
+            expectOneOf(flag, next(), {"off", "perChunk"});
+            o.inert.push_back(flag);
+        } else if (flag == "--output-dir") {
+            if (next().empty())
+                throw std::invalid_argument("--output-dir: value must not be empty");
+            o.unsupported.push_back(flag);
+        } else if (flag == "--trace-photons" || flag == "--trace-vertices") {
+            parseU32(flag, next(), true);
+            o.unsupported.push_back(flag);
+        } else {
+            throw std::invalid_argument("unknown argument '" + flag + "'");
+        }
+    }
+    return o;
+}
+
+int run(const Options& o)
+{
+    if (o.backend != "cuda")
+        throw std::invalid_argument("--backend: this build runs on CUDA (sm_100a) only, got '" + o.backend + "'");
+    if (!o.unsupported.empty())
+        throw std::invalid_argument(o.unsupported.front() + ": run outputs and path traces are not part of this build");
+    if (!(o.thickness > 0.0))
+        throw std::invalid_argument("--thickness: must be positive");
+    if (o.sigmaS < 0.0 || o.sigmaA < 0.0)
+        throw std::invalid_argument("--sigma-s / --sigma-a: must not be negative");
+    if (o.maxScatters > kMaxScatters)
+        throw std::invalid_argument("--max-scatters: at most 65535 in this build");
+    for (const auto& f : o.inert)
+        std::cerr << kName << ": note: " << f << " has no effect in this build\n";
+
+    cudaOrThrow(cudaSetDevice(static_cast<int>(o.device)), "cudaSetDevice");
+    cudaDeviceProp prop{};
+    cudaOrThrow(cudaGetDeviceProperties(&prop, static_cast<int>(o.device)), "cudaGetDeviceProperties");
+    const bool wideChunk = !o.chunkSize || *o.chunkSize >= kLogicalTileWidth;
+    gf_policy pol{};
+    if (gf_device_policy(nullptr, o.photons, o.chunkSize.value_or(0u), o.liveParticles.value_or(0u),
+                         o.tileSize.value_or(0u), wideChunk ? kAcceleratorLivePerChunk : 0u, 0u, 0u, &pol) != GF_OK)
+        throw std::invalid_argument(lastError());
+
+    gf_photon_params p{};
+    p.thickness = o.thickness;
+    p.sigma_s = o.sigmaS;
+    p.sigma_a = o.sigmaA;
+    p.max_scatters = o.maxScatters;
+    p.model = GF_PHOTON_ANALOG;
+    p.isotropic = o.mode == "isotropic" ? 1 : 0;
+    p.fp64 = 1;
+    const std::size_t m = o.photons ? o.photons : 1u;
+    std::vector<std::uint32_t> event(m), scatters(m);
+    std::vector<std::uint64_t> eventCounts(5, 0u);
+    gf_flow_stats st{};
+    if (gf_run_photon(o.seed, 0u, o.photons, &p, o.exec == "flow" ? GF_EXEC_FLOW : GF_EXEC_FUSED, pol.chunk_capacity,
+                      pol.live_particles, o.batchChunks, event.data(), scatters.data(), nullptr, nullptr, nullptr,
+                      nullptr, nullptr, eventCounts.data(), &st) != GF_OK)
+        throw std::runtime_error(lastError());
+
+    // outcome histogram over the delivered photons (PhotonScattering.hpp:132-156)
+    std::map<std::pair<std::uint32_t, std::uint32_t>, std::uint64_t> rows;
+    std::uint64_t counts[5] = {0u, 0u, 0u, 0u, 0u}, terminated = 0u, inconsistent = 0u;
+    for (std::uint64_t id = 0; id < o.photons; ++id) {
+        const std::uint32_t e = event[id];
+        if (e == 0u || e > 4u) {
+            ++inconsistent;
+            continue;
+        }
+        ++terminated;
+        ++counts[e];
+        ++rows[{e, scatters[id]}];
+    }
+
+    std::cout << "# graphFlow_photon_scattering backend=cuda device=" << o.device << " device-name=" << prop.name
+              << " photons=" << o.photons << " thickness=" << o.thickness << " sigma-s=" << o.sigmaS
+              << " sigma-a=" << o.sigmaA << " mode=" << o.mode << " max-scatters=" << o.maxScatters
+              << " seed=" << o.seed << " chunk-size=" << pol.chunk_capacity
+              << " live-particles=" << (o.photons ? pol.live_particles : 1u) << " tile-size=" << pol.tile_size
+              << " batch-chunks=" << o.batchChunks << " exec=" << o.exec << '\n';
+    std::cout << "# units length=1 coefficient=1/length\n";
+    std::cout << "# pool-chunks=" << st.pool_chunks << " peak-live-chunks=" << st.peak_live_chunks
+              << " peak-reserved-chunks=" << st.peak_reserved_chunks << '\n';
+    std::cout << "# scheduler completed-batches=" << st.completed_batches << " partition-batches="
+              << st.partition_batches << " kernel-launches=" << st.kernel_launches << " loop-iterations="
+              << st.loop_iterations << " seconds=" << st.seconds << '\n';
+    std::cout << "# event,count\n";
+    for (const std::uint32_t e : {1u, 2u, 3u, 4u})
+        std::cout << kEventName[e] << ',' << counts[e] << '\n';
+    std::cout << "# outcome,scatter-count,count\n";
+    for (const auto& [key, count] : rows)
+        std::cout << kEventName[key.first] << ',' << key.second << ',' << count << '\n';
+    std::cout << "# terminal-sum," << terminated << '\n';
+    std::cout << "# inconsistent," << inconsistent << '\n';
+    return EXIT_SUCCESS;
+}
+
+} // namespace
+
+int main(int argc, char** argv)
+{
+    Options o;
+    try {
+        o = parse(argc, argv);
+    } catch (const std::exception& e) {
+        std::cerr << kName << ": " << e.what() << '\n';
+        usage(std::cerr);
+        return 2;
+    }
+    if (o.help) {
+        usage(std::cout);
+        return EXIT_SUCCESS;
+    }
+    try {
+        return run(o);
+    } catch (const std::invalid_argument& e) {
+        std::cerr << kName << ": " << e.what() << '\n';
+        usage(std::cerr);
+        return 2;
+    } catch (const std::exception& e) {
+        std::cerr << kName << ": " << e.what() << '\n';
+        return 1;
+    }
+}

@@ -122,3 +122,85 @@ def test_cli_published_configuration_reproduces_the_published_rows():
     assert len(w) == 260 and int(c.sum()) == 100_000_000
     assert hashlib.sha256(text.encode()).hexdigest() == (
         "21ab0aeb9ec72d380af2ce6e9631f8fa7b9111d24ff7831f272aa9f6a7be9dab")
+
+
+# ---- graphflow_b200_photon_scattering (examples/photon_scattering/main.cpp, PhotonCli.hpp) ----
+
+def _prun(*args, timeout=600):
+    assert os.path.exists(capi.PHOTON_CLI_PATH), "build the library first (graphflow_b200.capi.build())"
+    return subprocess.run([capi.PHOTON_CLI_PATH, *args], capture_output=True, text=True, timeout=timeout)
+
+
+def _photon_report(stdout):
+    """(event counts by name, {(outcome, scatter count): count}, terminal-sum, inconsistent)."""
+    lines = stdout.splitlines()
+    ev_at, rows_at = lines.index("# event,count"), lines.index("# outcome,scatter-count,count")
+    events = {ln.split(",")[0]: int(ln.split(",")[1]) for ln in lines[ev_at + 1:rows_at]}
+    rows, term, bad = {}, None, None
+    for ln in lines[rows_at + 1:]:
+        if ln.startswith("# terminal-sum,"):
+            term = int(ln.split(",")[1])
+        elif ln.startswith("# inconsistent,"):
+            bad = int(ln.split(",")[1])
+        elif not ln.startswith("#"):
+            o, s, c = ln.split(",")
+            rows[(o, int(s))] = int(c)
+    return events, rows, term, bad
+
+
+def test_photon_cli_help():
+    r = _prun("--help")
+    assert r.returncode == 0 and r.stdout.startswith("usage: graphflow_b200_photon_scattering")
+
+
+@pytest.mark.parametrize("args", [
+    ["--bogus"],
+    ["--photons"],
+    ["--mode", "sideways"],
+    ["--thickness", "abc"],
+    ["--backend", "cpu"],
+    ["--backend", "cuda", "--thickness", "0"],
+    ["--backend", "cuda", "--sigma-s", "-1"],
+    ["--backend", "cuda", "--max-scatters", "70000"],            # the scatter counter is 16-bit here
+    ["--backend", "cuda", "--output-dir", "out"],                # no run-output directory in this build
+    ["--backend", "cuda", "--trace-photons", "4"],               # no path traces in this build
+    ["--backend", "cuda", "--pool-mode", "arena"],
+    ["--backend", "cuda", "--exec", "both"],
+])
+def test_photon_cli_rejects_bad_command_lines(args):
+    r = _prun(*args)
+    assert r.returncode == 2 and "usage:" in r.stderr and r.stdout == ""
+
+
+@pytest.mark.gpu
+def test_photon_cli_vacuum_transmits_every_photon_uncollided():
+    """sigma-s = sigma-a = 0 (the defaults): every photon leaves through the far face with no
+    scatter (the vacuum closed form of tests/integration/test_photon_scattering.cpp)."""
+    n = 10_000
+    r = _prun("--backend", "cuda", "--photons", str(n))
+    assert r.returncode == 0, r.stderr
+    events, rows, term, bad = _photon_report(r.stdout)
+    assert events == {"transmitted": n, "reflected": 0, "absorbed": 0, "capped": 0}
+    assert rows == {("transmitted", 0): n} and term == n and bad == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["forward", "isotropic"])
+def test_photon_cli_report_matches_the_library_and_both_execution_forms(mode):
+    """The printed outcome rows are the (event, scatter count) histogram of the same analog FP64
+    run through gf_run_photon, and --exec flow prints the same rows as --exec fused."""
+    n, seed = 100_000, 42
+    args = ["--backend", "cuda", "--photons", str(n), "--thickness", "1", "--sigma-s", "2", "--sigma-a", "0.5",
+            "--mode", mode, "--max-scatters", "64", "--seed", str(seed)]
+    fused, flow = _prun(*args), _prun(*args, "--exec", "flow", "--chunk-size", "4096", "--batch-chunks", "4")
+    assert fused.returncode == 0 and flow.returncode == 0, fused.stderr + flow.stderr
+    ev, rows, term, bad = _photon_report(fused.stdout)
+    assert _photon_report(flow.stdout) == (ev, rows, term, bad)
+    p = capi.photon_params(model=capi.PHOTON_ANALOG, thickness=1.0, sigma_s=2.0, sigma_a=0.5, max_scatters=64,
+                           isotropic=(mode == "isotropic"), fp64=True)
+    got = capi.run_photon(seed, n, p, exec_mode=capi.EXEC_FUSED)
+    names = {1: "transmitted", 2: "reflected", 3: "absorbed", 4: "capped"}
+    expect = {}
+    for e, s in zip(got["event"].tolist(), got["scatter_count"].tolist()):
+        expect[(names[e], s)] = expect.get((names[e], s), 0) + 1
+    assert rows == expect and term == n and bad == 0 and sum(ev.values()) == n
