@@ -743,11 +743,60 @@ def _cfg_tuning_and_graphs():
     return out
 
 
+def _cfg_histogram(n=100_000_000, cpu=True):
+    """The device histogram (ParticleTypes.hpp:206-219 histogramOf: sort + run-length encoding) of
+    N = 1e8 u32 values: the particle_feedback final weights (the published 260 rows) and uniform
+    values over the full 32-bit range (every 6-bit digit pass, ~1e8 rows). Device time with CUDA
+    events, buffers allocated beforehand; the oracle's host sort + RLE on a 1e7 sample beside it."""
+    import ctypes
+    import time
+    import numpy as np
+    import torch
+    from graphflow_b200 import capi
+    from oracle import oracle as O
+    L = capi.lib()
+    w, _, _ = capi.run_particle_feedback_kernel(42, n, 64)
+    gen = np.random.default_rng(SEED)
+    uniform = gen.integers(0, 1 << 32, size=n, dtype=np.uint64).astype(np.uint32)
+    need = ctypes.c_uint64()
+    capi.check(L.gf_histogram_scratch_bytes(n, ctypes.byref(need)), "scratch")
+    scratch = torch.empty((need.value + 255) // 8 + 32, dtype=torch.int64, device="cuda")
+    base = (scratch.data_ptr() + 255) & ~255
+    rows_v = torch.empty(n, dtype=torch.int32, device="cuda")
+    rows_c = torch.empty(n, dtype=torch.int64, device="cuda")
+    small = torch.zeros(2, dtype=torch.int32, device="cuda")
+    out = {"workload": f"histogramOf of N={n} u32 values on the device (radix passes of the stable "
+                       "cooperative partition + run-length encoding)"}
+    for name, vals in (("feedback_weights", w), ("uniform_u32", uniform)):
+        d = torch.from_numpy(vals.view(np.int32)).cuda()
+        stream = torch.cuda.current_stream()
+        times = []
+        for rep in range(4):
+            small.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            capi.check(L.gf_histogram_u32(stream.cuda_stream, d.data_ptr(), n, base, need.value, rows_v.data_ptr(),
+                                          rows_c.data_ptr(), small.data_ptr(), small[1:].data_ptr()), "histogram")
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if rep:
+                times.append(e0.elapsed_time(e1))
+        ms = float(np.median(times))
+        out[name] = {"ms": ms, "values_per_s": n / (ms / 1e3), "rows": int(small[0].item()),
+                     "status": int(small[1].item())}
+        del d
+    if cpu:
+        t = time.perf_counter()
+        O.histogram_u32(uniform[:10_000_000])
+        out["cpu_oracle_sort_rle_1e7_uniform"] = {"seconds": time.perf_counter() - t, "cores": 1, "kind": "port"}
+    return out
+
+
 def other_configs(peak):
     out = {}
     for name, f in (("particle_feedback", _cfg_particle_feedback), ("dense_flow", _cfg_dense_flow),
                     ("hash", lambda: _cfg_hash(peak)), ("photon", _cfg_photon), ("serving", _cfg_serving),
-                    ("tuning_and_graphs", _cfg_tuning_and_graphs)):
+                    ("tuning_and_graphs", _cfg_tuning_and_graphs), ("histogram", _cfg_histogram)):
         try:
             out[name] = f()
         except Exception as e:  # reported, never silent

@@ -26,11 +26,35 @@ struct DigitClassify {
     GF_D uint32_t operator()(uint32_t k) const { return (k >> shift) & (kHistBins - 1u); }
 };
 
+// AND and OR of all values (the digits that vary are the bits of AND ^ OR). A 16-byte-aligned
+// array is read as 128-bit words, four per thread in flight; the rest one value at a time.
 __global__ void and_or_kernel(const uint32_t* v, uint64_t n, uint32_t* ao)
 {
     uint32_t a = 0xFFFFFFFFu, o = 0u;
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint64_t scalar_from = 0u;
+    if ((reinterpret_cast<uintptr_t>(v) & 15u) == 0u) {
+        const uint4* v4 = reinterpret_cast<const uint4*>(v);
+        const uint64_t n4 = n / 4u;
+        auto take = [&](const uint4 x) {
+            a &= x.x & x.y & x.z & x.w;
+            o |= x.x | x.y | x.z | x.w;
+        };
+        uint64_t i = tid;
+        for (; i + 3u * stride < n4; i += 4u * stride) {
+            const uint4 x0 = __ldg(v4 + i), x1 = __ldg(v4 + i + stride), x2 = __ldg(v4 + i + 2u * stride),
+                        x3 = __ldg(v4 + i + 3u * stride);
+            take(x0);
+            take(x1);
+            take(x2);
+            take(x3);
+        }
+        for (; i < n4; i += stride)
+            take(__ldg(v4 + i));
+        scalar_from = n4 * 4u;
+    }
+    for (uint64_t i = scalar_from + tid; i < n; i += stride) {
         a &= v[i];
         o |= v[i];
     }
@@ -121,34 +145,54 @@ __global__ void hist_gather_kernel(const uint32_t* src, const gf_out_desc* descs
 }
 
 // Run-length encoding of a sorted array: a run starts at i = 0 and wherever s[i] != s[i - 1].
-GF_D uint32_t heads_of_thread(const uint32_t* s, uint64_t n, uint64_t first, uint32_t (&flag)[16])
+// Warp w of block b covers the 512 consecutive values [b kRleBlock + 512 w, + 512) in 16 rounds
+// of 32 lanes (coalesced loads); round k's heads are one ballot, so a head's run index is the
+// heads before it: the warp's base + the earlier rounds' popcounts + the lower lanes of this round.
+constexpr uint32_t kRleRounds = kRleBlock / 256u; // 256 threads = 8 warps x 512 values
+
+// Ballots of the warp's 16 rounds; v[k] = this lane's value of round k.
+GF_D void rle_heads(const uint32_t* s, uint64_t n, uint64_t base, uint32_t lane, uint32_t (&mask)[kRleRounds],
+                    uint32_t (&v)[kRleRounds])
 {
-    uint32_t c = 0;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        const uint64_t i = first + (uint64_t)k;
-        flag[k] = (i < n && (i == 0u || s[i] != s[i - 1u])) ? 1u : 0u;
-        c += flag[k];
+    for (uint32_t k = 0; k < kRleRounds; ++k) {
+        const uint64_t i = base + 32u * k + lane;
+        v[k] = i < n ? s[i] : 0u;
+        const bool head = i < n && (i == 0u || v[k] != s[i - 1u]);
+        mask[k] = __ballot_sync(0xFFFFFFFFu, head);
     }
-    return c;
+}
+
+// Heads before this warp in the block (exclusive over the 8 warps) and the block's total.
+GF_D uint32_t rle_block_prefix(uint32_t warp_heads, uint32_t w, uint32_t lane, uint32_t& total)
+{
+    __shared__ uint32_t ws[8];
+    if (lane == 0u)
+        ws[w] = warp_heads;
+    __syncthreads();
+    uint32_t before = 0;
+    total = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < 8u; ++i) {
+        before += i < w ? ws[i] : 0u;
+        total += ws[i];
+    }
+    return before;
 }
 
 __global__ void __launch_bounds__(256) rle_count_kernel(const uint32_t* s, uint64_t n, uint32_t* block_heads)
 {
-    uint32_t flag[16];
-    const uint64_t first = (uint64_t)blockIdx.x * kRleBlock + 16u * threadIdx.x;
-    uint32_t c = heads_of_thread(s, n, first, flag);
-    c = __reduce_add_sync(0xFFFFFFFFu, c);
-    __shared__ uint32_t ws[8];
-    if ((threadIdx.x & 31u) == 0u)
-        ws[threadIdx.x >> 5] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t t = 0;
-        for (int i = 0; i < 8; ++i)
-            t += ws[i];
-        block_heads[blockIdx.x] = t;
-    }
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    uint32_t mask[kRleRounds], v[kRleRounds];
+    rle_heads(s, n, (uint64_t)blockIdx.x * kRleBlock + 512u * w, lane, mask, v);
+    uint32_t c = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < kRleRounds; ++k)
+        c += (uint32_t)__popc(mask[k]);
+    uint32_t total = 0;
+    rle_block_prefix(c, w, lane, total);
+    if (threadIdx.x == 0)
+        block_heads[blockIdx.x] = total;
 }
 
 // Exclusive scan of the per-block head counts in place; *num_rows = the total (one CTA).
@@ -188,32 +232,25 @@ __global__ void __launch_bounds__(1024) rle_scan_kernel(uint32_t* block_heads, u
 __global__ void __launch_bounds__(256) rle_write_kernel(const uint32_t* s, uint64_t n, const uint32_t* block_base,
                                                         uint32_t* row_values, uint32_t* row_start)
 {
-    uint32_t flag[16];
-    const uint64_t first = (uint64_t)blockIdx.x * kRleBlock + 16u * threadIdx.x;
-    const uint32_t c = heads_of_thread(s, n, first, flag);
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
-    uint32_t incl = c;
+    const uint64_t base = (uint64_t)blockIdx.x * kRleBlock + 512u * w;
+    uint32_t mask[kRleRounds], v[kRleRounds];
+    rle_heads(s, n, base, lane, mask, v);
+    uint32_t c = 0;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if ((int)lane >= o)
-            incl += y;
-    }
-    __shared__ uint32_t ws[8];
-    if (lane == 31u)
-        ws[w] = incl;
-    __syncthreads();
-    uint32_t before = 0;
-    for (uint32_t i = 0; i < w; ++i)
-        before += ws[i];
-    uint32_t r = block_base[blockIdx.x] + before + incl - c;
+    for (uint32_t k = 0; k < kRleRounds; ++k)
+        c += (uint32_t)__popc(mask[k]);
+    uint32_t total = 0;
+    uint32_t r = block_base[blockIdx.x] + rle_block_prefix(c, w, lane, total);
+    const uint32_t below = (1u << lane) - 1u;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        if (flag[k]) {
-            row_values[r] = s[first + k];
-            row_start[r] = (uint32_t)(first + k);
-            ++r;
+    for (uint32_t k = 0; k < kRleRounds; ++k) {
+        if ((mask[k] >> lane) & 1u) {
+            const uint32_t q = r + (uint32_t)__popc(mask[k] & below);
+            row_values[q] = v[k];
+            row_start[q] = (uint32_t)(base + 32u * k + lane);
         }
+        r += (uint32_t)__popc(mask[k]);
     }
 }
 
@@ -352,19 +389,13 @@ gf_status gf_histogram_u32(void* stream, const uint32_t* d_values, uint64_t n, v
         const uint32_t n_chunks = any ? (uint32_t)L.R : (uint32_t)L.n_in;
         hist_tiles_kernel<<<(n_chunks + 255u) / 256u, 256, 0, s>>>(n, n_chunks, any ? descs : nullptr, num_out,
                                                                    tiles);
+        // the pass also writes its chunk table, descriptors and output count (no finish launch)
         e = launch_fused_coop<CoopShape<32>>(s, DigitClassify{shift}, in, out, kHistC, L.region, tiles,
                                                  2u * n_chunks, kHistBins, reserved, (uint32_t)L.R, totals,
-                                                 port_chunks, (uint32_t)L.max_k, ctl, kCoopScratch, d_status, sms);
+                                                 port_chunks, (uint32_t)L.max_k, ctl, kCoopScratch, d_status, sms,
+                                                 InlineFinish{table, descs, (uint32_t)L.R, num_out});
         if (e != cudaSuccess)
             return GF_ERR_CUDA;
-        constexpr int FT = 1024;
-        const size_t fsmem = sizeof(uint32_t) * (4096u * 2u + FT / 32 + 1);
-        e = cudaFuncSetAttribute(fused_finish_kernel<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem);
-        if (e != cudaSuccess)
-            return GF_ERR_CUDA;
-        fused_finish_kernel<FT><<<1, FT, fsmem, s>>>(totals, port_chunks, kHistBins, kHistC, FastDiv(kHistC),
-                                                      (uint32_t)L.max_k, ctl, table, descs, (uint32_t)L.R, num_out,
-                                                      d_status);
         any = true;
         std::swap(in, out); // the next pass reads this pass's output region
     }
