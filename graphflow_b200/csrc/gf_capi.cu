@@ -96,12 +96,6 @@ bool valid_classifier(int cls)
     return cls == GF_CLS_KEY_MOD || cls == GF_CLS_ID_BALANCED || cls == GF_CLS_ID_ONEHOT || cls == GF_CLS_ID_SKEWED;
 }
 
-uint32_t launch_frames(uint32_t n_tiles, size_t smem_bytes)
-{
-    (void)smem_bytes;
-    return n_tiles;
-}
-
 } // namespace
 } // namespace gf
 
@@ -162,7 +156,7 @@ gf_status gf_classify_dense_u32(void* stream, const uint32_t* d_keys, uint32_t c
             return cuda_status(e);
         Acc acc{d_keys, nullptr};
         KeyClassify<Acc> cls{key_classifier(classifier, bins)};
-        kernel<<<launch_frames(n_tiles, smem), Shape::kThreads, smem, as_stream(stream)>>>(
+        kernel<<<n_tiles, Shape::kThreads, smem, as_stream(stream)>>>(
             acc, cls, capacity, pool_slots, d_tiles, n_tiles, bins, d_bin_ids, d_counts, d_status);
         return cuda_status(cudaGetLastError());
     });
@@ -197,7 +191,7 @@ gf_status gf_scatter_dense_u32(void* stream, const uint32_t* d_keys_in, uint32_t
         cudaError_t e = allow_smem(kernel, smem);
         if (e != cudaSuccess)
             return cuda_status(e);
-        kernel<<<launch_frames(n_tiles, smem), Shape::kThreads, smem, as_stream(stream)>>>(
+        kernel<<<n_tiles, Shape::kThreads, smem, as_stream(stream)>>>(
             acc, NoUpdate{}, 0u, capacity, fdc, pool_slots, d_tiles, n_tiles, bins, d_bin_ids, d_table, d_next,
             d_counts, d_status);
         return cuda_status(cudaGetLastError());
