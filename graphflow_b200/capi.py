@@ -95,7 +95,8 @@ _SIGS = {
     "gf_histogram_scratch_bytes": [_U64, _VP],
     "gf_histogram_u32": [_VP, _VP, _U64, _VP, _U64, _VP, _VP, _VP, _VP],
     "gf_run_dense_chain": [_U64, _U64, _U32, _U32, _I32, C.c_double, _U32, _U32, _U32, _I32, _I32, _VP, _VP],
-    "gf_run_photon": [_U64, _U64, _U64, _VP, _I32, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP],
+    "gf_run_photon": [_U64, _U64, _U64, _VP, _I32, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
+                      _VP],
 }
 
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
@@ -142,6 +143,7 @@ def run_photon(seed, n, params, exec_mode=EXEC_FUSED, first_id=0, chunk_capacity
         out["weight"] = np.zeros(m, np.float64)
         out["cos_exit"] = np.zeros(m, np.float64)
         out["position"] = np.zeros(3 * m, np.float64)
+        out["direction"] = np.zeros(3 * m, np.float64)
     hb = max(params.hist_bins, 1)
     out["refl"] = np.zeros(hb, np.float64)
     out["trans"] = np.zeros(hb, np.float64)
@@ -150,7 +152,7 @@ def run_photon(seed, n, params, exec_mode=EXEC_FUSED, first_id=0, chunk_capacity
     ptr = (lambda k: out[k].ctypes.data) if records else (lambda k: None)
     rc = lib().gf_run_photon(seed, first_id, n, C.byref(params), exec_mode, chunk_capacity, live_particles,
                              batch_chunks, ptr("event"), ptr("scatter_count"), ptr("weight"), ptr("cos_exit"),
-                             ptr("position"), out["refl"].ctypes.data, out["trans"].ctypes.data,
+                             ptr("position"), ptr("direction"), out["refl"].ctypes.data, out["trans"].ctypes.data,
                              out["event_counts"].ctypes.data, C.byref(stats))
     if rc != GF_OK:
         raise GfError(rc, "photon: " + last_error())
@@ -158,6 +160,7 @@ def run_photon(seed, n, params, exec_mode=EXEC_FUSED, first_id=0, chunk_capacity
         for k in ("event", "scatter_count", "weight", "cos_exit"):
             out[k] = out[k][:n]
         out["position"] = out["position"][:3 * n].reshape(-1, 3)
+        out["direction"] = out["direction"][:3 * n].reshape(-1, 3)
     out["stats"] = stats
     return out
 

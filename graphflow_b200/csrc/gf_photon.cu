@@ -20,14 +20,15 @@ using namespace graphflow::photon;
 template <typename T>
 void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const gf_photon_params& P, int exec,
               std::uint32_t C, std::uint32_t live, std::uint32_t Q, uint32_t* hEvent, uint32_t* hSc, double* hW,
-              double* hCos, double* hPos, double* hRefl, double* hTrans, uint64_t* hCounts, gf_flow_stats* hStats)
+              double* hCos, double* hPos, double* hDir, double* hRefl, double* hTrans, uint64_t* hCounts,
+              gf_flow_stats* hStats)
 {
     if (exec == GF_EXEC_FLOW && firstId != 0u)
         throw std::invalid_argument("graphflow::photon: a Flow run starts at id 0");
     cuda::Device device = cuda::Device::current();
     device.makeCurrent();
     const std::size_t m = n ? n : 1u;
-    const bool wantRecords = hEvent || hSc || hW || hCos || hPos;
+    const bool wantRecords = hEvent || hSc || hW || hCos || hPos || hDir;
     cuda::Buffer<TerminalT<T>> records(wantRecords ? m : 1u);
     cuda::Buffer<std::uint32_t> visits(m);
     const std::uint32_t hb = P.model == GF_PHOTON_WEIGHTED ? P.hist_bins : 0u;
@@ -105,6 +106,11 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
                 hPos[3 * i + 1] = r[i].position.y;
                 hPos[3 * i + 2] = r[i].position.z;
             }
+            if (hDir) {
+                hDir[3 * i] = r[i].direction.x;
+                hDir[3 * i + 1] = r[i].direction.y;
+                hDir[3 * i + 2] = r[i].direction.z;
+            }
         }
     }
     if (hb && (hRefl || hTrans)) {
@@ -141,7 +147,8 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
 extern "C" gf_status gf_run_photon(uint64_t seed, uint64_t first_id, uint64_t n, const gf_photon_params* h_params,
                                    int exec, uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks,
                                    uint32_t* h_event, uint32_t* h_scatter_count, double* h_weight, double* h_cos_exit,
-                                   double* h_position, double* h_refl, double* h_trans, uint64_t* h_event_counts,
+                                   double* h_position, double* h_direction, double* h_refl, double* h_trans,
+                                   uint64_t* h_event_counts,
                                    gf_flow_stats* h_stats)
 {
     if (h_params == nullptr || (exec != GF_EXEC_FLOW && exec != GF_EXEC_FUSED) ||
@@ -157,11 +164,13 @@ extern "C" gf_status gf_run_photon(uint64_t seed, uint64_t first_id, uint64_t n,
     return gf_flows_guard([&] {
         if (P.fp64)
             runTyped<double>(seed, first_id, n, P, exec, chunk_capacity, live_particles, batch_chunks, h_event,
-                             h_scatter_count, h_weight, h_cos_exit, h_position, h_refl, h_trans, h_event_counts,
+                             h_scatter_count, h_weight, h_cos_exit, h_position, h_direction, h_refl, h_trans,
+                             h_event_counts,
                              h_stats);
         else
             runTyped<float>(seed, first_id, n, P, exec, chunk_capacity, live_particles, batch_chunks, h_event,
-                            h_scatter_count, h_weight, h_cos_exit, h_position, h_refl, h_trans, h_event_counts,
+                            h_scatter_count, h_weight, h_cos_exit, h_position, h_direction, h_refl, h_trans,
+                             h_event_counts,
                             h_stats);
     });
 }

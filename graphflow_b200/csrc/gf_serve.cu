@@ -72,9 +72,9 @@ __global__ void digest_feedback_kernel(const std::uint32_t* weights, const std::
     add_digest(acc, sum);
 }
 
-struct PhotonRecordF32 { // TerminalT<float> as stored (event, scatter count, weight, cos, position)
+struct PhotonRecordF32 { // TerminalT<float> as stored (event, scatter count, weight, cos, position, direction)
     std::uint32_t event, scatterCount;
-    float weight, cosExit, x, y, z;
+    float weight, cosExit, x, y, z, ux, uy, uz;
 };
 
 __global__ void digest_photon_kernel(const PhotonRecordF32* rec, std::uint64_t n, unsigned long long* acc)
@@ -440,7 +440,7 @@ gf_status runPlain(const gf_request& r, std::uint64_t& digest)
         std::vector<double> w(m), cs(m);
         gf_flow_stats st{};
         const gf_status rc = gf_run_photon(r.seed, 0u, r.n, &p, GF_EXEC_FLOW, 8192u, 0u, 8u, ev.data(), nullptr,
-                                           w.data(), cs.data(), nullptr, nullptr, nullptr, nullptr, &st);
+                                           w.data(), cs.data(), nullptr, nullptr, nullptr, nullptr, nullptr, &st);
         std::uint64_t d = 0;
         for (std::uint64_t i = 0; i < r.n; ++i) {
             const float wf = static_cast<float>(w[i]), cf = static_cast<float>(cs[i]);

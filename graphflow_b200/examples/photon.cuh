@@ -67,6 +67,7 @@ struct TerminalT {
     T weight;
     T cosExit;
     Vec3T<T> position;
+    Vec3T<T> direction; // at the terminal event (the exit direction for the two exits)
 };
 
 template <typename T>
@@ -308,7 +309,7 @@ struct RecordTerminalT {
         }
         const T c = fabs(p.direction.z);
         if (records != nullptr)
-            records[p.id] = TerminalT<T>{ev, p.scatterCount, p.weight, c, p.position};
+            records[p.id] = TerminalT<T>{ev, p.scatterCount, p.weight, c, p.position, p.direction};
         if (visits != nullptr && atomicAdd(&visits[p.id], 1u) != 0u)
             st.set(StatusCode::invalid);
         if (eventCounts != nullptr)

@@ -10,17 +10,26 @@
 // current CUDA device; C, P and T the command line leaves out come from the device policy as in
 // PhotonCli.hpp resolveOptions.
 //
+// --output-dir DIR writes the reference's run files (PhotonOutput.hpp:91-197 writeRunOutputs):
+// metadata.csv, outcomes.csv, scatter_histogram.csv, exits.csv (one row per transmitted or
+// reflected photon with its exit position and direction, 17 significant digits), and traces.csv /
+// trace_summary.csv with their headers only.
+//
 // Differences, by design: only --backend cuda runs. --exec fused (default) carries each photon
 // through the same functors in one kernel and --exec flow runs the graph through the Flow; both
-// give identical histories. The output directory (--output-dir) and path traces (--trace-photons,
-// --trace-vertices) are not part of this build (its terminal records keep the exit cosine, not the
-// full direction, and no path vertices). Pool, frame-cap, occupancy and per-chunk-schedule flags
-// are checked as the reference does and reported inert on stderr. At most 65535 scatters per
-// photon (16-bit counter).
+// give identical histories. Path traces are not recorded: --trace-photons / --trace-vertices take
+// 0 only. Pool, frame-cap, occupancy and per-chunk-schedule flags are checked as the reference does
+// and reported inert on stderr; provenance keys of metadata.csv that name the reference's build
+// (commit, alpaka pin, source directories) are written empty. At most 65535 scatters per photon
+// (16-bit counter).
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <cstdlib>
+#include <filesystem>
+#include <fstream>
+#include <iomanip>
 #include <iostream>
 #include <map>
 #include <optional>
@@ -59,6 +68,9 @@ struct Options {
     std::uint32_t batchChunks = 1u;
     std::uint32_t device = 0u;
     std::string exec = "fused";
+    std::uint32_t frameCap = 8u; // LaunchPolicy.hpp:18 defaultFrameCap (inert here, recorded in metadata)
+    std::optional<std::string> outputDir;
+    std::string command;
     std::vector<std::string> inert, unsupported;
 };
 
@@ -77,7 +89,9 @@ void usage(std::ostream& out)
            "       [--pool-mode fixed|slotArena] [--slot-arena-budget BYTES]\n"
            "       [--chunk-kernel-schedule off|perChunk] [--chunk-queue-depth D]\n"
            "       [--chunk-latency-cap-us U]\n"
-           "       not part of this build: [--output-dir DIR] [--trace-photons M] [--trace-vertices V]\n"
+           "       [--output-dir DIR]   the reference's run files (metadata, outcomes, scatter histogram,\n"
+           "                            exits; trace files with headers only)\n"
+           "       not part of this build: --trace-photons M / --trace-vertices V with M, V > 0\n"
            "       defaults: L = 1, sigma-s = sigma-a = 0, forward, 64 scatters, seed 0; C, P and T from\n"
            "       the device policy; --exec fused (the Flow and the fused kernel give identical results).\n";
 }
@@ -85,6 +99,8 @@ void usage(std::ostream& out)
 Options parse(int argc, char** argv)
 {
     Options o;
+    for (int i = 0; i < argc; ++i)
+        o.command += (i ? " " : "") + std::string(argv[i]);
     for (int i = 1; i < argc; ++i) {
         const std::string flag = argv[i];
         auto next = [&]() -> std::string {
@@ -125,7 +141,10 @@ Options parse(int argc, char** argv)
         } else if (flag == "--exec") {
             o.exec = next();
             expectOneOf(flag, o.exec, {"fused", "flow"});
-        } else if (flag == "--frame-cap" || flag == "--chunk-queue-depth") {
+        } else if (flag == "--frame-cap") {
+            o.frameCap = parseU32(flag, next());
+            o.inert.push_back(flag);
+        } else if (flag == "--chunk-queue-depth") {
             parseU32(flag, next());
             o.inert.push_back(flag);
         } else if (flag == "--occupancy-target" || flag == "--chunk-latency-cap-us") {
@@ -145,12 +164,12 @@ Options parse(int argc, char** argv)
             expectOneOf(flag, next(), {"off", "perChunk"});
             o.inert.push_back(flag);
         } else if (flag == "--output-dir") {
-            if (next().empty())
+            o.outputDir = next();
+            if (o.outputDir->empty())
                 throw std::invalid_argument("--output-dir: value must not be empty");
-            o.unsupported.push_back(flag);
         } else if (flag == "--trace-photons" || flag == "--trace-vertices") {
-            parseU32(flag, next(), true);
-            o.unsupported.push_back(flag);
+            if (parseU32(flag, next(), true) != 0u)
+                o.unsupported.push_back(flag);
         } else {
             throw std::invalid_argument("unknown argument '" + flag + "'");
         }
@@ -163,7 +182,7 @@ int run(const Options& o)
     if (o.backend != "cuda")
         throw std::invalid_argument("--backend: this build runs on CUDA (sm_100a) only, got '" + o.backend + "'");
     if (!o.unsupported.empty())
-        throw std::invalid_argument(o.unsupported.front() + ": run outputs and path traces are not part of this build");
+        throw std::invalid_argument(o.unsupported.front() + ": path traces are not part of this build");
     if (!(o.thickness > 0.0))
         throw std::invalid_argument("--thickness: must be positive");
     if (o.sigmaS < 0.0 || o.sigmaA < 0.0)
@@ -192,11 +211,13 @@ int run(const Options& o)
     p.fp64 = 1;
     const std::size_t m = o.photons ? o.photons : 1u;
     std::vector<std::uint32_t> event(m), scatters(m);
+    std::vector<double> position(o.outputDir ? 3u * m : 0u), direction(o.outputDir ? 3u * m : 0u);
     std::vector<std::uint64_t> eventCounts(5, 0u);
     gf_flow_stats st{};
     if (gf_run_photon(o.seed, 0u, o.photons, &p, o.exec == "flow" ? GF_EXEC_FLOW : GF_EXEC_FUSED, pol.chunk_capacity,
-                      pol.live_particles, o.batchChunks, event.data(), scatters.data(), nullptr, nullptr, nullptr,
-                      nullptr, nullptr, eventCounts.data(), &st) != GF_OK)
+                      pol.live_particles, o.batchChunks, event.data(), scatters.data(), nullptr, nullptr,
+                      o.outputDir ? position.data() : nullptr, o.outputDir ? direction.data() : nullptr, nullptr,
+                      nullptr, eventCounts.data(), &st) != GF_OK)
         throw std::runtime_error(lastError());
 
     // outcome histogram over the delivered photons (PhotonScattering.hpp:132-156)
@@ -233,6 +254,90 @@ int run(const Options& o)
         std::cout << kEventName[key.first] << ',' << key.second << ',' << count << '\n';
     std::cout << "# terminal-sum," << terminated << '\n';
     std::cout << "# inconsistent," << inconsistent << '\n';
+
+    if (o.outputDir) {
+        const std::filesystem::path dir(*o.outputDir);
+        std::filesystem::create_directories(dir);
+        std::ofstream meta(dir / "metadata.csv"), outcomes(dir / "outcomes.csv"), hist(dir / "scatter_histogram.csv"),
+            exits(dir / "exits.csv"), traces(dir / "traces.csv"), summary(dir / "trace_summary.csv");
+        if (!meta || !outcomes || !hist || !exits || !traces || !summary)
+            throw std::runtime_error("cannot create the output files in '" + *o.outputDir + "'");
+        outcomes << "event,count\n";
+        for (const std::uint32_t e : {1u, 2u, 3u, 4u})
+            outcomes << kEventName[e] << ',' << counts[e] << '\n';
+        hist << "event,scatter_count,count\n";
+        for (const auto& [key, count] : rows)
+            hist << kEventName[key.first] << ',' << key.second << ',' << count << '\n';
+        exits << "id,event,scatter_count,x,y,z,ux,uy,uz,cos_theta,phi_rad,transverse_x,transverse_y\n";
+        exits << std::setprecision(17);
+        for (std::uint64_t id = 0; id < o.photons; ++id) {
+            if (event[id] != 1u && event[id] != 2u)
+                continue;
+            const double* x = &position[3u * id];
+            const double* u = &direction[3u * id];
+            exits << id << ',' << kEventName[event[id]] << ',' << scatters[id] << ',' << x[0] << ',' << x[1] << ','
+                  << x[2] << ',' << u[0] << ',' << u[1] << ',' << u[2] << ',' << u[2] << ',' << std::atan2(u[1], u[0])
+                  << ',' << x[0] << ',' << x[1] << '\n';
+        }
+        traces << "id,step,kind,scatter_count,x,y,z,ux,uy,uz\n";
+        summary << "id,vertices,truncated\n";
+        auto quote = [](const std::string& v) {
+            std::string q = "\"";
+            for (const char c : v)
+                q += c == '"' ? std::string("\"\"") : std::string(1, c);
+            return q + "\"";
+        };
+        auto kv = [&](const char* key, const std::string& value) { meta << key << ',' << quote(value) << '\n'; };
+        auto kn = [&](const char* key, auto value) { kv(key, std::to_string(value)); };
+        meta << "key,value\n";
+        kv("schema_version", "1");
+        kv("graphflow_commit", "");
+        kv("alpaka_pin", "");
+        kv("graphflow_source_dir", "");
+        kv("alpaka_source_dir", "");
+        kv("backend", "cuda");
+        kn("device_index", o.device);
+        kv("device_name", prop.name);
+        kv("device_api", "cuda");
+        kn("multiprocessor_count", prop.multiProcessorCount);
+        kn("warp_size", prop.warpSize);
+        kn("global_mem_bytes", static_cast<std::uint64_t>(prop.totalGlobalMem));
+        kv("command", o.command);
+        kv("units", "length=1 coefficient=1/length angle=rad");
+        kn("photons", o.photons);
+        kn("thickness", o.thickness);
+        kn("sigma_s", o.sigmaS);
+        kn("sigma_a", o.sigmaA);
+        kn("sigma_t", o.sigmaS + o.sigmaA);
+        kv("mode", o.mode);
+        kn("max_scatters", o.maxScatters);
+        kn("seed", o.seed);
+        kn("chunk_size", pol.chunk_capacity);
+        kn("live_particles", o.photons ? pol.live_particles : 1u);
+        kn("tile_size", pol.tile_size);
+        kn("batch_chunks", o.batchChunks);
+        kn("frame_cap", o.frameCap);
+        kn("pool_chunks", st.pool_chunks);
+        kn("peak_live_chunks", st.peak_live_chunks);
+        kn("peak_reserved_chunks", st.peak_reserved_chunks);
+        kv("scheduler_stats", "completed-batches=" + std::to_string(st.completed_batches) +
+                                  " partition-batches=" + std::to_string(st.partition_batches) +
+                                  " kernel-launches=" + std::to_string(st.kernel_launches));
+        kn("count_terminated", terminated);
+        kn("count_inconsistent", inconsistent);
+        kn("count_transmitted", counts[1]);
+        kn("count_reflected", counts[2]);
+        kn("count_absorbed", counts[3]);
+        kn("count_capped", counts[4]);
+        kn("trace_enabled", 0);
+        kn("trace_photons", 0);
+        kn("trace_vertices", 0);
+        kn("trace_ids", 0);
+        kn("trace_truncated_ids", 0);
+        kn("detector_distance", o.thickness);
+        kn("detector_half_width", 2.0 * o.thickness);
+        std::cout << "# output-dir=" << *o.outputDir << '\n';
+    }
     return EXIT_SUCCESS;
 }
 

@@ -416,12 +416,14 @@ enum { GF_EXEC_FLOW = 0, GF_EXEC_FUSED = 1 };
 /* Runs photons first_id .. first_id + n - 1. exec GF_EXEC_FLOW runs the graph through the C++
  * Flow (partition + transforms + sink); GF_EXEC_FUSED carries each photon through the same
  * functors in one kernel (identical histories). Optional host outputs (NULL to skip):
- * h_event[n], h_scatter_count[n], h_weight[n], h_cos_exit[n], h_position[3n] (per id),
+ * h_event[n], h_scatter_count[n], h_weight[n], h_cos_exit[n], h_position[3n], h_direction[3n]
+ * (per id, at the terminal event),
  * h_refl[hist_bins], h_trans[hist_bins] (summed exit weights), h_event_counts[5]. */
 gf_status gf_run_photon(uint64_t seed, uint64_t first_id, uint64_t n, const gf_photon_params* h_params, int exec,
                         uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks, uint32_t* h_event,
                         uint32_t* h_scatter_count, double* h_weight, double* h_cos_exit, double* h_position,
-                        double* h_refl, double* h_trans, uint64_t* h_event_counts, gf_flow_stats* h_stats);
+                        double* h_direction, double* h_refl, double* h_trans, uint64_t* h_event_counts,
+                        gf_flow_stats* h_stats);
 
 /* Message of the last failed front-end call on this thread (empty if none). */
 size_t gf_last_error(char* h_buf, size_t cap);

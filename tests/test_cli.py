@@ -162,7 +162,7 @@ def test_photon_cli_help():
     ["--backend", "cuda", "--thickness", "0"],
     ["--backend", "cuda", "--sigma-s", "-1"],
     ["--backend", "cuda", "--max-scatters", "70000"],            # the scatter counter is 16-bit here
-    ["--backend", "cuda", "--output-dir", "out"],                # no run-output directory in this build
+    ["--backend", "cuda", "--output-dir", ""],
     ["--backend", "cuda", "--trace-photons", "4"],               # no path traces in this build
     ["--backend", "cuda", "--pool-mode", "arena"],
     ["--backend", "cuda", "--exec", "both"],
@@ -204,3 +204,39 @@ def test_photon_cli_report_matches_the_library_and_both_execution_forms(mode):
     for e, s in zip(got["event"].tolist(), got["scatter_count"].tolist()):
         expect[(names[e], s)] = expect.get((names[e], s), 0) + 1
     assert rows == expect and term == n and bad == 0 and sum(ev.values()) == n
+
+
+@pytest.mark.gpu
+def test_photon_cli_writes_the_reference_run_files(tmp_path):
+    """--output-dir writes metadata, outcomes, scatter histogram and exits as the reference does
+    (PhotonOutput.hpp:91-197): the outcome files equal the printed report, exits.csv has one row
+    per transmitted or reflected photon with a unit exit direction, cos_theta = uz, exits on the
+    slab faces; the trace files carry their headers only."""
+    import csv
+    import math
+    n, out = 20_000, tmp_path / "run"
+    r = _prun("--backend", "cuda", "--photons", str(n), "--sigma-s", "2", "--sigma-a", "0.5", "--mode", "isotropic",
+              "--seed", "3", "--output-dir", str(out))
+    assert r.returncode == 0, r.stderr
+    ev, rows, term, bad = _photon_report(r.stdout)
+    names = sorted(p.name for p in out.iterdir())
+    assert names == sorted(["metadata.csv", "outcomes.csv", "scatter_histogram.csv", "exits.csv", "traces.csv",
+                            "trace_summary.csv"])
+    outcomes = {row["event"]: int(row["count"]) for row in csv.DictReader(open(out / "outcomes.csv"))}
+    assert outcomes == ev
+    hist = {(row["event"], int(row["scatter_count"])): int(row["count"])
+            for row in csv.DictReader(open(out / "scatter_histogram.csv"))}
+    assert hist == rows
+    exits = list(csv.DictReader(open(out / "exits.csv")))
+    assert len(exits) == ev["transmitted"] + ev["reflected"]
+    for row in exits[:2000]:
+        ux, uy, uz = float(row["ux"]), float(row["uy"]), float(row["uz"])
+        assert abs(ux * ux + uy * uy + uz * uz - 1.0) < 1e-9 and float(row["cos_theta"]) == uz
+        assert abs(float(row["phi_rad"]) - math.atan2(uy, ux)) < 1e-12
+        z = float(row["z"])
+        assert (row["event"] == "transmitted" and abs(z - 1.0) < 1e-9 and uz > 0) or \
+               (row["event"] == "reflected" and abs(z) < 1e-9 and uz < 0)
+    meta = {row["key"]: row["value"] for row in csv.DictReader(open(out / "metadata.csv"))}
+    assert meta["photons"] == str(n) and meta["mode"] == "isotropic" and meta["count_terminated"] == str(n)
+    assert open(out / "traces.csv").read() == "id,step,kind,scatter_count,x,y,z,ux,uy,uz\n"
+    assert "# output-dir=" in r.stdout
