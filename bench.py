@@ -73,22 +73,42 @@ class ClockSampler:
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
-        self.index, self.proc, self.path = index, None, None
+        self.index, self.proc, self.path, self.start = index, None, None, None
 
     def __enter__(self):
+        import shutil
         try:
             self.path = f"/tmp/gf_clocks_{os.getpid()}.csv"
             self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.f,
-                                         stderr=subprocess.DEVNULL)
+            cmd = ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                   "-lms", "20"]
+            if shutil.which("stdbuf"):  # one line per sample reaches the file at once
+                cmd = ["stdbuf", "-oL"] + cmd
+            self.proc = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
 
+    def _lines(self):
+        try:
+            with open(self.path) as f:
+                return f.readlines()
+        except OSError:
+            return []
+
+    def begin(self, timeout=3.0):
+        """Wait for the first sample, then count only the samples from here on."""
+        if self.proc is None:
+            return
+        t = time.perf_counter()
+        while not self._lines() and time.perf_counter() - t < timeout and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.start = len(self._lines())
+
     def __exit__(self, *a):
+        import signal
         if self.proc is not None:
-            self.proc.terminate()
+            self.proc.send_signal(signal.SIGINT)  # lets nvidia-smi flush and exit
             try:
                 self.proc.wait(timeout=5)
             except Exception:
@@ -100,7 +120,10 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        lines = self._lines()
+        if self.start is not None and len(lines) > self.start:
+            lines = lines[self.start:]
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -348,6 +371,7 @@ def gpu_arm(args):
     torch.cuda.synchronize()
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
+        clocks.begin()
         with torch.cuda.stream(stream):
             t_start.record(stream)
             for i in range(args.steps):
