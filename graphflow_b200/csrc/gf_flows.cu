@@ -4,6 +4,7 @@
 #include <cstring>
 #include <string>
 
+#include "../examples/kernel_axes.cuh"
 #include "../examples/particle_feedback.cuh"
 
 namespace {
@@ -163,6 +164,55 @@ gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visit
             cuda::check(cudaMemcpy(h_weights, weights.data(), n * 4u, cudaMemcpyDeviceToHost), "D2H");
             cuda::check(cudaMemcpy(h_capped, capped.data(), n * 4u, cudaMemcpyDeviceToHost), "D2H");
         }
+        fill_stats(s, sec, h_stats);
+    });
+}
+
+gf_status gf_run_kernel_axes(uint64_t seed, uint64_t n, uint32_t bins, int distribution, int scatter_mode,
+                             uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks, int fused,
+                             uint32_t* h_weights, gf_flow_stats* h_stats)
+{
+    using namespace graphflow;
+    using namespace graphflow::particle;
+    if ((n != 0u && h_weights == nullptr) || (bins != 64u && bins != 1024u && bins != 4096u) ||
+        distribution < GF_KDIST_BALANCED || distribution > GF_KDIST_SPARSE ||
+        (scatter_mode != GF_SCATTER_SHARED && scatter_mode != GF_SCATTER_DIRECT) ||
+        (distribution == GF_KDIST_SPARSE && bins < 1024u) || (scatter_mode == GF_SCATTER_DIRECT && fused != 0))
+        return GF_ERR_ARGUMENT;
+    return guarded([&] {
+        cuda::Device device = cuda::Device::current();
+        device.makeCurrent();
+        const std::size_t m = n ? n : 1u;
+        cuda::Buffer<std::uint32_t> weights(m);
+        {
+            std::vector<std::uint32_t> init(m, missingWeight);
+            cuda::check(cudaMemcpy(weights.data(), init.data(), m * 4u, cudaMemcpyHostToDevice), "H2D");
+        }
+        Tuning t;
+        t.seed = seed;
+        if (chunk_capacity != 0u)
+            t.chunkCapacity = chunk_capacity;
+        if (live_particles != 0u)
+            t.liveParticles = live_particles;
+        t.batchChunks = batch_chunks;
+        t.fused = fused != 0;
+        t.scatterMode = scatter_mode == GF_SCATTER_DIRECT ? ScatterMode::Direct : ScatterMode::SharedStaging;
+        if (gf_runner_batched()) {
+            t.sinkBatchChunks = gf_runner_sink_batch();
+            t.multiDispatch = true;
+        }
+        const auto d = static_cast<Distribution>(distribution);
+        const auto t0 = std::chrono::steady_clock::now();
+        SchedulerStats s;
+        if (bins == 64u)
+            s = runKernelAxes<64u, SoAStorage<Particle>>(device, n, d, t, weights.data());
+        else if (bins == 1024u)
+            s = runKernelAxes<1024u, SoAStorage<Particle>>(device, n, d, t, weights.data());
+        else
+            s = runKernelAxes<4096u, SoAStorage<Particle>>(device, n, d, t, weights.data());
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (n != 0u)
+            cuda::check(cudaMemcpy(h_weights, weights.data(), n * 4u, cudaMemcpyDeviceToHost), "D2H");
         fill_stats(s, sec, h_stats);
     });
 }

@@ -15,8 +15,10 @@
 // the policy's C (a multiple of T) but the partition kernels keep their own 1024-particle tiles.
 // Flags that configure parts of the reference this build does not have (frame cap, occupancy
 // target, pool budget and mode, per-chunk transform schedule) are parsed and checked as the
-// reference does and reported as inert on stderr. The kernel workload (--workload kernel) is not
-// part of this build.
+// reference does and reported as inert on stderr. The kernel workload (--workload kernel,
+// KernelAxes.hpp runKernelAxes) runs through gf_run_kernel_axes with 64, 1024 or 4096 ports; 65536
+// ports and --bin-path hash need the reference's hash bin path, which this build's Flow does not
+// have, and are command-line errors here.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -56,6 +58,8 @@ struct Options {
     std::string workload = "feedback";
     std::vector<std::string> inert;     // accepted for CLI parity, no effect here
     std::vector<std::string> kernelOnly; // flags of the kernel workload
+    std::string scatter = "shared", binPath = "dense", distribution = "balanced"; // KernelOptions defaults
+    std::uint32_t bins = 64u;
 };
 
 void usage(std::ostream& out)
@@ -64,6 +68,9 @@ void usage(std::ostream& out)
            "                                        [--particles N] [--chunk-size C]\n"
            "                                        [--live-particles P] [--tile-size T]\n"
            "                                        [--batch-chunks Q] [--seed S] [--max-visits M]\n"
+           "                                        [--workload feedback|kernel]\n"
+           "       kernel workload only: [--scatter shared|direct] [--bin-path dense] [--bins 64|1024|4096]\n"
+           "                             [--distribution balanced|one-hot|skewed|sparse]\n"
            "       accepted for parity with graphFlow_particle_feedback, no effect here:\n"
            "       [--frame-cap F] [--occupancy-target D] [--pool-budget-bytes B]\n"
            "       [--pool-mode fixed|slotArena] [--slot-arena-budget BYTES]\n"
@@ -125,8 +132,20 @@ Options parse(int argc, char** argv)
         } else if (flag == "--chunk-kernel-schedule") {
             expectOneOf(flag, next(), {"off", "perChunk"});
             o.inert.push_back(flag);
-        } else if (flag == "--scatter" || flag == "--bin-path" || flag == "--bins" || flag == "--distribution") {
-            next();
+        } else if (flag == "--scatter") {
+            o.scatter = next();
+            expectOneOf(flag, o.scatter, {"shared", "direct"});
+            o.kernelOnly.push_back(flag);
+        } else if (flag == "--bin-path") {
+            o.binPath = next();
+            expectOneOf(flag, o.binPath, {"dense", "hash"});
+            o.kernelOnly.push_back(flag);
+        } else if (flag == "--bins") {
+            o.bins = parseU32(flag, next());
+            o.kernelOnly.push_back(flag);
+        } else if (flag == "--distribution") {
+            o.distribution = next();
+            expectOneOf(flag, o.distribution, {"balanced", "one-hot", "skewed", "sparse"});
             o.kernelOnly.push_back(flag);
         } else {
             throw std::invalid_argument("unknown flag '" + flag + "'");
@@ -191,8 +210,19 @@ int run(const Options& o)
 {
     if (o.backend != "cuda")
         throw std::invalid_argument("--backend: this build runs on CUDA (sm_100a) only, got '" + o.backend + "'");
-    if (o.workload == "kernel")
-        throw std::invalid_argument("--workload kernel: the kernel workload is not part of this build");
+    const bool kernel = o.workload == "kernel";
+    if (kernel) { // KernelAxes.hpp:169-214 checks, and this build's limits
+        if (o.bins != 64u && o.bins != 1024u && o.bins != 4096u && o.bins != 65536u)
+            throw std::invalid_argument("--bins: the kernel workload instantiates 64, 1024, 4096 and 65536 (got '" +
+                                        std::to_string(o.bins) + "')");
+        if (o.binPath == "hash" && o.scatter == "direct")
+            throw std::invalid_argument("--scatter direct is the dense-path variant; the hash path always stages");
+        if (o.distribution == "sparse" && o.bins < 1024u)
+            throw std::invalid_argument("--distribution sparse requires --bins 1024 or larger");
+        if (o.binPath == "hash" || o.bins == 65536u)
+            throw std::invalid_argument("--bin-path hash / --bins 65536: this build's Flow partitions through the "
+                                        "dense path only (at most 4096 ports in the kernel workload)");
+    }
     for (const auto& f : o.inert)
         std::cerr << kName << ": note: " << f << " has no effect in this build\n";
 
@@ -206,11 +236,21 @@ int run(const Options& o)
     cudaDeviceProp prop{};
     cudaOrThrow(cudaGetDeviceProperties(&prop, static_cast<int>(o.device)), "cudaGetDeviceProperties");
 
-    std::vector<std::uint32_t> weights(o.particles), capped(o.particles);
+    std::vector<std::uint32_t> weights(o.particles), capped(kernel ? 0u : o.particles);
     gf_flow_stats st{};
-    if (gf_run_particle_feedback(o.seed, o.particles, o.maxVisits, C, P, o.batchChunks, 1, GF_LAYOUT_SOA,
-                                 weights.data(), capped.data(), &st) != GF_OK)
+    if (kernel) {
+        const int dist = o.distribution == "one-hot" ? GF_KDIST_ONEHOT
+                         : o.distribution == "skewed" ? GF_KDIST_SKEWED
+                         : o.distribution == "sparse" ? GF_KDIST_SPARSE
+                                                      : GF_KDIST_BALANCED;
+        const bool direct = o.scatter == "direct"; // the plain form's one-atomic-per-particle scatter
+        if (gf_run_kernel_axes(o.seed, o.particles, o.bins, dist, direct ? GF_SCATTER_DIRECT : GF_SCATTER_SHARED, C,
+                               P, o.batchChunks, direct ? 0 : 1, weights.data(), &st) != GF_OK)
+            throw std::runtime_error(lastError());
+    } else if (gf_run_particle_feedback(o.seed, o.particles, o.maxVisits, C, P, o.batchChunks, 1, GF_LAYOUT_SOA,
+                                        weights.data(), capped.data(), &st) != GF_OK) {
         throw std::runtime_error(lastError());
+    }
     std::vector<std::uint32_t> values;
     std::vector<unsigned long long> counts;
     histogram(weights, values, counts);
@@ -219,9 +259,14 @@ int run(const Options& o)
         nCapped += c != 0u ? 1u : 0u;
 
     std::cout << "# graphFlow_particle_feedback backend=cuda device=" << o.device << " device-name=" << prop.name
-              << " particles=" << o.particles << " chunk-size=" << C << " live-particles=" << P
-              << " tile-size=" << T << " batch-chunks=" << o.batchChunks << " seed=" << o.seed
-              << " max-visits=" << o.maxVisits << '\n';
+              << (kernel ? " workload=kernel" : "") << " particles=" << o.particles << " chunk-size=" << C
+              << " live-particles=" << P << " tile-size=" << T << " batch-chunks=" << o.batchChunks
+              << " seed=" << o.seed;
+    if (kernel)
+        std::cout << " scatter=" << o.scatter << " bin-path=" << o.binPath << " bins=" << o.bins
+                  << " distribution=" << o.distribution << '\n';
+    else
+        std::cout << " max-visits=" << o.maxVisits << '\n';
     std::cout << "# pool-chunks=" << st.pool_chunks << " peak-live-chunks=" << st.peak_live_chunks
               << " peak-reserved-chunks=" << st.peak_reserved_chunks << '\n';
     std::cout << "# scheduler completed-batches=" << st.completed_batches << " partition-batches="

@@ -242,8 +242,10 @@ private:
 
 inline void check(cudaError_t e, const char* what)
 {
-    if (e != cudaSuccess)
+    if (e != cudaSuccess) {
+        cudaGetLastError(); // a reported failure does not linger as the thread's last error
         throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+    }
 }
 
 // Owning device buffer.

@@ -288,6 +288,7 @@ public:
                    std::uint32_t purpose)
         : m_st(st), m_cls(std::move(cls)), m_upd(std::move(upd)), m_seed(gf::mix64(c.seed)), m_purpose(purpose),
           m_bins(bins), m_C(c.chunkCapacity), m_Q(c.batchChunks), m_fused(c.fused),
+          m_direct(c.scatterMode == ScatterMode::Direct),
           m_tileCap(static_cast<std::uint32_t>(c.batchChunks) * ((c.chunkCapacity + kTile - 1u) / kTile)),
           m_bound(checkedOutputChunkBound(static_cast<std::uint64_t>(c.chunkCapacity) * c.batchChunks,
                                           c.chunkCapacity, bins)),
@@ -296,6 +297,20 @@ public:
     {
         if (bins > Config::denseBinLimit)
             throw std::invalid_argument("graphflow::PartitionStage: dense path supports at most 65535 bins");
+        const std::size_t smemFused = sizeof(P) * Shape::kTile + 4u * Shape::kTile + 4u * Shape::kWarps * bins +
+                                      4u * bins * 6u + 4u * (2u * Shape::kThreads + Shape::kWarps + 8u);
+        const std::size_t smemScatter = sizeof(P) * Shape::kTile + 4u * Shape::kTile +
+                                        4u * Shape::kWarps * bins + 4u * bins * 3u + 4u * (Shape::kWarps + 8u);
+        int dev = 0, smemLimit = 0;
+        cuda::check(cudaGetDevice(&dev), "cudaGetDevice");
+        cuda::check(cudaDeviceGetAttribute(&smemLimit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+                    "shared memory limit");
+        // many ports: the fused kernel's per-port tables no longer fit one block; the plain form's do
+        if (m_fused && smemFused > static_cast<std::size_t>(smemLimit))
+            m_fused = false;
+        if (!m_fused && !m_direct && smemScatter > static_cast<std::size_t>(smemLimit))
+            throw std::invalid_argument("graphflow::PartitionStage: " + std::to_string(bins) +
+                                        " ports need more shared memory per block than the device has");
         if (m_fused) {
             m_maxK = m_Q;
             m_portChunks = cuda::Buffer<unsigned long long>(static_cast<std::size_t>(bins) * m_maxK);
@@ -319,18 +334,16 @@ public:
         } else {
             m_binIds = cuda::Buffer<std::uint32_t>(st.slotCount());
         }
-        const std::size_t smemFused = sizeof(P) * Shape::kTile + 4u * Shape::kTile + 4u * Shape::kWarps * bins +
-                                      4u * bins * 6u + 4u * (2u * Shape::kThreads + Shape::kWarps + 8u);
-        const std::size_t smemScatter = sizeof(P) * Shape::kTile + 4u * Shape::kTile +
-                                        4u * Shape::kWarps * bins + 4u * bins * 3u + 4u * (Shape::kWarps + 8u);
         m_smemFused = smemFused;
         m_smemScatter = smemScatter;
-        cuda::check(cudaFuncSetAttribute(gf::fused_partition_kernel<Shape, Acc, Cls, Upd>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemFused)),
-                    "partition stage: fused kernel attribute");
-        cuda::check(cudaFuncSetAttribute(gf::scatter_kernel<Shape, Acc, Upd>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemScatter)),
-                    "partition stage: scatter kernel attribute");
+        if (m_fused)
+            cuda::check(cudaFuncSetAttribute(gf::fused_partition_kernel<Shape, Acc, Cls, Upd>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemFused)),
+                        "partition stage: fused kernel attribute");
+        if (!m_direct && smemScatter <= static_cast<std::size_t>(smemLimit))
+            cuda::check(cudaFuncSetAttribute(gf::scatter_kernel<Shape, Acc, Upd>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemScatter)),
+                        "partition stage: scatter kernel attribute");
     }
 
     std::uint32_t launch(cudaStream_t s, const Batch& b) override
@@ -526,9 +539,16 @@ private:
         if (m_numTiles) {
             const Acc acc{m_st.view()};
             const Upd upd{m_upd, m_purpose + 1u, m_status.dev.data()};
-            gf::scatter_kernel<Shape, Acc, Upd><<<m_numTiles, Shape::kThreads, m_smemScatter, s>>>(
-                acc, upd, m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(), m_tiles.dev.data(), m_numTiles, m_bins,
-                m_binIds.data(), m_table.dev.data(), m_next.dev.data(), m_counts.dev.data(), m_status.dev.data());
+            if (m_direct) // one device atomic per particle (Execution.hpp:1034-1095)
+                gf::scatter_direct_kernel<Shape, Acc, Upd><<<m_numTiles, Shape::kThreads, 0, s>>>(
+                    acc, upd, m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(), m_tiles.dev.data(), m_numTiles,
+                    m_bins, m_binIds.data(), m_table.dev.data(), m_next.dev.data(), m_counts.dev.data(),
+                    m_status.dev.data());
+            else
+                gf::scatter_kernel<Shape, Acc, Upd><<<m_numTiles, Shape::kThreads, m_smemScatter, s>>>(
+                    acc, upd, m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(), m_tiles.dev.data(), m_numTiles,
+                    m_bins, m_binIds.data(), m_table.dev.data(), m_next.dev.data(), m_counts.dev.data(),
+                    m_status.dev.data());
             cuda::check(cudaGetLastError(), "scatter launch");
             ++m_launches;
         }
@@ -553,6 +573,7 @@ private:
     std::uint64_t m_seed;
     std::uint32_t m_purpose, m_bins, m_C, m_Q;
     bool m_fused;
+    bool m_direct; // plain form: ScatterMode::Direct
     std::uint32_t m_tileCap, m_bound;
     detail::Staged<gf_tile> m_tiles;
     detail::Staged<std::uint32_t> m_counts, m_next, m_table, m_status, m_numOut;

@@ -47,7 +47,10 @@ def test_cli_help():
     ["--chunk-size", "0"],
     ["--chunk-size", "4294967296"],               # 2^32
     ["--backend", "cpu", "--particles", "10"],    # this build runs on CUDA only
-    ["--backend", "cuda", "--workload", "kernel"],
+    ["--backend", "cuda", "--workload", "kernel", "--bins", "65536"],   # needs the reference's hash bin path
+    ["--backend", "cuda", "--workload", "kernel", "--bin-path", "hash"],
+    ["--backend", "cuda", "--workload", "kernel", "--bins", "100"],
+    ["--backend", "cuda", "--workload", "kernel", "--distribution", "sparse"],  # sparse needs >= 1024 bins
     ["--backend", "cuda", "--bins", "64"],        # a kernel-workload flag without --workload kernel
     ["--backend", "cuda", "--pool-mode", "arena"],
     ["--backend", "cuda", "--workload", "both"],
@@ -57,6 +60,43 @@ def test_cli_rejects_bad_command_lines(args):
     device work (Cli.hpp: parseOptions / resolveOptions throw std::invalid_argument)."""
     r = _run(*args)
     assert r.returncode == 2 and "usage:" in r.stderr and r.stdout == ""
+
+
+def _distribution_bin(dist, ids, bins):
+    """KernelAxes.hpp:29-42 distributionBin."""
+    ids = ids.astype(np.uint64)
+    if dist == "one-hot":
+        return np.zeros(ids.size, np.uint32)
+    if dist == "skewed":
+        return np.where(ids % 8 == 0, ids % bins, 0).astype(np.uint32)
+    return (ids % bins).astype(np.uint32)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bins,dist,scatter", [(64, "balanced", "shared"), (64, "skewed", "direct"),
+                                               (1024, "sparse", "shared"), (1024, "one-hot", "direct"),
+                                               (4096, "balanced", "shared")])
+def test_kernel_workload_sends_every_particle_to_its_port(bins, dist, scatter):
+    """runKernelAxes (KernelAxes.hpp:115-167): each particle's final weight is the port its id
+    maps to, in the fused form and in the plain form with the direct (one atomic per particle) or
+    the shared-staging scatter."""
+    n = 300_007
+    for fused in ([False] if scatter == "direct" else [True, False]):
+        w, st = capi.run_kernel_axes(9, n, bins, dist, scatter, chunk_capacity=1024, live_particles=8192,
+                                     batch_chunks=4, fused=fused)
+        assert np.array_equal(w, _distribution_bin(dist, np.arange(n), bins)) and st.sunk == n
+
+
+@pytest.mark.gpu
+def test_cli_kernel_workload_prints_the_port_occupancy():
+    n, bins = 100_000, 1024
+    r = _run("--backend", "cuda", "--workload", "kernel", "--particles", str(n), "--bins", str(bins),
+             "--distribution", "skewed", "--chunk-size", "1024", "--live-particles", "8192", "--batch-chunks", "2")
+    assert r.returncode == 0, r.stderr
+    w, c, ncap, _ = _rows(r.stdout)
+    ev, ec = np.unique(_distribution_bin("skewed", np.arange(n), bins), return_counts=True)
+    assert np.array_equal(w, ev.astype(np.uint64)) and np.array_equal(c, ec.astype(np.uint64)) and ncap == 0
+    assert "workload=kernel" in r.stdout.splitlines()[0] and f"bins={bins}" in r.stdout.splitlines()[0]
 
 
 @pytest.mark.gpu
