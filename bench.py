@@ -767,6 +767,26 @@ def _cfg_tuning_and_graphs():
     return out
 
 
+def _cfg_kernel_workload():
+    """The particle example's kernel workload through the Flow (KernelAxes.hpp runKernelAxes):
+    N = 1e7 particles, one partition with B ports, every port into one sink; the fused form and the
+    plain form with the shared-staging or the direct (one device atomic per particle) scatter, for
+    the balanced and the one-hot distributions (the reference compares the scatter modes on one-hot,
+    docs/benchmarks.md:105-108, on its CPU backend)."""
+    from graphflow_b200 import capi
+    n, out = 10_000_000, {"workload": "kernel workload through the Flow, N=1e7, C=8192, P=65536, Q=8"}
+    for bins in (64, 1024):
+        for dist in ("balanced", "one-hot"):
+            for form, fused, scatter in (("fused", True, "shared"), ("plain_shared", False, "shared"),
+                                         ("plain_direct", False, "direct")):
+                for _ in range(2):  # the first run of a configuration loads its kernels
+                    _, st = capi.run_kernel_axes(7, n, bins, dist, scatter, chunk_capacity=8192,
+                                                 live_particles=65536, batch_chunks=8, fused=fused)
+                out[f"B{bins}_{dist}_{form}"] = {"seconds": st.seconds, "particles_per_s": n / st.seconds,
+                                                 "partition_batches": st.partition_batches}
+    return out
+
+
 def _cfg_histogram(n=100_000_000, cpu=True):
     """The device histogram (ParticleTypes.hpp:206-219 histogramOf: sort + run-length encoding) of
     N = 1e8 u32 values: the particle_feedback final weights (the published 260 rows) and uniform
@@ -820,7 +840,8 @@ def other_configs(peak):
     out = {}
     for name, f in (("particle_feedback", _cfg_particle_feedback), ("dense_flow", _cfg_dense_flow),
                     ("hash", lambda: _cfg_hash(peak)), ("photon", _cfg_photon), ("serving", _cfg_serving),
-                    ("tuning_and_graphs", _cfg_tuning_and_graphs), ("histogram", _cfg_histogram)):
+                    ("tuning_and_graphs", _cfg_tuning_and_graphs), ("histogram", _cfg_histogram),
+                    ("kernel_workload", _cfg_kernel_workload)):
         try:
             out[name] = f()
         except Exception as e:  # reported, never silent

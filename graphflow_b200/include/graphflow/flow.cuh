@@ -284,19 +284,24 @@ private:
         c.batchChunks = m_tuning.batchChunks.value_or(1u);
         c.sinkBatchChunks = std::min(std::max(m_tuning.sinkBatchChunks, 1u), Tuning::kMaxSinkBatchChunks);
         // C and P the caller left out come from the device policy (core/DevicePolicy.hpp:344-614)
-        // with the accelerator P/C ratio of 8 and this storage's slot size, as Flow does there
+        // with the accelerator P/C ratio of 8 and this storage's slot size, as Flow does there. The
+        // payload budget is one eighth of device memory: the reference caps it at 3 GiB for 24 GB
+        // devices, which on a B200 would clamp P below one chunk for records of 50 bytes and more.
         std::optional<DevicePolicy> policy;
         if (!m_tuning.chunkCapacity || !m_tuning.liveParticles) {
+            const DeviceProperties props = m_device.getDeviceProperties();
             DevicePolicyConfig pc;
             pc.liveParticlesPerChunk = DevicePolicyConfig::kAcceleratorLiveParticlesPerChunk;
             pc.slotBytes = TStorage::slotBytes();
+            pc.acceleratorBudgetCapBytes =
+                std::max(pc.acceleratorBudgetCapBytes, props.globalMemBytes / pc.memoryBudgetDivisor);
             DevicePolicyOverrides ov;
             ov.chunkCapacity = m_tuning.chunkCapacity;
             if (ov.chunkCapacity)
                 pc.maxChunkCapacity = std::max(pc.maxChunkCapacity, *ov.chunkCapacity);
             if (m_tuning.liveParticles && *m_tuning.liveParticles <= itemCount)
                 ov.liveParticles = m_tuning.liveParticles;
-            policy = makeDevicePolicy(m_device.getDeviceProperties(), itemCount, ov, pc);
+            policy = makeDevicePolicy(props, itemCount, ov, pc);
         }
         c.chunkCapacity = m_tuning.chunkCapacity.value_or(policy ? policy->chunkCapacity : 8192u);
         c.tileSize = m_tuning.tileSize.value_or(1024u);
