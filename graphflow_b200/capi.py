@@ -89,7 +89,7 @@ _SIGS = {
     "gf_generate_records16": [_VP, _U64, _U64, _U64, _VP, _U32, _U64, _VP, _I32],
     "gf_run_particle_feedback": [_U64, _U64, _U32, _U32, _U32, _U32, _I32, _I32, _VP, _VP, _VP],
     "gf_set_tuning": [C.c_char_p, _I32],
-    "gf_run_kernel_axes": [_U64, _U64, _U32, _I32, _I32, _U32, _U32, _U32, _I32, _VP, _VP],
+    "gf_run_kernel_axes": [_U64, _U64, _U32, _I32, _I32, _I32, _U32, _U32, _U32, _I32, _VP, _VP],
     "gf_device_policy": [_VP, _U64, _U32, _U32, _U32, _U32, _U64, _U64, _VP],
     "gf_run_particle_feedback_kernel": [_U64, _U64, _U32, _VP, _VP, _VP],
     "gf_serve": [_VP, _U32, _I32, _U64, _U32, _VP, _VP],
@@ -192,13 +192,14 @@ KDIST_NAMES = {"balanced": 0, "one-hot": 1, "skewed": 2, "sparse": 3}
 
 
 def run_kernel_axes(seed, n, bins, distribution="balanced", scatter="shared", chunk_capacity=1024,
-                    live_particles=4096, batch_chunks=1, fused=True):
+                    live_particles=4096, batch_chunks=1, fused=True, bin_path="dense"):
     """runKernelAxes through the C++ front end: each particle's port (its final weight) and the stats."""
     import numpy as np
     weights = np.zeros(max(n, 1), np.uint32)
     stats = FlowStats()
     rc = lib().gf_run_kernel_axes(seed, n, bins, KDIST_NAMES[distribution],
-                                  SCATTER_DIRECT if scatter == "direct" else SCATTER_SHARED, chunk_capacity,
+                                  SCATTER_DIRECT if scatter == "direct" else SCATTER_SHARED, int(bin_path == "hash"),
+                                  chunk_capacity,
                                   live_particles, batch_chunks, int(bool(fused)), weights.ctypes.data,
                                   C.byref(stats))
     if rc != GF_OK:

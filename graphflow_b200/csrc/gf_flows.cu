@@ -169,12 +169,13 @@ gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visit
 }
 
 gf_status gf_run_kernel_axes(uint64_t seed, uint64_t n, uint32_t bins, int distribution, int scatter_mode,
-                             uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks, int fused,
-                             uint32_t* h_weights, gf_flow_stats* h_stats)
+                             int hash_path, uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks,
+                             int fused, uint32_t* h_weights, gf_flow_stats* h_stats)
 {
     using namespace graphflow;
     using namespace graphflow::particle;
-    if ((n != 0u && h_weights == nullptr) || (bins != 64u && bins != 1024u && bins != 4096u) ||
+    if ((n != 0u && h_weights == nullptr) || (bins != 64u && bins != 1024u && bins != 4096u && bins != 65536u) ||
+        (scatter_mode == GF_SCATTER_DIRECT && (hash_path != 0 || bins > 4096u)) ||
         distribution < GF_KDIST_BALANCED || distribution > GF_KDIST_SPARSE ||
         (scatter_mode != GF_SCATTER_SHARED && scatter_mode != GF_SCATTER_DIRECT) ||
         (distribution == GF_KDIST_SPARSE && bins < 1024u) || (scatter_mode == GF_SCATTER_DIRECT && fused != 0))
@@ -197,6 +198,8 @@ gf_status gf_run_kernel_axes(uint64_t seed, uint64_t n, uint32_t bins, int distr
         t.batchChunks = batch_chunks;
         t.fused = fused != 0;
         t.scatterMode = scatter_mode == GF_SCATTER_DIRECT ? ScatterMode::Direct : ScatterMode::SharedStaging;
+        if (hash_path != 0)
+            t.binPath = BinPath::hash;
         if (gf_runner_batched()) {
             t.sinkBatchChunks = gf_runner_sink_batch();
             t.multiDispatch = true;
@@ -208,8 +211,10 @@ gf_status gf_run_kernel_axes(uint64_t seed, uint64_t n, uint32_t bins, int distr
             s = runKernelAxes<64u, SoAStorage<Particle>>(device, n, d, t, weights.data());
         else if (bins == 1024u)
             s = runKernelAxes<1024u, SoAStorage<Particle>>(device, n, d, t, weights.data());
-        else
+        else if (bins == 4096u)
             s = runKernelAxes<4096u, SoAStorage<Particle>>(device, n, d, t, weights.data());
+        else
+            s = runKernelAxes<65536u, SoAStorage<Particle>>(device, n, d, t, weights.data());
         const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (n != 0u)
             cuda::check(cudaMemcpy(h_weights, weights.data(), n * 4u, cudaMemcpyDeviceToHost), "D2H");

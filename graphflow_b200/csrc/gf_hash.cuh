@@ -128,8 +128,22 @@ GF_D void hash_reset(uint32_t* hkey, uint32_t* hcnt)
 // shared table, then one device atomic per occupied entry into counts[bin]. counts[bins] is the
 // status slot. `bin_ids == nullptr` skips the store (device-planned form recomputes the bin).
 // ---------------------------------------------------------------------------------------------
-template <typename Shape, typename Access>
-__global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) hash_classify_kernel(Access acc, UnmixClassify cls,
+// The per-tile kernels take the C ABI's key classifier (UnmixClassify: only the 8-byte key is
+// loaded) or any classifier of a whole payload (the front end's partition stages).
+template <typename Cls>
+inline constexpr bool kKeyClassifier = std::is_same_v<Cls, UnmixClassify>;
+
+template <typename Cls, typename P>
+GF_D uint32_t hash_bin_of(const Cls& cls, const P& p)
+{
+    if constexpr (kKeyClassifier<Cls>)
+        return cls(p.key);
+    else
+        return cls(p);
+}
+
+template <typename Shape, typename Access, typename Cls = UnmixClassify>
+__global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) hash_classify_kernel(Access acc, Cls cls,
                                                                         uint32_t capacity, uint64_t pool_slots,
                                                                         const gf_tile* tiles, uint32_t n_tiles,
                                                                         uint32_t B, uint32_t* bin_ids,
@@ -148,12 +162,17 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) hash_class
         if (threadIdx.x == 0)
             full = 0u;
         __syncthreads();
-        uint64_t keys[Shape::kIpt];
+        using In = std::conditional_t<kKeyClassifier<Cls>, uint64_t, typename Access::Payload>;
+        In keys[Shape::kIpt];
 #pragma unroll
         for (int r = 0; r < Shape::kIpt; ++r) {
             const uint32_t i = Shape::item(w, r, lane);
-            if (tile_ok && i < tile.count)
-                keys[r] = acc.load_key(base + i);
+            if (tile_ok && i < tile.count) {
+                if constexpr (kKeyClassifier<Cls>)
+                    keys[r] = acc.load_key(base + i);
+                else
+                    keys[r] = acc.load(base + i);
+            }
         }
 #pragma unroll
         for (int r = 0; r < Shape::kIpt; ++r) {
@@ -197,8 +216,8 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) hash_class
 // grouped by entry, apply the updater, write out through the dense table layout
 // out = table[B + table[bin] + j / C] * C + j % C.
 // ---------------------------------------------------------------------------------------------
-template <typename Shape, typename Access, typename Update>
-__global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) hash_scatter_kernel(Access acc, UnmixClassify cls, Update update,
+template <typename Shape, typename Access, typename Update, typename Cls = UnmixClassify>
+__global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) hash_scatter_kernel(Access acc, Cls cls, Update update,
                                                                        uint64_t seed_mixed, uint32_t capacity,
                                                                        FastDiv fdc, uint64_t pool_slots,
                                                                        const gf_tile* tiles, uint32_t n_tiles,
@@ -241,7 +260,7 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) hash_scatt
             const uint32_t i = Shape::item(w, r, lane);
             uint32_t bin = kNoBin;
             if (tile_ok && i < tile.count) {
-                bin = bin_ids != nullptr ? __ldg(bin_ids + base + i) : cls(p[r].key);
+                bin = bin_ids != nullptr ? __ldg(bin_ids + base + i) : hash_bin_of(cls, p[r]);
                 if (bin >= B) {
                     counts[B] = 1u;
                     set_status(status, GF_INVALID);

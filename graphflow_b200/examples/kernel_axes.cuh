@@ -5,8 +5,8 @@
 // Reference (examples/particle_feedback/ in graphFlow): KernelAxes.hpp:29-42 (distributionBin:
 // balanced and sparse id % B, one-hot 0, skewed id % 8 == 0 ? id % B : 0), :80-106 (classifier on
 // the id, updater weight = bin), :115-167 (topology and result buffer), :169-214 (supported B,
-// scatter and bin-path checks). The partition stages of this front end are dense (at most 65535
-// ports), so B is 64, 1024 or 4096 here; the reference's 65536 needs its hash bin path.
+// scatter and bin-path checks). B = 65536 (and any B with Tuning::binPath = hash) partitions
+// through the per-tile hash tables.
 #pragma once
 
 #include <cstdint>

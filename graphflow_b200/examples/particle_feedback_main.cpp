@@ -16,9 +16,8 @@
 // Flags that configure parts of the reference this build does not have (frame cap, occupancy
 // target, pool budget and mode, per-chunk transform schedule) are parsed and checked as the
 // reference does and reported as inert on stderr. The kernel workload (--workload kernel,
-// KernelAxes.hpp runKernelAxes) runs through gf_run_kernel_axes with 64, 1024 or 4096 ports; 65536
-// ports and --bin-path hash need the reference's hash bin path, which this build's Flow does not
-// have, and are command-line errors here.
+// KernelAxes.hpp runKernelAxes) runs through gf_run_kernel_axes with 64, 1024, 4096 or 65536 ports
+// on the dense or the hash bin path.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -69,7 +68,8 @@ void usage(std::ostream& out)
            "                                        [--live-particles P] [--tile-size T]\n"
            "                                        [--batch-chunks Q] [--seed S] [--max-visits M]\n"
            "                                        [--workload feedback|kernel]\n"
-           "       kernel workload only: [--scatter shared|direct] [--bin-path dense] [--bins 64|1024|4096]\n"
+           "       kernel workload only: [--scatter shared|direct] [--bin-path dense|hash]\n"
+           "                             [--bins 64|1024|4096|65536]\n"
            "                             [--distribution balanced|one-hot|skewed|sparse]\n"
            "       accepted for parity with graphFlow_particle_feedback, no effect here:\n"
            "       [--frame-cap F] [--occupancy-target D] [--pool-budget-bytes B]\n"
@@ -219,9 +219,9 @@ int run(const Options& o)
             throw std::invalid_argument("--scatter direct is the dense-path variant; the hash path always stages");
         if (o.distribution == "sparse" && o.bins < 1024u)
             throw std::invalid_argument("--distribution sparse requires --bins 1024 or larger");
-        if (o.binPath == "hash" || o.bins == 65536u)
-            throw std::invalid_argument("--bin-path hash / --bins 65536: this build's Flow partitions through the "
-                                        "dense path only (at most 4096 ports in the kernel workload)");
+        if (o.binPath == "dense" && o.bins > 4096u)
+            throw std::invalid_argument("--bin-path dense supports at most 4096 bins here; use --bin-path hash above "
+                                        "that");
     }
     for (const auto& f : o.inert)
         std::cerr << kName << ": note: " << f << " has no effect in this build\n";
@@ -244,8 +244,9 @@ int run(const Options& o)
                          : o.distribution == "sparse" ? GF_KDIST_SPARSE
                                                       : GF_KDIST_BALANCED;
         const bool direct = o.scatter == "direct"; // the plain form's one-atomic-per-particle scatter
-        if (gf_run_kernel_axes(o.seed, o.particles, o.bins, dist, direct ? GF_SCATTER_DIRECT : GF_SCATTER_SHARED, C,
-                               P, o.batchChunks, direct ? 0 : 1, weights.data(), &st) != GF_OK)
+        if (gf_run_kernel_axes(o.seed, o.particles, o.bins, dist, direct ? GF_SCATTER_DIRECT : GF_SCATTER_SHARED,
+                               o.binPath == "hash" ? 1 : 0, C, P, o.batchChunks, direct ? 0 : 1, weights.data(),
+                               &st) != GF_OK)
             throw std::runtime_error(lastError());
     } else if (gf_run_particle_feedback(o.seed, o.particles, o.maxVisits, C, P, o.batchChunks, 1, GF_LAYOUT_SOA,
                                         weights.data(), capped.data(), &st) != GF_OK) {

@@ -16,6 +16,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "gf_hash.cuh"
 #include "kernels.cuh"
 #include "storage.cuh"
 
@@ -295,8 +296,6 @@ public:
           m_tiles(m_tileCap), m_counts(bins + 1u), m_next(bins), m_table(bins + m_bound), m_status(1),
           m_numOut(1), m_descs(m_bound ? m_bound : 1)
     {
-        if (bins > Config::denseBinLimit)
-            throw std::invalid_argument("graphflow::PartitionStage: dense path supports at most 65535 bins");
         const std::size_t smemFused = sizeof(P) * Shape::kTile + 4u * Shape::kTile + 4u * Shape::kWarps * bins +
                                       4u * bins * 6u + 4u * (2u * Shape::kThreads + Shape::kWarps + 8u);
         const std::size_t smemScatter = sizeof(P) * Shape::kTile + 4u * Shape::kTile +
@@ -305,12 +304,24 @@ public:
         cuda::check(cudaGetDevice(&dev), "cudaGetDevice");
         cuda::check(cudaDeviceGetAttribute(&smemLimit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
                     "shared memory limit");
-        // many ports: the fused kernel's per-port tables no longer fit one block; the plain form's do
-        if (m_fused && smemFused > static_cast<std::size_t>(smemLimit))
+        const auto limit = static_cast<std::size_t>(smemLimit);
+        // the hash bin path (per-tile open-addressing tables, Execution.hpp:1208-1502): asked for,
+        // more ports than 16-bit dense bins hold, or (automatic path) more than the dense kernels'
+        // per-port tables fit in one block
+        m_hash = c.binPath == BinPath::hash || bins > Config::denseBinLimit ||
+                 (c.binPath == BinPath::automatic && smemFused > limit && smemScatter > limit && !m_direct);
+        if (m_hash) {
+            if (m_direct)
+                throw std::invalid_argument("graphflow::PartitionStage: the hash path has no direct scatter");
             m_fused = false;
-        if (!m_fused && !m_direct && smemScatter > static_cast<std::size_t>(smemLimit))
-            throw std::invalid_argument("graphflow::PartitionStage: " + std::to_string(bins) +
-                                        " ports need more shared memory per block than the device has");
+        } else {
+            // many ports: the fused kernel's per-port tables no longer fit one block; the plain form's do
+            if (m_fused && smemFused > limit)
+                m_fused = false;
+            if (!m_fused && !m_direct && smemScatter > limit)
+                throw std::invalid_argument("graphflow::PartitionStage: " + std::to_string(bins) +
+                                            " ports need more shared memory per block than the device has");
+        }
         if (m_fused) {
             m_maxK = m_Q;
             m_portChunks = cuda::Buffer<unsigned long long>(static_cast<std::size_t>(bins) * m_maxK);
@@ -340,10 +351,18 @@ public:
             cuda::check(cudaFuncSetAttribute(gf::fused_partition_kernel<Shape, Acc, Cls, Upd>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemFused)),
                         "partition stage: fused kernel attribute");
-        if (!m_direct && smemScatter <= static_cast<std::size_t>(smemLimit))
+        if (!m_hash && !m_direct && smemScatter <= limit)
             cuda::check(cudaFuncSetAttribute(gf::scatter_kernel<Shape, Acc, Upd>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemScatter)),
                         "partition stage: scatter kernel attribute");
+        if (m_hash) {
+            constexpr std::size_t E = 2u * Shape::kTile; // table entries per tile
+            m_smemScatter = sizeof(P) * Shape::kTile + 4u * Shape::kTile + 4u * 4u * E + 4u * (Shape::kWarps + 2u) + 16u;
+            cuda::check(cudaFuncSetAttribute(gf::hash_scatter_kernel<Shape, Acc, Upd, Cls>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(m_smemScatter)),
+                        "partition stage: hash scatter kernel attribute");
+        }
     }
 
     std::uint32_t launch(cudaStream_t s, const Batch& b) override
@@ -408,7 +427,11 @@ public:
         cuda::check(cudaMemsetAsync(m_status.dev.data(), 0, 4, s), "memset");
         const Cls cls{m_cls, m_seed, m_purpose, m_status.dev.data()};
         cuda::check(cudaMemsetAsync(m_counts.dev.data(), 0, 4u * (m_bins + 1u), s), "memset");
-        if (m_numTiles)
+        if (m_numTiles && m_hash)
+            gf::hash_classify_kernel<Shape, Acc, Cls><<<m_numTiles, Shape::kThreads, 0, s>>>(
+                acc, cls, m_C, m_st.slotCount(), m_tiles.dev.data(), m_numTiles, m_bins, m_binIds.data(),
+                m_counts.dev.data(), m_status.dev.data());
+        else if (m_numTiles)
             gf::classify_kernel<Shape, Acc, Cls><<<m_numTiles, Shape::kThreads, 4u * m_bins, s>>>(
                 acc, cls, m_C, m_st.slotCount(), m_tiles.dev.data(), m_numTiles, m_bins, m_binIds.data(),
                 m_counts.dev.data(), m_status.dev.data());
@@ -539,7 +562,12 @@ private:
         if (m_numTiles) {
             const Acc acc{m_st.view()};
             const Upd upd{m_upd, m_purpose + 1u, m_status.dev.data()};
-            if (m_direct) // one device atomic per particle (Execution.hpp:1034-1095)
+            if (m_hash) // per-tile tables again, one range per occupied entry (Execution.hpp:1336-1502)
+                gf::hash_scatter_kernel<Shape, Acc, Upd, Cls><<<m_numTiles, Shape::kThreads, m_smemScatter, s>>>(
+                    acc, Cls{m_cls, m_seed, m_purpose, m_status.dev.data()}, upd, m_seed, m_C, gf::FastDiv(m_C),
+                    m_st.slotCount(), m_tiles.dev.data(), m_numTiles, m_bins, m_binIds.data(), m_table.dev.data(),
+                    m_next.dev.data(), m_counts.dev.data(), m_status.dev.data());
+            else if (m_direct) // one device atomic per particle (Execution.hpp:1034-1095)
                 gf::scatter_direct_kernel<Shape, Acc, Upd><<<m_numTiles, Shape::kThreads, 0, s>>>(
                     acc, upd, m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(), m_tiles.dev.data(), m_numTiles,
                     m_bins, m_binIds.data(), m_table.dev.data(), m_next.dev.data(), m_counts.dev.data(),
@@ -573,7 +601,8 @@ private:
     std::uint64_t m_seed;
     std::uint32_t m_purpose, m_bins, m_C, m_Q;
     bool m_fused;
-    bool m_direct; // plain form: ScatterMode::Direct
+    bool m_direct;       // plain form: ScatterMode::Direct
+    bool m_hash = false; // plain form through the per-tile hash tables
     std::uint32_t m_tileCap, m_bound;
     detail::Staged<gf_tile> m_tiles;
     detail::Staged<std::uint32_t> m_counts, m_next, m_table, m_status, m_numOut;

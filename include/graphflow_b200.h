@@ -311,15 +311,16 @@ typedef struct gf_flow_stats {
 } gf_flow_stats;
 
 /* examples/particle_feedback/KernelAxes.hpp:115-214 runKernelAxes: Generate -> one partition with
- * `bins` ports (64, 1024 or 4096; the classifier is distributionBin of the particle id) -> one sink
- * on every port, the updater writing the port into the weight: h_weights[n] = each particle's port.
- * distribution GF_KDIST_*; scatter_mode GF_SCATTER_SHARED / _DIRECT (direct only with fused = 0:
- * one device atomic per particle in the plain form's scatter); sparse needs bins >= 1024.
- * Errors as gf_run_particle_feedback. */
+ * `bins` ports (64, 1024, 4096 or 65536; the classifier is distributionBin of the particle id) ->
+ * one sink on every port, the updater writing the port into the weight: h_weights[n] = each
+ * particle's port. distribution GF_KDIST_*; scatter_mode GF_SCATTER_SHARED / _DIRECT (direct only
+ * with fused = 0 and the dense path: one device atomic per particle in the plain form's scatter);
+ * hash_path != 0 partitions through the per-tile hash tables (the bin path 65536 ports always take);
+ * sparse needs bins >= 1024. Errors as gf_run_particle_feedback. */
 enum { GF_KDIST_BALANCED = 0, GF_KDIST_ONEHOT = 1, GF_KDIST_SKEWED = 2, GF_KDIST_SPARSE = 3 };
 gf_status gf_run_kernel_axes(uint64_t seed, uint64_t n, uint32_t bins, int distribution, int scatter_mode,
-                             uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks, int fused,
-                             uint32_t* h_weights, gf_flow_stats* h_stats);
+                             int hash_path, uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks,
+                             int fused, uint32_t* h_weights, gf_flow_stats* h_stats);
 
 /* The same feedback graph with the same functors and RNG streams, run as one per-particle kernel
  * (every particle carried from the source to its sink by one thread, no batches): h_weights and

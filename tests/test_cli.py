@@ -47,8 +47,8 @@ def test_cli_help():
     ["--chunk-size", "0"],
     ["--chunk-size", "4294967296"],               # 2^32
     ["--backend", "cpu", "--particles", "10"],    # this build runs on CUDA only
-    ["--backend", "cuda", "--workload", "kernel", "--bins", "65536"],   # needs the reference's hash bin path
-    ["--backend", "cuda", "--workload", "kernel", "--bin-path", "hash"],
+    ["--backend", "cuda", "--workload", "kernel", "--bin-path", "dense", "--bins", "65536"],
+    ["--backend", "cuda", "--workload", "kernel", "--bin-path", "hash", "--scatter", "direct"],
     ["--backend", "cuda", "--workload", "kernel", "--bins", "100"],
     ["--backend", "cuda", "--workload", "kernel", "--distribution", "sparse"],  # sparse needs >= 1024 bins
     ["--backend", "cuda", "--bins", "64"],        # a kernel-workload flag without --workload kernel
@@ -73,17 +73,22 @@ def _distribution_bin(dist, ids, bins):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("bins,dist,scatter", [(64, "balanced", "shared"), (64, "skewed", "direct"),
-                                               (1024, "sparse", "shared"), (1024, "one-hot", "direct"),
-                                               (4096, "balanced", "shared")])
-def test_kernel_workload_sends_every_particle_to_its_port(bins, dist, scatter):
+@pytest.mark.parametrize("bins,dist,scatter,path", [(64, "balanced", "shared", "dense"),
+                                                    (64, "skewed", "direct", "dense"),
+                                                    (1024, "sparse", "shared", "dense"),
+                                                    (1024, "one-hot", "direct", "dense"),
+                                                    (4096, "balanced", "shared", "dense"),
+                                                    (1024, "skewed", "shared", "hash"),
+                                                    (65536, "balanced", "shared", "hash"),
+                                                    (65536, "sparse", "shared", "hash")])
+def test_kernel_workload_sends_every_particle_to_its_port(bins, dist, scatter, path):
     """runKernelAxes (KernelAxes.hpp:115-167): each particle's final weight is the port its id
     maps to, in the fused form and in the plain form with the direct (one atomic per particle) or
-    the shared-staging scatter."""
+    the shared-staging scatter, and through the per-tile hash tables (65536 ports always)."""
     n = 300_007
     for fused in ([False] if scatter == "direct" else [True, False]):
         w, st = capi.run_kernel_axes(9, n, bins, dist, scatter, chunk_capacity=1024, live_particles=8192,
-                                     batch_chunks=4, fused=fused)
+                                     batch_chunks=4, fused=fused, bin_path=path)
         assert np.array_equal(w, _distribution_bin(dist, np.arange(n), bins)) and st.sunk == n
 
 
@@ -97,6 +102,12 @@ def test_cli_kernel_workload_prints_the_port_occupancy():
     ev, ec = np.unique(_distribution_bin("skewed", np.arange(n), bins), return_counts=True)
     assert np.array_equal(w, ev.astype(np.uint64)) and np.array_equal(c, ec.astype(np.uint64)) and ncap == 0
     assert "workload=kernel" in r.stdout.splitlines()[0] and f"bins={bins}" in r.stdout.splitlines()[0]
+    h = _run("--backend", "cuda", "--workload", "kernel", "--particles", str(n), "--bins", "65536",
+             "--bin-path", "hash", "--chunk-size", "1024", "--live-particles", "8192")
+    assert h.returncode == 0, h.stderr
+    w, c, _, _ = _rows(h.stdout)
+    ev, ec = np.unique(_distribution_bin("balanced", np.arange(n), 65536), return_counts=True)
+    assert np.array_equal(w, ev.astype(np.uint64)) and np.array_equal(c, ec.astype(np.uint64))
 
 
 @pytest.mark.gpu
