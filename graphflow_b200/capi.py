@@ -98,6 +98,8 @@ _SIGS = {
     "gf_run_dense_chain": [_U64, _U64, _U32, _U32, _I32, C.c_double, _U32, _U32, _U32, _I32, _I32, _VP, _VP],
     "gf_run_photon": [_U64, _U64, _U64, _VP, _I32, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                       _VP],
+    "gf_run_photon_traced": [_U64, _U64, _U64, _VP, _I32, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
+                             _VP, _VP, _VP, _U32, _U32, _VP, _VP, _VP],
 }
 
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
@@ -132,9 +134,18 @@ def photon_params(model=PHOTON_WEIGHTED, thickness=1.0, sigma_s=10.0, sigma_a=0.
                         model, int(isotropic), int(fp64))
 
 
+TRACE_VERTEX_DTYPE = [("kind", "<u4"), ("scatter_count", "<u4"), ("x", "<f8"), ("y", "<f8"), ("z", "<f8"),
+                      ("ux", "<f8"), ("uy", "<f8"), ("uz", "<f8")]  # gf_trace_vertex, 56 bytes
+TRACE_KIND_NAMES = ("source", "scatter", "transmitted", "reflected", "absorbed", "capped")
+
+
 def run_photon(seed, n, params, exec_mode=EXEC_FUSED, first_id=0, chunk_capacity=8192, live_particles=0,
-               batch_chunks=8, records=True):
-    """photon_scattering transform bodies on the GPU. Returns a dict of numpy arrays."""
+               batch_chunks=8, records=True, trace_photons=0, trace_vertices=64):
+    """photon_scattering transform bodies on the GPU. Returns a dict of numpy arrays.
+
+    trace_photons > 0 also records the bounded path trace of ids < min(n, trace_photons)
+    (gf_run_photon_traced): out["trace_vertices"] (M, trace_vertices) TRACE_VERTEX_DTYPE,
+    out["trace_counts"] (M,) and out["trace_truncated"] (M,)."""
     import numpy as np
     m = max(n, 1)
     out = {}
@@ -151,10 +162,21 @@ def run_photon(seed, n, params, exec_mode=EXEC_FUSED, first_id=0, chunk_capacity
     out["event_counts"] = np.zeros(5, np.uint64)
     stats = FlowStats()
     ptr = (lambda k: out[k].ctypes.data) if records else (lambda k: None)
-    rc = lib().gf_run_photon(seed, first_id, n, C.byref(params), exec_mode, chunk_capacity, live_particles,
-                             batch_chunks, ptr("event"), ptr("scatter_count"), ptr("weight"), ptr("cos_exit"),
-                             ptr("position"), ptr("direction"), out["refl"].ctypes.data, out["trans"].ctypes.data,
-                             out["event_counts"].ctypes.data, C.byref(stats))
+    args = (seed, first_id, n, C.byref(params), exec_mode, chunk_capacity, live_particles, batch_chunks, ptr("event"),
+            ptr("scatter_count"), ptr("weight"), ptr("cos_exit"), ptr("position"), ptr("direction"),
+            out["refl"].ctypes.data, out["trans"].ctypes.data, out["event_counts"].ctypes.data, C.byref(stats))
+    if trace_photons:
+        ids = min(n, trace_photons)
+        out["trace_vertices"] = np.zeros((max(ids, 1), max(trace_vertices, 1)), TRACE_VERTEX_DTYPE)
+        out["trace_counts"] = np.zeros(max(ids, 1), np.uint32)
+        out["trace_truncated"] = np.zeros(max(ids, 1), np.uint32)
+        rc = lib().gf_run_photon_traced(*args, trace_photons, trace_vertices, out["trace_vertices"].ctypes.data,
+                                        out["trace_counts"].ctypes.data, out["trace_truncated"].ctypes.data)
+        out["trace_vertices"] = out["trace_vertices"][:ids, :trace_vertices]
+        out["trace_counts"] = out["trace_counts"][:ids]
+        out["trace_truncated"] = out["trace_truncated"][:ids]
+    else:
+        rc = lib().gf_run_photon(*args)
     if rc != GF_OK:
         raise GfError(rc, "photon: " + last_error())
     if records:

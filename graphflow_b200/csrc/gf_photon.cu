@@ -17,11 +17,20 @@ namespace {
 using namespace graphflow;
 using namespace graphflow::photon;
 
+// Path trace of ids [0, ids) with up to `vertices` vertices each; ids = 0 traces nothing.
+struct TraceRequest {
+    std::uint64_t ids = 0u;
+    std::uint32_t vertices = 0u;
+    gf_trace_vertex* hVertices = nullptr;
+    std::uint32_t* hCounts = nullptr;
+    std::uint32_t* hTruncated = nullptr;
+};
+
 template <typename T>
 void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const gf_photon_params& P, int exec,
               std::uint32_t C, std::uint32_t live, std::uint32_t Q, uint32_t* hEvent, uint32_t* hSc, double* hW,
               double* hCos, double* hPos, double* hDir, double* hRefl, double* hTrans, uint64_t* hCounts,
-              gf_flow_stats* hStats)
+              gf_flow_stats* hStats, const TraceRequest& tr = {})
 {
     if (exec == GF_EXEC_FLOW && firstId != 0u)
         throw std::invalid_argument("graphflow::photon: a Flow run starts at id 0");
@@ -44,11 +53,16 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
         cuda::check(cudaMemset(records.data(), 0xFF, sizeof(TerminalT<T>) * m), "memset");
 
     const SlabT<T> slab{static_cast<T>(P.thickness), static_cast<T>(P.sigma_s), static_cast<T>(P.sigma_a)};
-    RecordTerminalT<T> terminal{wantRecords ? records.data() : nullptr, visits.data(), refl.data(), trans.data(), hb,
-                                counts.data()};
+    const std::size_t traceSlots = static_cast<std::size_t>(tr.ids) * tr.vertices;
+    cuda::Buffer<TraceVertexT<T>> traceVertices(traceSlots);
+    cuda::Buffer<std::uint32_t> traceCounts(tr.ids), traceTruncated(tr.ids);
+    if (tr.ids != 0u) {
+        cuda::check(cudaMemset(traceCounts.data(), 0, 4u * tr.ids), "memset");
+        cuda::check(cudaMemset(traceTruncated.data(), 0, 4u * tr.ids), "memset");
+    }
     SchedulerStats stats;
     const auto t0 = std::chrono::steady_clock::now();
-    auto run = [&](auto propose, auto scatter) {
+    auto run = [&](auto propose, auto scatter, auto terminal) {
         if (exec == GF_EXEC_FLOW) {
             Tuning t;
             t.seed = seed;
@@ -70,14 +84,29 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
             cuda::check(cudaDeviceSynchronize(), "transport");
         }
     };
-    if (P.model == GF_PHOTON_ANALOG)
-        run(ProposeFlightT<T>{slab, P.max_scatters}, ScatterT<T>{P.isotropic != 0});
+    // an untraced run instantiates the functors without trace code (NoTraceT)
+    auto withTrace = [&](auto trace) {
+        using Tr = decltype(trace);
+        const RecordTerminalT<T, Tr> terminal{wantRecords ? records.data() : nullptr,
+                                              visits.data(),
+                                              refl.data(),
+                                              trans.data(),
+                                              hb,
+                                              counts.data(),
+                                              trace};
+        if (P.model == GF_PHOTON_ANALOG)
+            run(ProposeFlightT<T>{slab, P.max_scatters}, ScatterT<T, Tr>{P.isotropic != 0, trace}, terminal);
+        else
+            run(ProposeWeightedT<T>{slab,
+                                    WeightedT<T>{static_cast<T>(P.g), static_cast<T>(P.roulette_threshold),
+                                                 static_cast<T>(P.roulette_survival)},
+                                    P.max_scatters},
+                ScatterHGT<T, Tr>{static_cast<T>(P.g), trace}, terminal);
+    };
+    if (tr.ids != 0u)
+        withTrace(TraceT<T>{traceVertices.data(), traceCounts.data(), traceTruncated.data(), tr.vertices, tr.ids});
     else
-        run(ProposeWeightedT<T>{slab,
-                                WeightedT<T>{static_cast<T>(P.g), static_cast<T>(P.roulette_threshold),
-                                             static_cast<T>(P.roulette_survival)},
-                                P.max_scatters},
-            ScatterHGT<T>{static_cast<T>(P.g)});
+        withTrace(NoTraceT<T>{});
     const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     std::uint32_t st = 0;
     cuda::check(cudaMemcpy(&st, status.data(), 4, cudaMemcpyDeviceToHost), "D2H");
@@ -126,6 +155,37 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
     }
     if (hCounts)
         cuda::check(cudaMemcpy(hCounts, counts.data(), 40, cudaMemcpyDeviceToHost), "D2H");
+    if (tr.ids != 0u) {
+        std::vector<std::uint32_t> kept(tr.ids);
+        cuda::check(cudaMemcpy(kept.data(), traceCounts.data(), 4u * tr.ids, cudaMemcpyDeviceToHost), "D2H");
+        if (tr.hCounts)
+            std::memcpy(tr.hCounts, kept.data(), 4u * tr.ids);
+        if (tr.hTruncated)
+            cuda::check(cudaMemcpy(tr.hTruncated, traceTruncated.data(), 4u * tr.ids, cudaMemcpyDeviceToHost), "D2H");
+        if (tr.hVertices && traceSlots != 0u) {
+            std::vector<TraceVertexT<T>> v(traceSlots);
+            cuda::check(cudaMemcpy(v.data(), traceVertices.data(), sizeof(TraceVertexT<T>) * traceSlots,
+                                   cudaMemcpyDeviceToHost),
+                        "D2H");
+            for (std::uint64_t id = 0; id < tr.ids; ++id)
+                for (std::uint32_t j = 0; j < tr.vertices; ++j) {
+                    const std::size_t k = static_cast<std::size_t>(id) * tr.vertices + j;
+                    gf_trace_vertex out{};
+                    if (j < kept[id]) {
+                        const TraceVertexT<T>& a = v[k];
+                        out.kind = static_cast<std::uint32_t>(a.kind);
+                        out.scatter_count = a.scatterCount;
+                        out.position[0] = a.position.x;
+                        out.position[1] = a.position.y;
+                        out.position[2] = a.position.z;
+                        out.direction[0] = a.direction.x;
+                        out.direction[1] = a.direction.y;
+                        out.direction[2] = a.direction.z;
+                    }
+                    tr.hVertices[k] = out;
+                }
+        }
+    }
     if (hStats) {
         std::memset(hStats, 0, sizeof(*hStats));
         hStats->completed_batches = stats.completedBatches;
@@ -144,12 +204,13 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
 
 } // namespace
 
-extern "C" gf_status gf_run_photon(uint64_t seed, uint64_t first_id, uint64_t n, const gf_photon_params* h_params,
-                                   int exec, uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks,
-                                   uint32_t* h_event, uint32_t* h_scatter_count, double* h_weight, double* h_cos_exit,
-                                   double* h_position, double* h_direction, double* h_refl, double* h_trans,
-                                   uint64_t* h_event_counts,
-                                   gf_flow_stats* h_stats)
+namespace {
+
+gf_status runPhoton(uint64_t seed, uint64_t first_id, uint64_t n, const gf_photon_params* h_params, int exec,
+                    uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks, uint32_t* h_event,
+                    uint32_t* h_scatter_count, double* h_weight, double* h_cos_exit, double* h_position,
+                    double* h_direction, double* h_refl, double* h_trans, uint64_t* h_event_counts,
+                    gf_flow_stats* h_stats, const TraceRequest& tr)
 {
     if (h_params == nullptr || (exec != GF_EXEC_FLOW && exec != GF_EXEC_FUSED) ||
         (h_params->model != GF_PHOTON_ANALOG && h_params->model != GF_PHOTON_WEIGHTED))
@@ -165,14 +226,50 @@ extern "C" gf_status gf_run_photon(uint64_t seed, uint64_t first_id, uint64_t n,
         if (P.fp64)
             runTyped<double>(seed, first_id, n, P, exec, chunk_capacity, live_particles, batch_chunks, h_event,
                              h_scatter_count, h_weight, h_cos_exit, h_position, h_direction, h_refl, h_trans,
-                             h_event_counts,
-                             h_stats);
+                             h_event_counts, h_stats, tr);
         else
             runTyped<float>(seed, first_id, n, P, exec, chunk_capacity, live_particles, batch_chunks, h_event,
                             h_scatter_count, h_weight, h_cos_exit, h_position, h_direction, h_refl, h_trans,
-                             h_event_counts,
-                            h_stats);
+                            h_event_counts, h_stats, tr);
     });
+}
+
+} // namespace
+
+extern "C" gf_status gf_run_photon(uint64_t seed, uint64_t first_id, uint64_t n, const gf_photon_params* h_params,
+                                   int exec, uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks,
+                                   uint32_t* h_event, uint32_t* h_scatter_count, double* h_weight, double* h_cos_exit,
+                                   double* h_position, double* h_direction, double* h_refl, double* h_trans,
+                                   uint64_t* h_event_counts, gf_flow_stats* h_stats)
+{
+    return runPhoton(seed, first_id, n, h_params, exec, chunk_capacity, live_particles, batch_chunks, h_event,
+                     h_scatter_count, h_weight, h_cos_exit, h_position, h_direction, h_refl, h_trans, h_event_counts,
+                     h_stats, TraceRequest{});
+}
+
+extern "C" gf_status gf_run_photon_traced(uint64_t seed, uint64_t first_id, uint64_t n,
+                                          const gf_photon_params* h_params, int exec, uint32_t chunk_capacity,
+                                          uint32_t live_particles, uint32_t batch_chunks, uint32_t* h_event,
+                                          uint32_t* h_scatter_count, double* h_weight, double* h_cos_exit,
+                                          double* h_position, double* h_direction, double* h_refl, double* h_trans,
+                                          uint64_t* h_event_counts, gf_flow_stats* h_stats, uint32_t trace_photons,
+                                          uint32_t trace_vertices, gf_trace_vertex* h_trace_vertices,
+                                          uint32_t* h_trace_counts, uint32_t* h_trace_truncated)
+{
+    TraceRequest tr;
+    tr.ids = trace_photons < n ? trace_photons : n;
+    tr.vertices = trace_vertices;
+    tr.hVertices = h_trace_vertices;
+    tr.hCounts = h_trace_counts;
+    tr.hTruncated = h_trace_truncated;
+    if (tr.ids != 0u && first_id != 0u)
+        return GF_ERR_ARGUMENT;
+    // the id-major vertex array must be addressable: ids x vertices x 56 bytes within 2^62
+    if (tr.ids != 0u && trace_vertices != 0u && tr.ids > (std::uint64_t{1} << 56) / trace_vertices)
+        return GF_ERR_RANGE;
+    return runPhoton(seed, first_id, n, h_params, exec, chunk_capacity, live_particles, batch_chunks, h_event,
+                     h_scatter_count, h_weight, h_cos_exit, h_position, h_direction, h_refl, h_trans, h_event_counts,
+                     h_stats, tr);
 }
 
 // Enqueues the FP32 transport of photons [0, n) with the parameters' model on `stream`, writing one

@@ -70,6 +70,58 @@ struct TerminalT {
     Vec3T<T> direction; // at the terminal event (the exit direction for the two exits)
 };
 
+// Path trace vertex kinds (PhotonTypes.hpp:189-197): the source, each scatter, then the terminal
+// event as Event + 1.
+enum class TraceKind : std::uint32_t {
+    source = 0u,
+    scatter = 1u,
+    transmitted = 2u,
+    reflected = 3u,
+    absorbed = 4u,
+    capped = 5u
+};
+
+template <typename T>
+struct TraceVertexT {
+    TraceKind kind;
+    std::uint32_t scatterCount; // completed scatters, this one included
+    Vec3T<T> position;
+    Vec3T<T> direction; // outgoing
+};
+
+// Trace writer of untraced runs (PhotonFunctors.hpp:188-199): the functors' default, so their
+// kernels carry no trace code at all.
+template <typename T>
+struct NoTraceT {
+    __device__ void record(std::uint64_t, TraceKind, std::uint32_t, const Vec3T<T>&, const Vec3T<T>&) const {}
+};
+
+// Bounded path trace (PhotonFunctors.hpp:201-234): photons with id < limit own maxVertices
+// consecutive vertex slots; a vertex past the bound sets the id's truncation flag instead and
+// leaves the history alone. A photon's events run one after another on one thread at a time, in
+// the Flow and in the fused kernel alike, so its counter needs no atomic.
+template <typename T>
+struct TraceT {
+    TraceVertexT<T>* vertices = nullptr;
+    std::uint32_t* counts = nullptr;
+    std::uint32_t* truncated = nullptr;
+    std::uint32_t maxVertices = 0u;
+    std::uint64_t limit = 0u;
+    __device__ void record(std::uint64_t id, TraceKind kind, std::uint32_t scatterCount, const Vec3T<T>& position,
+                           const Vec3T<T>& direction) const
+    {
+        if (id >= limit)
+            return;
+        const std::uint32_t index = counts[id];
+        if (index >= maxVertices) {
+            truncated[id] = 1u;
+            return;
+        }
+        vertices[id * maxVertices + index] = TraceVertexT<T>{kind, scatterCount, position, direction};
+        counts[id] = index + 1u;
+    }
+};
+
 template <typename T>
 __device__ inline T dlog(T x)
 {
@@ -96,8 +148,9 @@ __device__ inline bool faceHit(const SlabT<T>& s, const PhotonT<T>& p, T& dist, 
     return false;
 }
 
-template <typename T>
+template <typename T, typename TTrace = NoTraceT<T>>
 struct GeneratePhotonT {
+    TTrace trace;
     __device__ PhotonT<T> operator()(const Acc&, std::uint64_t id) const
     {
         PhotonT<T> p{};
@@ -107,6 +160,7 @@ struct GeneratePhotonT {
         p.weight = T(1);
         p.scatterCount = 0u;
         p.proposal = ProposalT<T>{Event::absorbed, T(0), T(1), 0u};
+        trace.record(id, TraceKind::source, 0u, p.position, p.direction);
         return p;
     }
 };
@@ -230,9 +284,10 @@ struct AdvanceToEventT {
 };
 
 // PhotonFunctors.hpp:172-186 isotropicDirection, :338-372 Scatter (analog model).
-template <typename T>
+template <typename T, typename TTrace = NoTraceT<T>>
 struct ScatterT {
     bool isotropic;
+    TTrace trace;
     __device__ void operator()(const Acc&, rng::Engine& e, Status& st, PhotonT<T>& p) const
     {
         if (!p.proposal.valid || p.proposal.event != Event::scatter) {
@@ -250,14 +305,16 @@ struct ScatterT {
             st.set(StatusCode::overflow);
             return;
         }
+        trace.record(p.id, TraceKind::scatter, p.scatterCount + 1u, p.position, p.direction);
         ++p.scatterCount;
     }
 };
 
 // Henyey-Greenstein scattering with the MCML direction update.
-template <typename T>
+template <typename T, typename TTrace = NoTraceT<T>>
 struct ScatterHGT {
     T g;
+    TTrace trace;
     __device__ void operator()(const Acc&, rng::Engine& e, Status& st, PhotonT<T>& p) const
     {
         if (!p.proposal.valid || p.proposal.event != Event::scatter) {
@@ -287,12 +344,13 @@ struct ScatterHGT {
             const T nz = -st2 * cp * tmp + u.z * ct;
             u = {nx, ny, nz};
         }
+        trace.record(p.id, TraceKind::scatter, p.scatterCount + 1u, p.position, p.direction);
         ++p.scatterCount;
     }
 };
 
 // PhotonFunctors.hpp:377-415 RecordTerminal (+ exit-weight histograms of the weighted model).
-template <typename T>
+template <typename T, typename TTrace = NoTraceT<T>>
 struct RecordTerminalT {
     TerminalT<T>* records;
     std::uint32_t* visits;
@@ -300,6 +358,7 @@ struct RecordTerminalT {
     T* transHist;  // may be null
     std::uint32_t histBins;
     unsigned long long* eventCounts; // [5], may be null
+    TTrace trace;                    // also the source's, so both execution forms trace alike
     __device__ void operator()(const Acc&, Status& st, const PhotonT<T>& p) const
     {
         const std::uint32_t ev = static_cast<std::uint32_t>(p.proposal.event);
@@ -310,6 +369,7 @@ struct RecordTerminalT {
         const T c = fabs(p.direction.z);
         if (records != nullptr)
             records[p.id] = TerminalT<T>{ev, p.scatterCount, p.weight, c, p.position, p.direction};
+        trace.record(p.id, static_cast<TraceKind>(ev + 1u), p.scatterCount, p.position, p.direction);
         if (visits != nullptr && atomicAdd(&visits[p.id], 1u) != 0u)
             st.set(StatusCode::invalid);
         if (eventCounts != nullptr)
@@ -323,10 +383,10 @@ struct RecordTerminalT {
 };
 
 // The walks of one thread's photons (grid-stride over [0, n)).
-template <typename T, typename TPropose, typename TScatter>
+template <typename T, typename TPropose, typename TScatter, typename TTrace>
 __device__ void transport_walks(const TPropose& propose, const AdvanceToEventT<T>& advance, const TScatter& scatter,
-                                const RecordTerminalT<T>& terminal, std::uint64_t seedMixed, std::uint64_t firstId,
-                                std::uint64_t n, std::uint32_t* status)
+                                const RecordTerminalT<T, TTrace>& terminal, std::uint64_t seedMixed,
+                                std::uint64_t firstId, std::uint64_t n, std::uint32_t* status)
 {
     const Acc acc{};
     Status st(status);
@@ -334,7 +394,8 @@ __device__ void transport_walks(const TPropose& propose, const AdvanceToEventT<T
     std::uint64_t i = (std::uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    PhotonT<T> p = GeneratePhotonT<T>{}(acc, firstId + i);
+    const GeneratePhotonT<T, TTrace> generate{terminal.trace};
+    PhotonT<T> p = generate(acc, firstId + i);
     std::uint32_t scatters = 0;
     // One event per iteration; a lane whose photon ends (or reaches 0x10001 scatters) starts its
     // next photon at once, so a warp stays full instead of waiting for its longest walk. Every
@@ -358,7 +419,7 @@ __device__ void transport_walks(const TPropose& propose, const AdvanceToEventT<T
             i += stride;
             if (i >= n)
                 break;
-            p = GeneratePhotonT<T>{}(acc, firstId + i);
+            p = generate(acc, firstId + i);
             scatters = 0;
         }
     }
@@ -367,9 +428,9 @@ __device__ void transport_walks(const TPropose& propose, const AdvanceToEventT<T
 // Fused transport: a thread carries photons through propose -> advance -> scatter until their
 // terminal events (transport_walks), calling the very functors the graph runs at the same stream
 // positions, so a history is identical to the one the Flow produces.
-template <typename T, typename TPropose, typename TScatter>
+template <typename T, typename TPropose, typename TScatter, typename TTrace>
 __global__ void __launch_bounds__(256) transport_kernel(TPropose propose, AdvanceToEventT<T> advance, TScatter scatter,
-                                                        RecordTerminalT<T> terminal, std::uint64_t seedMixed,
+                                                        RecordTerminalT<T, TTrace> terminal, std::uint64_t seedMixed,
                                                         std::uint64_t firstId, std::uint64_t n, std::uint32_t* status)
 {
     // The event counts and exit histograms of this CTA's photons accumulate in shared memory
@@ -385,7 +446,7 @@ __global__ void __launch_bounds__(256) transport_kernel(TPropose propose, Advanc
     for (std::uint32_t k = threadIdx.x; k < eventBins; k += blockDim.x)
         s_counts[k] = 0ull;
     __syncthreads();
-    RecordTerminalT<T> local = terminal;
+    RecordTerminalT<T, TTrace> local = terminal;
     if (localHist) {
         local.transHist = s_hist[0];
         local.reflHist = s_hist[1];
@@ -426,12 +487,12 @@ struct graphflow::SoAFields<graphflow::photon::PhotonT<T>> {
 namespace graphflow::photon {
 
 // Builds and runs the photon graph (PhotonScattering.hpp:37-181).
-template <typename T, typename TStorage, typename TPropose, typename TScatter>
+template <typename T, typename TStorage, typename TPropose, typename TScatter, typename TTrace>
 SchedulerStats runPhotonFlow(cuda::Device device, std::uint64_t n, TPropose propose, SlabT<T> slab, TScatter scatter,
-                             RecordTerminalT<T> terminal, Tuning tuning)
+                             RecordTerminalT<T, TTrace> terminal, Tuning tuning)
 {
     Flow<PhotonT<T>, cuda::Device, TStorage> flow{device};
-    auto source = flow.source("generate", GeneratePhotonT<T>{});
+    auto source = flow.source("generate", GeneratePhotonT<T, TTrace>{terminal.trace});
     auto flight = flow.transform("propose flight", propose);
     auto route = flow.partition("advance and route", ClassifyEventT<T>{}, AdvanceToEventT<T>{slab});
     auto scat = flow.transform("scatter", scatter);

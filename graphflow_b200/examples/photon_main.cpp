@@ -12,18 +12,20 @@
 //
 // --output-dir DIR writes the reference's run files (PhotonOutput.hpp:91-197 writeRunOutputs):
 // metadata.csv, outcomes.csv, scatter_histogram.csv, exits.csv (one row per transmitted or
-// reflected photon with its exit position and direction, 17 significant digits), and traces.csv /
-// trace_summary.csv with their headers only.
+// reflected photon with its exit position and direction, 17 significant digits), traces.csv (the
+// path trace vertices of the photons with id < --trace-photons, at most --trace-vertices each:
+// source, every scatter with its outgoing direction, the terminal event) and trace_summary.csv
+// (vertices kept and the truncation flag per traced id), through gf_run_photon_traced.
 //
 // Differences, by design: only --backend cuda runs. --exec fused (default) carries each photon
 // through the same functors in one kernel and --exec flow runs the graph through the Flow; both
-// give identical histories. Path traces are not recorded: --trace-photons / --trace-vertices take
-// 0 only. Pool, frame-cap, occupancy and per-chunk-schedule flags are checked as the reference does
-// and reported inert on stderr; provenance keys of metadata.csv that name the reference's build
-// (commit, alpaka pin, source directories) are written empty. At most 65535 scatters per photon
-// (16-bit counter).
+// give identical histories, traced or not. Pool, frame-cap, occupancy and per-chunk-schedule flags
+// are checked as the reference does and reported inert on stderr; provenance keys of metadata.csv
+// that name the reference's build (commit, alpaka pin, source directories) are written empty. At
+// most 65535 scatters per photon (16-bit counter).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -70,8 +72,9 @@ struct Options {
     std::string exec = "fused";
     std::uint32_t frameCap = 8u; // LaunchPolicy.hpp:18 defaultFrameCap (inert here, recorded in metadata)
     std::optional<std::string> outputDir;
+    std::uint32_t tracePhotons = 0u, traceVertices = 64u; // PhotonCli.hpp:46-47
     std::string command;
-    std::vector<std::string> inert, unsupported;
+    std::vector<std::string> inert;
 };
 
 void usage(std::ostream& out)
@@ -90,8 +93,9 @@ void usage(std::ostream& out)
            "       [--chunk-kernel-schedule off|perChunk] [--chunk-queue-depth D]\n"
            "       [--chunk-latency-cap-us U]\n"
            "       [--output-dir DIR]   the reference's run files (metadata, outcomes, scatter histogram,\n"
-           "                            exits; trace files with headers only)\n"
-           "       not part of this build: --trace-photons M / --trace-vertices V with M, V > 0\n"
+           "                            exits, path traces)\n"
+           "       [--trace-photons M] [--trace-vertices V]   trace ids < M, at most V vertices each\n"
+           "                            (default 0 and 64)\n"
            "       defaults: L = 1, sigma-s = sigma-a = 0, forward, 64 scatters, seed 0; C, P and T from\n"
            "       the device policy; --exec fused (the Flow and the fused kernel give identical results).\n";
 }
@@ -167,9 +171,10 @@ Options parse(int argc, char** argv)
             o.outputDir = next();
             if (o.outputDir->empty())
                 throw std::invalid_argument("--output-dir: value must not be empty");
-        } else if (flag == "--trace-photons" || flag == "--trace-vertices") {
-            if (parseU32(flag, next(), true) != 0u)
-                o.unsupported.push_back(flag);
+        } else if (flag == "--trace-photons") {
+            o.tracePhotons = parseU32(flag, next(), true);
+        } else if (flag == "--trace-vertices") {
+            o.traceVertices = parseU32(flag, next(), true);
         } else {
             throw std::invalid_argument("unknown argument '" + flag + "'");
         }
@@ -181,8 +186,6 @@ int run(const Options& o)
 {
     if (o.backend != "cuda")
         throw std::invalid_argument("--backend: this build runs on CUDA (sm_100a) only, got '" + o.backend + "'");
-    if (!o.unsupported.empty())
-        throw std::invalid_argument(o.unsupported.front() + ": path traces are not part of this build");
     if (!(o.thickness > 0.0))
         throw std::invalid_argument("--thickness: must be positive");
     if (o.sigmaS < 0.0 || o.sigmaA < 0.0)
@@ -214,11 +217,20 @@ int run(const Options& o)
     std::vector<double> position(o.outputDir ? 3u * m : 0u), direction(o.outputDir ? 3u * m : 0u);
     std::vector<std::uint64_t> eventCounts(5, 0u);
     gf_flow_stats st{};
-    if (gf_run_photon(o.seed, 0u, o.photons, &p, o.exec == "flow" ? GF_EXEC_FLOW : GF_EXEC_FUSED, pol.chunk_capacity,
-                      pol.live_particles, o.batchChunks, event.data(), scatters.data(), nullptr, nullptr,
-                      o.outputDir ? position.data() : nullptr, o.outputDir ? direction.data() : nullptr, nullptr,
-                      nullptr, eventCounts.data(), &st) != GF_OK)
+    // path trace of ids < M (PhotonScattering.hpp:49-57: M = min(N, --trace-photons))
+    const std::uint64_t traceIds = std::min<std::uint64_t>(o.photons, o.tracePhotons);
+    std::vector<gf_trace_vertex> traceVertices(traceIds * o.traceVertices);
+    std::vector<std::uint32_t> traceCounts(traceIds), traceTruncated(traceIds);
+    if (gf_run_photon_traced(o.seed, 0u, o.photons, &p, o.exec == "flow" ? GF_EXEC_FLOW : GF_EXEC_FUSED,
+                             pol.chunk_capacity, pol.live_particles, o.batchChunks, event.data(), scatters.data(),
+                             nullptr, nullptr, o.outputDir ? position.data() : nullptr,
+                             o.outputDir ? direction.data() : nullptr, nullptr, nullptr, eventCounts.data(), &st,
+                             o.tracePhotons, o.traceVertices, traceVertices.data(), traceCounts.data(),
+                             traceTruncated.data()) != GF_OK)
         throw std::runtime_error(lastError());
+    std::uint64_t traceTruncatedIds = 0u;
+    for (const std::uint32_t t : traceTruncated)
+        traceTruncatedIds += t != 0u;
 
     // outcome histogram over the delivered photons (PhotonScattering.hpp:132-156)
     std::map<std::pair<std::uint32_t, std::uint32_t>, std::uint64_t> rows;
@@ -279,8 +291,21 @@ int run(const Options& o)
                   << x[2] << ',' << u[0] << ',' << u[1] << ',' << u[2] << ',' << u[2] << ',' << std::atan2(u[1], u[0])
                   << ',' << x[0] << ',' << x[1] << '\n';
         }
+        // PhotonOutput.hpp:56-75 traceName, :131-146 the trace rows
+        static const char* const kTraceName[6] = {"source",   "scatter",  "transmitted",
+                                                  "reflected", "absorbed", "capped"};
         traces << "id,step,kind,scatter_count,x,y,z,ux,uy,uz\n";
+        traces << std::setprecision(17);
         summary << "id,vertices,truncated\n";
+        for (std::uint64_t id = 0; id < traceIds; ++id) {
+            summary << id << ',' << traceCounts[id] << ',' << (traceTruncated[id] != 0u ? 1 : 0) << '\n';
+            for (std::uint32_t step = 0; step < traceCounts[id]; ++step) {
+                const gf_trace_vertex& v = traceVertices[id * o.traceVertices + step];
+                traces << id << ',' << step << ',' << (v.kind < 6u ? kTraceName[v.kind] : "unknown") << ','
+                       << v.scatter_count << ',' << v.position[0] << ',' << v.position[1] << ',' << v.position[2]
+                       << ',' << v.direction[0] << ',' << v.direction[1] << ',' << v.direction[2] << '\n';
+            }
+        }
         auto quote = [](const std::string& v) {
             std::string q = "\"";
             for (const char c : v)
@@ -329,11 +354,11 @@ int run(const Options& o)
         kn("count_reflected", counts[2]);
         kn("count_absorbed", counts[3]);
         kn("count_capped", counts[4]);
-        kn("trace_enabled", 0);
-        kn("trace_photons", 0);
-        kn("trace_vertices", 0);
-        kn("trace_ids", 0);
-        kn("trace_truncated_ids", 0);
+        kn("trace_enabled", o.tracePhotons != 0u ? 1 : 0);
+        kn("trace_photons", o.tracePhotons);
+        kn("trace_vertices", o.traceVertices);
+        kn("trace_ids", traceIds);
+        kn("trace_truncated_ids", traceTruncatedIds);
         kn("detector_distance", o.thickness);
         kn("detector_half_width", 2.0 * o.thickness);
         std::cout << "# output-dir=" << *o.outputDir << '\n';

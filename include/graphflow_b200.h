@@ -437,6 +437,31 @@ gf_status gf_run_photon(uint64_t seed, uint64_t first_id, uint64_t n, const gf_p
                         double* h_direction, double* h_refl, double* h_trans, uint64_t* h_event_counts,
                         gf_flow_stats* h_stats);
 
+/* One path trace vertex (examples/photon_scattering/PhotonTypes.hpp:189-207 TraceVertexT): kind
+ * 0 source, 1 scatter, 2 transmitted, 3 reflected, 4 absorbed, 5 capped; the completed scatters
+ * (the scatter's own included); position and outgoing direction. */
+typedef struct gf_trace_vertex {
+    uint32_t kind;
+    uint32_t scatter_count;
+    double position[3];
+    double direction[3];
+} gf_trace_vertex;
+
+/* gf_run_photon with the reference's bounded path trace (PhotonFunctors.hpp:201-234 TraceWriter,
+ * recorded at the source, every scatter and the terminal event; PhotonScattering.hpp:49-82,
+ * 158-174): photons with id < M = min(n, trace_photons) keep up to trace_vertices vertices each.
+ * first_id must be 0 when trace_photons > 0. Extra host outputs (NULL to skip):
+ * h_trace_vertices[M * trace_vertices] (id-major; vertex j of id i at i * trace_vertices + j),
+ * h_trace_counts[M] (vertices kept), h_trace_truncated[M] (1 when a vertex did not fit).
+ * trace_photons = 0 runs exactly gf_run_photon. Histories are the same with or without a trace. */
+gf_status gf_run_photon_traced(uint64_t seed, uint64_t first_id, uint64_t n, const gf_photon_params* h_params,
+                               int exec, uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks,
+                               uint32_t* h_event, uint32_t* h_scatter_count, double* h_weight, double* h_cos_exit,
+                               double* h_position, double* h_direction, double* h_refl, double* h_trans,
+                               uint64_t* h_event_counts, gf_flow_stats* h_stats, uint32_t trace_photons,
+                               uint32_t trace_vertices, gf_trace_vertex* h_trace_vertices, uint32_t* h_trace_counts,
+                               uint32_t* h_trace_truncated);
+
 /* Message of the last failed front-end call on this thread (empty if none). */
 size_t gf_last_error(char* h_buf, size_t cap);
 

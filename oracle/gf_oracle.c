@@ -639,8 +639,34 @@ uint64_t gfo_histogram_u32(uint32_t* values, uint64_t n, uint32_t* row_weight, u
 /* purposes: flight 2, scatter 6 (ScalarTransport.hpp:30-32)                                  */
 /* ------------------------------------------------------------------------------------------ */
 
-int gfo_photon_analog(uint64_t seed, uint64_t n, double thickness, double sigma_s, double sigma_a, int isotropic,
-                      uint32_t max_scatters, gfo_photon_terminal* out, int threads)
+/* Bounded path trace of one id (PhotonFunctors.hpp:201-234): a vertex past the bound sets the
+ * truncation flag; ids at or above trace_ids record nothing. */
+typedef struct {
+    uint64_t ids;
+    uint32_t max_vertices;
+    gfo_trace_vertex* vertices;
+    uint32_t* counts;
+    uint32_t* truncated;
+} photon_trace;
+
+static void trace_record(const photon_trace* tr, uint64_t id, uint32_t kind, uint32_t sc, double x, double y,
+                         double z, double ux, double uy, double uz)
+{
+    if (id >= tr->ids)
+        return;
+    uint32_t index = tr->counts[id];
+    if (index >= tr->max_vertices) {
+        tr->truncated[id] = 1u;
+        return;
+    }
+    gfo_trace_vertex v = {kind, sc, x, y, z, ux, uy, uz};
+    tr->vertices[id * tr->max_vertices + index] = v;
+    tr->counts[id] = index + 1u;
+}
+
+static int photon_analog_run(uint64_t seed, uint64_t n, double thickness, double sigma_s, double sigma_a,
+                             int isotropic, uint32_t max_scatters, gfo_photon_terminal* out, const photon_trace* tr,
+                             int threads)
 {
     if (!(thickness > 0.0) || !isfinite(thickness) || sigma_s < 0.0 || sigma_a < 0.0)
         return GFO_INVALID;
@@ -653,6 +679,7 @@ int gfo_photon_analog(uint64_t seed, uint64_t n, double thickness, double sigma_
         double x = 0, y = 0, z = 0, ux = 0, uy = 0, uz = 1;
         uint32_t sc = 0;
         gfo_photon_terminal t;
+        trace_record(tr, id, 0u, 0u, x, y, z, ux, uy, uz);
         for (;;) {
             int reach = 0;
             double fd = 0.0;
@@ -712,8 +739,10 @@ int gfo_photon_analog(uint64_t seed, uint64_t n, double thickness, double sigma_
                 uy = tr * sin(phi);
                 uz = mu;
             }
+            trace_record(tr, id, 1u, sc + 1u, x, y, z, ux, uy, uz);
             ++sc;
         }
+        trace_record(tr, id, t.event + 1u, sc, x, y, z, ux, uy, uz);
         t.scatter_count = sc;
         t.x = x;
         t.y = y;
@@ -724,6 +753,24 @@ int gfo_photon_analog(uint64_t seed, uint64_t n, double thickness, double sigma_
         out[i] = t;
     }
     return bad ? GFO_INVALID : GFO_OK;
+}
+
+int gfo_photon_analog(uint64_t seed, uint64_t n, double thickness, double sigma_s, double sigma_a, int isotropic,
+                      uint32_t max_scatters, gfo_photon_terminal* out, int threads)
+{
+    photon_trace none = {0u, 0u, NULL, NULL, NULL};
+    return photon_analog_run(seed, n, thickness, sigma_s, sigma_a, isotropic, max_scatters, out, &none, threads);
+}
+
+int gfo_photon_analog_traced(uint64_t seed, uint64_t n, double thickness, double sigma_s, double sigma_a,
+                             int isotropic, uint32_t max_scatters, gfo_photon_terminal* out, uint32_t trace_photons,
+                             uint32_t trace_vertices, gfo_trace_vertex* vertices, uint32_t* counts,
+                             uint32_t* truncated, int threads)
+{
+    photon_trace tr = {trace_photons < n ? trace_photons : n, trace_vertices, vertices, counts, truncated};
+    for (uint64_t id = 0; id < tr.ids; ++id)
+        counts[id] = truncated[id] = 0u;
+    return photon_analog_run(seed, n, thickness, sigma_s, sigma_a, isotropic, max_scatters, out, &tr, threads);
 }
 
 /* ------------------------------------------------------------------------------------------ */

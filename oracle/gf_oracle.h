@@ -122,6 +122,19 @@ typedef struct {
 } gfo_photon_terminal;
 int gfo_photon_analog(uint64_t seed, uint64_t n, double thickness, double sigma_s, double sigma_a,
                       int isotropic, uint32_t max_scatters, gfo_photon_terminal* out, int threads);
+/* The same transport with the bounded path trace (examples/photon_scattering/PhotonFunctors.hpp
+ * :201-234 TraceWriter; records at :255 source, :364-369 scatter, :401-406 terminal as event + 1):
+ * ids < min(n, trace_photons) keep up to trace_vertices vertices (vertices[id * trace_vertices + j]),
+ * counts[id] the vertices kept, truncated[id] = 1 when one did not fit. */
+typedef struct {
+    uint32_t kind; /* 0 source, 1 scatter, 2 transmitted, 3 reflected, 4 absorbed, 5 capped */
+    uint32_t scatter_count;
+    double x, y, z, ux, uy, uz;
+} gfo_trace_vertex;
+int gfo_photon_analog_traced(uint64_t seed, uint64_t n, double thickness, double sigma_s, double sigma_a,
+                             int isotropic, uint32_t max_scatters, gfo_photon_terminal* out, uint32_t trace_photons,
+                             uint32_t trace_vertices, gfo_trace_vertex* vertices, uint32_t* counts,
+                             uint32_t* truncated, int threads);
 
 /* ---- weighted slab model of the FP32 Monte Carlo sweep (Henyey-Greenstein, implicit capture,
  *      Russian roulette); FP64 restatement, structure of ScalarTransport.hpp ---- */

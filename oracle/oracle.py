@@ -125,6 +125,10 @@ def _declare(L):
     L.gfo_photon_analog.restype = i32
     L.gfo_photon_analog.argtypes = [u64, u64, C.c_double, C.c_double, C.c_double, i32, u32,
                                     C.POINTER(PhotonTerminal), i32]
+    L.gfo_photon_analog_traced.restype = i32
+    L.gfo_photon_analog_traced.argtypes = [u64, u64, C.c_double, C.c_double, C.c_double, i32, u32,
+                                           C.POINTER(PhotonTerminal), u32, u32, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, i32]
     L.gfo_photon_hg.restype = i32
     L.gfo_photon_hg.argtypes = [u64, u64, u64, C.POINTER(HgParams), C.c_void_p, _f64p, _f64p, _u64p, i32]
 
@@ -300,6 +304,24 @@ def photon_analog(seed, n, thickness, sigma_s, sigma_a, isotropic, max_scatters,
            "photon analog")
     out = np.ctypeslib.as_array(arr)[:n]
     return out
+
+
+TRACE_VERTEX_DTYPE = [("kind", "<u4"), ("scatter_count", "<u4"), ("x", "<f8"), ("y", "<f8"), ("z", "<f8"),
+                      ("ux", "<f8"), ("uy", "<f8"), ("uz", "<f8")]  # gfo_trace_vertex
+
+
+def photon_analog_traced(seed, n, thickness, sigma_s, sigma_a, isotropic, max_scatters, trace_photons,
+                         trace_vertices, threads=0):
+    """photon_analog plus the bounded path trace: (terminals, vertices (M, V), counts (M,), truncated (M,))."""
+    ids = min(n, trace_photons)
+    arr = (PhotonTerminal * max(n, 1))()
+    v = np.zeros((max(ids, 1), max(trace_vertices, 1)), TRACE_VERTEX_DTYPE)
+    counts = np.zeros(max(ids, 1), np.uint32)
+    truncated = np.zeros(max(ids, 1), np.uint32)
+    _check(lib().gfo_photon_analog_traced(seed, n, thickness, sigma_s, sigma_a, int(isotropic), max_scatters, arr,
+                                          trace_photons, trace_vertices, v.ctypes.data, counts.ctypes.data,
+                                          truncated.ctypes.data, threads), "photon analog traced")
+    return np.ctypeslib.as_array(arr)[:n], v[:ids, :trace_vertices], counts[:ids], truncated[:ids]
 
 
 def hg_params(thickness=1.0, mu_a=0.1, mu_s=10.0, g=0.9, roulette_threshold=1e-4, roulette_survival=0.1,

@@ -214,7 +214,7 @@ def test_photon_cli_help():
     ["--backend", "cuda", "--sigma-s", "-1"],
     ["--backend", "cuda", "--max-scatters", "70000"],            # the scatter counter is 16-bit here
     ["--backend", "cuda", "--output-dir", ""],
-    ["--backend", "cuda", "--trace-photons", "4"],               # no path traces in this build
+    ["--backend", "cuda", "--trace-vertices", "-1"],
     ["--backend", "cuda", "--pool-mode", "arena"],
     ["--backend", "cuda", "--exec", "both"],
 ])
@@ -262,7 +262,8 @@ def test_photon_cli_writes_the_reference_run_files(tmp_path):
     """--output-dir writes metadata, outcomes, scatter histogram and exits as the reference does
     (PhotonOutput.hpp:91-197): the outcome files equal the printed report, exits.csv has one row
     per transmitted or reflected photon with a unit exit direction, cos_theta = uz, exits on the
-    slab faces; the trace files carry their headers only."""
+    slab faces; without --trace-photons the trace files carry their headers only and metadata.csv
+    reports the trace defaults (0 photons, 64 vertices)."""
     import csv
     import math
     n, out = 20_000, tmp_path / "run"
@@ -290,4 +291,7 @@ def test_photon_cli_writes_the_reference_run_files(tmp_path):
     meta = {row["key"]: row["value"] for row in csv.DictReader(open(out / "metadata.csv"))}
     assert meta["photons"] == str(n) and meta["mode"] == "isotropic" and meta["count_terminated"] == str(n)
     assert open(out / "traces.csv").read() == "id,step,kind,scatter_count,x,y,z,ux,uy,uz\n"
+    assert open(out / "trace_summary.csv").read() == "id,vertices,truncated\n"
+    assert (meta["trace_enabled"], meta["trace_photons"], meta["trace_vertices"], meta["trace_ids"]) == \
+        ("0", "0", "64", "0")
     assert "# output-dir=" in r.stdout
