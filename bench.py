@@ -316,32 +316,49 @@ class DenseBench:
         totals, table, descs = self.plain.run(self.chunks, self.fills, stream)
         self.pool.release([int(c) for c in descs[:, 0]])
 
-    def check_fused(self):
-        """Size-independent properties at full size: counts sum to N, each port's keys are
-        congruent to the port, the plan matches the totals, the output multiset is the input."""
+    def _gather(self, descs):
+        """Output keys in descriptor (port) order and each key's port, on the device."""
+        torch = self.torch
+        d = torch.from_numpy(descs.astype(self.np.int64)).to(self.pool.column.device)
+        rows = self.pool.column.view(-1, CAPACITY)[d[:, 0]]
+        valid = torch.arange(CAPACITY, device=d.device)[None, :] < d[:, 1:2]
+        return rows[valid], torch.repeat_interleave(d[:, 2], d[:, 1])
+
+    def _expected(self):
+        """The stable partition of the input keys by key mod B (a torch restatement on the device,
+        not the product path): per-port totals and the keys in port order, input order inside a
+        port."""
+        torch = self.torch
+        keys = self.pool.column[: self.n]
+        port = (keys.to(torch.int64) & 0xFFFFFFFF) % self.bins
+        order = torch.argsort(port, stable=True)
+        return torch.bincount(port, minlength=self.bins), keys[order], port[order]
+
+    def check(self, totals, descs, status, exact_order):
+        """Every output slot of the batch against the expected partition: totals, each output
+        chunk's port and fill (the plan), and each port's keys (the sequence for the fused form, the
+        multiset for the plain form, whose in-port order is atomic order)."""
         np, torch = self.np, self.torch
-        st = int(self.fused.status.item())
-        totals = self.fused.totals.cpu().numpy().view(np.uint32)
+        if status != 0 or int(np.asarray(totals, np.uint64).sum()) != self.n:
+            return False
+        exp_tot, exp_keys, exp_port = self._expected()
+        if not np.array_equal(np.asarray(totals, np.int64), exp_tot.cpu().numpy()):
+            return False
+        got_keys, got_port = self._gather(descs)
+        if got_keys.numel() != self.n or not torch.equal(got_port, exp_port):
+            return False
+        if exact_order:
+            return bool(torch.equal(got_keys, exp_keys))
+        m = 0xFFFFFFFF
+        a = torch.sort((got_port << 32) | (got_keys.to(torch.int64) & m)).values
+        b = torch.sort((exp_port << 32) | (exp_keys.to(torch.int64) & m)).values
+        return bool(torch.equal(a, b))
+
+    def check_fused(self):
+        np = self.np
         r = int(self.fused.num_out.item())
         descs = self.fused.descs.cpu().numpy().view(np.uint32)[:3 * r].reshape(-1, 3)
-        ok = st == 0 and int(totals.sum(dtype=np.uint64)) == self.n
-        col = self.pool.column
-        if ok and self.dist != "zipf":
-            # port check on device: key % B == port for every output slot
-            ch = torch.from_numpy(descs[:, 0].astype(np.int64)).to(col.device)
-            fl = torch.from_numpy(descs[:, 1].astype(np.int64)).to(col.device)
-            bn = torch.from_numpy(descs[:, 2].astype(np.int64)).to(col.device)
-            view = col.view(-1, CAPACITY)[ch]
-            idx = torch.arange(CAPACITY, device=col.device)[None, :]
-            valid = idx < fl[:, None]
-            keys = view.to(torch.int64) & 0xFFFFFFFF
-            ok &= bool(((keys % self.bins == bn[:, None]) | ~valid).all().item())
-            ok &= int(valid.sum().item()) == self.n
-            # checksum of checksums: sum of all output keys == sum of all input keys (mod 2^64)
-            out_sum = int((keys * valid).sum().item())
-            in_sum = int((col[: self.n_in * CAPACITY].view(-1, CAPACITY).to(torch.int64) & 0xFFFFFFFF).sum().item())
-            ok &= out_sum == in_sum
-        return ok
+        return self.check(self.fused.totals.cpu().numpy().view(np.uint32), descs, int(self.fused.status.item()), True)
 
 
 def gpu_arm(args):
@@ -411,19 +428,21 @@ def gpu_arm(args):
     correct &= bench.check_fused()
 
     # -------- plain (reference's two-launch form) --------
-    plain_ms = None
-    if rank == 0 or True:
-        for _ in range(max(1, args.warmup // 2)):
-            bench.plain_step(stream)
-        stream.synchronize()
-        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = max(3, min(args.steps // 4, 100))
-        p0.record(stream)
-        for _ in range(reps):
-            bench.plain_step(stream)
-        p1.record(stream)
-        stream.synchronize()
-        plain_ms = max_over_ranks(p0.elapsed_time(p1) / reps)
+    # every rank runs it: the max over ranks is a collective
+    for _ in range(max(1, args.warmup // 2)):
+        bench.plain_step(stream)
+    stream.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = max(3, min(args.steps // 4, 100))
+    p0.record(stream)
+    for _ in range(reps):
+        bench.plain_step(stream)
+    p1.record(stream)
+    stream.synchronize()
+    plain_ms = max_over_ranks(p0.elapsed_time(p1) / reps)
+    totals, _, pdescs = bench.plain.run(bench.chunks, bench.fills, stream)
+    plain_correct = bench.check(totals, pdescs, 0, False)
+    bench.pool.release([int(c) for c in pdescs[:, 0]])
 
     # -------- e2e through the C ABI from pinned host buffers --------
     host_keys = torch.empty(args.n, dtype=torch.int32, pin_memory=True)
@@ -535,12 +554,22 @@ def gpu_arm(args):
         "clocks": clocks.summary(),
         "gpu_launches": args.steps,  # one fused_partition_coop_kernel launch per timed step
         "fused_per_tile_kernel": {"value": world * args.n / (per_tile_ms / 1e3), "ms_per_step": per_tile_ms},
-        "plain": {"value": world * args.n / (plain_ms / 1e3), "ms_per_step": plain_ms,
+        "plain": {"value": world * args.n / (plain_ms / 1e3), "ms_per_step": plain_ms, "correct": plain_correct,
                   "form": "classify kernel + host plan + scatter kernel (reference structure)"},
-        "correct": bool(correct),
-        "sweep": sweep,
-        "configs": extra,
+        # every output slot of the timed batch (and of every sweep case) against the stable partition
+        "correct": bool(correct and plain_correct and all(e["correct"] for e in sweep)),
+        "correct_check": "exact: totals, plan and every port's key sequence vs a torch stable partition on the device",
     }
+    if sweep:
+        fr = [e["hbm_frac"] for e in sweep]
+        line["sweep"] = {"cases": len(sweep), "hbm_frac_min": min(fr), "hbm_frac_max": max(fr),
+                         "ms_min": min(e["ms"] for e in sweep), "ms_max": max(e["ms"] for e in sweep),
+                         "all_correct": all(e["correct"] for e in sweep)}
+    if extra is not None:
+        # the full record of the other configurations first, on its own line; the result line last
+        print("# configs " + json.dumps({"sweep": sweep, "configs": extra}), flush=True)
+        line["serving"] = extra.get("serving", {}).get("summary")
+        line["kernel_workload"] = extra.get("kernel_workload", {}).get("summary")
     print(json.dumps(line), flush=True)
 
 
@@ -702,10 +731,12 @@ def _cfg_photon():
 
 def _cfg_serving():
     """Served mixed stream: whole-flow requests (particle_feedback; photon at 1/100 size; two-node
-    dense chain, B in {2, 8, 32}), N log-uniform, Poisson arrivals, device memory cap 40 GB, 32
-    streams. Both forms run a 256-request stream (N in [1e3, 1e5]); the served form also runs the
-    full 4096-request stream (N in [1e3, 1e7]), at 2000 arrivals/s and with every request arriving
-    at once (capacity). The plain form on the full stream would take tens of minutes."""
+    dense chain, B in {2, 8, 32}), N log-uniform, Poisson arrivals, device memory cap 40 GB. The
+    same streams three ways: the served form with continuous batching (up to 32 requests in
+    flight), the served form one request at a time (max_inflight = 1: the same device-resident
+    per-request work without batching) and the plain form (each request through the Flow, one at a
+    time). The plain form runs the 256-request stream (N in [1e3, 1e5]) only; on the full
+    4096-request stream (N in [1e3, 1e7]) it would take tens of minutes."""
     import numpy as np
     from graphflow_b200 import capi
 
@@ -716,21 +747,40 @@ def _cfg_serving():
                 "p99_latency_ms": float(np.percentile(lat, 99) * 1e3),
                 "peak_inflight": int(st.peak_inflight), "peak_bytes": int(st.peak_bytes),
                 "all_ok": bool(np.all(res["status"] == 0))}
-    out = {"workload": "mixed flow requests, Poisson arrivals, memory cap 40 GB, 32 streams"}
+
+    def short(x):
+        return {"flows_per_s": round(x["flows_per_s"], 1), "p50_ms": round(x["p50_latency_ms"], 2),
+                "p99_ms": round(x["p99_latency_ms"], 2)}
+    out = {"workload": "mixed flow requests, Poisson arrivals at 2000/s, memory cap 40 GB"}
     small = capi.make_requests(256, seed=7, n_min=1_000, n_max=100_000, rate_per_s=2000.0)
-    served, st_s = capi.serve(small, capi.SERVE_BATCHED, max_inflight=32)
-    plain, st_p = capi.serve(small, capi.SERVE_PLAIN)
-    out["stream256_n1e3_1e5_rate2000"] = {"served": summary(small, served, st_s), "plain": summary(small, plain, st_p),
-                                          "results_identical": bool(np.array_equal(served["digest"],
-                                                                                   plain["digest"]))}
+    s32, st32 = capi.serve(small, capi.SERVE_BATCHED, max_inflight=32)
+    s1, st1 = capi.serve(small, capi.SERVE_BATCHED, max_inflight=1)
+    pl, stp = capi.serve(small, capi.SERVE_PLAIN)
+    out["stream256_n1e3_1e5"] = {
+        "served_batched32": summary(small, s32, st32), "served_one_at_a_time": summary(small, s1, st1),
+        "plain": summary(small, pl, stp),
+        "results_identical": bool(np.array_equal(s32["digest"], pl["digest"]) and
+                                  np.array_equal(s1["digest"], pl["digest"]))}
     full = capi.make_requests(4096, seed=8, n_min=1_000, n_max=10_000_000, rate_per_s=2000.0)
-    res, st = capi.serve(full, capi.SERVE_BATCHED, max_inflight=32)
-    out["stream4096_n1e3_1e7_rate2000_served"] = summary(full, res, st)
+    f32, ft32 = capi.serve(full, capi.SERVE_BATCHED, max_inflight=32)
+    f1, ft1 = capi.serve(full, capi.SERVE_BATCHED, max_inflight=1)
+    out["stream4096_n1e3_1e7"] = {"served_batched32": summary(full, f32, ft32),
+                                  "served_one_at_a_time": summary(full, f1, ft1),
+                                  "results_identical": bool(np.array_equal(f32["digest"], f1["digest"]))}
     burst = full.copy()
     burst["arrival_s"] = 0.0
-    res2, st2 = capi.serve(burst, capi.SERVE_BATCHED, max_inflight=32)
-    out["stream4096_n1e3_1e7_all_at_once_served"] = summary(burst, res2, st2)
-    out["stream4096_results_identical_across_arrivals"] = bool(np.array_equal(res["digest"], res2["digest"]))
+    b32, bt32 = capi.serve(burst, capi.SERVE_BATCHED, max_inflight=32)
+    out["stream4096_all_at_once_batched32"] = summary(burst, b32, bt32)
+    a, b, c = (out["stream256_n1e3_1e5"][k] for k in ("served_batched32", "served_one_at_a_time", "plain"))
+    d, e = (out["stream4096_n1e3_1e7"][k] for k in ("served_batched32", "served_one_at_a_time"))
+    out["summary"] = {
+        "s256": {"batched32": short(a), "one_at_a_time": short(b), "plain": short(c),
+                 "identical": out["stream256_n1e3_1e5"]["results_identical"],
+                 "batched_over_plain": round(a["flows_per_s"] / c["flows_per_s"], 1),
+                 "batching_over_one_at_a_time": round(a["flows_per_s"] / b["flows_per_s"], 2)},
+        "s4096": {"batched32": short(d), "one_at_a_time": short(e),
+                  "identical": out["stream4096_n1e3_1e7"]["results_identical"],
+                  "batching_over_one_at_a_time": round(d["flows_per_s"] / e["flows_per_s"], 2)}}
     return out
 
 
@@ -772,18 +822,29 @@ def _cfg_kernel_workload():
     N = 1e7 particles, one partition with B ports, every port into one sink; the fused form and the
     plain form with the shared-staging or the direct (one device atomic per particle) scatter, for
     the balanced and the one-hot distributions (the reference compares the scatter modes on one-hot,
-    docs/benchmarks.md:105-108, on its CPU backend)."""
+    docs/benchmarks.md:105-108, on its CPU backend). One warm-up run per case, then five timed runs
+    (median, min, max): whole runs from Flow construction to the final synchronisation."""
+    import numpy as np
     from graphflow_b200 import capi
-    n, out = 10_000_000, {"workload": "kernel workload through the Flow, N=1e7, C=8192, P=65536, Q=8"}
+    n, out = 10_000_000, {"workload": "kernel workload through the Flow, N=1e7, C=8192, P=65536, Q=8, 5 runs"}
+    summ = {}
     for bins in (64, 1024):
         for dist in ("balanced", "one-hot"):
             for form, fused, scatter in (("fused", True, "shared"), ("plain_shared", False, "shared"),
                                          ("plain_direct", False, "direct")):
-                for _ in range(2):  # the first run of a configuration loads its kernels
+                capi.run_kernel_axes(7, n, bins, dist, scatter, chunk_capacity=8192, live_particles=65536,
+                                     batch_chunks=8, fused=fused)  # loads the configuration's kernels
+                secs = []
+                for _ in range(5):
                     _, st = capi.run_kernel_axes(7, n, bins, dist, scatter, chunk_capacity=8192,
                                                  live_particles=65536, batch_chunks=8, fused=fused)
-                out[f"B{bins}_{dist}_{form}"] = {"seconds": st.seconds, "particles_per_s": n / st.seconds,
-                                                 "partition_batches": st.partition_batches}
+                    secs.append(st.seconds)
+                med = float(np.median(secs))
+                key = f"B{bins}_{dist}_{form}"
+                out[key] = {"seconds_median": med, "seconds_min": min(secs), "seconds_max": max(secs),
+                            "particles_per_s": n / med, "partition_batches": st.partition_batches}
+                summ[key] = round(med * 1e3, 1)
+    out["summary"] = {"ms_median": summ}
     return out
 
 

@@ -119,6 +119,12 @@ gf_status gf_set_tuning(const char* name, int value)
         g_hash_persistent = value != 0;
         return GF_OK;
     }
+    if (std::string(name) == "spin_limit") {
+        // polls a wait between CTAs of the dense fused partition entry points makes before it gives
+        // up with GF_ERR_TIMEOUT; <= 0 restores the default (a synchronous 4-byte copy to the device)
+        const uint32_t v = value <= 0 ? kSpinLimit : (uint32_t)value;
+        return cuda_status(cudaMemcpyToSymbol(g_spin_limit, &v, sizeof(v)));
+    }
     if (std::string(name) == "sink_batch_chunks") {
         if (value < 1 || value > 256)
             return GF_ERR_ARGUMENT;
@@ -363,6 +369,8 @@ gf_status gf_generate_keys_u32(void* stream, int dist, uint64_t seed, uint64_t f
 // file-scope array below, sized kNoAllocScratchBytes, which every GPU that loads this library
 // holds until the process exits.
 // ---------------------------------------------------------------------------------------------
+void gf_set_last_error(const char* message); // gf_flows.cu
+
 namespace {
 
 constexpr uint64_t kNoAllocScratchBytes = 8ull << 20; // 8 MiB
@@ -377,13 +385,21 @@ void* g_noalloc_ptr[kNoAllocMaxDevices];
 cudaError_t g_noalloc_err[kNoAllocMaxDevices];
 
 // Set-up of the current device, done by its first call: take the array's device address and
-// zero the control block (a 64-byte synchronous cudaMemset; it allocates nothing).
+// zero the control block (a 64-byte synchronous cudaMemset; it allocates nothing). The address is
+// kept for the life of the process's primary context on that device.
 void* noalloc_scratch(gf_status* rc)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
-        *rc = e != cudaSuccess ? cuda_status(e) : GF_ERR_RANGE;
+    if (e != cudaSuccess) {
+        *rc = cuda_status(e);
+        return nullptr;
+    }
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        gf_set_last_error(("gf_partition_fused_u32_noalloc: device " + std::to_string(dev) +
+                           " is beyond the " + std::to_string(kNoAllocMaxDevices) + " devices it serves")
+                              .c_str());
+        *rc = GF_ERR_RANGE;
         return nullptr;
     }
     std::call_once(g_noalloc_once[dev], [dev] {
@@ -404,8 +420,6 @@ void* noalloc_scratch(gf_status* rc)
 
 } // namespace
 
-void gf_set_last_error(const char* message); // gf_flows.cu
-
 extern "C" gf_status gf_partition_fused_u32_noalloc(
     void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out, uint32_t capacity, uint64_t pool_slots,
     const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size, uint32_t bins, int classifier,
@@ -423,17 +437,18 @@ extern "C" gf_status gf_partition_fused_u32_noalloc(
                               .c_str());
         return GF_ERR_RANGE;
     }
+    // the finish outputs are checked before anything runs, so a bad argument changes no output
+    if (d_table == nullptr || d_num_out == nullptr || (desc_cap != 0u && d_descs == nullptr))
+        return GF_ERR_ARGUMENT;
     gf_status rc = GF_OK;
     void* scratch = noalloc_scratch(&rc);
     if (scratch == nullptr)
         return rc;
-    rc = gf_partition_fused_u32(stream, d_keys_in, d_keys_out, capacity, pool_slots, d_tiles, n_tiles, tile_size, bins,
-                                classifier, d_reserved, n_reserved, d_totals, d_port_chunks, max_chunks_per_port,
-                                scratch, kNoAllocScratchBytes, d_status);
-    if (rc != GF_OK)
-        return rc;
-    return gf_fused_finish(stream, d_totals, d_port_chunks, bins, capacity, max_chunks_per_port, scratch, d_table,
-                           d_descs, desc_cap, d_num_out, d_status);
+    // partition and finish in one launch where the kernel allows it (same results as the two calls)
+    return gf_partition_fused_full_u32(stream, d_keys_in, d_keys_out, capacity, pool_slots, d_tiles, n_tiles,
+                                       tile_size, bins, classifier, d_reserved, n_reserved, d_totals, d_port_chunks,
+                                       max_chunks_per_port, scratch, kNoAllocScratchBytes, d_table, d_descs, desc_cap,
+                                       d_num_out, d_status);
 }
 
 // Read by the flow entry points (gf_flows.cu, gf_dense_flow.cu, gf_photon.cu).

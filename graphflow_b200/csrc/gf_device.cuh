@@ -168,6 +168,13 @@ GF_D void set_status(uint32_t* status, uint32_t code)
 // one failed tile cannot make the others spin. A wait that gives up records GF_ERR_TIMEOUT.
 constexpr uint32_t kSpinLimit = 1u << 20;
 
+// Poll budget of the waits between CTAs (look-back descriptors, chunk claims, the cooperative
+// grid barrier): kSpinLimit unless a front end lowers it for a failure test. One copy per
+// translation unit (internal linkage); the C ABI's tuning knob "spin_limit" sets the copy of the
+// dense partition entry points (gf_capi.cu). Waits on this CTA's own bulk copies keep kSpinLimit:
+// they always complete, and a CTA must not leave with a copy into its shared memory in flight.
+static __device__ uint32_t g_spin_limit = kSpinLimit;
+
 // ---------------------------------------------------------------------------------------------
 // Synthetic key of stream position (id, 0, 0x100 + dist): uniform (the position's first draw),
 // Zipf over `bins` ports (inverse CDF of a uniform double; cdf[b] = P(rank <= b)), all in port 0,

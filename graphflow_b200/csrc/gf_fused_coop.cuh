@@ -89,10 +89,10 @@ GF_D void bulk_load(void* sdst, const void* gsrc, uint32_t bytes, uint64_t* bar)
                  : "memory");
 }
 
-GF_D uint32_t ld_acquire_u32(const uint32_t* p)
+GF_D unsigned long long ld_acquire_u64(const unsigned long long* p)
 {
-    uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 
@@ -123,14 +123,18 @@ constexpr bool always_valid()
 }
 
 // Control block of the cooperative kernel, right after the FusedCtl in the scratch; the launcher
-// zeroes its first kCoopHdrResetBytes on the stream before every launch. The per-CTA port totals
-// follow it.
+// zeroes it on the stream before every launch. The per-CTA port totals follow it. The scratch may
+// later serve the per-tile look-back kernel, which reads the same bytes as 64-bit descriptors
+// whose bits 33..32 are a publication flag (gf_partition.cuh); everything this kernel leaves
+// there reads as "not published": the control block holds 64-bit words below 2^32 and the per-CTA
+// rows hold counts times four.
 struct CoopHdr {
-    uint32_t total[64]; // batch per-port totals: atomic sums of the CTAs' counts
-    uint32_t done;      // grid-barrier arrivals
-    uint32_t pad[63];
+    unsigned long long total[64]; // batch per-port totals: atomic sums of the CTAs' counts
+    unsigned long long done;      // grid-barrier arrivals
+    unsigned long long pad[7];    // the per-CTA rows behind it start 64-byte aligned (128-bit loads)
 };
-constexpr uint32_t kCoopHdrResetBytes = 65u * sizeof(uint32_t);
+static_assert(sizeof(CoopHdr) % 64u == 0u && sizeof(FusedCtl) % 64u == 0u, "row alignment");
+constexpr uint32_t kCoopHdrResetBytes = sizeof(CoopHdr);
 
 // 128 threads; LANES counter rows with two 16-bit port counters per word (up to 2 * LANES ports).
 template <int LANES>
@@ -178,15 +182,15 @@ struct CoopShape {
 
 // Grid-wide barrier of a cooperative launch on a counter reset before the launch. Bounded: a wait
 // that gives up sets GF_ERR_TIMEOUT and returns.
-GF_D void coop_grid_barrier(uint32_t* counter, uint32_t* status)
+GF_D void coop_grid_barrier(unsigned long long* counter, uint32_t* status)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        atomicAdd(counter, 1u);
+        atomicAdd(counter, 1ull);
         uint32_t polls = 0;
-        while (ld_acquire_u32(counter) < gridDim.x) {
-            if (++polls >= kSpinLimit) {
+        while (ld_acquire_u64(counter) < gridDim.x) {
+            if (++polls >= g_spin_limit) {
                 set_status(status, GF_ERR_TIMEOUT);
                 break;
             }
@@ -357,9 +361,9 @@ __global__ void __launch_bounds__(S::kThreads, 4)
         const uint32_t v = tid < B ? acc[tid] : 0u;
         own[tid] = v;
         if (tid < MB) {
-            cta_tot[(size_t)c * MB + tid] = v;
+            cta_tot[(size_t)c * MB + tid] = v << 2; // see CoopHdr: v < 2^30 (checked by the launcher)
             if (v != 0u)
-                atomicAdd(&hdr->total[tid], v);
+                atomicAdd(&hdr->total[tid], (unsigned long long)v);
         }
     }
     // phase 2 walks the tiles last to first through the same two buffers; its first two tiles are
@@ -391,10 +395,10 @@ __global__ void __launch_bounds__(S::kThreads, 4)
             }
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-                s.x += v[u].x;
-                s.y += v[u].y;
-                s.z += v[u].z;
-                s.w += v[u].w;
+                s.x += v[u].x >> 2;
+                s.y += v[u].y >> 2;
+                s.z += v[u].z >> 2;
+                s.w += v[u].w >> 2;
             }
         }
         uint4* red = reinterpret_cast<uint4*>(cnt); // the counters are zero now and are zeroed again below
@@ -409,7 +413,7 @@ __global__ void __launch_bounds__(S::kThreads, 4)
                     part += e == 0u ? x.x : e == 1u ? x.y : e == 2u ? x.z : x.w;
                 }
             }
-            const uint32_t tot = tid < B ? ld_relaxed_u32(&hdr->total[tid]) : 0u;
+            const uint32_t tot = tid < B ? (uint32_t)ld_relaxed_u64(&hdr->total[tid]) : 0u;
             total[tid] = tot;
             cbase[tid] = tid < B ? (before ? part : tot - own[tid] - part) : 0u;
         }
@@ -756,7 +760,8 @@ __global__ void __launch_bounds__(S::kThreads, 4)
 
 // Host side: one cooperative launch of the kernel with classifier `cls`; the grid is as many CTAs
 // as fit on the device at once, capped by the tiles and by the scratch (the control block, then
-// 4 * 2 * LANES bytes per CTA). The control block's reset words are zeroed here, on the stream.
+// 4 * 2 * LANES bytes per CTA); a batch whose CTAs would own 2^30 keys or more is refused. The
+// control block is zeroed here, on the stream.
 // With `fin` set, the launch also writes the chunk table, descriptors and output count.
 template <typename S, typename Cls>
 cudaError_t launch_fused_coop(cudaStream_t stream, Cls cls, const uint32_t* in, uint32_t* out, uint32_t capacity,
@@ -787,6 +792,9 @@ cudaError_t launch_fused_coop(cudaStream_t stream, Cls cls, const uint32_t* in, 
     const uint64_t cap_ctas = (scratch_bytes - kHead) / kRow;
     g = g < cap_ctas ? g : cap_ctas;
     if (g == 0u)
+        return cudaErrorInvalidConfiguration;
+    // every CTA owns at most ceil(n_tiles / g) tiles of at most kMaxCount keys: below 2^30 (CoopHdr)
+    if (((uint64_t)n_tiles + g - 1u) / g * S::kMaxCount >= (1ull << 30))
         return cudaErrorInvalidConfiguration;
     CoopHdr* hdr = reinterpret_cast<CoopHdr*>(ctl + 1);
     uint32_t* cta_tot = reinterpret_cast<uint32_t*>(hdr + 1);

@@ -18,7 +18,7 @@ constexpr uint32_t kHistC = 8192u;    // chunk capacity of the radix passes
 constexpr uint32_t kHistTile = 4096u; // keys per tile
 constexpr uint32_t kHistBins = 64u;   // 6-bit digits
 constexpr uint32_t kRleBlock = 4096u; // values per run-length block (256 threads x 16)
-constexpr uint64_t kCoopScratch = 64u + 512u + (1u << 18); // control blocks + up to 1024 CTAs x 64 words
+constexpr uint64_t kCoopScratch = 64u + sizeof(CoopHdr) + (1u << 18); // control blocks + up to 1024 CTAs x 64 words
 
 struct DigitClassify {
     static constexpr bool kAlwaysValid = true;

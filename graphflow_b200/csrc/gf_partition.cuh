@@ -382,7 +382,7 @@ constexpr uint32_t kClaimed = 0xFFFFFFFEu;
 // batch's status word already reports a failure).
 GF_D bool poll_again(uint32_t& polls, const uint32_t* status)
 {
-    if (++polls >= kSpinLimit)
+    if (++polls >= g_spin_limit)
         return false;
     if ((polls & 255u) == 0u && ld_relaxed_u32(status) != 0u)
         return false;

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "runner.hpp"
+#include "stages.cuh"
 
 namespace graphflow {
 
@@ -106,6 +107,14 @@ public:
         m_tuning = std::move(t);
     }
     const Tuning& tuning() const { return m_tuning; }
+
+    // Flow.hpp:95-104: receives the per-node detail of a scheduler stall (node names, ready lists,
+    // in-flight batches) just before SchedulerStallError is thrown; the exception's message itself
+    // holds aggregate counters only.
+    void setStallDetailCallback(std::function<void(const std::string&)> callback)
+    {
+        m_stallDetailCallback = std::move(callback);
+    }
 
     template <typename F>
     SourceHandle source(std::string name, F f)
@@ -199,9 +208,8 @@ public:
         runner.setMultiDispatch(m_tuning.multiDispatch);
         if (m_tuning.stallTimeout)
             runner.setStallTimeout(*m_tuning.stallTimeout);
+        runner.setStallDetailCallback(m_stallDetailCallback);
         Stats stats = runner.run();
-        for (const auto& s : stages)
-            stats.kernelLaunches += 0u;
         stats.poolBytes = stats.poolSlots * TStorage::slotBytes();
         cuda::check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
         return stats;
@@ -336,6 +344,7 @@ private:
     std::optional<std::size_t> m_sourceKey;
     std::vector<NodeRecord> m_nodes;
     Tuning m_tuning;
+    std::function<void(const std::string&)> m_stallDetailCallback;
 };
 
 // flow/Flow.hpp:761-762: SoA storage deduced from the payload's field list.

@@ -115,29 +115,29 @@ inline DevicePolicy makeDevicePolicy(const DeviceProperties& d, std::uint64_t n,
                                      const DevicePolicyConfig& c = {})
 {
     using namespace policy_detail;
-    auto fail = [](const std::string& what) { throw std::invalid_argument("graphflow::DevicePolicy: " + what); };
+    auto fail = [](const std::string& what) { throw std::invalid_argument("graphflow device policy rejected: " + what); };
     if (c.waves == 0u || c.targetBlocksPerSm == 0u || c.logicalTileWidth == 0u || c.maxChunkCapacity == 0u ||
         c.liveParticlesPerChunk == 0u || c.memoryBudgetDivisor == 0u || c.hostBudgetBytes == 0u ||
         c.acceleratorBudgetCapBytes == 0u || c.slotBytes == 0u)
-        fail("every policy knob must be non-zero");
+        fail("a zero policy setting (every limit and factor has to be positive)");
     const std::uint64_t warp = d.warpSize == 0u ? 1u : d.warpSize;
     const std::uint64_t threads = d.maxThreadsPerBlock;
     if (threads == 0u)
-        fail("device reports maxThreadsPerBlock == 0");
+        fail("the device properties give zero threads per block");
     if (threads < warp)
-        fail("maxThreadsPerBlock is smaller than the warp size");
+        fail("fewer threads per block than one warp holds");
     if (d.maxBlocksPerGrid == 0u)
-        fail("device reports maxBlocksPerGrid == 0");
+        fail("the device properties give a zero grid limit");
     if (o.liveParticles && (*o.liveParticles == 0u || *o.liveParticles > n))
-        fail("liveParticles must be non-zero and not exceed numParticles");
+        fail("the live-particle count is zero or larger than the run's particles");
 
     // T
     std::uint64_t tile = 0u;
     if (o.tileSize) {
         if (*o.tileSize == 0u)
-            fail("tileSize must be non-zero");
+            fail("a zero tile size was requested");
         if (*o.tileSize > threads)
-            fail("tileSize exceeds maxThreadsPerBlock");
+            fail("the requested tile size needs more threads than one block may have");
         tile = *o.tileSize;
     } else {
         std::uint64_t t = std::max<std::uint64_t>(floorTo(std::max<std::uint64_t>(c.logicalTileWidth, warp), warp), warp);
@@ -153,18 +153,18 @@ inline DevicePolicy makeDevicePolicy(const DeviceProperties& d, std::uint64_t n,
     const std::uint64_t grid = satMul(d.maxBlocksPerGrid, tile);
     const std::uint64_t launch = std::min<std::uint64_t>(c.maxChunkCapacity, grid);
     if (!o.chunkCapacity && launch < tile)
-        fail("maxChunkCapacity and maxBlocksPerGrid cannot hold one tile");
+        fail("no chunk capacity fits a whole tile under the capacity and grid limits");
     const std::uint64_t sms = d.multiProcessorCount == 0u ? 1u : d.multiProcessorCount;
     const std::uint64_t wave = satMul(satMul(satMul(c.waves, sms), c.targetBlocksPerSm), tile);
     std::uint64_t chunk = 0u;
     std::string cap = "explicit";
     if (o.chunkCapacity) {
         if (*o.chunkCapacity == 0u)
-            fail("chunkCapacity must be non-zero");
+            fail("a zero chunk capacity was requested");
         if (*o.chunkCapacity > c.maxChunkCapacity)
-            fail("chunkCapacity exceeds the configured maximum of " + std::to_string(c.maxChunkCapacity));
+            fail("the requested chunk capacity is above the limit of " + std::to_string(c.maxChunkCapacity) + " slots");
         if (*o.chunkCapacity > grid)
-            fail("chunkCapacity needs more tiles than maxBlocksPerGrid allows");
+            fail("one chunk of the requested capacity would need a grid larger than the device allows");
         chunk = *o.chunkCapacity;
     } else {
         std::uint64_t v = std::min(wave, launch);
@@ -195,7 +195,7 @@ inline DevicePolicy makeDevicePolicy(const DeviceProperties& d, std::uint64_t n,
         }
         v = floorTo(v, tile);
         if (v < tile)
-            fail("the payload memory budget cannot hold one tile of the chunk");
+            fail("the memory budget is smaller than one tile of payload");
         chunk = v;
     }
 
@@ -211,24 +211,23 @@ inline DevicePolicy makeDevicePolicy(const DeviceProperties& d, std::uint64_t n,
         if (most == 0u && !o.chunkCapacity) {
             const std::uint64_t shrunk = floorTo(std::min<std::uint64_t>(chunk, budget / c.slotBytes), tile);
             if (shrunk < tile)
-                fail("the payload memory budget cannot hold one tile of the chunk");
+                fail("the memory budget is smaller than one tile of payload");
             chunk = shrunk;
             cap = "memory";
             most = maxLive(chunk, budget, tile, c.slotBytes);
         }
         if (most == 0u)
-            fail("the payload memory budget is too small for one live particle");
+            fail("the memory budget has no room for a single live particle");
         if (liveExplicit && live > most)
-            fail("explicit liveParticles " + std::to_string(live) + " with chunkCapacity " + std::to_string(chunk) +
-                 " exceeds the payload budget of " + std::to_string(budget) + " bytes; the largest feasible P is " +
-                 std::to_string(most));
+            fail(std::to_string(live) + " live particles at " + std::to_string(chunk) + " slots per chunk do not fit " +
+                 std::to_string(budget) + " budget bytes; at most " + std::to_string(most) + " do");
         if (!liveExplicit && live > most) {
             live = most;
             cap = "memory";
         }
     }
     if (!fits(live, chunk, budget, c.slotBytes))
-        fail("liveParticles and chunkCapacity exceed the payload memory budget");
+        fail("the live particles at this chunk capacity need more memory than the budget");
 
     DevicePolicy p;
     p.chunkCapacity = static_cast<std::uint32_t>(chunk);

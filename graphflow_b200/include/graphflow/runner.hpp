@@ -13,39 +13,100 @@
 //                the prefix until outputChunkBound(sum(fill), C, B) fits the available chunks;
 //   4. stop    - source exhausted, all ready lists and in-flight batches empty, no credit left;
 //   5. back off- yield after 64 idle iterations, SchedulerStallError after the stall timeout.
+// On any exception the runner drains every stream, aborts the in-flight stages, releases their
+// leases and chunks and every queued chunk, then rethrows the original exception
+// (GraphRunner.hpp:1173-1185).
+//
+// The queue operations are a policy (CudaQueueOps on the device; the scheduler's CPU tests use a
+// fake), so the scheduling and failure paths are testable without a GPU.
 #pragma once
 
 #include <chrono>
+#include <cstdio>
 #include <deque>
+#include <exception>
+#include <functional>
 #include <memory>
 #include <optional>
+#include <sstream>
 #include <string>
 #include <thread>
 #include <vector>
 
-#include <cuda_runtime.h>
+#include <cuda_runtime_api.h>
 
 #include "core.hpp"
-#include "stages.cuh"
+#include "stage.hpp"
 
 namespace graphflow {
 
 enum class NodeRole { source, transform, sink };
 
-class GraphRunner {
-public:
-    explicit GraphRunner(ChunkLedger& ledger) : m_ledger(ledger) {}
-    GraphRunner(const GraphRunner&) = delete;
-    GraphRunner& operator=(const GraphRunner&) = delete;
+// Failure-injection points of the failure-path tests (the reference's FailurePoint,
+// sched/GraphRunner.hpp:54-59): before a node's completion event is enqueued (item = the node's
+// 1-based enqueue count), before the lease on a batch's i-th chunk is taken (item = i, 0-based),
+// before a stage launch (item = the node's 1-based launch count). The hook may throw; production
+// callers leave it empty.
+enum class FailurePoint { eventEnqueue, leaseAcquire, launch };
 
-    ~GraphRunner()
+// Queue operations on the CUDA device: one non-blocking stream and one completion event per node.
+struct CudaQueueOps {
+    using Event = cudaEvent_t;
+    static void check(cudaError_t e, const char* what)
     {
-        for (auto& n : m_nodes) {
-            if (n.event)
-                cudaEventDestroy(n.event);
-            if (n.stream)
-                cudaStreamDestroy(n.stream);
-        }
+        if (e != cudaSuccess)
+            throw CudaError(std::string("graphflow: ") + what + ": " + cudaGetErrorString(e));
+    }
+    static cudaStream_t makeStream()
+    {
+        cudaStream_t s = nullptr;
+        check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+        return s;
+    }
+    static Event makeEvent()
+    {
+        cudaEvent_t e = nullptr;
+        check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        return e;
+    }
+    static void destroy(cudaStream_t s, Event e) noexcept
+    {
+        if (e)
+            cudaEventDestroy(e);
+        if (s)
+            cudaStreamDestroy(s);
+    }
+    static void record(Event e, cudaStream_t s) { check(cudaEventRecord(e, s), "cudaEventRecord"); }
+    // true once the work recorded before `e` completed
+    static bool done(Event e)
+    {
+        const cudaError_t q = cudaEventQuery(e);
+        if (q == cudaErrorNotReady)
+            return false;
+        check(q, "cudaEventQuery");
+        return true;
+    }
+    static void drain(cudaStream_t s) noexcept
+    {
+        if (s)
+            cudaStreamSynchronize(s);
+    }
+};
+
+template <typename Ops = CudaQueueOps>
+class BasicGraphRunner {
+public:
+    using Event = typename Ops::Event;
+    using FailureHook = std::function<void(FailurePoint, std::uint32_t node, std::uint32_t item)>;
+
+    explicit BasicGraphRunner(ChunkLedger& ledger) : m_ledger(ledger) {}
+    BasicGraphRunner(const BasicGraphRunner&) = delete;
+    BasicGraphRunner& operator=(const BasicGraphRunner&) = delete;
+
+    ~BasicGraphRunner()
+    {
+        for (auto& n : m_nodes)
+            Ops::destroy(n.stream, n.event);
     }
 
     // Adds a node; `route[bin]` is the destination node index (transforms and the source), the
@@ -58,9 +119,10 @@ public:
         n.bins = bins;
         n.route = std::move(route);
         n.stage = stage;
-        cuda::check(cudaStreamCreateWithFlags(&n.stream, cudaStreamNonBlocking), "cudaStreamCreate");
-        cuda::check(cudaEventCreateWithFlags(&n.event, cudaEventDisableTiming), "cudaEventCreate");
         m_nodes.push_back(std::move(n));
+        Node& added = m_nodes.back();
+        added.stream = Ops::makeStream();
+        added.event = Ops::makeEvent();
         return m_nodes.size() - 1u;
     }
 
@@ -79,6 +141,17 @@ public:
     void setStallTimeout(std::chrono::milliseconds t) { m_stallTimeout = t; }
     void setSinkBatchChunks(std::uint32_t q) { m_sinkQ = q == 0u ? 1u : q; }
     void setMultiDispatch(bool on) { m_multiDispatch = on; }
+    // Test hook (see FailurePoint); it runs before the injected operation and may throw.
+    void setFailureHook(FailureHook hook) { m_failureHook = std::move(hook); }
+    // Receives the per-node detail of a stall (names, ready lists, in-flight batches) before
+    // SchedulerStallError is thrown; the exception's message holds aggregate counters only
+    // (Flow.hpp:95-104).
+    void setStallDetailCallback(std::function<void(const std::string&)> callback)
+    {
+        m_stallDetail = std::move(callback);
+    }
+    // Batches node k completed in the last run.
+    std::uint64_t nodeCompleted(std::size_t k) const { return m_nodes.at(k).completed; }
 
     SchedulerStats run()
     {
@@ -104,12 +177,8 @@ public:
                 // 1) retire
                 for (std::size_t k = 0; k < m_nodes.size(); ++k) {
                     Node& node = m_nodes[k];
-                    if (!node.armed)
+                    if (!node.armed || !Ops::done(node.event))
                         continue;
-                    const cudaError_t q = cudaEventQuery(node.event);
-                    if (q == cudaErrorNotReady)
-                        continue;
-                    cuda::check(q, "cudaEventQuery");
                     node.armed = false;
                     std::uint32_t allocated = 0;
                     const bool more = node.stage->advance(node.stream, *node.inflight, allocated);
@@ -124,11 +193,21 @@ public:
                             node.reserved = 0u;
                         }
                         ++stats.completedBatches;
-                        for (const auto& out : outputs) {
-                            if (out.bin >= node.route.size() || node.route[out.bin] < 0)
-                                throw std::runtime_error("graphflow: node '" + node.name + "' produced an unroutable bin");
+                        ++node.completed;
+                        // every route is checked before any output moves: an unroutable bin fails
+                        // the run with the published outputs released (the inputs are still the
+                        // in-flight batch's, released by the teardown)
+                        for (const auto& out : outputs)
+                            if (out.bin >= node.route.size() || node.route[out.bin] < 0) {
+                                for (const auto& o : outputs)
+                                    if (m_ledger.valid(o.handle) &&
+                                        (node.role != NodeRole::source || !inputOf(*node.inflight, o.handle)))
+                                        m_ledger.release(o.handle);
+                                throw std::runtime_error("graphflow: node '" + node.name +
+                                                         "' produced an unroutable bin");
+                            }
+                        for (const auto& out : outputs)
                             m_nodes[static_cast<std::size_t>(node.route[out.bin])].ready.push_back(out);
-                        }
                         if (node.role == NodeRole::sink)
                             sunk += node.inflight->particles();
                         if (node.role != NodeRole::source) {
@@ -137,6 +216,7 @@ public:
                                 m_ledger.release(in.handle);
                             }
                         }
+                        node.leaseHeld = false;
                         node.inflight.reset();
                     }
                     progress = true;
@@ -159,9 +239,9 @@ public:
                     Batch batch{{ChunkDescriptor{h, static_cast<std::uint32_t>(budget), 0u}}, generated};
                     generated += budget;
                     src.inflight = batch;
-                    src.stage->launch(src.stream, *src.inflight);
+                    launch(src, *m_source);
                     ++stats.kernelLaunches;
-                    arm(src);
+                    arm(src, *m_source);
                     progress = true;
                 }
 
@@ -197,11 +277,14 @@ public:
                         std::this_thread::yield();
                         ++stats.yields;
                     }
-                    if (std::chrono::steady_clock::now() - lastProgress > m_stallTimeout)
+                    if (std::chrono::steady_clock::now() - lastProgress > m_stallTimeout) {
+                        if (m_stallDetail)
+                            m_stallDetail(stallDetail());
                         throw SchedulerStallError("graphflow: scheduler stalled (generated=" +
                                                   std::to_string(generated) + " sunk=" + std::to_string(sunk) +
                                                   " free=" + std::to_string(m_ledger.freeCount()) +
                                                   " reserved=" + std::to_string(reservedTotal) + ")");
+                    }
                 } else {
                     idle = 0;
                     lastProgress = std::chrono::steady_clock::now();
@@ -209,13 +292,12 @@ public:
                 ++stats.loopIterations;
             }
         } catch (...) {
-            teardown();
-            throw;
+            const std::exception_ptr original = std::current_exception();
+            teardown(); // noexcept: a teardown failure must not hide the original error
+            std::rethrow_exception(original);
         }
         stats.sourceGenerated = generated;
         stats.sourceSunk = sunk;
-        for (const auto& n : m_nodes)
-            stats.kernelLaunches += 0u;
         return stats;
     }
 
@@ -227,17 +309,50 @@ private:
         std::vector<int> route;
         Stage* stage = nullptr;
         cudaStream_t stream = nullptr;
-        cudaEvent_t event = nullptr;
+        Event event{};
         std::deque<ChunkDescriptor> ready;
         std::optional<Batch> inflight;
         bool armed = false;
+        bool leaseHeld = false; // the in-flight batch's input leases are taken
         std::uint32_t reserved = 0u;
+        std::uint32_t launchCount = 0u, eventEnqueues = 0u;
+        std::uint64_t completed = 0u;
     };
 
-    void arm(Node& n)
+    void arm(Node& n, std::size_t k)
     {
-        cuda::check(cudaEventRecord(n.event, n.stream), "cudaEventRecord");
+        ++n.eventEnqueues;
+        if (m_failureHook)
+            m_failureHook(FailurePoint::eventEnqueue, static_cast<std::uint32_t>(k), n.eventEnqueues);
+        Ops::record(n.event, n.stream);
         n.armed = true;
+    }
+    void arm(Node& n) { arm(n, static_cast<std::size_t>(&n - m_nodes.data())); }
+
+    std::uint32_t launch(Node& n, std::size_t k)
+    {
+        ++n.launchCount;
+        if (m_failureHook)
+            m_failureHook(FailurePoint::launch, static_cast<std::uint32_t>(k), n.launchCount);
+        return n.stage->launch(n.stream, *n.inflight);
+    }
+
+    static bool inputOf(const Batch& b, ChunkHandle h)
+    {
+        for (const auto& c : b.chunks)
+            if (c.handle == h)
+                return true;
+        return false;
+    }
+
+    std::string stallDetail() const
+    {
+        std::ostringstream o;
+        for (const auto& n : m_nodes)
+            o << "node '" << n.name << "': ready=" << n.ready.size() << " inflight=" << (n.inflight ? 1 : 0)
+              << " armed=" << (n.armed ? 1 : 0) << " reserved=" << n.reserved << " completed=" << n.completed
+              << "\n";
+        return o.str();
     }
 
     void convertCredit(Node& n, std::uint32_t allocated, std::uint32_t& reservedTotal)
@@ -280,19 +395,35 @@ private:
         }
         Batch batch;
         batch.chunks.assign(node.ready.begin(), node.ready.begin() + static_cast<std::ptrdiff_t>(wanted));
-        for (const auto& c : batch.chunks)
-            m_ledger.acquireLease(c.handle);
+        // leases on the inputs (not for a source, which owns its chunk); a failure rolls back the
+        // leases taken so far and leaves the chunks in the ready list (GraphRunner.hpp:1046-1059)
+        std::size_t leased = 0;
+        try {
+            if (node.role != NodeRole::source)
+                for (std::size_t i = 0; i < batch.chunks.size(); ++i) {
+                    if (m_failureHook)
+                        m_failureHook(FailurePoint::leaseAcquire, static_cast<std::uint32_t>(k),
+                                      static_cast<std::uint32_t>(i));
+                    m_ledger.acquireLease(batch.chunks[i].handle);
+                    leased = i + 1u;
+                }
+        } catch (...) {
+            for (std::size_t i = 0; i < leased; ++i)
+                m_ledger.releaseLease(batch.chunks[i].handle);
+            throw;
+        }
         node.inflight = std::move(batch);
+        node.leaseHeld = node.role != NodeRole::source;
         node.reserved = reserve;
         reservedTotal += reserve;
         for (std::size_t i = 0; i < wanted; ++i)
             node.ready.pop_front();
-        const std::uint32_t allocated = node.stage->launch(node.stream, *node.inflight);
+        const std::uint32_t allocated = launch(node, k);
         ++stats.kernelLaunches;
         if (node.role == NodeRole::transform && node.bins > 1u)
             ++stats.partitionBatches;
         convertCredit(node, allocated, reservedTotal);
-        arm(node);
+        arm(node, k);
         if (reservedTotal > stats.peakReservedChunks)
             stats.peakReservedChunks = reservedTotal;
         return true;
@@ -314,18 +445,19 @@ private:
     void teardown() noexcept
     {
         for (auto& n : m_nodes)
-            if (n.stream)
-                cudaStreamSynchronize(n.stream);
+            Ops::drain(n.stream);
         for (auto& n : m_nodes) {
             try {
+                n.armed = false;
                 if (n.inflight) {
                     n.stage->abort();
                     for (const auto& c : n.inflight->chunks) {
-                        if (n.role != NodeRole::source)
+                        if (n.leaseHeld && m_ledger.valid(c.handle))
                             m_ledger.releaseLease(c.handle);
                         if (m_ledger.valid(c.handle))
                             m_ledger.release(c.handle);
                     }
+                    n.leaseHeld = false;
                     n.inflight.reset();
                 }
                 for (const auto& c : n.ready)
@@ -347,6 +479,10 @@ private:
     bool m_multiDispatch = false;
     std::size_t m_roundRobin = 0;
     std::chrono::milliseconds m_stallTimeout{60000};
+    FailureHook m_failureHook;
+    std::function<void(const std::string&)> m_stallDetail;
 };
+
+using GraphRunner = BasicGraphRunner<CudaQueueOps>;
 
 } // namespace graphflow

@@ -18,39 +18,10 @@
 
 #include "gf_hash.cuh"
 #include "kernels.cuh"
+#include "stage.hpp"
 #include "storage.cuh"
 
 namespace graphflow {
-
-struct Batch {
-    std::vector<ChunkDescriptor> chunks;
-    std::uint64_t firstId = 0u;
-    std::uint64_t particles() const
-    {
-        std::uint64_t n = 0;
-        for (const auto& c : chunks)
-            n += c.fill;
-        return n;
-    }
-};
-
-class Stage {
-public:
-    virtual ~Stage() = default;
-    // Enqueue the batch's first device stage on `s`. Returns the output chunks it acquired.
-    virtual std::uint32_t launch(cudaStream_t s, const Batch& b) = 0;
-    // Called after the last enqueued device work completed. Returns true when it enqueued more;
-    // `allocated` receives the output chunks acquired by this call.
-    virtual bool advance(cudaStream_t s, const Batch& b, std::uint32_t& allocated) = 0;
-    // Publish the batch's outputs (Execution.hpp:2457-2461).
-    virtual void finish(const Batch& b, std::vector<ChunkDescriptor>& outputs) = 0;
-    // Release every unpublished output; the stage is single-use afterwards (Execution.hpp:2652-2656).
-    virtual void abort() = 0;
-    virtual std::uint64_t launches() const { return m_launches; }
-
-protected:
-    std::uint64_t m_launches = 0;
-};
 
 namespace detail {
 

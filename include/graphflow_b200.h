@@ -185,11 +185,15 @@ gf_status gf_partition_fused_full_u32(void* stream, const uint32_t* d_keys_in, u
  * every input and output buffer. The scratch is a fixed 8 MiB array inside the library, held by
  * every GPU that loads it until the process exits, so one batch may use at most
  * 64 + 8 x tiles x ports <= 8 MiB (e.g. 24,415 tiles of 4096 keys x 32 ports); larger batches
- * get GF_ERR_RANGE and a message from gf_last_error(). The first call on a device sets the array
- * up (takes its device address, zeroes its 64-byte control block with a synchronous memset);
- * make that first call before any stream capture. Every call on a device shares the array and
- * it keeps the last call's contents: calls that overlap on the GPU race, so order them on one
- * stream or synchronise between them. No call allocates or frees device memory. */
+ * get GF_ERR_RANGE and a message from gf_last_error(). Devices 0..63 are served (others get
+ * GF_ERR_RANGE and a message). The first call on a device sets the array up (takes its device
+ * address, zeroes its 64-byte control block with a synchronous memset); make that first call
+ * before any stream capture. The set-up holds for the life of the process's primary context on
+ * that device: after cudaDeviceReset (or anything else that destroys the primary context) this
+ * entry point must not be called again in the process. Every call on a device shares the array
+ * and it keeps the last call's contents: calls that overlap on the GPU race, so order them on
+ * one stream or synchronise between them. The finish outputs (d_table, d_num_out, d_descs) are
+ * checked before anything runs. No call allocates or frees device memory. */
 gf_status gf_partition_fused_u32_noalloc(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_out,
                                          uint32_t capacity, uint64_t pool_slots, const gf_tile* d_tiles,
                                          uint32_t n_tiles, uint32_t tile_size, uint32_t bins, int classifier,
@@ -450,7 +454,9 @@ typedef struct gf_trace_vertex {
 /* gf_run_photon with the reference's bounded path trace (PhotonFunctors.hpp:201-234 TraceWriter,
  * recorded at the source, every scatter and the terminal event; PhotonScattering.hpp:49-82,
  * 158-174): photons with id < M = min(n, trace_photons) keep up to trace_vertices vertices each.
- * first_id must be 0 when trace_photons > 0. Extra host outputs (NULL to skip):
+ * first_id must be 0 when trace_photons > 0 (GF_ERR_ARGUMENT otherwise, in both execution
+ * forms); with trace_vertices = 0 no vertex fits, so every traced id reports truncated = 1.
+ * Extra host outputs (NULL to skip):
  * h_trace_vertices[M * trace_vertices] (id-major; vertex j of id i at i * trace_vertices + j),
  * h_trace_counts[M] (vertices kept), h_trace_truncated[M] (1 when a vertex did not fit).
  * trace_photons = 0 runs exactly gf_run_photon. Histories are the same with or without a trace. */

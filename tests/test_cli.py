@@ -159,7 +159,7 @@ def test_cli_defaults_come_from_the_device_policy():
 @pytest.mark.gpu
 def test_cli_rejects_a_live_particle_count_above_the_run():
     r = _run("--backend", "cuda", "--particles", "1000", "--live-particles", "2000")
-    assert r.returncode == 2 and "liveParticles" in r.stderr
+    assert r.returncode == 2 and "live-particle count" in r.stderr
 
 
 @pytest.mark.gpu

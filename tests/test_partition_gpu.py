@@ -230,3 +230,69 @@ def test_oversized_tile_sets_status_invalid():
     torch.cuda.synchronize()
     assert int(status.item()) == capi.GF_INVALID
     assert int(counts[:bins].sum().item()) == 0
+
+
+def test_cooperative_scratch_reads_unpublished_to_the_per_tile_kernel():
+    """A caller scratch serves the cooperative kernel, then the per-tile look-back kernel. The
+    per-tile kernel reads the scratch as 64-bit (epoch, flag, value) descriptors and accepts a word
+    whose flag bits (33..32) are non-zero and whose epoch is its own; whatever the cooperative
+    kernel leaves there must carry flag 0. The first batch's port-1 total is 9 = 4 x 2 + 1, the
+    flag-1 word of the next launch's epoch (2) in a layout that stored raw 32-bit totals."""
+    capacity, bins = 8192, 2
+    n_odd, n_even = 9, 300_000
+    keys = np.concatenate([np.full(n_even, 4, np.uint32), np.full(n_odd, 7, np.uint32)])
+    n_in = -(-keys.size // capacity)
+    pool = ChunkPool(n_in + capi.output_chunk_bound(keys.size, capacity, bins) + 8, capacity)
+    chunks = list(range(n_in))
+    fills = [capacity] * (n_in - 1) + [keys.size - capacity * (n_in - 1)]
+    _fill_pool(pool, chunks, fills, keys)
+    for c in chunks:
+        pool.free.remove(c)
+    part = FusedPartition(pool, bins, tile_size=4096, max_batch_particles=8_000_000)
+    part.scratch.zero_()
+    totals, _, descs = part.run(chunks, fills)
+    assert list(totals) == [n_even, n_odd]
+    words = part.scratch.cpu().numpy().view(np.uint64)[8:]  # after the 64-byte control block
+    assert not np.any(words & np.uint64(3 << 32)), "a cooperative word reads as a published descriptor"
+    # the next batch on the same scratch runs the per-tile kernel (chunks of 1024 slots)
+    pool2 = ChunkPool(400, 1024)
+    part2 = FusedPartition(pool2, bins, tile_size=1024, max_batch_particles=200_003)
+    assert part.scratch_bytes >= part2.scratch_bytes
+    part2.scratch, part2.scratch_bytes = part.scratch, part.scratch_bytes
+    k2 = O.generate_keys_u32("uniform", 5, 200_003, bins)
+    chunks2 = pool2.acquire(-(-k2.size // 1024))
+    fills2 = [1024] * (len(chunks2) - 1) + [k2.size - 1024 * (len(chunks2) - 1)]
+    _fill_pool(pool2, chunks2, fills2, k2)
+    col = pool2.column.cpu().numpy().view(np.uint32)
+    snap = {c: col[c * 1024:(c + 1) * 1024].copy() for c in chunks2}
+    _check(pool2, chunks2, fills2, k2, bins, part2.run(chunks2, fills2), True, snap)
+
+
+def test_cooperative_barrier_wait_gives_up_under_a_short_limit():
+    """Failure detection without a fault: with the poll budget of the waits between CTAs cut to
+    one poll (tuning knob spin_limit), every CTA of the cooperative launch but the last to arrive
+    gives up at the grid barrier. The batch reports GF_ERR_TIMEOUT, nothing is published (the
+    reservation goes back to the pool), and with the default budget restored the next batch on the
+    same scratch is exact."""
+    n, capacity, bins = 4_000_003, 8192, 64
+    keys = O.generate_keys_u32("uniform", 9, n, bins)
+    n_in = -(-n // capacity)
+    pool = ChunkPool(n_in + capi.output_chunk_bound(n, capacity, bins), capacity)
+    chunks = list(range(n_in))
+    fills = [capacity] * (n_in - 1) + [n - capacity * (n_in - 1)]
+    _fill_pool(pool, chunks, fills, keys)
+    for c in chunks:
+        pool.free.remove(c)
+    col = pool.column.cpu().numpy().view(np.uint32)
+    snap = {c: col[c * capacity:(c + 1) * capacity].copy() for c in chunks}
+    part = FusedPartition(pool, bins, tile_size=4096, max_batch_particles=n)
+    free_before = len(pool.free)
+    capi.check(capi.lib().gf_set_tuning(b"spin_limit", 1), "tuning")
+    try:
+        with pytest.raises(BatchError):
+            part.run(chunks, fills)
+        assert int(part.status.item()) == capi.GF_ERR_TIMEOUT
+        assert len(pool.free) == free_before
+    finally:
+        capi.check(capi.lib().gf_set_tuning(b"spin_limit", 0), "tuning")
+    _check(pool, chunks, fills, keys, bins, part.run(chunks, fills), True, snap)

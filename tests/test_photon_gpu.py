@@ -86,7 +86,10 @@ def test_weighted_fp64_matches_fp64_oracle():
     same = (got["event"] == terms["event"]) & (got["scatter_count"] == terms["scatter_count"])
     assert same.mean() >= 0.999
     assert np.allclose(got["weight"][same], terms["weight"][same], rtol=1e-9, atol=0)
-    assert np.array_equal(got["event_counts"], ev)  or same.mean() < 1.0
+    # every photon is counted once under its terminal event, so each history that differs moves at
+    # most one count from one event to another
+    diff = np.abs(got["event_counts"].astype(np.int64) - ev.astype(np.int64)).sum()
+    assert int(got["event_counts"].sum()) == n and diff <= 2 * int((~same).sum())
 
 
 def test_photon_argument_errors():
