@@ -100,7 +100,29 @@ _SIGS = {
                       _VP],
     "gf_run_photon_traced": [_U64, _U64, _U64, _VP, _I32, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                              _VP, _VP, _VP, _U32, _U32, _VP, _VP, _VP],
+    "gf_classify_dense": [_VP, _VP, _U32, _U64, _VP, _U32, _U32, _U32, _I32, _VP, _VP, _VP, _VP],
+    "gf_scatter": [_VP, _VP, _VP, _U32, _U64, _VP, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _I32, _I32, _VP, _VP],
+    "gf_transform": [_VP, _VP, _VP, _U32, _U64, _VP, _U32, _VP, _U32, _I32, _VP, _VP],
+    "gf_partition_fused": [_VP, _VP, _U32, _U64, _VP, _U32, _U32, _I32, _I32, _VP, _VP, _U32, _VP, _VP, _U32, _VP,
+                           _U64, _VP, _VP, _U32, _VP, _VP],
 }
+
+# generic ABI (gf_generic.cu): record types, classifiers, updaters, transforms
+REC_U32, REC_KEYREC, REC_PARTICLE, REC_R16 = 0, 1, 2, 3
+CLS_FEEDBACK_FILTER, CLS_FEEDBACK_SELECT = 16, 17
+UPD_NONE, UPD_SET_BIN, UPD_FEEDBACK = 0, 1, 2
+XF_IDENTITY, XF_ADD_WEIGHT = 0, 1
+
+
+class Columns(C.Structure):
+    """gf_columns: a registered record type, its layout and device column pointers."""
+    _fields_ = [("record", C.c_int32), ("layout", C.c_int32), ("column", C.c_void_p * 4)]
+
+
+class FunctorParams(C.Structure):
+    """gf_functor_params: seed, stream purpose and the registered functors' constants."""
+    _fields_ = [("seed", C.c_uint64), ("purpose", C.c_uint32), ("max_visits", C.c_uint32),
+                ("increment", C.c_uint32), ("pad", C.c_uint32)]
 
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
 
@@ -110,7 +132,8 @@ class FlowStats(C.Structure):
     _fields_ = [("completed_batches", C.c_uint64), ("partition_batches", C.c_uint64),
                 ("kernel_launches", C.c_uint64), ("loop_iterations", C.c_uint64), ("generated", C.c_uint64),
                 ("sunk", C.c_uint64), ("pool_chunks", C.c_uint32), ("peak_live_chunks", C.c_uint32),
-                ("peak_reserved_chunks", C.c_uint32), ("peak_ready_chunks", C.c_uint32), ("seconds", C.c_double)]
+                ("peak_reserved_chunks", C.c_uint32), ("peak_ready_chunks", C.c_uint32), ("seconds", C.c_double),
+                ("setup_seconds", C.c_double), ("loop_seconds", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

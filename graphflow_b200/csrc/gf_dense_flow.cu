@@ -87,6 +87,8 @@ extern "C" gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins
             h_stats->peak_reserved_chunks = s.peakReservedChunks;
             h_stats->peak_ready_chunks = s.peakReadyChunks;
             h_stats->seconds = sec;
+            h_stats->setup_seconds = s.setupSeconds;
+            h_stats->loop_seconds = s.loopSeconds;
         }
     });
 }

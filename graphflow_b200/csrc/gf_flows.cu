@@ -57,6 +57,8 @@ void fill_stats(const graphflow::SchedulerStats& s, double seconds, gf_flow_stat
     out->peak_reserved_chunks = s.peakReservedChunks;
     out->peak_ready_chunks = s.peakReadyChunks;
     out->seconds = seconds;
+    out->setup_seconds = s.setupSeconds;
+    out->loop_seconds = s.loopSeconds;
 }
 
 } // namespace

@@ -199,6 +199,8 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
         hStats->peak_reserved_chunks = stats.peakReservedChunks;
         hStats->peak_ready_chunks = stats.peakReadyChunks;
         hStats->seconds = sec;
+        hStats->setup_seconds = stats.setupSeconds;
+        hStats->loop_seconds = stats.loopSeconds;
     }
 }
 

@@ -178,6 +178,8 @@ struct SchedulerStats {
     std::uint32_t chunkCapacity = 0u;
     std::uint64_t kernelLaunches = 0u;
     std::uint64_t partitionBatches = 0u;
+    double setupSeconds = 0.0; // Flow::run: storage, stages and runner built
+    double loopSeconds = 0.0;  // Flow::run: the scheduler loop
 };
 
 inline std::string formatSchedulerStats(const SchedulerStats& s)

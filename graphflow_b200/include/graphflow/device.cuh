@@ -7,6 +7,8 @@
 #pragma once
 
 #include <cstdint>
+#include <map>
+#include <mutex>
 #include <type_traits>
 #include <utility>
 
@@ -248,25 +250,94 @@ inline void check(cudaError_t e, const char* what)
     }
 }
 
-// Owning device buffer.
+namespace detail {
+// Blocks of the front end's buffers kept for reuse, keyed by (device, exact size): a Flow run
+// allocates the same storage and stage buffers as the previous run of its configuration, and
+// cudaMalloc / cudaMallocHost (which pin, map and sometimes wait on the driver) cost up to
+// hundreds of milliseconds where reuse costs nothing. A released block keeps the semantics of
+// cudaFree: the device is synchronised first, so no queued work can still use it when it is
+// handed out again. Blocks beyond the cap are freed; cached blocks are held until process exit.
+class BlockCache {
+public:
+    BlockCache(bool host, std::size_t cap) : m_host(host), m_cap(cap) {}
+    void* take(std::size_t bytes, int dev)
+    {
+        std::lock_guard<std::mutex> lock(m_mutex);
+        auto range = m_blocks.equal_range(bytes);
+        for (auto it = range.first; it != range.second; ++it)
+            if (it->second.first == dev) {
+                void* p = it->second.second;
+                m_blocks.erase(it);
+                m_cached -= bytes;
+                return p;
+            }
+        return nullptr;
+    }
+    void give(void* p, std::size_t bytes, int dev)
+    {
+        cudaDeviceSynchronize();
+        {
+            std::lock_guard<std::mutex> lock(m_mutex);
+            if (m_cached + bytes <= m_cap) {
+                m_blocks.emplace(bytes, std::make_pair(dev, p));
+                m_cached += bytes;
+                return;
+            }
+        }
+        if (m_host)
+            cudaFreeHost(p);
+        else
+            cudaFree(p);
+    }
+
+private:
+    bool m_host;
+    std::size_t m_cap, m_cached = 0;
+    std::mutex m_mutex;
+    std::multimap<std::size_t, std::pair<int, void*>> m_blocks;
+};
+inline BlockCache& deviceBlocks()
+{
+    static BlockCache* c = new BlockCache(false, std::size_t(2) << 30); // never destroyed: no CUDA calls at exit
+    return *c;
+}
+inline BlockCache& hostBlocks()
+{
+    static BlockCache* c = new BlockCache(true, std::size_t(256) << 20);
+    return *c;
+}
+inline int currentDevice()
+{
+    int d = 0;
+    cudaGetDevice(&d);
+    return d;
+}
+} // namespace detail
+
+// Owning device buffer (blocks reused through detail::deviceBlocks).
 template <typename T>
 class Buffer {
 public:
     Buffer() = default;
     explicit Buffer(std::size_t n) : m_n(n)
     {
-        if (n != 0u)
-            check(cudaMalloc(&m_p, n * sizeof(T)), "cudaMalloc");
+        if (n != 0u) {
+            m_dev = detail::currentDevice();
+            m_p = static_cast<T*>(detail::deviceBlocks().take(n * sizeof(T), m_dev));
+            if (m_p == nullptr)
+                check(cudaMalloc(&m_p, n * sizeof(T)), "cudaMalloc");
+        }
     }
     Buffer(const Buffer&) = delete;
     Buffer& operator=(const Buffer&) = delete;
-    Buffer(Buffer&& o) noexcept : m_p(o.m_p), m_n(o.m_n) { o.m_p = nullptr, o.m_n = 0; }
+    Buffer(Buffer&& o) noexcept : m_p(o.m_p), m_n(o.m_n), m_dev(o.m_dev) { o.m_p = nullptr, o.m_n = 0; }
     Buffer& operator=(Buffer&& o) noexcept
     {
         if (this != &o) {
             reset();
             m_p = o.m_p;
             m_n = o.m_n;
+            m_dev = o.m_dev;
             o.m_p = nullptr;
             o.m_n = 0;
         }
@@ -280,11 +351,12 @@ private:
     void reset()
     {
         if (m_p != nullptr)
-            cudaFree(m_p);
+            detail::deviceBlocks().give(m_p, m_n * sizeof(T), m_dev);
         m_p = nullptr;
     }
     T* m_p = nullptr;
     std::size_t m_n = 0;
+    int m_dev = 0;
 };
 
 // Owning pinned host buffer (the mapped staging of the reference's stages).
@@ -294,8 +366,11 @@ public:
     HostBuffer() = default;
     explicit HostBuffer(std::size_t n) : m_n(n)
     {
-        if (n != 0u)
-            check(cudaMallocHost(&m_p, n * sizeof(T)), "cudaMallocHost");
+        if (n != 0u) {
+            m_p = static_cast<T*>(detail::hostBlocks().take(n * sizeof(T), -1));
+            if (m_p == nullptr)
+                check(cudaMallocHost(&m_p, n * sizeof(T)), "cudaMallocHost");
+        }
     }
     HostBuffer(const HostBuffer&) = delete;
     HostBuffer& operator=(const HostBuffer&) = delete;
@@ -304,7 +379,7 @@ public:
     {
         if (this != &o) {
             if (m_p != nullptr)
-                cudaFreeHost(m_p);
+                detail::hostBlocks().give(m_p, m_n * sizeof(T), -1);
             m_p = o.m_p;
             m_n = o.m_n;
             o.m_p = nullptr;
@@ -315,7 +390,7 @@ public:
     ~HostBuffer()
     {
         if (m_p != nullptr)
-            cudaFreeHost(m_p);
+            detail::hostBlocks().give(m_p, m_n * sizeof(T), -1);
     }
     T* data() const { return m_p; }
     T& operator[](std::size_t i) const { return m_p[i]; }

@@ -189,6 +189,7 @@ public:
         validateForRun(source);
         if (itemCount != 0u && itemCount - 1u > rng::maxStreamId)
             throw std::overflow_error("graphflow: item count exceeds the 32 bit RNG stream-id range");
+        const auto t0 = std::chrono::steady_clock::now();
         const Config config = resolveConfig(itemCount);
         m_device.makeCurrent();
         TStorage storage(m_device, config.numChunks, config.chunkCapacity);
@@ -209,7 +210,10 @@ public:
         if (m_tuning.stallTimeout)
             runner.setStallTimeout(*m_tuning.stallTimeout);
         runner.setStallDetailCallback(m_stallDetailCallback);
+        const auto t1 = std::chrono::steady_clock::now();
         Stats stats = runner.run();
+        stats.setupSeconds = std::chrono::duration<double>(t1 - t0).count();
+        stats.loopSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
         stats.poolBytes = stats.poolSlots * TStorage::slotBytes();
         cuda::check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
         return stats;

@@ -202,6 +202,102 @@ gf_status gf_partition_fused_u32_noalloc(void* stream, const uint32_t* d_keys_in
                                          uint32_t* d_table, gf_out_desc* d_descs, uint32_t desc_cap,
                                          uint32_t* d_num_out, uint32_t* d_status);
 
+/* ---- generic partition and transform over registered record types ---------------------------
+ * The entry points the reference's stages bind for any payload (flow/Execution.hpp:709-776
+ * TransformKernel, :870-954 classify, :985-1189 scatter), over a column descriptor instead of the
+ * u32 key column. User functors cannot cross a C ABI: each record type below and each classifier,
+ * updater and transform id is a compile-time instantiation of the same kernels the C++ Flow runs
+ * (the explicit instantiation table of gf_generic.cu). A record/functor pair the table does not
+ * list returns GF_ERR_ARGUMENT. */
+enum {
+    GF_REC_U32 = 0,      /* {u32 key}                                                          */
+    GF_REC_KEYREC = 1,   /* {u32 id, u32 key} (the dense chain's record)                       */
+    GF_REC_PARTICLE = 2, /* {u64 id, u32 property, u32 weight, u32 visit}: particle_feedback's
+                          * record (examples/particle_feedback/ParticleTypes.hpp:35-47); AoS
+                          * slots are 24 bytes (the C struct's alignment padding)             */
+    GF_REC_R16 = 3       /* {u64 key, f32 weight, u32 tag} (the hash path's record)            */
+};
+/* Device columns of a pool of one record type: SoA = column[i] holds field i (in the record's
+ * field order above) of every slot; AoS = column[0] holds the slots. */
+typedef struct gf_columns {
+    int32_t record; /* GF_REC_* */
+    int32_t layout; /* GF_LAYOUT_SOA / GF_LAYOUT_AOS */
+    void* column[4];
+} gf_columns;
+
+/* Further registered classifiers (GF_CLS_KEY_MOD and GF_CLS_ID_* above apply to the records with
+ * a key / an id field): */
+enum {
+    GF_CLS_FEEDBACK_FILTER = 16, /* particle_feedback Filter: bin = draw >= property ? 1 : 0
+                                  * (ParticleFunctors.hpp FilterByProperty)                       */
+    GF_CLS_FEEDBACK_SELECT = 17  /* A/B: draw < 2^31 ? sink (0) : visit < max_visits ? feedback (1)
+                                  * : capped (2) (SelectOutcome)                                  */
+};
+/* Registered updaters, applied to every payload the scatter emits (purpose + 1 engine). */
+enum {
+    GF_UPD_NONE = 0,
+    GF_UPD_SET_BIN = 1,  /* weight = bin (KernelAxes.hpp:80-106, particle records)               */
+    GF_UPD_FEEDBACK = 2  /* on bin 1 (feedback): checked weight += increment, visit += 1
+                          * (ParticleFunctors.hpp UpdateWeight; overflow sets GF_OVERFLOW)        */
+};
+/* Registered transforms (out-of-place, dense concatenation of the batch). */
+enum {
+    GF_XF_IDENTITY = 0,   /* copy                                                              */
+    GF_XF_ADD_WEIGHT = 1  /* particle records: checked weight += increment, visit += 1            */
+};
+/* Functor parameters: seed (the keyed RNG streams, rng/ParticleRng.hpp), the node's stream
+ * purpose (functor purpose; its updater uses purpose + 1), and the functor's constants. */
+typedef struct gf_functor_params {
+    uint64_t seed;
+    uint32_t purpose;
+    uint32_t max_visits; /* GF_CLS_FEEDBACK_SELECT */
+    uint32_t increment;  /* GF_UPD_FEEDBACK, GF_XF_ADD_WEIGHT */
+    uint32_t pad;
+} gf_functor_params;
+
+/* One <= tile slice of one input chunk and its position in the batch's dense output (the
+ * reference's transform tile: TileDescriptor plus outPosition, Execution.hpp:709-776). */
+typedef struct gf_move_tile {
+    uint32_t in_chunk;
+    uint32_t in_offset;
+    uint32_t count;
+    uint32_t out_pos;
+} gf_move_tile;
+
+/* flow/Execution.hpp:870-954 PartitionClassifyKernel for any registered record: per-port counts
+ * in d_counts[0..bins) and the status slot d_counts[bins] (a result >= bins), d_bin_ids per slot. */
+gf_status gf_classify_dense(void* stream, const gf_columns* h_cols, uint32_t capacity, uint64_t pool_slots,
+                            const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size, uint32_t bins,
+                            int classifier, const gf_functor_params* h_params, uint32_t* d_bin_ids,
+                            uint32_t* d_counts, uint32_t* d_status);
+
+/* flow/Execution.hpp:985-1189 PartitionScatterKernel for any registered record: every field of
+ * each payload moves from h_in's slot to the planned slot of h_out (table = [binBase, chunkIndex]
+ * of the plan, next[bins] zeroed), the updater applied on the way. mode GF_SCATTER_SHARED or
+ * _DIRECT. h_in and h_out may describe the same columns. */
+gf_status gf_scatter(void* stream, const gf_columns* h_in, const gf_columns* h_out, uint32_t capacity,
+                     uint64_t pool_slots, const gf_tile* d_tiles, uint32_t n_tiles, uint32_t tile_size, uint32_t bins,
+                     const uint32_t* d_bin_ids, const uint32_t* d_table, uint32_t* d_next, uint32_t* d_counts,
+                     int mode, int updater, const gf_functor_params* h_params, uint32_t* d_status);
+
+/* flow/Execution.hpp:709-776 TransformKernel: input item i of tile t goes, transformed, to dense
+ * output position t.out_pos + i, i.e. chunk d_out_chunks[pos / C] at offset pos % C. */
+gf_status gf_transform(void* stream, const gf_columns* h_in, const gf_columns* h_out, uint32_t capacity,
+                       uint64_t pool_slots, const gf_move_tile* d_tiles, uint32_t n_tiles,
+                       const uint32_t* d_out_chunks, uint32_t n_out, int transform,
+                       const gf_functor_params* h_params, uint32_t* d_status);
+
+/* gf_partition_fused_full_u32 for any registered record, classifier and updater: one fused
+ * classify -> plan -> scatter launch plus its device finish (the per-tile look-back kernel;
+ * ports < 4096), output chunks from the caller's reservation, per-port sequences in input order.
+ * Scratch: gf_fused_scratch_bytes(n_tiles, bins). */
+gf_status gf_partition_fused(void* stream, const gf_columns* h_cols, uint32_t capacity, uint64_t pool_slots,
+                             const gf_tile* d_tiles, uint32_t n_tiles, uint32_t bins, int classifier, int updater,
+                             const gf_functor_params* h_params, const uint32_t* d_reserved, uint32_t n_reserved,
+                             uint32_t* d_totals, unsigned long long* d_port_chunks, uint32_t max_chunks_per_port,
+                             void* d_scratch, uint64_t scratch_bytes, uint32_t* d_table, gf_out_desc* d_descs,
+                             uint32_t desc_cap, uint32_t* d_num_out, uint32_t* d_status);
+
 /* ---- hash partition of 16-byte records (large port counts) ---------------------------------- */
 
 /* Columns of the 16-byte record {u64 key, f32 weight, u32 tag}: SoA uses key/weight/tag, AoS
@@ -311,7 +407,9 @@ typedef struct gf_flow_stats {
     uint32_t peak_live_chunks;
     uint32_t peak_reserved_chunks;
     uint32_t peak_ready_chunks;
-    double seconds; /* wall time of Flow::run */
+    double seconds;       /* wall time of the entry point's run, Flow built and destroyed included */
+    double setup_seconds; /* of it: the Flow's storage, stages and runner built */
+    double loop_seconds;  /* of it: the scheduler loop (the rest: final synchronisation, teardown) */
 } gf_flow_stats;
 
 /* examples/particle_feedback/KernelAxes.hpp:115-214 runKernelAxes: Generate -> one partition with

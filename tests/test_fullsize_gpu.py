@@ -12,13 +12,16 @@
   weight bits of its tag), and the per-port tag multisets equal the oracle's partition.
   Reference bar: tests/integration/test_hash_bins.cpp:286-502.
 * photon_scattering, weighted Henyey-Greenstein slab in FP32 (N = 2e6) against the FP64 oracle:
-  photon counts conserve N; every one of the 2 x 256 exit-weight bins agrees within
-      |h32 - h64| <= 6 sqrt(2 f S) + 2e-4 h64 + 6 sqrt(2 f) w_max
-  where f is the fraction of photons whose event or scatter count differs between the two runs
-  (FP32 rounding flips a decision near a tie; required <= 3 %), S the bin's sum of squared FP64
-  weights and w_max the largest terminal weight: histories that agree carry weights within 1e-4
-  relative, and the diverged ones are a random subset of about f of the bin's photons whose
-  weight sum has variance at most 2 f S.
+  photon counts conserve N; the FP32 run's histograms equal the sums of its own per-photon exit
+  records (FP32 accumulation, 5e-5 relative); and every one of the 2 x 256 exit-weight bins agrees
+  with the oracle within
+      |h32 - h64| <= 2e-4 h64 + k_i w_max,   k_i = the 1 - 1e-7 quantile of Poisson(2 f N_i),
+  where f is the fraction of photons whose terminal event, scatter count or exit bin differs
+  between the runs (FP32 rounding moves a photon across a bin edge or, rarely, flips a decision;
+  required <= 1e-3), N_i the oracle's photon count in the bin and w_max the largest terminal
+  weight. Photons that agree carry weights within 1e-4 relative (the 2e-4 term); a bin differs
+  otherwise by the weights of the photons that moved in or out, whose number is Poisson with mean
+  at most 2 f N_i.
 The comparisons run on the device with torch (gathers, sorts, equality), fed by the oracle's
 host results.
 """
@@ -189,22 +192,40 @@ def test_hash_k2e20_s08_matches_oracle():
         assert np.array_equal(np.sort((got_port << 32) | got_tag), exp)
 
 
+def _poisson_quantile(lam, tail=1e-7):
+    """Smallest k with P(X > k) <= tail for X ~ Poisson(lam)."""
+    k, pmf = 0, np.exp(-lam)
+    cdf = pmf
+    while 1.0 - cdf > tail:
+        k += 1
+        pmf *= lam / k
+        cdf += pmf
+    return k
+
+
 def test_photon_fp32_exit_histograms_per_bin():
     n = 2_000_000
     p = capi.photon_params(model=capi.PHOTON_WEIGHTED, fp64=False)
     got = capi.run_photon(42, n, p, capi.EXEC_FUSED)
     refl, trans, ev, terms = O.photon_hg(42, n, O.hg_params(), want_terminals=True)
     assert int(got["event_counts"].sum()) == n and int(ev.sum()) == n
-    same = (got["event"] == terms["event"]) & (got["scatter_count"] == terms["scatter_count"])
-    f = 1.0 - same.mean()
-    assert f <= 0.03
     nb = len(refl)
-    bins = np.minimum((terms["cos_exit"] * nb).astype(np.int64), nb - 1)
-    w_max = float(terms["weight"].max())
+    b64 = np.minimum((terms["cos_exit"] * nb).astype(np.int64), nb - 1)
+    b32 = np.minimum((got["cos_exit"] * nb).astype(np.int64), nb - 1)
+    same = (got["event"] == terms["event"]) & (got["scatter_count"] == terms["scatter_count"]) & (b32 == b64)
+    f = 1.0 - same.mean()
+    assert f <= 1e-3
+    w_ref = terms["weight"][same]
+    assert np.all(np.abs(got["weight"][same] - w_ref) <= 1e-4 * w_ref)
+    w_max = float(max(terms["weight"].max(), got["weight"].max()))
     for event, h32, h64 in ((2, got["refl"], refl), (1, got["trans"], trans)):
-        sel = terms["event"] == event
-        s = np.bincount(bins[sel], weights=terms["weight"][sel] ** 2, minlength=nb)
-        assert np.allclose(np.bincount(bins[sel], weights=terms["weight"][sel], minlength=nb), h64, rtol=1e-12,
+        s64, s32 = terms["event"] == event, got["event"] == event
+        # each run's histogram is the sum of its photons' exit records
+        assert np.allclose(np.bincount(b64[s64], weights=terms["weight"][s64], minlength=nb), h64, rtol=1e-12,
                            atol=1e-9)
-        tol = 6.0 * np.sqrt(2.0 * f * s) + 2e-4 * h64 + 6.0 * np.sqrt(2.0 * f) * w_max
+        assert np.allclose(np.bincount(b32[s32], weights=got["weight"][s32], minlength=nb), h32, rtol=5e-5,
+                           atol=1e-6)
+        count = np.bincount(b64[s64], minlength=nb)
+        k = np.array([_poisson_quantile(2.0 * f * c) for c in count])
+        tol = 2e-4 * h64 + k * w_max
         assert np.all(np.abs(h32 - h64) <= tol), np.max(np.abs(h32 - h64) / tol)
