@@ -244,16 +244,18 @@ def test_transform_dense_concatenation(layout):
     d_out = torch.from_numpy(out_chunks.view(np.int32)).cuda()
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
     L = capi.lib()
+    inc = 20  # the three planted weights (2^32 - 11) overflow, every other weight does not
     for xf in (capi.XF_IDENTITY, capi.XF_ADD_WEIGHT):
         status.zero_()
         capi.check(L.gf_transform(None, C.byref(pool.cols), C.byref(pool.cols), CAP, pool.slots, tiles.data_ptr(),
-                                  len(mt), d_out.data_ptr(), n_out, xf, C.byref(_params(0, increment=7)),
+                                  len(mt), d_out.data_ptr(), n_out, xf, C.byref(_params(0, increment=inc)),
                                   status.data_ptr()), "transform")
         got = np.concatenate([pool.get(int(c) * CAP, min(CAP, n - k * CAP)) for k, c in enumerate(out_chunks)])
         exp = parts.copy()
         if xf == capi.XF_ADD_WEIGHT:
-            ok = exp["weight"] <= 0xFFFFFFFF - 7
-            exp["weight"][ok] += 7
+            ok = exp["weight"] <= 0xFFFFFFFF - inc
+            assert (~ok).sum() == 3
+            exp["weight"][ok] += inc
             exp["visit"][ok] += 1
             assert int(status.item()) == capi.GF_OVERFLOW
             keep = ok
