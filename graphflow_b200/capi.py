@@ -133,7 +133,7 @@ class FlowStats(C.Structure):
                 ("kernel_launches", C.c_uint64), ("loop_iterations", C.c_uint64), ("generated", C.c_uint64),
                 ("sunk", C.c_uint64), ("pool_chunks", C.c_uint32), ("peak_live_chunks", C.c_uint32),
                 ("peak_reserved_chunks", C.c_uint32), ("peak_ready_chunks", C.c_uint32), ("seconds", C.c_double),
-                ("setup_seconds", C.c_double), ("loop_seconds", C.c_double)]
+                ("setup_seconds", C.c_double), ("loop_seconds", C.c_double), ("partition_launches", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

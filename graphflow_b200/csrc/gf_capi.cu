@@ -21,6 +21,10 @@ int g_runner_batched = 1;
 // counter per port and CTA); 0 = the per-tile open-addressing kernels.
 int g_hash_persistent = 1;
 int g_sink_batch = 256;
+// Tuning knob: 1 = with the B200 runner options, the fused partition nodes of one type run as one
+// partition group (one multi-batch launch drains every member's ready batches); 0 = one runner node
+// per partition node.
+int g_group_partitions = 1;
 
 constexpr int kThreads = 256;
 constexpr uint32_t kMaxDenseBins = 65535u;
@@ -113,6 +117,10 @@ gf_status gf_set_tuning(const char* name, int value)
     }
     if (std::string(name) == "runner_batched") {
         g_runner_batched = value != 0;
+        return GF_OK;
+    }
+    if (std::string(name) == "group_partitions") {
+        g_group_partitions = value != 0;
         return GF_OK;
     }
     if (std::string(name) == "hash_persistent") {
@@ -455,5 +463,7 @@ extern "C" gf_status gf_partition_fused_u32_noalloc(
 bool gf_runner_batched() { return gf::g_runner_batched != 0; }
 // Chunks a sink takes per launch in the batched runner (gf_flows.cu, gf_dense_flow.cu, gf_photon.cu).
 uint32_t gf_runner_sink_batch() { return (uint32_t)gf::g_sink_batch; }
+// Read by the flow entry points (gf_dense_flow.cu, gf_flows.cu).
+bool gf_group_partitions() { return gf::g_group_partitions != 0; }
 // Read by the hash entry points (gf_capi_hash.cu).
 bool gf_hash_persistent() { return gf::g_hash_persistent != 0; }

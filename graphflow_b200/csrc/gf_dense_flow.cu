@@ -8,7 +8,8 @@
 
 gf_status gf_flows_guard(const std::function<void()>& body); // gf_flows.cu
 bool gf_runner_batched();                                       // gf_capi.cu
-uint32_t gf_runner_sink_batch();                                // gf_capi.cu
+uint32_t gf_runner_sink_batch();
+bool gf_group_partitions();                                // gf_capi.cu
 
 namespace {
 
@@ -66,6 +67,7 @@ extern "C" gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins
         if (gf_runner_batched()) {
             t.sinkBatchChunks = gf_runner_sink_batch();
             t.multiDispatch = true;
+            t.groupPartitions = gf_group_partitions();
         }
         const auto t0 = std::chrono::steady_clock::now();
         const SchedulerStats s =
@@ -89,6 +91,7 @@ extern "C" gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins
             h_stats->seconds = sec;
             h_stats->setup_seconds = s.setupSeconds;
             h_stats->loop_seconds = s.loopSeconds;
+            h_stats->partition_launches = s.partitionLaunches;
         }
     });
 }

@@ -59,12 +59,14 @@ void fill_stats(const graphflow::SchedulerStats& s, double seconds, gf_flow_stat
     out->seconds = seconds;
     out->setup_seconds = s.setupSeconds;
     out->loop_seconds = s.loopSeconds;
+    out->partition_launches = s.partitionLaunches;
 }
 
 } // namespace
 
 bool gf_runner_batched();        // gf_capi.cu
-uint32_t gf_runner_sink_batch(); // gf_capi.cu
+uint32_t gf_runner_sink_batch();
+bool gf_group_partitions(); // gf_capi.cu
 
 // Runs a front-end call, mapping its exceptions to gf_status and the last-error message.
 gf_status gf_flows_guard(const std::function<void()>& body) { return guarded(body); }
@@ -154,6 +156,7 @@ gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visit
         if (gf_runner_batched()) {
             t.sinkBatchChunks = gf_runner_sink_batch();
             t.multiDispatch = true;
+            t.groupPartitions = gf_group_partitions();
         }
         const auto t0 = std::chrono::steady_clock::now();
         SchedulerStats s = layout == GF_LAYOUT_SOA
@@ -205,6 +208,7 @@ gf_status gf_run_kernel_axes(uint64_t seed, uint64_t n, uint32_t bins, int distr
         if (gf_runner_batched()) {
             t.sinkBatchChunks = gf_runner_sink_batch();
             t.multiDispatch = true;
+            t.groupPartitions = gf_group_partitions();
         }
         const auto d = static_cast<Distribution>(distribution);
         const auto t0 = std::chrono::steady_clock::now();

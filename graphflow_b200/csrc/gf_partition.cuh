@@ -395,7 +395,7 @@ GF_D bool poll_again(uint32_t& polls, const uint32_t* status)
 // publishes it; later touchers read it, waiting (bounded) only while a claim is in flight.
 // Because any toucher may claim, no tile waits for the look-back of the tile that owns the
 // chunk's first position.
-GF_D uint32_t claim_chunk(unsigned long long* slot, uint32_t epoch, FusedCtl* ctl, const uint32_t* reserved,
+GF_D uint32_t claim_chunk(unsigned long long* slot, uint32_t epoch, uint32_t* alloc_cursor, const uint32_t* reserved,
                           uint32_t n_reserved, uint32_t* status)
 {
     const unsigned long long tag = (unsigned long long)epoch << 32;
@@ -403,7 +403,7 @@ GF_D uint32_t claim_chunk(unsigned long long* slot, uint32_t epoch, FusedCtl* ct
     if ((uint32_t)(v >> 32) != epoch) {
         const unsigned long long old = atomicCAS(slot, v, tag | kClaimed);
         if (old == v) {
-            const uint32_t idx = atomicAdd(&ctl->alloc_cursor, 1u);
+            const uint32_t idx = atomicAdd(alloc_cursor, 1u);
             uint32_t chunk = kNoChunk;
             if (idx < n_reserved)
                 chunk = __ldg(reserved + idx);
@@ -694,10 +694,11 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
             if (kb >= max_k) {
                 set_status(status, GF_OVERFLOW);
             } else {
-                lo = claim_chunk(port_chunks + (size_t)b * max_k + ka, epoch, ctl, reserved, n_reserved, status);
+                lo = claim_chunk(port_chunks + (size_t)b * max_k + ka, epoch, &ctl->alloc_cursor, reserved,
+                                 n_reserved, status);
                 if (kb != ka)
-                    hi = claim_chunk(port_chunks + (size_t)b * max_k + kb, epoch, ctl, reserved, n_reserved,
-                                     status);
+                    hi = claim_chunk(port_chunks + (size_t)b * max_k + kb, epoch, &ctl->alloc_cursor, reserved,
+                                     n_reserved, status);
             }
         }
         chunk_lo[b] = lo;
@@ -708,6 +709,213 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
     __syncthreads();
     if (s_tile[2] != 0u) {
         retire(); // the batch failed somewhere: write nothing, the host discards it
+        return;
+    }
+
+    // 7. coalesced write-out
+    for (uint32_t q = threadIdx.x; q < n_valid; q += Shape::kThreads) {
+        const uint32_t b = stage_bin[q];
+        const uint32_t j = gbase[b] + q;
+        const uint32_t k = fdc.div(j);
+        const uint32_t chunk = k == k0[b] ? chunk_lo[b] : chunk_hi[b];
+        if (chunk == kNoChunk)
+            continue;
+        const uint64_t slot = (uint64_t)chunk * capacity + (j - k * capacity);
+        if (slot < pool_slots)
+            acc.store(slot, stage[q]);
+        else
+            set_status(status, GF_OVERFLOW);
+    }
+    retire();
+}
+
+// One partition batch of a multi-batch fused launch (several nodes' ready batches in one grid):
+// its tiles in the launch's tile list, the node (member) whose classifier and updater it uses,
+// its output-chunk reservation, and its own outputs and scratch. The host zeroes `counters`
+// (allocation cursor, retired tiles) before every launch.
+struct MultiBatch {
+    uint32_t tile_begin;
+    uint32_t n_tiles;
+    uint32_t member;
+    uint32_t n_reserved;
+    const uint32_t* reserved;
+    uint32_t* totals;                // [B]
+    unsigned long long* port_chunks; // [B * max_k]
+    unsigned long long* desc;        // [n_tiles * B] look-back descriptors
+    uint32_t* counters;              // [2]
+    uint32_t* table;                 // [B + desc_cap]
+    gf_out_desc* descs;              // [desc_cap]
+    uint32_t desc_cap;
+    uint32_t* num_out;
+};
+
+// Multi-batch form of fused_partition_kernel: one CTA per tile of the concatenated tile list
+// (`tile_batch[t]` = the tile's batch). A tile looks back only over the predecessors of its own
+// batch, which claimed their tiles earlier from the launch-wide counter, so every wait ends. The
+// batch's last tile to retire builds that batch's chunk table and descriptors; the launch's last
+// CTA publishes the epoch. The batches of one launch share the epoch, so their descriptor and
+// chunk-claim words from earlier launches read as stale.
+template <typename Shape, typename Access, typename Classify, typename Update>
+__global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_partition_multi_kernel(
+    Access acc, const Classify* classify_of, const Update* update_of, uint64_t seed_mixed, uint32_t capacity,
+    FastDiv fdc, uint64_t pool_slots, const gf_tile* tiles, const uint32_t* tile_batch, uint32_t n_tiles, uint32_t B,
+    const MultiBatch* batches, uint32_t n_batches, uint32_t max_k, FusedCtl* ctl, uint32_t* status)
+{
+    using P = typename Access::Payload;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    P* stage = reinterpret_cast<P*>(smem_raw);
+    uint32_t* stage_bin = reinterpret_cast<uint32_t*>(stage + Shape::kTile);
+    uint32_t* warp_cnt = stage_bin + Shape::kTile;            // [W][B]
+    uint32_t* bin_tot = warp_cnt + (size_t)Shape::kWarps * B; // [B]
+    uint32_t* bin_excl = bin_tot + B;                         // [B]
+    uint32_t* gbase = bin_excl + B;                           // [B]
+    uint32_t* k0 = gbase + B;                                 // [B]
+    uint32_t* chunk_lo = k0 + B;                              // [B]
+    uint32_t* chunk_hi = chunk_lo + B;                        // [B]
+    uint32_t* lb_flag = chunk_hi + B;                         // [THREADS]
+    uint32_t* lb_val = lb_flag + Shape::kThreads;             // [THREADS]
+    uint32_t* scan_tmp = lb_val + Shape::kThreads;            // [W+1]
+    uint32_t* s_tile = scan_tmp + Shape::kWarps + 1;          // [3]
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+
+    if (threadIdx.x == 0) {
+        s_tile[0] = atomicAdd(&ctl->tile_counter, 1u);
+        s_tile[1] = next_epoch(ld_relaxed_u32(&ctl->epoch));
+    }
+    __syncthreads();
+    const uint32_t gt = s_tile[0];
+    const uint32_t epoch = s_tile[1];
+    const uint32_t bi = gt < n_tiles ? __ldg(tile_batch + gt) : 0u;
+    const bool in_range = gt < n_tiles && bi < n_batches;
+    if (gt < n_tiles && !in_range && threadIdx.x == 0)
+        set_status(status, GF_INVALID);
+    const MultiBatch mb = in_range ? batches[bi] : MultiBatch{};
+    const uint32_t t = gt - mb.tile_begin; // the tile's index inside its batch
+    const bool batch_ok = in_range && gt >= mb.tile_begin && t < mb.n_tiles;
+    if (in_range && !batch_ok && threadIdx.x == 0)
+        set_status(status, GF_INVALID);
+
+    // retire: the batch's last tile builds the batch's table and descriptors; the launch's last
+    // CTA publishes the epoch
+    auto retire = [&]() {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            uint32_t last_of_batch = 0u;
+            if (batch_ok)
+                last_of_batch = atomicAdd(mb.counters + 1, 1u) + 1u == mb.n_tiles ? 1u : 0u;
+            if (atomicAdd(&ctl->done, 1u) + 1u == gridDim.x)
+                atomicExch(&ctl->epoch, epoch);
+            s_tile[2] = last_of_batch;
+        }
+        __syncthreads();
+        if (s_tile[2] == 0u)
+            return;
+        __threadfence(); // the batch's other tiles published their totals and claims before arriving
+        constexpr uint32_t kSeg = (uint32_t)(sizeof(P) * Shape::kTile / 8u);
+        uint32_t* scratch = reinterpret_cast<uint32_t*>(smem_raw);
+        finish_plan<Shape::kThreads>(mb.totals, mb.port_chunks, B, capacity, fdc, max_k, epoch, mb.table, mb.descs,
+                                     mb.desc_cap, mb.num_out, status, scratch, scratch + kSeg, kSeg, lb_flag);
+    };
+    if (!batch_ok) {
+        retire();
+        return;
+    }
+    const Classify classify = classify_of[mb.member];
+    const Update update = update_of[mb.member];
+
+    const gf_tile tile = tiles[gt];
+    const uint64_t base = (uint64_t)tile.chunk_index * capacity + tile.tile_offset;
+    const bool tile_ok = tile.count <= (uint32_t)Shape::kTile && base + tile.count <= pool_slots &&
+                         tile.tile_offset + tile.count <= capacity;
+    if (!tile_ok && threadIdx.x == 0)
+        set_status(status, GF_INVALID);
+
+    // 1. load and classify
+    uint32_t bp[Shape::kIpt];
+    P p[Shape::kIpt];
+#pragma unroll
+    for (int r = 0; r < Shape::kIpt; ++r) {
+        const uint32_t i = Shape::item(w, r, lane);
+        bp[r] = kNoBin16;
+        if (tile_ok && i < tile.count)
+            p[r] = acc.load(base + i);
+    }
+#pragma unroll
+    for (int r = 0; r < Shape::kIpt; ++r) {
+        const uint32_t i = Shape::item(w, r, lane);
+        if (tile_ok && i < tile.count) {
+            const uint32_t b = classify(p[r]);
+            if (b >= B)
+                set_status(status, GF_INVALID);
+            else
+                bp[r] = b;
+        }
+    }
+    // 2. stable rank inside the tile, per-bin tile totals
+    warp_rank<Shape>(bp, warp_cnt, B);
+    __syncthreads();
+    warp_offsets<Shape>(warp_cnt, bin_tot, B);
+    __syncthreads();
+
+    // 3. publish the tile aggregate, then look back (inside the batch) for the exclusive prefixes
+    unsigned long long* my_desc = mb.desc + (size_t)t * B;
+    for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads)
+        st_relaxed_u64(my_desc + b, make_desc(epoch, t == 0 ? 2u : 1u, bin_tot[b]));
+    const uint32_t n_valid = block_exclusive_scan<Shape::kThreads>(bin_tot, bin_excl, B, scan_tmp);
+
+    // 4. updater, stage in bin order
+#pragma unroll
+    for (int r = 0; r < Shape::kIpt; ++r) {
+        const uint32_t b = bp_bin(bp[r]);
+        if (b != kNoBin16) {
+            const uint32_t q = bin_excl[b] + warp_cnt[(size_t)w * B + b] + bp_pos(bp[r]);
+            const uint32_t res = update(b, p[r], seed_mixed);
+            if (res != kUpdateSuccess)
+                set_status(status, res == kUpdateOverflow ? GF_OVERFLOW : GF_INVALID);
+            stage[q] = p[r];
+            stage_bin[q] = b;
+        }
+    }
+
+    // 5. look-back
+    if (t != 0u)
+        block_lookback<Shape::kThreads>(mb.desc, t, B, epoch, gbase, chunk_lo, lb_flag, lb_val, status);
+    else
+        for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads)
+            gbase[b] = 0u;
+    __syncthreads();
+
+    // 6. inclusive prefixes, batch totals, output chunks by first-touch claim
+    for (uint32_t b = threadIdx.x; b < B; b += Shape::kThreads) {
+        const uint32_t excl = gbase[b], tot = bin_tot[b];
+        if (t != 0u)
+            st_relaxed_u64(my_desc + b, make_desc(epoch, 2u, excl + tot));
+        if (t + 1u == mb.n_tiles)
+            mb.totals[b] = excl + tot;
+        gbase[b] = excl - bin_excl[b];
+        uint32_t lo = kNoChunk, hi = kNoChunk;
+        if (tot != 0u) {
+            const uint32_t ka = fdc.div(excl), kb = fdc.div(excl + tot - 1u);
+            k0[b] = ka;
+            if (kb >= max_k) {
+                set_status(status, GF_OVERFLOW);
+            } else {
+                lo = claim_chunk(mb.port_chunks + (size_t)b * max_k + ka, epoch, mb.counters, mb.reserved,
+                                 mb.n_reserved, status);
+                if (kb != ka)
+                    hi = claim_chunk(mb.port_chunks + (size_t)b * max_k + kb, epoch, mb.counters, mb.reserved,
+                                     mb.n_reserved, status);
+            }
+        }
+        chunk_lo[b] = lo;
+        chunk_hi[b] = hi;
+    }
+    if (threadIdx.x == 0)
+        s_tile[2] = ld_relaxed_u32(status);
+    __syncthreads();
+    if (s_tile[2] != 0u) {
+        retire(); // the launch failed somewhere: write nothing, the host discards every batch
         return;
     }
 

@@ -201,6 +201,7 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
         hStats->seconds = sec;
         hStats->setup_seconds = stats.setupSeconds;
         hStats->loop_seconds = stats.loopSeconds;
+        hStats->partition_launches = stats.partitionLaunches;
     }
 }
 

@@ -92,6 +92,11 @@ struct Tuning {
     // same loop iteration (the reference dispatches one node per iteration, GraphRunner.hpp:985).
     std::uint32_t sinkBatchChunks = 1u;
     bool multiDispatch = false;
+    // B200: the fused partition nodes of one classifier and updater type run as one runner node
+    // whose launches drain every member's ready batches (at most groupChunks input chunks, cut into
+    // batches of at most Q chunks per member) in one multi-batch kernel.
+    bool groupPartitions = false;
+    std::uint32_t groupChunks = 1024u;
     static constexpr std::uint32_t kMaxSinkBatchChunks = 256u;
 
     void validate() const
@@ -107,6 +112,8 @@ struct Tuning {
         nz(numChunks, "numChunks");
         nz(frameCap, "frameCap");
         nz(poolPayloadBudgetBytes, "poolPayloadBudgetBytes");
+        if (groupChunks == 0u)
+            throw std::invalid_argument("graphflow::Tuning: groupChunks must be non-zero");
     }
 };
 
@@ -121,6 +128,7 @@ struct Config {
     std::uint32_t liveParticles = 0u;
     std::uint32_t batchChunks = 1u;
     std::uint32_t sinkBatchChunks = 1u; // chunks per sink launch (B200 runner option)
+    std::uint32_t groupChunks = 1024u;  // input chunks per partition-group launch (B200 runner option)
     std::uint32_t tileSize = 4096u;
     std::uint32_t numChunks = 0u;
     std::uint32_t maxBins = 1u;
@@ -178,6 +186,7 @@ struct SchedulerStats {
     std::uint32_t chunkCapacity = 0u;
     std::uint64_t kernelLaunches = 0u;
     std::uint64_t partitionBatches = 0u;
+    std::uint64_t partitionLaunches = 0u; // launches that ran partition batches (a group runs many per launch)
     double setupSeconds = 0.0; // Flow::run: storage, stages and runner built
     double loopSeconds = 0.0;  // Flow::run: the scheduler loop
 };
@@ -186,7 +195,7 @@ inline std::string formatSchedulerStats(const SchedulerStats& s)
 {
     std::ostringstream o;
     o << "batches=" << s.completedBatches << " partitionBatches=" << s.partitionBatches
-      << " launches=" << s.kernelLaunches << " iterations=" << s.loopIterations << " yields=" << s.yields
+      << " partitionLaunches=" << s.partitionLaunches << " launches=" << s.kernelLaunches << " iterations=" << s.loopIterations << " yields=" << s.yields
       << " poolChunks=" << s.poolChunks << " peakLive=" << s.peakLiveChunks << " peakReserved="
       << s.peakReservedChunks << " peakReady=" << s.peakReadyChunks << " peakInflight=" << s.peakInflightBatches
       << " generated=" << s.sourceGenerated << " sunk=" << s.sourceSunk;

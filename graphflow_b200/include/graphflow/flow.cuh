@@ -38,6 +38,12 @@ inline std::uint64_t nextGraphIdentity()
     static std::uint64_t next = 1u;
     return next++;
 }
+// One address per classifier and updater type pair: partition nodes that share it (and their port
+// count) can run as one partition group.
+template <typename TClassifier, typename TUpdate>
+struct PartitionGroupKey {
+    static constexpr char id = 0;
+};
 } // namespace detail
 
 // flow/NodeHandle.hpp: opaque handle bound to its Flow instance.
@@ -142,6 +148,17 @@ public:
                                   st, c, cls, upd, static_cast<std::uint32_t>(TClassifier::maxBins), purpose);
                           });
         m_nodes[key].partition = true;
+        m_nodes[key].groupKey = &detail::PartitionGroupKey<TClassifier, TUpdate>::id;
+        m_nodes[key].makeGroup = [](TStorage& st, const Config& c, std::uint32_t b) -> std::unique_ptr<Stage> {
+            using G = PartitionGroupStage<TStorage, TClassifier, TUpdate, TBin>;
+            if (!G::feasible(c, b))
+                return nullptr;
+            return std::make_unique<G>(st, c, b);
+        };
+        m_nodes[key].joinGroup = [cls, upd](Stage& g, std::uint32_t purpose) -> std::uint32_t {
+            return static_cast<PartitionGroupStage<TStorage, TClassifier, TUpdate, TBin>&>(g).addMember(cls, upd,
+                                                                                                        purpose);
+        };
         return TypedNodeHandle<bins, TBin>(m_identity, key, bins, m_nodes[key].name);
     }
 
@@ -193,17 +210,79 @@ public:
         const Config config = resolveConfig(itemCount);
         m_device.makeCurrent();
         TStorage storage(m_device, config.numChunks, config.chunkCapacity);
-        std::vector<std::unique_ptr<Stage>> stages;
-        for (std::size_t k = 0; k < m_nodes.size(); ++k)
-            stages.push_back(m_nodes[k].make(storage, config, rng::streamPurposeForNode(k)));
-        GraphRunner runner(storage.ledger());
-        for (std::size_t k = 0; k < m_nodes.size(); ++k) {
-            std::vector<int> route;
-            for (auto r : m_nodes[k].routes)
-                route.push_back(static_cast<int>(r));
-            runner.addNode(m_nodes[k].name, m_nodes[k].role, m_nodes[k].bins, std::move(route), stages[k].get());
+        // partition groups: fused partition nodes of one classifier/updater type and port count run
+        // as one runner node (Tuning::groupPartitions)
+        const std::size_t N = m_nodes.size();
+        std::vector<int> groupOf(N, -1);
+        std::vector<std::uint32_t> memberOf(N, 0u);
+        std::vector<std::unique_ptr<Stage>> groupStages;
+        std::vector<std::vector<std::size_t>> groupMembers;
+        if (m_tuning.groupPartitions)
+            for (std::size_t k = 0; k < N; ++k) {
+                if (!m_nodes[k].partition || groupOf[k] >= 0)
+                    continue;
+                std::vector<std::size_t> members;
+                for (std::size_t j = k; j < N; ++j)
+                    if (m_nodes[j].partition && groupOf[j] < 0 && m_nodes[j].groupKey == m_nodes[k].groupKey &&
+                        m_nodes[j].bins == m_nodes[k].bins)
+                        members.push_back(j);
+                if (members.size() < 2u)
+                    continue;
+                std::unique_ptr<Stage> g = m_nodes[k].makeGroup(storage, config, m_nodes[k].bins);
+                if (!g)
+                    continue;
+                for (std::size_t j : members) {
+                    memberOf[j] = m_nodes[j].joinGroup(*g, rng::streamPurposeForNode(j));
+                    groupOf[j] = static_cast<int>(groupStages.size());
+                }
+                groupStages.push_back(std::move(g));
+                groupMembers.push_back(std::move(members));
+            }
+        // runner node of every Flow node (a group's runner node sits at its first member)
+        std::vector<std::size_t> runnerOf(N);
+        std::vector<int> groupRunner(groupStages.size(), -1);
+        std::size_t next = 0;
+        for (std::size_t k = 0; k < N; ++k) {
+            if (groupOf[k] >= 0) {
+                int& r = groupRunner[static_cast<std::size_t>(groupOf[k])];
+                if (r < 0)
+                    r = static_cast<int>(next++);
+                runnerOf[k] = static_cast<std::size_t>(r);
+            } else {
+                runnerOf[k] = next++;
+            }
         }
-        runner.setSource(*m_sourceKey, itemCount, config.liveParticles);
+        auto routeOf = [&](std::size_t k, std::vector<int>& route, std::vector<std::uint32_t>& tag) {
+            for (auto r : m_nodes[k].routes) {
+                route.push_back(static_cast<int>(runnerOf[r]));
+                tag.push_back(groupOf[r] >= 0 ? memberOf[r] : 0u);
+            }
+        };
+        std::vector<std::unique_ptr<Stage>> stages;
+        GraphRunner runner(storage.ledger());
+        for (std::size_t k = 0; k < N; ++k) {
+            std::vector<int> route;
+            std::vector<std::uint32_t> tag;
+            if (groupOf[k] >= 0) {
+                const std::size_t g = static_cast<std::size_t>(groupOf[k]);
+                if (groupMembers[g].front() != k)
+                    continue;
+                std::string name = "group(";
+                for (std::size_t j : groupMembers[g]) {
+                    routeOf(j, route, tag);
+                    name += (j == k ? "" : ", ") + m_nodes[j].name;
+                }
+                runner.addNode(name + ")", NodeRole::transform,
+                               m_nodes[k].bins * static_cast<std::uint32_t>(groupMembers[g].size()), std::move(route),
+                               groupStages[g].get(), std::move(tag));
+                continue;
+            }
+            stages.push_back(m_nodes[k].make(storage, config, rng::streamPurposeForNode(k)));
+            routeOf(k, route, tag);
+            runner.addNode(m_nodes[k].name, m_nodes[k].role, m_nodes[k].bins, std::move(route), stages.back().get(),
+                           std::move(tag));
+        }
+        runner.setSource(runnerOf[*m_sourceKey], itemCount, config.liveParticles);
         runner.setBatchChunks(config.batchChunks);
         runner.setSinkBatchChunks(config.sinkBatchChunks);
         runner.setMultiDispatch(m_tuning.multiDispatch);
@@ -232,6 +311,9 @@ private:
         std::vector<std::size_t> routes;
         Factory make;
         bool partition = false;
+        const void* groupKey = nullptr; // partition nodes: classifier/updater type identity
+        std::function<std::unique_ptr<Stage>(TStorage&, const Config&, std::uint32_t)> makeGroup;
+        std::function<std::uint32_t(Stage&, std::uint32_t)> joinGroup;
     };
 
     std::size_t append(std::string name, NodeRole role, std::uint32_t bins, Factory make)
@@ -295,6 +377,7 @@ private:
         c.maxBins = maxBins;
         c.batchChunks = m_tuning.batchChunks.value_or(1u);
         c.sinkBatchChunks = std::min(std::max(m_tuning.sinkBatchChunks, 1u), Tuning::kMaxSinkBatchChunks);
+        c.groupChunks = m_tuning.groupChunks;
         // C and P the caller left out come from the device policy (core/DevicePolicy.hpp:344-614)
         // with the accelerator P/C ratio of 8 and this storage's slot size, as Flow does there. The
         // payload budget is one eighth of device memory: the reference caps it at 3 GiB for 24 GB

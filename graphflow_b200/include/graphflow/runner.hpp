@@ -110,14 +110,20 @@ public:
     }
 
     // Adds a node; `route[bin]` is the destination node index (transforms and the source), the
-    // stage is owned by the caller. Returns the node index.
-    std::size_t addNode(std::string name, NodeRole role, std::uint32_t bins, std::vector<int> route, Stage* stage)
+    // stage is owned by the caller. `tag[bin]`, when given, is written into the routed chunk's
+    // descriptor bin (a partition group reads it as the member the chunk is for). Returns the node
+    // index.
+    std::size_t addNode(std::string name, NodeRole role, std::uint32_t bins, std::vector<int> route, Stage* stage,
+                        std::vector<std::uint32_t> tag = {})
     {
+        if (!tag.empty() && tag.size() != route.size())
+            throw std::invalid_argument("graphflow::GraphRunner: one tag per route");
         Node n;
         n.name = std::move(name);
         n.role = role;
         n.bins = bins;
         n.route = std::move(route);
+        n.tag = std::move(tag);
         n.stage = stage;
         m_nodes.push_back(std::move(n));
         Node& added = m_nodes.back();
@@ -206,8 +212,12 @@ public:
                                 throw std::runtime_error("graphflow: node '" + node.name +
                                                          "' produced an unroutable bin");
                             }
-                        for (const auto& out : outputs)
-                            m_nodes[static_cast<std::size_t>(node.route[out.bin])].ready.push_back(out);
+                        for (const auto& out : outputs) {
+                            ChunkDescriptor d = out;
+                            if (!node.tag.empty())
+                                d.bin = node.tag[out.bin];
+                            m_nodes[static_cast<std::size_t>(node.route[out.bin])].ready.push_back(d);
+                        }
                         if (node.role == NodeRole::sink)
                             sunk += node.inflight->particles();
                         if (node.role != NodeRole::source) {
@@ -307,6 +317,7 @@ private:
         NodeRole role = NodeRole::transform;
         std::uint32_t bins = 1u;
         std::vector<int> route;
+        std::vector<std::uint32_t> tag;
         Stage* stage = nullptr;
         cudaStream_t stream = nullptr;
         Event event{};
@@ -377,7 +388,11 @@ private:
         else if (node.role == NodeRole::sink)
             wanted = std::min<std::size_t>(m_sinkQ, node.ready.size());
         std::uint32_t reserve = 0u;
-        if (node.role == NodeRole::transform) {
+        if (node.role == NodeRole::transform && node.stage->plansBatches()) {
+            wanted = node.stage->planBatch(node.ready, available(), reserve);
+            if (wanted == 0u || wanted > node.ready.size())
+                return false;
+        } else if (node.role == NodeRole::transform) {
             std::uint64_t n = 0;
             for (std::size_t i = 0; i < wanted; ++i)
                 n += node.ready[i].fill;
@@ -420,8 +435,10 @@ private:
             node.ready.pop_front();
         const std::uint32_t allocated = launch(node, k);
         ++stats.kernelLaunches;
-        if (node.role == NodeRole::transform && node.bins > 1u)
-            ++stats.partitionBatches;
+        if (node.role == NodeRole::transform && node.bins > 1u) {
+            stats.partitionBatches += node.stage->lastLaunchBatches();
+            ++stats.partitionLaunches;
+        }
         convertCredit(node, allocated, reservedTotal);
         arm(node, k);
         if (reservedTotal > stats.peakReservedChunks)

@@ -3,7 +3,9 @@
 // scheduler and its tests compile without the device code.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
+#include <deque>
 #include <vector>
 
 #include <cuda_runtime_api.h>
@@ -37,6 +39,18 @@ public:
     // Release every unpublished output; the stage is single-use afterwards (Execution.hpp:2652-2656).
     virtual void abort() = 0;
     virtual std::uint64_t launches() const { return m_launches; }
+    // A stage that sizes its own batches (a partition group) answers true and plans them:
+    // planBatch returns how many chunks of `ready` (a prefix) to take with at most `available`
+    // output chunks reserved, and the reservation in `reserve`; 0 takes nothing. Other stages
+    // leave batch sizing to the runner.
+    virtual bool plansBatches() const { return false; }
+    virtual std::size_t planBatch(const std::deque<ChunkDescriptor>&, std::uint32_t, std::uint32_t& reserve) const
+    {
+        reserve = 0u;
+        return 0u;
+    }
+    // Partition batches the last launch ran (a partition group runs several per launch).
+    virtual std::uint32_t lastLaunchBatches() const { return 1u; }
 
 protected:
     std::uint64_t m_launches = 0;

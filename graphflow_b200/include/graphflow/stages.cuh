@@ -595,4 +595,351 @@ private:
     bool m_failed = false;
 };
 
+// Several fused partition nodes of one classifier and updater type, run as one runner node.
+// Each input chunk carries its member node in ChunkDescriptor::bin (the runner's route tags). A
+// launch cuts every member's chunks, in arrival order, into batches of at most Q chunks, reserves
+// outputChunkBound output chunks per batch and runs all of them in one multi-batch fused kernel
+// (gf::fused_partition_multi_kernel): the per-node batches of GraphRunner.hpp:985-1133 drained by a
+// single launch. Every batch's plan, table and outputs are those its node would produce alone;
+// outputs carry bin = member * B + port for the group's route table.
+template <typename TStorage, typename TClassifier, typename TUpdate, typename TBin>
+class PartitionGroupStage final : public Stage {
+    using View = typename TStorage::View;
+    using P = typename TStorage::Payload;
+    using Acc = ViewAccess<View>;
+    using Cls = ClassifyAdapter<TClassifier, P>;
+    using Upd = UpdateAdapter<TUpdate, TBin, P>;
+    using Shape = gf::TileShape<256, 4, 2>; // 1024-particle tiles
+    static constexpr std::uint32_t kTile = 1024u;
+
+public:
+    static std::size_t smemBytes(std::uint32_t bins)
+    {
+        return sizeof(P) * Shape::kTile + 4u * Shape::kTile + 4u * Shape::kWarps * bins + 4u * bins * 6u +
+               4u * (2u * Shape::kThreads + Shape::kWarps + 8u);
+    }
+    // The group runs the dense fused kernel only: fused form, shared-memory staging, dense bins
+    // whose per-port tables fit one block.
+    static bool feasible(const Config& c, std::uint32_t bins)
+    {
+        if (!c.fused || c.scatterMode == ScatterMode::Direct || c.binPath == BinPath::hash ||
+            bins > Config::denseBinLimit)
+            return false;
+        int dev = 0, limit = 0;
+        cuda::check(cudaGetDevice(&dev), "cudaGetDevice");
+        cuda::check(cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "smem limit");
+        return smemBytes(bins) <= static_cast<std::size_t>(limit);
+    }
+
+    PartitionGroupStage(TStorage& st, const Config& c, std::uint32_t bins)
+        : m_st(st), m_seed(gf::mix64(c.seed)), m_bins(bins), m_C(c.chunkCapacity), m_Q(c.batchChunks),
+          m_maxChunks(c.groupChunks), m_maxBatches(c.groupChunks),
+          m_tilesPerChunk((c.chunkCapacity + kTile - 1u) / kTile),
+          m_maxTiles(c.groupChunks * ((c.chunkCapacity + kTile - 1u) / kTile)),
+          m_tilesPerBatch(c.batchChunks * ((c.chunkCapacity + kTile - 1u) / kTile)),
+          m_boundMax(checkedOutputChunkBound(static_cast<std::uint64_t>(c.chunkCapacity) * c.batchChunks,
+                                             c.chunkCapacity, bins))
+    {
+        static_assert(sizeof(gf::MultiBatch) % 8u == 0u, "8-byte aligned batch records");
+        static_assert(sizeof(gf_tile) == 12 && sizeof(gf_out_desc) == 12, "packed layout");
+        if (!feasible(c, bins))
+            throw std::invalid_argument("graphflow::PartitionGroupStage: the fused dense kernel does not apply");
+        m_portChunks = cuda::Buffer<unsigned long long>(static_cast<std::size_t>(m_maxBatches) * bins * m_Q);
+        m_desc = cuda::Buffer<unsigned long long>(static_cast<std::size_t>(m_maxBatches) * m_tilesPerBatch * bins);
+        m_totals = cuda::Buffer<std::uint32_t>(static_cast<std::size_t>(m_maxBatches) * bins);
+        m_table = cuda::Buffer<std::uint32_t>(static_cast<std::size_t>(m_maxBatches) * (bins + m_boundMax));
+        cuda::check(cudaMemset(m_portChunks.data(), 0, m_portChunks.size() * 8u), "memset");
+        cuda::check(cudaMemset(m_desc.data(), 0, m_desc.size() * 8u), "memset");
+        // mirrored words: [status | numOut[maxBatches] | descs[maxBatches][boundMax] | ctl (4 words) |
+        // payload: tiles, tile batch, batch records, reserved chunks, batch counters]; a launch uploads
+        // ctl + payload in one copy and downloads status, numOut and the descriptors in one copy
+        m_oNum = 1u;
+        m_oDescs = m_oNum + m_maxBatches;
+        m_oCtl = (m_oDescs + 3u * m_maxBatches * m_boundMax + 3u) & ~3u;
+        m_oPay = m_oCtl + 4u;
+        const std::size_t payMax = 4u * static_cast<std::size_t>(m_maxTiles) +
+                                   m_maxBatches * (sizeof(gf::MultiBatch) / 4u + m_boundMax + 2u) + 4u;
+        m_io = detail::Staged<std::uint32_t>(m_oPay + payMax);
+        cuda::check(cudaMemset(m_io.dev.data(), 0, m_io.dev.size() * 4u), "memset");
+        std::fill(m_io.host.data(), m_io.host.data() + m_io.host.size(), 0u);
+        m_smem = smemBytes(bins);
+        cuda::check(cudaFuncSetAttribute(gf::fused_partition_multi_kernel<Shape, Acc, Cls, Upd>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(m_smem)),
+                    "partition group: kernel attribute");
+    }
+
+    // A member node's classifier, updater and stream purpose; its index is the route tag of the
+    // chunks routed to it.
+    std::uint32_t addMember(TClassifier cls, TUpdate upd, std::uint32_t purpose)
+    {
+        std::uint32_t* status = m_io.dev.data();
+        m_cls.push_back(Cls{cls, m_seed, purpose, status});
+        m_upd.push_back(Upd{upd, purpose + 1u, status});
+        m_membersDirty = true;
+        return static_cast<std::uint32_t>(m_cls.size() - 1u);
+    }
+    std::uint32_t members() const { return static_cast<std::uint32_t>(m_cls.size()); }
+
+    bool plansBatches() const override { return true; }
+    std::uint32_t lastLaunchBatches() const override { return static_cast<std::uint32_t>(m_sub.size()); }
+
+    // The longest prefix of `ready` (at most groupChunks chunks, tiles and batches within the
+    // launch's capacity) whose batches' output bounds fit `available`.
+    std::size_t planBatch(const std::deque<ChunkDescriptor>& ready, std::uint32_t available,
+                          std::uint32_t& reserve) const override
+    {
+        reserve = 0u;
+        const std::size_t m = m_cls.size();
+        m_openChunks.assign(m, 0u);
+        m_openN.assign(m, 0u);
+        std::uint64_t closed = 0, open = 0;
+        std::uint32_t batches = 0, tiles = 0;
+        std::size_t take = 0;
+        const std::size_t limit = std::min<std::size_t>(ready.size(), m_maxChunks);
+        for (std::size_t j = 0; j < limit; ++j) {
+            const ChunkDescriptor& d = ready[j];
+            if (d.bin >= m)
+                break; // not a member's chunk: launch() rejects it
+            const std::uint32_t mb = d.bin;
+            const std::uint32_t t = (d.fill + kTile - 1u) / kTile;
+            std::uint64_t o = open, c = closed;
+            std::uint32_t nb = batches;
+            if (m_openChunks[mb] == 0u || m_openChunks[mb] == m_Q) {
+                if (m_openChunks[mb] == m_Q) {
+                    const std::uint32_t bnd = checkedOutputChunkBound(m_openN[mb], m_C, m_bins);
+                    o -= bnd;
+                    c += bnd;
+                }
+                ++nb;
+            } else {
+                o -= checkedOutputChunkBound(m_openN[mb], m_C, m_bins);
+            }
+            const std::uint64_t n = (m_openChunks[mb] == m_Q ? 0u : m_openN[mb]) + d.fill;
+            o += checkedOutputChunkBound(n, m_C, m_bins);
+            if (c + o > available || nb > m_maxBatches || tiles + t > m_maxTiles)
+                break;
+            open = o;
+            closed = c;
+            batches = nb;
+            tiles += t;
+            m_openChunks[mb] = m_openChunks[mb] == m_Q ? 1u : m_openChunks[mb] + 1u;
+            m_openN[mb] = n;
+            take = j + 1u;
+        }
+        reserve = static_cast<std::uint32_t>(closed + open);
+        return take;
+    }
+
+    std::uint32_t launch(cudaStream_t s, const Batch& b) override
+    {
+        if (m_failed)
+            throw std::logic_error("graphflow::PartitionGroupStage: single-use after a failed batch");
+        if (m_cls.empty())
+            throw std::logic_error("graphflow::PartitionGroupStage: no member nodes");
+        ++m_launches;
+        if (m_membersDirty) {
+            m_clsDev = cuda::Buffer<Cls>(m_cls.size());
+            m_updDev = cuda::Buffer<Upd>(m_upd.size());
+            cuda::check(cudaMemcpy(m_clsDev.data(), m_cls.data(), sizeof(Cls) * m_cls.size(), cudaMemcpyHostToDevice),
+                        "H2D");
+            cuda::check(cudaMemcpy(m_updDev.data(), m_upd.data(), sizeof(Upd) * m_upd.size(), cudaMemcpyHostToDevice),
+                        "H2D");
+            m_membersDirty = false;
+        }
+        // batches: every member's chunks in arrival order, at most Q per batch
+        m_sub.clear();
+        m_cur.assign(m_cls.size(), -1);
+        for (const auto& c : b.chunks) {
+            if (c.bin >= m_cls.size())
+                throw BatchError("partition group: chunk routed to an unknown member");
+            int& k = m_cur[c.bin];
+            if (k < 0 || m_sub[static_cast<std::size_t>(k)].chunks.size() == m_Q) {
+                k = static_cast<int>(m_sub.size());
+                m_sub.push_back(Sub{c.bin, {}, 0u, 0u, 0u, 0u, 0u});
+            }
+            m_sub[static_cast<std::size_t>(k)].chunks.push_back(c);
+        }
+        if (m_sub.size() > m_maxBatches)
+            throw BatchError("partition group: more batches than one launch holds");
+        // reservations, tiles and batch records
+        std::uint32_t* h = m_io.host.data();
+        std::uint32_t* d = m_io.dev.data();
+        std::uint32_t nTiles = 0, nReserved = 0;
+        m_reserved.clear();
+        for (auto& sb : m_sub) {
+            sb.n = 0u;
+            for (const auto& c : sb.chunks)
+                sb.n += c.fill;
+            sb.bound = checkedOutputChunkBound(sb.n, m_C, m_bins);
+            sb.resBegin = nReserved;
+            for (std::uint32_t k = 0; k < sb.bound; ++k)
+                m_reserved.push_back(m_st.ledger().acquire());
+            nReserved += sb.bound;
+            sb.tileBegin = nTiles;
+            for (const auto& c : sb.chunks)
+                nTiles += (c.fill + kTile - 1u) / kTile;
+            sb.tiles = nTiles - sb.tileBegin;
+        }
+        if (nTiles > m_maxTiles)
+            throw BatchError("partition group: more tiles than one launch holds");
+        const std::uint32_t nb = static_cast<std::uint32_t>(m_sub.size());
+        const std::uint32_t oTiles = m_oPay, oTileBatch = oTiles + 3u * nTiles;
+        const std::uint32_t oBatches = (oTileBatch + nTiles + 1u) & ~1u;
+        const std::uint32_t oRes = oBatches + nb * static_cast<std::uint32_t>(sizeof(gf::MultiBatch) / 4u);
+        const std::uint32_t oCnt = oRes + nReserved, oEnd = oCnt + 2u * nb;
+        auto* tiles = reinterpret_cast<gf_tile*>(h + oTiles);
+        auto* recs = reinterpret_cast<gf::MultiBatch*>(h + oBatches);
+        std::uint32_t t = 0;
+        for (std::uint32_t i = 0; i < nb; ++i) {
+            const Sub& sb = m_sub[i];
+            for (const auto& c : sb.chunks)
+                for (std::uint32_t off = 0; off < c.fill; off += kTile) {
+                    tiles[t] = gf_tile{c.handle.index, off, c.fill - off < kTile ? c.fill - off : kTile};
+                    h[oTileBatch + t] = i;
+                    ++t;
+                }
+            for (std::uint32_t k = 0; k < sb.bound; ++k)
+                h[oRes + sb.resBegin + k] = m_reserved[sb.resBegin + k].index;
+            h[oCnt + 2u * i] = 0u;
+            h[oCnt + 2u * i + 1u] = 0u;
+            gf::MultiBatch r{};
+            r.tile_begin = sb.tileBegin;
+            r.n_tiles = sb.tiles;
+            r.member = sb.member;
+            r.n_reserved = sb.bound;
+            r.reserved = d + oRes + sb.resBegin;
+            r.totals = m_totals.data() + static_cast<std::size_t>(i) * m_bins;
+            r.port_chunks = m_portChunks.data() + static_cast<std::size_t>(i) * m_bins * m_Q;
+            r.desc = m_desc.data() + static_cast<std::size_t>(i) * m_tilesPerBatch * m_bins;
+            r.counters = d + oCnt + 2u * i;
+            r.table = m_table.data() + static_cast<std::size_t>(i) * (m_bins + m_boundMax);
+            r.descs = reinterpret_cast<gf_out_desc*>(d + m_oDescs) + static_cast<std::size_t>(i) * m_boundMax;
+            r.desc_cap = m_boundMax;
+            r.num_out = d + m_oNum + i;
+            recs[i] = r;
+            h[m_oNum + i] = 0u;
+        }
+        // control block: tile counter, (unused) cursor, retired CTAs, the last published epoch
+        h[m_oCtl] = h[m_oCtl + 1u] = h[m_oCtl + 2u] = 0u;
+        h[m_oCtl + 3u] = m_epoch;
+        h[0] = 0u;
+        cuda::check(cudaMemcpyAsync(d + m_oCtl, h + m_oCtl, 4u * (oEnd - m_oCtl), cudaMemcpyHostToDevice, s), "H2D");
+        if (nTiles) {
+            const Acc acc{m_st.view()};
+            gf::fused_partition_multi_kernel<Shape, Acc, Cls, Upd><<<nTiles, Shape::kThreads, m_smem, s>>>(
+                acc, m_clsDev.data(), m_updDev.data(), m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(),
+                reinterpret_cast<const gf_tile*>(d + oTiles), d + oTileBatch, nTiles, m_bins,
+                reinterpret_cast<const gf::MultiBatch*>(d + oBatches), nb, m_Q,
+                reinterpret_cast<gf::FusedCtl*>(d + m_oCtl), d);
+            cuda::check(cudaGetLastError(), "partition group launch");
+            m_epoch = gf::next_epoch(m_epoch);
+        }
+        cuda::check(cudaMemcpyAsync(h, d, 4u * (m_oDescs + 3u * nb * m_boundMax), cudaMemcpyDeviceToHost, s), "D2H");
+        return nReserved;
+    }
+
+    bool advance(cudaStream_t, const Batch&, std::uint32_t& allocated) override
+    {
+        allocated = 0u;
+        detail::checkStatusWord(m_io.host[0], "partition group");
+        return false;
+    }
+
+    void finish(const Batch&, std::vector<ChunkDescriptor>& outputs) override
+    {
+        if (m_slotOf.size() != m_st.ledger().numChunks())
+            m_slotOf.assign(m_st.ledger().numChunks(), -1);
+        for (std::size_t k = 0; k < m_reserved.size(); ++k)
+            m_slotOf[m_reserved[k].index] = static_cast<std::int32_t>(k);
+        m_used.assign(m_reserved.size(), false);
+        std::vector<ChunkHandle> reserved = std::move(m_reserved);
+        m_reserved.clear();
+        struct Clear { // on every exit: the table is all -1 again, unused reservations are released
+            std::vector<std::int32_t>& slot;
+            const std::vector<ChunkHandle>& r;
+            const std::vector<bool>& used;
+            ChunkLedger& ledger;
+            bool committed = false; // outputs handed to the runner; otherwise every reservation goes back
+            ~Clear()
+            {
+                for (std::size_t k = 0; k < r.size(); ++k) {
+                    slot[r[k].index] = -1;
+                    if ((!committed || !used[k]) && ledger.valid(r[k]))
+                        ledger.release(r[k]);
+                }
+            }
+        } clear{m_slotOf, reserved, m_used, m_st.ledger()};
+        std::vector<ChunkDescriptor> out;
+        const auto* descs = reinterpret_cast<const gf_out_desc*>(m_io.host.data() + m_oDescs);
+        for (std::size_t i = 0; i < m_sub.size(); ++i) {
+            const Sub& sb = m_sub[i];
+            if (sb.n == 0u)
+                continue;
+            const std::uint32_t r = m_io.host[m_oNum + i];
+            if (r > sb.bound)
+                throw BatchError("partition group: more output chunks than the reservation bound");
+            std::uint64_t placed = 0;
+            const gf_out_desc* d = descs + i * m_boundMax;
+            for (std::uint32_t q = 0; q < r; ++q) {
+                const std::int32_t k = d[q].chunk_index < m_slotOf.size() ? m_slotOf[d[q].chunk_index] : -1;
+                if (k < static_cast<std::int32_t>(sb.resBegin) || k >= static_cast<std::int32_t>(sb.resBegin + sb.bound) ||
+                    m_used[static_cast<std::size_t>(k)])
+                    throw BatchError("partition group: output chunk outside the batch's reservation");
+                if (d[q].bin >= m_bins)
+                    throw BatchError("partition group: output bin out of range");
+                m_used[static_cast<std::size_t>(k)] = true;
+                placed += d[q].fill;
+                out.push_back(ChunkDescriptor{reserved[static_cast<std::size_t>(k)], d[q].fill,
+                                              sb.member * m_bins + d[q].bin});
+            }
+            if (placed != sb.n)
+                throw BatchError("partition group: placed particle count does not match the batch");
+        }
+        outputs.insert(outputs.end(), out.begin(), out.end());
+        clear.committed = true;
+        m_sub.clear();
+    }
+
+    void abort() override
+    {
+        m_failed = true;
+        for (const auto& h : m_reserved)
+            if (m_st.ledger().valid(h))
+                m_st.ledger().release(h);
+        m_reserved.clear();
+        m_sub.clear();
+    }
+
+private:
+    struct Sub {
+        std::uint32_t member;
+        std::vector<ChunkDescriptor> chunks;
+        std::uint64_t n;
+        std::uint32_t bound, resBegin, tileBegin, tiles;
+    };
+
+    TStorage& m_st;
+    std::uint64_t m_seed;
+    std::uint32_t m_bins, m_C, m_Q, m_maxChunks, m_maxBatches, m_tilesPerChunk, m_maxTiles, m_tilesPerBatch, m_boundMax;
+    std::vector<Cls> m_cls;
+    std::vector<Upd> m_upd;
+    cuda::Buffer<Cls> m_clsDev;
+    cuda::Buffer<Upd> m_updDev;
+    bool m_membersDirty = true;
+    cuda::Buffer<unsigned long long> m_portChunks, m_desc;
+    cuda::Buffer<std::uint32_t> m_totals, m_table;
+    detail::Staged<std::uint32_t> m_io;
+    std::uint32_t m_oNum = 0, m_oDescs = 0, m_oCtl = 0, m_oPay = 0;
+    std::size_t m_smem = 0;
+    std::uint32_t m_epoch = 0;
+    std::vector<Sub> m_sub;
+    std::vector<int> m_cur;
+    std::vector<ChunkHandle> m_reserved;
+    std::vector<std::int32_t> m_slotOf;
+    std::vector<bool> m_used;
+    mutable std::vector<std::uint32_t> m_openChunks;
+    mutable std::vector<std::uint64_t> m_openN;
+    bool m_failed = false;
+};
+
 } // namespace graphflow

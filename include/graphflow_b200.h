@@ -410,6 +410,8 @@ typedef struct gf_flow_stats {
     double seconds;       /* wall time of the entry point's run, Flow built and destroyed included */
     double setup_seconds; /* of it: the Flow's storage, stages and runner built */
     double loop_seconds;  /* of it: the scheduler loop (the rest: final synchronisation, teardown) */
+    uint64_t partition_launches; /* launches that ran partition batches; a partition group runs many
+                                  * nodes' batches per launch (partition_batches counts the batches) */
 } gf_flow_stats;
 
 /* examples/particle_feedback/KernelAxes.hpp:115-214 runKernelAxes: Generate -> one partition with
