@@ -630,22 +630,30 @@ def _cfg_particle_feedback():
 
 
 def _cfg_dense_flow():
-    """The dense sweep through the public Flow: B = 64 uniform keys, C = 8192, P = 16384, Q = 8."""
+    """The dense sweep through the public Flow: B = 64 uniform keys, C = 8192, P = 16384, Q = 8, at 1
+    node and at 4 chained nodes. The 4-node chain runs with its partition nodes grouped (one
+    multi-batch launch drains every node's ready batches) and, for comparison, with one runner node
+    per partition node."""
     from graphflow_b200 import capi
+    L = capi.lib()
     out = {"workload": "dense chain through Flow, B=64 uniform, C=8192 P=16384 Q=8 (records {u32 id, u32 key})"}
 
-    def run(nodes, n, fused, batched):
-        capi.check(capi.lib().gf_set_tuning(b"runner_batched", int(batched)), "tuning")
+    def run(nodes, n, fused, batched, grouped=True):
+        capi.check(L.gf_set_tuning(b"runner_batched", int(batched)), "tuning")
+        capi.check(L.gf_set_tuning(b"group_partitions", int(grouped)), "tuning")
         try:
             _, st = capi.run_dense_chain(42, n, 64, nodes=nodes, dist="uniform", chunk_capacity=8192,
                                          live_particles=16384, batch_chunks=8, fused=fused, want_ports=False)
         finally:
-            capi.check(capi.lib().gf_set_tuning(b"runner_batched", 1), "tuning")
+            capi.check(L.gf_set_tuning(b"runner_batched", 1), "tuning")
+            capi.check(L.gf_set_tuning(b"group_partitions", 1), "tuning")
         return {"n": n, "seconds": st.seconds, "particles_per_s": n / st.seconds,
-                "partition_batches": st.partition_batches, "kernel_launches": st.kernel_launches}
+                "partition_batches": st.partition_batches, "partition_launches": st.partition_launches,
+                "kernel_launches": st.kernel_launches, "loop_iterations": st.loop_iterations}
     out["nodes1_fused_b200_runner"] = run(1, 100_000_000, True, True)
     out["nodes1_plain_reference_runner"] = run(1, 10_000_000, False, False)
-    out["nodes4_fused_b200_runner"] = run(4, 1_000_000, True, True)
+    out["nodes4_grouped_b200_runner"] = run(4, 100_000_000, True, True, grouped=True)
+    out["nodes4_per_node_b200_runner"] = run(4, 1_000_000, True, True, grouped=False)
     out["nodes4_plain_reference_runner"] = run(4, 200_000, False, False)
     return out
 

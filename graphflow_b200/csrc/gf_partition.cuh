@@ -500,7 +500,42 @@ struct InlineFinish {
     gf_out_desc* descs = nullptr;
     uint32_t desc_cap = 0u;
     uint32_t* num_out = nullptr;
+    // Host-polled completion (per-tile kernel only): a record in mapped host memory,
+    // [0] sequence, [1] status, [2] output count, [3, 3 + B) totals, then the descriptors. The
+    // finishing CTA fills it, resets the launch counters for the next launch and writes `done_seq`
+    // last, so a host that sees the sequence reads a complete record without a copy or an event.
+    uint32_t* done_rec = nullptr;
+    uint32_t done_seq = 0u;
 };
+
+// The finishing CTA of a launch with a host-polled completion record (see InlineFinish).
+GF_D void publish_done(const InlineFinish& fin, FusedCtl* ctl, const uint32_t* totals, uint32_t B,
+                       uint32_t* status)
+{
+    __syncthreads(); // the finish's table, descriptors and output count are written
+    uint32_t* rec = fin.done_rec;
+    const uint32_t r = ld_relaxed_u32(fin.num_out);
+    const uint32_t nd = 3u * (r < fin.desc_cap ? r : fin.desc_cap);
+    const uint32_t* d = reinterpret_cast<const uint32_t*>(fin.descs);
+    for (uint32_t i = threadIdx.x; i < B; i += blockDim.x)
+        rec[3u + i] = ld_relaxed_u32(totals + i);
+    for (uint32_t i = threadIdx.x; i < nd; i += blockDim.x)
+        rec[3u + B + i] = ld_relaxed_u32(d + i);
+    if (threadIdx.x == 0) {
+        // every CTA has counted itself: the counters are free for the next launch
+        ctl->tile_counter = 0u;
+        ctl->alloc_cursor = 0u;
+        ctl->done = 0u;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        rec[1] = ld_relaxed_u32(status);
+        rec[2] = r;
+        *status = 0u; // read into the record: the word is clean for the next launch
+        __threadfence_system();
+        *reinterpret_cast<volatile uint32_t*>(rec) = fin.done_seq;
+    }
+}
 
 // Device form of planDenseBins + buildDenseTable + the output-descriptor loop
 // (DenseBinTable.hpp:39-91, Execution.hpp:2558-2581) for a fused launch, by one CTA of THREADS
@@ -576,14 +611,22 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
     uint32_t* lb_flag = chunk_hi + B;                         // [THREADS]
     uint32_t* lb_val = lb_flag + Shape::kThreads;             // [THREADS]
     uint32_t* scan_tmp = lb_val + Shape::kThreads;            // [W+1]
-    uint32_t* s_tile = scan_tmp + Shape::kWarps + 1;          // [3]
+    uint32_t* s_tile = scan_tmp + Shape::kWarps + 1;          // [6]
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 
     // The launch epoch is the successor of the last completed launch's epoch; the last CTA to
-    // finish publishes it, so CUDA-graph replays of this launch get a fresh epoch each time.
+    // finish publishes it, so CUDA-graph replays of this launch get a fresh epoch each time. One
+    // thread reads the tile descriptor (the list may sit in mapped host memory).
     if (threadIdx.x == 0) {
-        s_tile[0] = atomicAdd(&ctl->tile_counter, 1u);
+        const uint32_t tt = atomicAdd(&ctl->tile_counter, 1u);
+        s_tile[0] = tt;
         s_tile[1] = next_epoch(ld_relaxed_u32(&ctl->epoch));
+        if (tt < n_tiles) {
+            const gf_tile tl = tiles[tt];
+            s_tile[3] = tl.chunk_index;
+            s_tile[4] = tl.tile_offset;
+            s_tile[5] = tl.count;
+        }
     }
     __syncthreads();
     const uint32_t t = s_tile[0];
@@ -610,13 +653,15 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
         uint32_t* scratch = reinterpret_cast<uint32_t*>(smem_raw);
         finish_plan<Shape::kThreads>(totals, port_chunks, B, capacity, fdc, max_k, epoch, fin.table, fin.descs,
                                      fin.desc_cap, fin.num_out, status, scratch, scratch + kSeg, kSeg, lb_flag);
+        if (fin.done_rec != nullptr)
+            publish_done(fin, ctl, totals, B, status);
     };
     if (t >= n_tiles) {
         retire();
         return;
     }
 
-    const gf_tile tile = tiles[t];
+    const gf_tile tile{s_tile[3], s_tile[4], s_tile[5]};
     const uint64_t base = (uint64_t)tile.chunk_index * capacity + tile.tile_offset;
     const bool tile_ok = tile.count <= (uint32_t)Shape::kTile && base + tile.count <= pool_slots &&
                          tile.tile_offset + tile.count <= capacity;
@@ -752,14 +797,18 @@ struct MultiBatch {
 // Multi-batch form of fused_partition_kernel: one CTA per tile of the concatenated tile list
 // (`tile_batch[t]` = the tile's batch). A tile looks back only over the predecessors of its own
 // batch, which claimed their tiles earlier from the launch-wide counter, so every wait ends. The
-// batch's last tile to retire builds that batch's chunk table and descriptors; the launch's last
-// CTA publishes the epoch. The batches of one launch share the epoch, so their descriptor and
-// chunk-claim words from earlier launches read as stale.
+// batch's last tile to retire builds that batch's chunk table and descriptors and resets the
+// batch's counters; the launch's last CTA publishes the epoch and resets the launch counters. The
+// batches of one launch share the epoch, so their descriptor and chunk-claim words from earlier
+// launches read as stale. With `done_rec` (mapped host memory: [0] sequence, [1] status), the last
+// of the `live_batches` batches to finish copies the status word there and then writes `done_seq`,
+// so the host polls one word instead of an event.
 template <typename Shape, typename Access, typename Classify, typename Update>
 __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_partition_multi_kernel(
     Access acc, const Classify* classify_of, const Update* update_of, uint64_t seed_mixed, uint32_t capacity,
     FastDiv fdc, uint64_t pool_slots, const gf_tile* tiles, const uint32_t* tile_batch, uint32_t n_tiles, uint32_t B,
-    const MultiBatch* batches, uint32_t n_batches, uint32_t max_k, FusedCtl* ctl, uint32_t* status)
+    const MultiBatch* batches, uint32_t n_batches, uint32_t max_k, FusedCtl* ctl, uint32_t* status,
+    uint32_t* done_rec, uint32_t done_seq, uint32_t live_batches)
 {
     using P = typename Access::Payload;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -778,22 +827,41 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
     uint32_t* s_tile = scan_tmp + Shape::kWarps + 1;          // [3]
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 
+    // one thread reads the tile's batch record and descriptor (they sit in mapped host memory) into
+    // the stage area, which is free until step 4
+    uint32_t* s_rec = reinterpret_cast<uint32_t*>(smem_raw);
+    constexpr uint32_t kRecWords = (uint32_t)(sizeof(MultiBatch) / 4u);
     if (threadIdx.x == 0) {
-        s_tile[0] = atomicAdd(&ctl->tile_counter, 1u);
+        const uint32_t g0 = atomicAdd(&ctl->tile_counter, 1u);
+        s_tile[0] = g0;
         s_tile[1] = next_epoch(ld_relaxed_u32(&ctl->epoch));
+        const uint32_t b0 = g0 < n_tiles ? tile_batch[g0] : 0u;
+        s_tile[2] = b0;
+        if (g0 < n_tiles && b0 < n_batches) {
+            const uint2* src = reinterpret_cast<const uint2*>(batches + b0);
+            uint2* dst = reinterpret_cast<uint2*>(s_rec);
+            for (uint32_t i = 0; i < kRecWords / 2u; ++i)
+                dst[i] = src[i];
+            const gf_tile tl = tiles[g0];
+            s_rec[kRecWords] = tl.chunk_index;
+            s_rec[kRecWords + 1u] = tl.tile_offset;
+            s_rec[kRecWords + 2u] = tl.count;
+        }
     }
     __syncthreads();
     const uint32_t gt = s_tile[0];
     const uint32_t epoch = s_tile[1];
-    const uint32_t bi = gt < n_tiles ? __ldg(tile_batch + gt) : 0u;
+    const uint32_t bi = s_tile[2];
     const bool in_range = gt < n_tiles && bi < n_batches;
     if (gt < n_tiles && !in_range && threadIdx.x == 0)
         set_status(status, GF_INVALID);
-    const MultiBatch mb = in_range ? batches[bi] : MultiBatch{};
+    const MultiBatch mb = in_range ? *reinterpret_cast<const MultiBatch*>(s_rec) : MultiBatch{};
+    const gf_tile tile{s_rec[kRecWords], s_rec[kRecWords + 1u], s_rec[kRecWords + 2u]};
     const uint32_t t = gt - mb.tile_begin; // the tile's index inside its batch
     const bool batch_ok = in_range && gt >= mb.tile_begin && t < mb.n_tiles;
     if (in_range && !batch_ok && threadIdx.x == 0)
         set_status(status, GF_INVALID);
+    __syncthreads(); // the record is in registers: the stage area is free again
 
     // retire: the batch's last tile builds the batch's table and descriptors; the launch's last
     // CTA publishes the epoch
@@ -804,8 +872,12 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
             uint32_t last_of_batch = 0u;
             if (batch_ok)
                 last_of_batch = atomicAdd(mb.counters + 1, 1u) + 1u == mb.n_tiles ? 1u : 0u;
-            if (atomicAdd(&ctl->done, 1u) + 1u == gridDim.x)
+            if (atomicAdd(&ctl->done, 1u) + 1u == gridDim.x) {
+                // every CTA has counted itself: the launch counters are free for the next launch
                 atomicExch(&ctl->epoch, epoch);
+                ctl->tile_counter = 0u;
+                ctl->done = 0u;
+            }
             s_tile[2] = last_of_batch;
         }
         __syncthreads();
@@ -816,6 +888,22 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
         uint32_t* scratch = reinterpret_cast<uint32_t*>(smem_raw);
         finish_plan<Shape::kThreads>(mb.totals, mb.port_chunks, B, capacity, fdc, max_k, epoch, mb.table, mb.descs,
                                      mb.desc_cap, mb.num_out, status, scratch, scratch + kSeg, kSeg, lb_flag);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            mb.counters[0] = 0u; // the batch's claims and tiles are all counted
+            mb.counters[1] = 0u;
+            if (done_rec != nullptr) {
+                __threadfence_system(); // this batch's descriptors and output count reach the host first
+                if (atomicAdd(&ctl->alloc_cursor, 1u) + 1u == live_batches) {
+                    ctl->alloc_cursor = 0u;
+                    __threadfence(); // every other batch's finish came before its count
+                    done_rec[1] = ld_relaxed_u32(status);
+                    *status = 0u;
+                    __threadfence_system();
+                    *reinterpret_cast<volatile uint32_t*>(done_rec) = done_seq;
+                }
+            }
+        }
     };
     if (!batch_ok) {
         retire();
@@ -824,7 +912,6 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
     const Classify classify = classify_of[mb.member];
     const Update update = update_of[mb.member];
 
-    const gf_tile tile = tiles[gt];
     const uint64_t base = (uint64_t)tile.chunk_index * capacity + tile.tile_offset;
     const bool tile_ok = tile.count <= (uint32_t)Shape::kTile && base + tile.count <= pool_slots &&
                          tile.tile_offset + tile.count <= capacity;

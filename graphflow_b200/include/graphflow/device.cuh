@@ -401,5 +401,15 @@ private:
     std::size_t m_n = 0;
 };
 
+// Device address of pinned host memory (cudaMallocHost memory is mapped; under unified addressing
+// the address is the host pointer itself).
+template <typename T>
+T* mappedDevicePointer(T* host)
+{
+    void* d = nullptr;
+    check(cudaHostGetDevicePointer(&d, host, 0), "cudaHostGetDevicePointer");
+    return static_cast<T*>(d);
+}
+
 } // namespace cuda
 } // namespace graphflow

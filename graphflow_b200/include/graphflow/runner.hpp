@@ -183,7 +183,8 @@ public:
                 // 1) retire
                 for (std::size_t k = 0; k < m_nodes.size(); ++k) {
                     Node& node = m_nodes[k];
-                    if (!node.armed || !Ops::done(node.event))
+                    if (!node.armed ||
+                        !(node.stage->pollsCompletion() ? node.stage->completed() : Ops::done(node.event)))
                         continue;
                     node.armed = false;
                     std::uint32_t allocated = 0;
@@ -335,7 +336,8 @@ private:
         ++n.eventEnqueues;
         if (m_failureHook)
             m_failureHook(FailurePoint::eventEnqueue, static_cast<std::uint32_t>(k), n.eventEnqueues);
-        Ops::record(n.event, n.stream);
+        if (!n.stage->pollsCompletion())
+            Ops::record(n.event, n.stream);
         n.armed = true;
     }
     void arm(Node& n) { arm(n, static_cast<std::size_t>(&n - m_nodes.data())); }

@@ -51,6 +51,10 @@ public:
     }
     // Partition batches the last launch ran (a partition group runs several per launch).
     virtual std::uint32_t lastLaunchBatches() const { return 1u; }
+    // A stage whose device work reports its own completion in host memory answers true; the
+    // runner then polls completed() instead of recording and querying the node's event.
+    virtual bool pollsCompletion() const { return false; }
+    virtual bool completed() const { return true; }
 
 protected:
     std::uint64_t m_launches = 0;

@@ -10,6 +10,7 @@
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -313,6 +314,15 @@ public:
             m_io = detail::Staged<std::uint32_t>(m_oCtl + (m_scratchBytes + 3u) / 4u);
             cuda::check(cudaMemset(m_io.dev.data(), 0, m_io.dev.size() * 4u), "memset");
             std::fill(m_io.host.data(), m_io.host.data() + m_io.host.size(), 0u);
+            // per batch, no copies and no event: the kernel reads its tiles and reserved chunks from
+            // mapped pinned memory and its finishing CTA writes a completion record there (status,
+            // output count, totals, descriptors, then the batch's sequence number), which the runner
+            // polls with a plain load; the launch counters reset themselves
+            m_hin = cuda::HostBuffer<std::uint32_t>(3u * m_tileCap + (m_bound ? m_bound : 1u));
+            m_rec = cuda::HostBuffer<std::uint32_t>(3u + bins + 3u * (m_bound ? m_bound : 1u));
+            std::fill(m_rec.data(), m_rec.data() + m_rec.size(), 0u);
+            m_hinDev = cuda::mappedDevicePointer(m_hin.data());
+            m_recDev = cuda::mappedDevicePointer(m_rec.data());
         } else {
             m_binIds = cuda::Buffer<std::uint32_t>(st.slotCount());
         }
@@ -360,38 +370,33 @@ public:
             const Cls cls{m_cls, m_seed, m_purpose, status};
             const Upd upd{m_upd, m_purpose + 1u, status};
             const std::uint32_t bound = checkedOutputChunkBound(m_n, m_C, m_bins);
-            std::memcpy(m_io.host.data() + m_oTiles, m_tiles.host.data(), sizeof(gf_tile) * m_numTiles);
+            std::memcpy(m_hin.data(), m_tiles.host.data(), sizeof(gf_tile) * m_numTiles);
             m_reserved.clear();
             for (std::uint32_t k = 0; k < bound; ++k) {
                 m_reserved.push_back(m_st.ledger().acquire());
-                m_io.host[m_oReserved + k] = m_reserved.back().index;
+                m_hin.data()[3u * m_tileCap + k] = m_reserved.back().index;
             }
-            m_io.host[m_oStatus] = 0u;
-            for (std::uint32_t i = 0; i < 3u; ++i)
-                m_io.host[m_oCtl + i] = 0u; // FusedCtl tile counter, allocation cursor, done
-            cuda::check(cudaMemcpyAsync(io + m_oTiles, m_io.host.data() + m_oTiles, 4u * (m_oCtl + 3u - m_oTiles),
-                                        cudaMemcpyHostToDevice, s),
-                        "H2D");
+            ++m_seq;
             auto* ctl = reinterpret_cast<gf::FusedCtl*>(io + m_oCtl);
             auto* desc = reinterpret_cast<unsigned long long*>(ctl + 1);
-            auto* tiles = reinterpret_cast<const gf_tile*>(io + m_oTiles);
+            auto* tiles = reinterpret_cast<const gf_tile*>(m_hinDev);
             auto* descs = reinterpret_cast<gf_out_desc*>(io + m_oDescs);
             if (m_numTiles) {
-                // the launch's last CTA builds the table and descriptors (no separate finish launch)
+                // the launch's last CTA builds the table and descriptors and publishes the record
+                gf::InlineFinish fin{m_table.dev.data(), descs, m_bound, io};
+                fin.done_rec = m_recDev;
+                fin.done_seq = m_seq;
                 gf::fused_partition_kernel<Shape, Acc, Cls, Upd><<<m_numTiles, Shape::kThreads, m_smemFused, s>>>(
                     acc, cls, upd, m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(), tiles, m_numTiles, m_bins,
-                    io + m_oReserved, bound, io + m_oTotals, m_portChunks.data(), m_maxK, ctl, desc, status,
-                    gf::InlineFinish{m_table.dev.data(), descs, m_bound, io});
+                    m_hinDev + 3u * m_tileCap, bound, io + m_oTotals, m_portChunks.data(), m_maxK, ctl, desc, status,
+                    fin);
                 cuda::check(cudaGetLastError(), "fused partition kernel launch");
             } else {
-                cuda::check(cudaMemsetAsync(io + m_oTotals, 0, 4u * m_bins, s), "memset");
-                // the finish kernel of the C ABI builds the (empty) table and descriptors
-                throw_on(gf_fused_finish(s, io + m_oTotals, m_portChunks.data(), m_bins, m_C, m_maxK, ctl,
-                                         m_table.dev.data(), descs, m_bound, io, status),
-                         "fused partition finish");
+                // an empty batch: nothing to run, the record is complete at once
+                std::uint32_t* rec = m_rec.data();
+                std::fill(rec + 1, rec + 3 + m_bins, 0u);
+                reinterpret_cast<volatile std::uint32_t*>(rec)[0] = m_seq;
             }
-            cuda::check(cudaMemcpyAsync(m_io.host.data(), io, 4u * (m_oStatus + 1u), cudaMemcpyDeviceToHost, s),
-                        "D2H");
             return bound;
         }
         m_tiles.upload(s, m_numTiles);
@@ -410,6 +415,15 @@ public:
         m_status.download(s, 1);
         m_counts.download(s, m_bins + 1u);
         return 0u;
+    }
+
+    bool pollsCompletion() const override { return m_fused; }
+    bool completed() const override
+    {
+        const bool done = reinterpret_cast<const volatile std::uint32_t*>(m_rec.data())[0] == m_seq;
+        if (done)
+            std::atomic_thread_fence(std::memory_order_acquire);
+        return done;
     }
 
     bool advance(cudaStream_t s, const Batch& b, std::uint32_t& allocated) override
@@ -456,11 +470,12 @@ private:
 
     bool finishFused(const Batch&)
     {
-        detail::checkStatusWord(m_io.host[m_oStatus], "fused partition");
-        const std::uint32_t r = m_io.host[0];
+        const std::uint32_t* rec = m_rec.data();
+        detail::checkStatusWord(rec[1], "fused partition");
+        const std::uint32_t r = rec[2];
         std::uint64_t total = 0;
         for (std::uint32_t b = 0; b < m_bins; ++b)
-            total += m_io.host[m_oTotals + b];
+            total += rec[3u + b];
         if (total != m_n)
             throw BatchError("fused partition: classified particle count does not match the batch");
         // reservation slot of every reserved chunk index (a flat table over the pool, cleared after use)
@@ -480,7 +495,7 @@ private:
         m_reservedCopy = m_reserved;
         if (r > m_bound)
             throw BatchError("fused partition: more output chunks than the reservation bound");
-        const gf_out_desc* d = reinterpret_cast<const gf_out_desc*>(m_io.host.data() + m_oDescs);
+        const gf_out_desc* d = reinterpret_cast<const gf_out_desc*>(rec + 3u + m_bins);
         std::vector<bool>& used = m_usedSlot;
         used.assign(m_reserved.size(), false);
         for (std::uint32_t i = 0; i < r; ++i) {
@@ -579,6 +594,10 @@ private:
     detail::Staged<std::uint32_t> m_counts, m_next, m_table, m_status, m_numOut;
     detail::Staged<gf_out_desc> m_descs;
     detail::Staged<std::uint32_t> m_io; // fused form: the packed per-batch buffer (layout in the constructor)
+    cuda::HostBuffer<std::uint32_t> m_hin, m_rec; // fused form: mapped tiles + reserved chunks, completion record
+    std::uint32_t* m_hinDev = nullptr;
+    std::uint32_t* m_recDev = nullptr;
+    std::uint32_t m_seq = 0;
     std::uint32_t m_oTotals = 0, m_oDescs = 0, m_oTiles = 0, m_oReserved = 0, m_oStatus = 0, m_oCtl = 0;
     cuda::Buffer<std::uint32_t> m_binIds;
     cuda::Buffer<unsigned long long> m_portChunks;
@@ -650,18 +669,23 @@ public:
         m_table = cuda::Buffer<std::uint32_t>(static_cast<std::size_t>(m_maxBatches) * (bins + m_boundMax));
         cuda::check(cudaMemset(m_portChunks.data(), 0, m_portChunks.size() * 8u), "memset");
         cuda::check(cudaMemset(m_desc.data(), 0, m_desc.size() * 8u), "memset");
-        // mirrored words: [status | numOut[maxBatches] | descs[maxBatches][boundMax] | ctl (4 words) |
-        // payload: tiles, tile batch, batch records, reserved chunks, batch counters]; a launch uploads
-        // ctl + payload in one copy and downloads status, numOut and the descriptors in one copy
-        m_oNum = 1u;
+        // a launch makes no copy and records no event: the kernel reads its payload (tiles, tile
+        // batch, batch records, reserved chunks) from mapped pinned memory, every batch's finish
+        // writes its output count and descriptors into the mapped record [sequence | status |
+        // numOut[maxBatches] | descs[maxBatches][boundMax]], and the last batch to finish writes
+        // the status and then the sequence number, which the runner polls. The device words
+        // [status | pad | control block (4) | per-batch counters (2 each)] reset themselves.
+        m_dev = cuda::Buffer<std::uint32_t>(8u + 2u * static_cast<std::size_t>(m_maxBatches));
+        cuda::check(cudaMemset(m_dev.data(), 0, m_dev.size() * 4u), "memset");
+        m_oNum = 2u;
         m_oDescs = m_oNum + m_maxBatches;
-        m_oCtl = (m_oDescs + 3u * m_maxBatches * m_boundMax + 3u) & ~3u;
-        m_oPay = m_oCtl + 4u;
+        m_rec = cuda::HostBuffer<std::uint32_t>(m_oDescs + 3u * static_cast<std::size_t>(m_maxBatches) * m_boundMax);
+        std::fill(m_rec.data(), m_rec.data() + m_rec.size(), 0u);
         const std::size_t payMax = 4u * static_cast<std::size_t>(m_maxTiles) +
-                                   m_maxBatches * (sizeof(gf::MultiBatch) / 4u + m_boundMax + 2u) + 4u;
-        m_io = detail::Staged<std::uint32_t>(m_oPay + payMax);
-        cuda::check(cudaMemset(m_io.dev.data(), 0, m_io.dev.size() * 4u), "memset");
-        std::fill(m_io.host.data(), m_io.host.data() + m_io.host.size(), 0u);
+                                   m_maxBatches * (sizeof(gf::MultiBatch) / 4u + m_boundMax) + 4u;
+        m_pay = cuda::HostBuffer<std::uint32_t>(payMax);
+        m_payDev = cuda::mappedDevicePointer(m_pay.data());
+        m_recDev = cuda::mappedDevicePointer(m_rec.data());
         m_smem = smemBytes(bins);
         cuda::check(cudaFuncSetAttribute(gf::fused_partition_multi_kernel<Shape, Acc, Cls, Upd>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(m_smem)),
@@ -672,7 +696,7 @@ public:
     // chunks routed to it.
     std::uint32_t addMember(TClassifier cls, TUpdate upd, std::uint32_t purpose)
     {
-        std::uint32_t* status = m_io.dev.data();
+        std::uint32_t* status = m_dev.data();
         m_cls.push_back(Cls{cls, m_seed, purpose, status});
         m_upd.push_back(Upd{upd, purpose + 1u, status});
         m_membersDirty = true;
@@ -681,6 +705,14 @@ public:
     std::uint32_t members() const { return static_cast<std::uint32_t>(m_cls.size()); }
 
     bool plansBatches() const override { return true; }
+    bool pollsCompletion() const override { return true; }
+    bool completed() const override
+    {
+        const bool done = reinterpret_cast<const volatile std::uint32_t*>(m_rec.data())[0] == m_seq;
+        if (done)
+            std::atomic_thread_fence(std::memory_order_acquire);
+        return done;
+    }
     std::uint32_t lastLaunchBatches() const override { return static_cast<std::uint32_t>(m_sub.size()); }
 
     // The longest prefix of `ready` (at most groupChunks chunks, tiles and batches within the
@@ -762,9 +794,9 @@ public:
         if (m_sub.size() > m_maxBatches)
             throw BatchError("partition group: more batches than one launch holds");
         // reservations, tiles and batch records
-        std::uint32_t* h = m_io.host.data();
-        std::uint32_t* d = m_io.dev.data();
-        std::uint32_t nTiles = 0, nReserved = 0;
+        std::uint32_t* h = m_pay.data();
+        std::uint32_t* d = m_payDev;
+        std::uint32_t nTiles = 0, nReserved = 0, live = 0;
         m_reserved.clear();
         for (auto& sb : m_sub) {
             sb.n = 0u;
@@ -779,16 +811,17 @@ public:
             for (const auto& c : sb.chunks)
                 nTiles += (c.fill + kTile - 1u) / kTile;
             sb.tiles = nTiles - sb.tileBegin;
+            live += sb.tiles != 0u ? 1u : 0u;
         }
         if (nTiles > m_maxTiles)
             throw BatchError("partition group: more tiles than one launch holds");
         const std::uint32_t nb = static_cast<std::uint32_t>(m_sub.size());
-        const std::uint32_t oTiles = m_oPay, oTileBatch = oTiles + 3u * nTiles;
+        const std::uint32_t oTiles = 0u, oTileBatch = oTiles + 3u * nTiles;
         const std::uint32_t oBatches = (oTileBatch + nTiles + 1u) & ~1u;
         const std::uint32_t oRes = oBatches + nb * static_cast<std::uint32_t>(sizeof(gf::MultiBatch) / 4u);
-        const std::uint32_t oCnt = oRes + nReserved, oEnd = oCnt + 2u * nb;
         auto* tiles = reinterpret_cast<gf_tile*>(h + oTiles);
         auto* recs = reinterpret_cast<gf::MultiBatch*>(h + oBatches);
+        std::uint32_t* rec = m_rec.data();
         std::uint32_t t = 0;
         for (std::uint32_t i = 0; i < nb; ++i) {
             const Sub& sb = m_sub[i];
@@ -800,8 +833,6 @@ public:
                 }
             for (std::uint32_t k = 0; k < sb.bound; ++k)
                 h[oRes + sb.resBegin + k] = m_reserved[sb.resBegin + k].index;
-            h[oCnt + 2u * i] = 0u;
-            h[oCnt + 2u * i + 1u] = 0u;
             gf::MultiBatch r{};
             r.tile_begin = sb.tileBegin;
             r.n_tiles = sb.tiles;
@@ -811,37 +842,34 @@ public:
             r.totals = m_totals.data() + static_cast<std::size_t>(i) * m_bins;
             r.port_chunks = m_portChunks.data() + static_cast<std::size_t>(i) * m_bins * m_Q;
             r.desc = m_desc.data() + static_cast<std::size_t>(i) * m_tilesPerBatch * m_bins;
-            r.counters = d + oCnt + 2u * i;
+            r.counters = m_dev.data() + 8u + 2u * i;
             r.table = m_table.data() + static_cast<std::size_t>(i) * (m_bins + m_boundMax);
-            r.descs = reinterpret_cast<gf_out_desc*>(d + m_oDescs) + static_cast<std::size_t>(i) * m_boundMax;
+            r.descs = reinterpret_cast<gf_out_desc*>(m_recDev + m_oDescs) + static_cast<std::size_t>(i) * m_boundMax;
             r.desc_cap = m_boundMax;
-            r.num_out = d + m_oNum + i;
+            r.num_out = m_recDev + m_oNum + i;
             recs[i] = r;
-            h[m_oNum + i] = 0u;
+            rec[m_oNum + i] = 0u;
         }
-        // control block: tile counter, (unused) cursor, retired CTAs, the last published epoch
-        h[m_oCtl] = h[m_oCtl + 1u] = h[m_oCtl + 2u] = 0u;
-        h[m_oCtl + 3u] = m_epoch;
-        h[0] = 0u;
-        cuda::check(cudaMemcpyAsync(d + m_oCtl, h + m_oCtl, 4u * (oEnd - m_oCtl), cudaMemcpyHostToDevice, s), "H2D");
-        if (nTiles) {
+        ++m_seq;
+        if (live != 0u) {
             const Acc acc{m_st.view()};
             gf::fused_partition_multi_kernel<Shape, Acc, Cls, Upd><<<nTiles, Shape::kThreads, m_smem, s>>>(
                 acc, m_clsDev.data(), m_updDev.data(), m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(),
                 reinterpret_cast<const gf_tile*>(d + oTiles), d + oTileBatch, nTiles, m_bins,
                 reinterpret_cast<const gf::MultiBatch*>(d + oBatches), nb, m_Q,
-                reinterpret_cast<gf::FusedCtl*>(d + m_oCtl), d);
+                reinterpret_cast<gf::FusedCtl*>(m_dev.data() + 4u), m_dev.data(), m_recDev, m_seq, live);
             cuda::check(cudaGetLastError(), "partition group launch");
-            m_epoch = gf::next_epoch(m_epoch);
+        } else {
+            rec[1] = 0u; // no particle: the record is complete at once
+            reinterpret_cast<volatile std::uint32_t*>(rec)[0] = m_seq;
         }
-        cuda::check(cudaMemcpyAsync(h, d, 4u * (m_oDescs + 3u * nb * m_boundMax), cudaMemcpyDeviceToHost, s), "D2H");
         return nReserved;
     }
 
     bool advance(cudaStream_t, const Batch&, std::uint32_t& allocated) override
     {
         allocated = 0u;
-        detail::checkStatusWord(m_io.host[0], "partition group");
+        detail::checkStatusWord(m_rec.data()[1], "partition group");
         return false;
     }
 
@@ -870,12 +898,12 @@ public:
             }
         } clear{m_slotOf, reserved, m_used, m_st.ledger()};
         std::vector<ChunkDescriptor> out;
-        const auto* descs = reinterpret_cast<const gf_out_desc*>(m_io.host.data() + m_oDescs);
+        const auto* descs = reinterpret_cast<const gf_out_desc*>(m_rec.data() + m_oDescs);
         for (std::size_t i = 0; i < m_sub.size(); ++i) {
             const Sub& sb = m_sub[i];
             if (sb.n == 0u)
                 continue;
-            const std::uint32_t r = m_io.host[m_oNum + i];
+            const std::uint32_t r = m_rec.data()[m_oNum + i];
             if (r > sb.bound)
                 throw BatchError("partition group: more output chunks than the reservation bound");
             std::uint64_t placed = 0;
@@ -928,10 +956,13 @@ private:
     bool m_membersDirty = true;
     cuda::Buffer<unsigned long long> m_portChunks, m_desc;
     cuda::Buffer<std::uint32_t> m_totals, m_table;
-    detail::Staged<std::uint32_t> m_io;
-    std::uint32_t m_oNum = 0, m_oDescs = 0, m_oCtl = 0, m_oPay = 0;
+    cuda::Buffer<std::uint32_t> m_dev;
+    cuda::HostBuffer<std::uint32_t> m_pay, m_rec;
+    std::uint32_t* m_payDev = nullptr;
+    std::uint32_t* m_recDev = nullptr;
+    std::uint32_t m_oNum = 0, m_oDescs = 0;
     std::size_t m_smem = 0;
-    std::uint32_t m_epoch = 0;
+    std::uint32_t m_seq = 0;
     std::vector<Sub> m_sub;
     std::vector<int> m_cur;
     std::vector<ChunkHandle> m_reserved;
