@@ -92,6 +92,7 @@ _SIGS = {
     "gf_run_kernel_axes": [_U64, _U64, _U32, _I32, _I32, _I32, _U32, _U32, _U32, _I32, _VP, _VP],
     "gf_device_policy": [_VP, _U64, _U32, _U32, _U32, _U32, _U64, _U64, _VP],
     "gf_run_particle_feedback_kernel": [_U64, _U64, _U32, _VP, _VP, _VP],
+    "gf_run_set_transform": [_U64, _U64, _U32, _U32, _U32, _U32, _VP, _VP, _VP],
     "gf_serve": [_VP, _U32, _I32, _U64, _U32, _VP, _VP],
     "gf_histogram_scratch_bytes": [_U64, _VP],
     "gf_histogram_u32": [_VP, _VP, _U64, _VP, _U64, _VP, _VP, _VP, _VP],
@@ -125,6 +126,7 @@ class FunctorParams(C.Structure):
                 ("increment", C.c_uint32), ("pad", C.c_uint32)]
 
 LAYOUT_SOA, LAYOUT_AOS = 0, 1
+LAYOUT_RECORD = 2  # gf_run_particle_feedback only: the graph over a Record payload
 
 
 class FlowStats(C.Structure):
@@ -250,6 +252,20 @@ def run_kernel_axes(seed, n, bins, distribution="balanced", scatter="shared", ch
     if rc != GF_OK:
         raise GfError(rc, "kernel axes: " + last_error())
     return weights[:n], stats
+
+
+def run_set_transform(seed, n, increment, chunk_capacity=1024, live_particles=4096, batch_chunks=1):
+    """Generate -> transform<Set<WeightTag, VisitTag>> -> sink over a Record payload. Returns
+    (weights, visits, stats)."""
+    import numpy as np
+    weights = np.zeros(max(n, 1), np.uint32)
+    visits = np.zeros(max(n, 1), np.uint32)
+    stats = FlowStats()
+    rc = lib().gf_run_set_transform(seed, n, increment, chunk_capacity, live_particles, batch_chunks,
+                                    weights.ctypes.data, visits.ctypes.data, C.byref(stats))
+    if rc != GF_OK:
+        raise GfError(rc, "set transform: " + last_error())
+    return weights[:n], visits[:n], stats
 
 
 def run_particle_feedback_kernel(seed, n, max_visits=64):

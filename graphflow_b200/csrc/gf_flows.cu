@@ -70,6 +70,13 @@ bool gf_group_partitions(); // gf_capi.cu
 
 // Runs a front-end call, mapping its exceptions to gf_status and the last-error message.
 gf_status gf_flows_guard(const std::function<void()>& body) { return guarded(body); }
+void gf_fill_flow_stats(const graphflow::SchedulerStats& s, double seconds, gf_flow_stats* out)
+{
+    fill_stats(s, seconds, out);
+}
+gf_status gf_run_particle_feedback_record_form(std::uint64_t n, std::uint32_t max_visits, graphflow::Tuning t,
+                                               std::uint32_t* h_weights, std::uint32_t* h_capped,
+                                               gf_flow_stats* h_stats); // gf_record_flows.cu
 
 gf_status gf_device_policy(const gf_device_props* h_props, uint64_t n, uint32_t chunk_capacity,
                            uint32_t live_particles, uint32_t tile_size, uint32_t live_per_chunk,
@@ -133,8 +140,24 @@ gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visit
     using namespace graphflow;
     using namespace graphflow::particle;
     if ((n != 0u && (h_weights == nullptr || h_capped == nullptr)) ||
-        (layout != GF_LAYOUT_SOA && layout != GF_LAYOUT_AOS))
+        (layout != GF_LAYOUT_SOA && layout != GF_LAYOUT_AOS && layout != GF_LAYOUT_RECORD))
         return GF_ERR_ARGUMENT;
+    if (layout == GF_LAYOUT_RECORD) {
+        Tuning t;
+        t.seed = seed;
+        if (chunk_capacity != 0u)
+            t.chunkCapacity = chunk_capacity;
+        if (live_particles != 0u)
+            t.liveParticles = live_particles;
+        t.batchChunks = batch_chunks;
+        t.fused = fused != 0;
+        if (gf_runner_batched()) {
+            t.sinkBatchChunks = gf_runner_sink_batch();
+            t.multiDispatch = true;
+            t.groupPartitions = gf_group_partitions();
+        }
+        return gf_run_particle_feedback_record_form(n, max_visits, t, h_weights, h_capped, h_stats);
+    }
     return guarded([&] {
         cuda::Device device = cuda::Device::current();
         device.makeCurrent();

@@ -24,6 +24,7 @@
 #include <string>
 #include <vector>
 
+#include "record.hpp"
 #include "runner.hpp"
 #include "stages.cuh"
 
@@ -38,6 +39,26 @@ inline std::uint64_t nextGraphIdentity()
     static std::uint64_t next = 1u;
     return next++;
 }
+template <typename T>
+inline constexpr bool isSet = false;
+template <typename... Tags>
+inline constexpr bool isSet<Set<Tags...>> = true;
+
+// A transform restricted to the attributes of TSet (flow/Flow.hpp:235-242): the functor receives
+// the record as a MutableRecordProxy<TRecord, TSet> (after the usual optional accelerator,
+// engine and status arguments) and changes it in place; attributes outside the set are moved
+// unchanged and are out of the functor's reach at compile time.
+template <typename F, typename TSet>
+struct SetTransform {
+    F f;
+    template <typename TRecord>
+    __device__ void operator()(const Acc&, rng::Engine& engine, Status& status, TRecord& p) const
+    {
+        auto view = p.template proxy<TSet>();
+        invokeWithContext(f, engine, status, view);
+    }
+};
+
 // One address per classifier and updater type pair: partition nodes that share it (and their port
 // count) can run as one partition group.
 template <typename TClassifier, typename TUpdate>
@@ -170,6 +191,16 @@ public:
                               return std::make_unique<TransformStage<TStorage, F>>(st, c, f, purpose);
                           });
         return NodeHandle(m_identity, key, 1u, m_nodes[key].name);
+    }
+
+    template <typename TSet, typename F>
+        requires detail::isSet<TSet>
+    TransformHandle transform(std::string name, F f)
+    {
+        static_assert(isRecord<TPayload>, "graphflow: transform<Set<...>> needs a graphflow::Record payload");
+        static_assert(detail::SetCompatible<TSet, typename TPayload::attribute_list>::value,
+                      "graphflow: transform<Set<...>> names a tag that is not an attribute of the payload");
+        return transform(std::move(name), detail::SetTransform<F, TSet>{f});
     }
 
     template <typename F>
@@ -439,3 +470,7 @@ template <typename TPayload, typename TDevice = cuda::Device>
 using SoAFlow = Flow<TPayload, TDevice, SoAStorage<TPayload, TDevice>>;
 
 } // namespace graphflow
+
+// The reference's namespace spelling, for callers written against graphFlow::Flow, Record, Field,
+// Set and rng::StreamTraits.
+namespace graphFlow = graphflow;

@@ -315,6 +315,9 @@ typedef struct gf_rec16_columns {
     void* records;
 } gf_rec16_columns;
 enum { GF_LAYOUT_SOA = 0, GF_LAYOUT_AOS = 1 };
+/* gf_run_particle_feedback only: the graph over a graphFlow::Record payload (named attributes, one
+ * device column each; examples/particle_feedback/ParticleTypes.hpp:20-47 in the reference). */
+enum { GF_LAYOUT_RECORD = 2 };
 
 /* Tile sizes the hash kernels are compiled for (the shared table has 2 x tile entries). */
 uint32_t gf_supported_hash_tile_sizes(uint32_t* h_sizes, uint32_t cap);
@@ -431,6 +434,15 @@ gf_status gf_run_kernel_axes(uint64_t seed, uint64_t n, uint32_t bins, int distr
                              int hash_path, uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks,
                              int fused, uint32_t* h_weights, gf_flow_stats* h_stats);
 
+/* A transform restricted to an attribute subset (flow/Flow.hpp:235-242 transform<Set<Tags...>>):
+ * Generate (the particle_feedback source over a Record payload) -> transform<Set<WeightTag,
+ * VisitTag>> adding `increment` to the weight and 1 to the visit -> sink. h_weights[id] and
+ * h_visits[id] receive every particle's weight (= increment) and visit (= 1). No reference entry
+ * point; it runs the front end's attribute-subset transform. Errors as gf_run_particle_feedback. */
+gf_status gf_run_set_transform(uint64_t seed, uint64_t n, uint32_t increment, uint32_t chunk_capacity,
+                               uint32_t live_particles, uint32_t batch_chunks, uint32_t* h_weights,
+                               uint32_t* h_visits, gf_flow_stats* h_stats);
+
 /* The same feedback graph with the same functors and RNG streams, run as one per-particle kernel
  * (every particle carried from the source to its sink by one thread, no batches): h_weights and
  * h_capped as gf_run_particle_feedback, identical values. No reference counterpart as an entry
@@ -509,7 +521,8 @@ gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins, uint32_t 
 /* examples/particle_feedback/ParticleFeedback.hpp:41-108 runParticleFeedback: the
  * Generate -> Filter -> {A, B} -> sink feedback graph with the example's functors, on the GPU.
  * h_weights[n] receives each particle's final weight (0xDEADBEEF if it never reached a sink),
- * h_capped[n] is 1 for particles stopped by the visit cap. layout: GF_LAYOUT_SOA / _AOS.
+ * h_capped[n] is 1 for particles stopped by the visit cap. layout: GF_LAYOUT_SOA / _AOS, or
+ * GF_LAYOUT_RECORD for the same graph written over a Record payload (identical results).
  * fused != 0 runs each partition batch as one fused launch, else classify + host plan + scatter.
  * Errors: GF_ERR_ARGUMENT (configuration), GF_ERR_RANGE (32/16-bit stream limits),
  * GF_INVALID / GF_OVERFLOW (a batch failed), GF_ERR_TIMEOUT (scheduler stall), GF_ERR_CUDA;
