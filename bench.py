@@ -593,7 +593,17 @@ def _cfg_particle_feedback():
     (w, c, st), _ = _timed(lambda: capi.run_particle_feedback(42, n, chunk_capacity=1024, live_particles=4096,
                                                              batch_chunks=1, fused=True))
     out["flow_fused"] = {"seconds": st.seconds, "particles_per_s": n / st.seconds,
-                         "partition_batches": st.partition_batches, "kernel_launches": st.kernel_launches}
+                         "partition_batches": st.partition_batches, "partition_launches": st.partition_launches,
+                         "kernel_launches": st.kernel_launches, "form": "partition groups (B200 runner)"}
+    capi.check(capi.lib().gf_set_tuning(b"group_partitions", 0), "tuning")
+    try:
+        (_, _, su), _ = _timed(lambda: capi.run_particle_feedback(42, n, chunk_capacity=1024, live_particles=4096,
+                                                                 batch_chunks=1, fused=True))
+    finally:
+        capi.check(capi.lib().gf_set_tuning(b"group_partitions", 1), "tuning")
+    out["flow_fused_one_node_per_partition"] = {"seconds": su.seconds, "particles_per_s": n / su.seconds,
+                                                "partition_batches": su.partition_batches,
+                                                "partition_launches": su.partition_launches}
     capi.check(capi.lib().gf_set_tuning(b"runner_batched", 0), "tuning")
     try:
         (w0, c0, st0), _ = _timed(lambda: capi.run_particle_feedback(42, n, chunk_capacity=1024, live_particles=4096,

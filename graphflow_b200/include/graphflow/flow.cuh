@@ -257,8 +257,7 @@ public:
                     if (m_nodes[j].partition && groupOf[j] < 0 && m_nodes[j].groupKey == m_nodes[k].groupKey &&
                         m_nodes[j].bins == m_nodes[k].bins)
                         members.push_back(j);
-                if (members.size() < 2u)
-                    continue;
+                // a group of one still drains all of its node's ready batches per launch
                 std::unique_ptr<Stage> g = m_nodes[k].makeGroup(storage, config, m_nodes[k].bins);
                 if (!g)
                     continue;

@@ -12,6 +12,34 @@
 
 namespace graphflow {
 
+// Host-polled completion of a front-end kernel: the launch's last CTA copies the status word into
+// a record in mapped host memory ([0] sequence, [1] status), clears the status word and the CTA
+// counter for the next launch, and writes the sequence number last, so the host reads a complete
+// record with a plain load and needs neither a copy nor an event.
+struct Completion {
+    std::uint32_t* ctas = nullptr; // device counter of retired CTAs, zero between launches
+    std::uint32_t* rec = nullptr;  // mapped host record
+    std::uint32_t seq = 0u;
+};
+
+__device__ inline void complete(const Completion& c, std::uint32_t* status)
+{
+    if (c.rec == nullptr)
+        return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(c.ctas, 1u) + 1u == gridDim.x) {
+            *c.ctas = 0u;
+            __threadfence(); // every other CTA's status write came before its count
+            c.rec[1] = gf::ld_relaxed_u32(status);
+            *status = 0u;
+            __threadfence_system();
+            *reinterpret_cast<volatile std::uint32_t*>(c.rec) = c.seq;
+        }
+    }
+}
+
 // One <= tile slice of one input chunk with its position in the batch's dense output.
 struct MoveTile {
     std::uint32_t in_chunk;
@@ -23,7 +51,8 @@ struct MoveTile {
 template <typename TFunctor, typename TView>
 __global__ void __launch_bounds__(256) source_kernel(TFunctor f, TView view, std::uint64_t seed_mixed,
                                                      std::uint32_t purpose, std::uint64_t first_id,
-                                                     std::uint64_t base, std::uint32_t fill, std::uint32_t* status)
+                                                     std::uint64_t base, std::uint32_t fill, std::uint32_t* status,
+                                                     Completion done = {})
 {
     for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < fill; i += gridDim.x * blockDim.x) {
         const std::uint64_t id = first_id + i;
@@ -32,6 +61,7 @@ __global__ void __launch_bounds__(256) source_kernel(TFunctor f, TView view, std
         auto payload = invokeWithContext(f, engine, st, id);
         view.store(base + i, static_cast<typename TView::Payload>(payload));
     }
+    complete(done, status);
 }
 
 // Out-of-place transform over a batch: input item i of tile t goes to dense output position
@@ -41,7 +71,8 @@ __global__ void __launch_bounds__(256) transform_kernel(TFunctor f, TView view, 
                                                         std::uint32_t purpose, const MoveTile* tiles,
                                                         std::uint32_t n_tiles, const std::uint32_t* out_chunks,
                                                         std::uint32_t n_out, std::uint32_t capacity, gf::FastDiv fdc,
-                                                        std::uint64_t slots, std::uint32_t* status)
+                                                        std::uint64_t slots, std::uint32_t* status,
+                                                        Completion done = {})
 {
     for (std::uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
         const MoveTile tile = tiles[t];
@@ -65,6 +96,7 @@ __global__ void __launch_bounds__(256) transform_kernel(TFunctor f, TView view, 
             view.store(out, p);
         }
     }
+    complete(done, status);
 }
 
 // Sink over a batch of input chunks (the reference launches one per chunk).
@@ -72,7 +104,7 @@ template <typename TFunctor, typename TView>
 __global__ void __launch_bounds__(256) sink_kernel(TFunctor f, TView view, std::uint64_t seed_mixed,
                                                    std::uint32_t purpose, const MoveTile* tiles,
                                                    std::uint32_t n_tiles, std::uint32_t capacity,
-                                                   std::uint64_t slots, std::uint32_t* status)
+                                                   std::uint64_t slots, std::uint32_t* status, Completion done = {})
 {
     for (std::uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
         const MoveTile tile = tiles[t];
@@ -88,6 +120,7 @@ __global__ void __launch_bounds__(256) sink_kernel(TFunctor f, TView view, std::
             invokeWithContext(f, engine, st, p);
         }
     }
+    complete(done, status);
 }
 
 // Storage view as a partition-kernel access policy (same columns in and out: the batch reads

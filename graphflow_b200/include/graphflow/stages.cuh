@@ -78,6 +78,41 @@ struct StatusWord {
     }
 };
 
+// A front-end stage's host-polled completion record (Completion in kernels.cuh): [0] sequence,
+// [1] status in mapped pinned memory, and the device counter the kernel's last CTA is elected by.
+struct CompletionRecord {
+    cuda::HostBuffer<std::uint32_t> rec{2};
+    cuda::Buffer<std::uint32_t> ctas{1};
+    std::uint32_t* recDev = nullptr;
+    std::uint32_t seq = 0u;
+    CompletionRecord()
+    {
+        rec.data()[0] = rec.data()[1] = 0u;
+        cuda::check(cudaMemset(ctas.data(), 0, 4u), "memset");
+        recDev = cuda::mappedDevicePointer(rec.data());
+    }
+    // the next launch's completion
+    Completion arm()
+    {
+        ++seq;
+        return Completion{ctas.data(), recDev, seq};
+    }
+    // a launch with nothing to run is complete at once
+    void completeOnHost()
+    {
+        rec.data()[1] = 0u;
+        reinterpret_cast<volatile std::uint32_t*>(rec.data())[0] = seq;
+    }
+    bool done() const
+    {
+        const bool d = reinterpret_cast<const volatile std::uint32_t*>(rec.data())[0] == seq;
+        if (d)
+            std::atomic_thread_fence(std::memory_order_acquire);
+        return d;
+    }
+    std::uint32_t status() const { return rec.data()[1]; }
+};
+
 inline void checkStatusWord(std::uint32_t w, const char* stage)
 {
     if (w != 0u)
@@ -99,20 +134,23 @@ public:
         if (b.chunks.size() != 1u)
             throw BatchError("source: a source batch is exactly one chunk");
         const auto& c = b.chunks[0];
-        m_status.prepare(s);
+        const Completion done = m_done.arm();
         const unsigned blocks = (c.fill + 255u) / 256u;
         if (blocks)
             source_kernel<<<blocks, 256, 0, s>>>(m_f, m_st.view(), m_seed, m_purpose, b.firstId,
-                                                  m_st.base(c.handle), c.fill, m_status.dev());
+                                                  m_st.base(c.handle), c.fill, m_status.dev(), done);
+        else
+            m_done.completeOnHost();
         cuda::check(cudaGetLastError(), "source launch");
-        m_status.download(s);
         ++m_launches;
         return 0u;
     }
+    bool pollsCompletion() const override { return true; }
+    bool completed() const override { return m_done.done(); }
     bool advance(cudaStream_t, const Batch&, std::uint32_t& allocated) override
     {
         allocated = 0u;
-        detail::checkStatusWord(m_status.read(), "source");
+        detail::checkStatusWord(m_done.status(), "source");
         return false;
     }
     void finish(const Batch& b, std::vector<ChunkDescriptor>& outputs) override
@@ -127,6 +165,7 @@ private:
     std::uint64_t m_seed;
     std::uint32_t m_purpose;
     detail::StatusWord m_status;
+    detail::CompletionRecord m_done;
 };
 
 template <typename TStorage, typename TFunctor>
@@ -135,9 +174,10 @@ public:
     TransformStage(TStorage& st, const Config& c, TFunctor f, std::uint32_t purpose)
         : m_st(st), m_f(std::move(f)), m_seed(gf::mix64(c.seed)), m_purpose(purpose), m_tile(1024u),
           m_tileCap(static_cast<std::uint32_t>(c.batchChunks) * ((c.chunkCapacity + 1023u) / 1024u)),
-          m_io(4u * m_tileCap + c.batchChunks) // [tiles (4 words each) | output chunk indices]
+          m_io(4u * m_tileCap + c.batchChunks) // mapped: [tiles (4 words each) | output chunk indices]
     {
         static_assert(sizeof(MoveTile) == 16, "packed layout");
+        m_ioDev = cuda::mappedDevicePointer(m_io.data());
     }
     std::uint32_t launch(cudaStream_t s, const Batch& b) override
     {
@@ -150,29 +190,31 @@ public:
         m_pending.clear();
         for (std::uint32_t k = 0; k < r; ++k) {
             const ChunkHandle h = m_st.ledger().acquire();
-            m_io.host[4u * m_tileCap + k] = h.index;
+            m_io.data()[4u * m_tileCap + k] = h.index;
             const std::uint64_t left = n - static_cast<std::uint64_t>(k) * C;
             m_pending.push_back(ChunkDescriptor{h, static_cast<std::uint32_t>(left < C ? left : C), 0u});
         }
         if (!tiles.empty())
-            std::memcpy(m_io.host.data(), tiles.data(), sizeof(MoveTile) * tiles.size());
-        // one upload: the whole tile region and the output chunk indices after it
-        m_io.upload(s, 4u * m_tileCap + r);
-        m_status.prepare(s);
-        auto* dtiles = reinterpret_cast<const MoveTile*>(m_io.dev.data());
+            std::memcpy(m_io.data(), tiles.data(), sizeof(MoveTile) * tiles.size());
+        // the kernel reads the tiles and output chunk indices from mapped memory
+        const Completion done = m_done.arm();
+        auto* dtiles = reinterpret_cast<const MoveTile*>(m_ioDev);
         if (!tiles.empty())
             transform_kernel<<<static_cast<unsigned>(tiles.size()), 256, 0, s>>>(
                 m_f, m_st.view(), m_seed, m_purpose, dtiles, static_cast<std::uint32_t>(tiles.size()),
-                m_io.dev.data() + 4u * m_tileCap, r, C, gf::FastDiv(C), m_st.slotCount(), m_status.dev());
+                m_ioDev + 4u * m_tileCap, r, C, gf::FastDiv(C), m_st.slotCount(), m_status.dev(), done);
+        else
+            m_done.completeOnHost();
         cuda::check(cudaGetLastError(), "transform launch");
-        m_status.download(s);
         ++m_launches;
         return r;
     }
+    bool pollsCompletion() const override { return true; }
+    bool completed() const override { return m_done.done(); }
     bool advance(cudaStream_t, const Batch&, std::uint32_t& allocated) override
     {
         allocated = 0u;
-        const std::uint32_t st = m_status.read();
+        const std::uint32_t st = m_done.status();
         if (st != 0u) {
             abort();
             detail::checkStatusWord(st, "transform");
@@ -196,8 +238,10 @@ private:
     TFunctor m_f;
     std::uint64_t m_seed;
     std::uint32_t m_purpose, m_tile, m_tileCap;
-    detail::Staged<std::uint32_t> m_io;
+    cuda::HostBuffer<std::uint32_t> m_io;
+    std::uint32_t* m_ioDev = nullptr;
     detail::StatusWord m_status;
+    detail::CompletionRecord m_done;
     std::vector<ChunkDescriptor> m_pending;
 };
 
@@ -208,28 +252,31 @@ public:
         : m_st(st), m_f(std::move(f)), m_seed(gf::mix64(c.seed)), m_purpose(purpose),
           m_tiles(static_cast<std::size_t>(c.sinkBatchChunks) * ((c.chunkCapacity + 1023u) / 1024u))
     {
+        m_tilesDev = cuda::mappedDevicePointer(m_tiles.data());
     }
     std::uint32_t launch(cudaStream_t s, const Batch& b) override
     {
         const auto tiles = detail::moveTiles(b, 1024u);
-        if (tiles.size() > m_tiles.host.size())
+        if (tiles.size() > m_tiles.size())
             throw BatchError("sink: tile capacity exceeded");
-        std::copy(tiles.begin(), tiles.end(), m_tiles.host.data());
-        m_tiles.upload(s, tiles.size());
-        m_status.prepare(s);
+        std::copy(tiles.begin(), tiles.end(), m_tiles.data());
+        const Completion done = m_done.arm();
         if (!tiles.empty())
             sink_kernel<<<static_cast<unsigned>(tiles.size()), 256, 0, s>>>(
-                m_f, m_st.view(), m_seed, m_purpose, m_tiles.dev.data(), static_cast<std::uint32_t>(tiles.size()),
-                m_st.chunkCapacity(), m_st.slotCount(), m_status.dev());
+                m_f, m_st.view(), m_seed, m_purpose, m_tilesDev, static_cast<std::uint32_t>(tiles.size()),
+                m_st.chunkCapacity(), m_st.slotCount(), m_status.dev(), done);
+        else
+            m_done.completeOnHost();
         cuda::check(cudaGetLastError(), "sink launch");
-        m_status.download(s);
         ++m_launches;
         return 0u;
     }
+    bool pollsCompletion() const override { return true; }
+    bool completed() const override { return m_done.done(); }
     bool advance(cudaStream_t, const Batch&, std::uint32_t& allocated) override
     {
         allocated = 0u;
-        detail::checkStatusWord(m_status.read(), "sink");
+        detail::checkStatusWord(m_done.status(), "sink");
         return false;
     }
     void finish(const Batch&, std::vector<ChunkDescriptor>&) override {}
@@ -240,8 +287,10 @@ private:
     TFunctor m_f;
     std::uint64_t m_seed;
     std::uint32_t m_purpose;
-    detail::Staged<MoveTile> m_tiles;
+    cuda::HostBuffer<MoveTile> m_tiles; // mapped: the kernel reads the batch's tiles in place
+    MoveTile* m_tilesDev = nullptr;
     detail::StatusWord m_status;
+    detail::CompletionRecord m_done;
 };
 
 // Dense partition stage. Plain form: classify -> (host) plan -> scatter -> finalise, two device
