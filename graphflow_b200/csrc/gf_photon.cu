@@ -12,6 +12,8 @@ gf_status gf_flows_guard(const std::function<void()>& body); // gf_flows.cu
 bool gf_runner_batched();                                       // gf_capi.cu
 uint32_t gf_runner_sink_batch();                                // gf_capi.cu
 
+bool gf_group_partitions(); // gf_capi.cu
+
 namespace {
 
 using namespace graphflow;
@@ -74,6 +76,7 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
             if (gf_runner_batched()) {
                 t.sinkBatchChunks = gf_runner_sink_batch();
                 t.multiDispatch = true;
+                t.groupPartitions = gf_group_partitions();
             }
             stats = runPhotonFlow<T, SoAStorage<PhotonT<T>>>(device, n, propose, slab, scatter, terminal, t);
         } else if (n != 0u) {

@@ -701,7 +701,7 @@ public:
 
     PartitionGroupStage(TStorage& st, const Config& c, std::uint32_t bins)
         : m_st(st), m_seed(gf::mix64(c.seed)), m_bins(bins), m_C(c.chunkCapacity), m_Q(c.batchChunks),
-          m_maxChunks(c.groupChunks), m_maxBatches(c.groupChunks),
+          m_maxChunks(c.groupChunks), m_maxBatches(maxBatchesFor(c, bins)),
           m_tilesPerChunk((c.chunkCapacity + kTile - 1u) / kTile),
           m_maxTiles(c.groupChunks * ((c.chunkCapacity + kTile - 1u) / kTile)),
           m_tilesPerBatch(c.batchChunks * ((c.chunkCapacity + kTile - 1u) / kTile)),
@@ -739,6 +739,16 @@ public:
         cuda::check(cudaFuncSetAttribute(gf::fused_partition_multi_kernel<Shape, Acc, Cls, Upd>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(m_smem)),
                     "partition group: kernel attribute");
+    }
+
+    // Batches one launch holds: one per input chunk at most, and the batches' look-back descriptor
+    // scratch (tiles x ports x 8 bytes each) within 64 MiB.
+    static std::uint32_t maxBatchesFor(const Config& c, std::uint32_t bins)
+    {
+        const std::uint64_t perBatch = static_cast<std::uint64_t>(c.batchChunks) *
+                                       ((c.chunkCapacity + kTile - 1u) / kTile) * bins * 8u;
+        const std::uint64_t cap = std::max<std::uint64_t>(1u, (64ull << 20) / std::max<std::uint64_t>(perBatch, 1u));
+        return static_cast<std::uint32_t>(std::min<std::uint64_t>(c.groupChunks, cap));
     }
 
     // A member node's classifier, updater and stream purpose; its index is the route tag of the

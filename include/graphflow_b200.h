@@ -108,11 +108,12 @@ uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap);
  *                0 = the reference runner's one-chunk sinks and one dispatch per iteration.
  *                Results are identical.
  *   "sink_batch_chunks" 1..256 (default 256) = chunks per sink launch in the batched runner.
- *   "group_partitions" 1 (default) = with "runner_batched", gf_run_dense_chain and
- *                gf_run_particle_feedback run their fused partition nodes of one type as one
- *                partition group: one launch drains every member node's ready batches
- *                (sched/GraphRunner.hpp:985-1133 launches once per node batch); 0 = one runner node
- *                per partition node. Results are identical.
+ *   "group_partitions" 1 (default) = with "runner_batched", the flow entry points
+ *                (gf_run_dense_chain, gf_run_particle_feedback, gf_run_kernel_axes, gf_run_photon)
+ *                run their fused partition nodes of one type as one partition group (a group may be
+ *                one node): one launch drains every member node's ready batches, each of at most Q
+ *                chunks (sched/GraphRunner.hpp:985-1133 launches once per node batch); 0 = one
+ *                runner node per partition node. Results are identical.
  *   "hash_persistent" 1 (default) = gf_classify_hash_r16 and gf_scatter_hash_r16 use the
  *                persistent kernels (one shared-memory counter per port and CTA for the count;
  *                the scatter groups each tile's records of ports below 2048 by port and places
