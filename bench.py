@@ -54,6 +54,9 @@ def parse():
     p.add_argument("--hash", type=int, default=0, metavar="K",
                    help="only run the device-planned hash partition of --n records over K keys (Zipf 1.2, "
                         "tiles of 2048) --steps times after --warmup batches and print its timing; for profiling")
+    p.add_argument("--flow-chain", type=int, default=0, metavar="NODES",
+                   help="only run the dense chain of NODES partition nodes through the Flow on --n keys (--bins, "
+                        "--dist, C=8192, P=16384, Q=8, partition groups) and print its counters; for profiling")
     return p.parse_args()
 
 
@@ -995,8 +998,22 @@ def hash_only(args):
                       "status": int(part.status.item())}))
 
 
+def flow_chain_only(args):
+    """One run of the dense chain through the Flow, for profiling its launches."""
+    from graphflow_b200 import capi
+    _, st = capi.run_dense_chain(SEED, args.n, args.bins, nodes=args.flow_chain, dist=args.dist, chunk_capacity=8192,
+                                 live_particles=16384, batch_chunks=8, want_ports=False)
+    print(json.dumps({"workload": f"dense chain through the Flow, {args.flow_chain} nodes, N={args.n}, B={args.bins}, "
+                                  f"{args.dist}, C=8192 P=16384 Q=8", "seconds": st.seconds,
+                      "partition_batches": st.partition_batches, "partition_launches": st.partition_launches,
+                      "kernel_launches": st.kernel_launches, "sunk": st.sunk}))
+
+
 def main():
     args = parse()
+    if args.flow_chain:
+        flow_chain_only(args)
+        return
     if args.hash:
         hash_only(args)
         return
