@@ -681,8 +681,25 @@ def _cfg_hash(peak):
     import torch
     from graphflow_b200 import capi
     from graphflow_b200.hashpart import HashPartition, RecordPool
+    from graphflow_b200.autotune import tune_hash
     n, salt, out = 100_000_000, 0x5EED, {}
-    for k, cap in ((1 << 10, 8192), (1 << 16, 2048), (1 << 20, 512)):
+    free_bytes = torch.cuda.mem_get_info()[0]
+    tuned = {}
+    for k in (1 << 10, 1 << 16, 1 << 20):
+        # C and tile from the autotuner on a 2e7-record sample, among the capacities whose pool at the
+        # full N fits in half the free device memory
+        def pool_slots(c):
+            return (-(-n // c) + capi.output_chunk_bound(n, c, k)) * c
+        caps = tuple(c for c in (512, 1024, 2048, 4096, 8192)
+                     if pool_slots(c) < (1 << 32) and pool_slots(c) * 16 <= free_bytes // 2)
+        best, table = tune_hash(20_000_000, k, capacities=caps, tiles=(1024, 2048))
+        tuned[k] = (best["capacity"], best["tile"])
+        out[f"K{k}_autotune"] = {"chosen_C": best["capacity"], "chosen_tile": best["tile"], "sample_n": 20_000_000,
+                                 "candidates_ms": {f"C{t['capacity']}_T{t['tile']}": round(t["ms"], 3)
+                                                   for t in table if "ms" in t}}
+        torch.cuda.empty_cache()
+    for k in (1 << 10, 1 << 16, 1 << 20):
+        cap, tile = tuned[k]
         for layout in (capi.LAYOUT_SOA, capi.LAYOUT_AOS):
             if layout == capi.LAYOUT_AOS and k != (1 << 16):
                 continue
@@ -697,7 +714,7 @@ def _cfg_hash(peak):
             chunks = np.arange(n_in, dtype=np.uint32)
             for _ in range(n_in):
                 pool.free.popleft()
-            part = HashPartition(pool, k, salt, tile_size=2048, form="device", max_batch_particles=n)
+            part = HashPartition(pool, k, salt, tile_size=tile, form="device", max_batch_particles=n)
             tiles, d_tiles = part._tiles(chunks, fills)
             part.reserved[:bound].copy_(torch.from_numpy(np.arange(n_in, n_in + bound, dtype=np.uint32).view(np.int32)))
             for _ in range(2):
@@ -710,11 +727,11 @@ def _cfg_hash(peak):
             e1.record()
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1) / 5
-            name = f"K{k}_{'soa' if layout == capi.LAYOUT_SOA else 'aos'}_C{cap}"
+            name = f"K{k}_{'soa' if layout == capi.LAYOUT_SOA else 'aos'}_C{cap}_T{tile}"
             entry = {"device_form_ms": ms, "records_per_s": n / (ms / 1e3),
                      "hbm_frac": n * 32 / (ms / 1e3) / 1e9 / peak, "status": int(part.status.item())}
             if layout == capi.LAYOUT_SOA:
-                plain = HashPartition(pool, k, salt, tile_size=2048, form="plain")
+                plain = HashPartition(pool, k, salt, tile_size=tile, form="plain")
                 descs = plain.run(list(chunks), list(fills))[2]
                 pool.release([int(x) for x in descs[:, 0]])
                 (_, _, descs), sec = _timed(lambda: plain.run(list(chunks), list(fills)))
@@ -724,7 +741,8 @@ def _cfg_hash(peak):
             out[name] = entry
             del pool, part
             torch.cuda.empty_cache()
-    out["workload"] = "hash partition, N=1e8 16-byte records, Zipf 1.2 over K keys, tiles of 2048"
+    out["workload"] = ("hash partition, N=1e8 16-byte records, Zipf 1.2 over K keys; C and tile from the autotuner "
+                       "(device-planned form on a 2e7-record sample)")
     return out
 
 
