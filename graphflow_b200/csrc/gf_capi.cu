@@ -5,6 +5,7 @@
 #include <mutex>
 #include <string>
 
+#include "gf_fused_bulk.cuh"
 #include "gf_fused_coop.cuh"
 
 namespace gf {
@@ -13,6 +14,10 @@ namespace {
 // Tuning knob: 1 = gf_partition_fused_u32 uses the cooperative count/plan/scatter kernel where it
 // applies (default); 0 = always the per-tile look-back kernel.
 int g_fused_coop = 1;
+// Tuning knob: 1 = for up to 16 ports the cooperative kernel writes tiles out with bulk copies
+// (fused_partition_coop_bulk_kernel) when the scratch holds its tile histograms (default); 0 = the
+// warp-store write-out of fused_partition_coop_kernel for every port count.
+int g_fused_coop_bulk = 1;
 // Tuning knob: 1 = the flow entry points run the B200 runner options (sinks take up to Q chunks,
 // every idle node is dispatched per loop iteration); 0 = the reference's one-chunk sinks and one
 // dispatch per iteration.
@@ -113,6 +118,10 @@ gf_status gf_set_tuning(const char* name, int value)
         return GF_ERR_ARGUMENT;
     if (std::string(name) == "fused_coop") {
         g_fused_coop = value != 0;
+        return GF_OK;
+    }
+    if (std::string(name) == "fused_coop_bulk") {
+        g_fused_coop_bulk = value != 0;
         return GF_OK;
     }
     if (std::string(name) == "runner_batched") {
@@ -216,7 +225,8 @@ gf_status gf_fused_scratch_bytes(uint32_t n_tiles, uint32_t bins, uint64_t* h_by
 {
     if (h_bytes == nullptr || bins == 0u)
         return GF_ERR_ARGUMENT;
-    *h_bytes = sizeof(FusedCtl) + (uint64_t)n_tiles * bins * sizeof(unsigned long long);
+    // at least four ports' worth per tile: room for the cooperative kernels' tile histograms
+    *h_bytes = sizeof(FusedCtl) + (uint64_t)n_tiles * std::max(bins, 4u) * sizeof(unsigned long long);
     return GF_OK;
 }
 
@@ -255,10 +265,16 @@ gf_status fused_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_ou
         // the cooperative control block and the per-CTA port totals live in the descriptor area of
         // the scratch; the launcher zeroes the control block's reset words
         auto launch = [&]<typename S, typename Cls>(Cls cls) -> gf_status {
-            return cuda_status(launch_fused_coop<S>(as_stream(stream), cls, d_keys_in, d_keys_out, capacity,
-                                                    pool_slots, d_tiles, n_tiles, bins, d_reserved, n_reserved,
-                                                    d_totals, d_port_chunks, max_chunks_per_port, ctl, scratch_bytes,
-                                                    d_status, device_sms(), fin));
+            if constexpr (requires { S::kHistWords; })
+                return cuda_status(launch_fused_coop_bulk<S>(
+                    as_stream(stream), cls, d_keys_in, d_keys_out, capacity, pool_slots, d_tiles, n_tiles, bins,
+                    d_reserved, n_reserved, d_totals, d_port_chunks, max_chunks_per_port, ctl, scratch_bytes,
+                    d_status, device_sms(), fin));
+            else
+                return cuda_status(launch_fused_coop<S>(as_stream(stream), cls, d_keys_in, d_keys_out, capacity,
+                                                        pool_slots, d_tiles, n_tiles, bins, d_reserved, n_reserved,
+                                                        d_totals, d_port_chunks, max_chunks_per_port, ctl,
+                                                        scratch_bytes, d_status, device_sms(), fin));
         };
         auto with_cls = [&]<typename S>() -> gf_status {
             if (classifier == GF_CLS_KEY_MOD || classifier == GF_CLS_ID_BALANCED) {
@@ -268,8 +284,13 @@ gf_status fused_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_ou
             }
             return launch.template operator()<S>(AnyKeyClassify{key_classifier(classifier, bins)});
         };
+        const int sms = device_sms();
+        if (bins <= 4u && g_fused_coop_bulk != 0 && coop_bulk_fits<CoopBulkShape<2>>(n_tiles, scratch_bytes, sms))
+            return with_cls.template operator()<CoopBulkShape<2>>();
         if (bins <= 4u)
             return with_cls.template operator()<CoopShape<2>>();
+        if (bins <= 16u && g_fused_coop_bulk != 0 && coop_bulk_fits<CoopBulkShape<8>>(n_tiles, scratch_bytes, sms))
+            return with_cls.template operator()<CoopBulkShape<8>>();
         if (bins <= 16u)
             return with_cls.template operator()<CoopShape<8>>();
         return with_cls.template operator()<CoopShape<32>>();
@@ -440,7 +461,7 @@ extern "C" gf_status gf_partition_fused_u32_noalloc(
         return GF_ERR_ARGUMENT;
     if (need > kNoAllocScratchBytes) {
         gf_set_last_error(("gf_partition_fused_u32_noalloc: the batch needs " + std::to_string(need) +
-                           " scratch bytes (64 + 8 x tiles x ports) but the static scratch holds " +
+                           " scratch bytes (64 + 8 x tiles x max(ports, 4)) but the static scratch holds " +
                            std::to_string(kNoAllocScratchBytes) + "; use gf_partition_fused_u32 with caller scratch")
                               .c_str());
         return GF_ERR_RANGE;

@@ -102,6 +102,10 @@ uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap);
  *                per-tile look-back kernel. Per-port counts, the plan and every port's sequence are
  *                identical either way; the cooperative kernel also takes the output chunks in plan
  *                order (table[B + f] = reserved[f]).
+ *   "fused_coop_bulk" 1 (default) = for up to 16 ports the cooperative kernel writes each tile's
+ *                port runs with bulk copies (shared -> global) when the scratch also holds one
+ *                histogram per tile (gf_fused_scratch_bytes sizes it so); 0 = warp stores.
+ *                Results are identical.
  *   "runner_batched" 1 (default) = the flow entry points (gf_run_particle_feedback,
  *                gf_run_dense_chain, gf_run_photon) let a sink take up to "sink_batch_chunks"
  *                ready chunks per launch and dispatch every idle node in one scheduler iteration;
