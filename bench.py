@@ -668,6 +668,15 @@ def _cfg_dense_flow():
     out["nodes4_grouped_b200_runner"] = run(4, 100_000_000, True, True, grouped=True)
     out["nodes4_per_node_b200_runner"] = run(4, 1_000_000, True, True, grouped=False)
     out["nodes4_plain_reference_runner"] = run(4, 200_000, False, False)
+    # the same chain run entirely on the device (device-resident chunk pool, one launch per node,
+    # no host round trip): device time over three runs, and the wall time of the whole call
+    runs = [capi.run_dense_chain_device(42, 100_000_000, 64, nodes=4, want_ports=False) for _ in range(3)]
+    dev = sorted(r[3].loop_seconds for r in runs)[1]
+    out["nodes4_device_chain"] = {"n": 100_000_000, "device_seconds": dev, "particles_per_s": 1e8 / dev,
+                                  "wall_seconds": sorted(r[3].seconds for r in runs)[1],
+                                  "kernel_launches": runs[0][3].kernel_launches,
+                                  "pool_chunks": runs[0][2].num_chunks, "peak_live_chunks": runs[0][2].peak_live,
+                                  "all_chunks_free": all(r[2].free_chunks == r[2].num_chunks for r in runs)}
     return out
 
 

@@ -97,6 +97,12 @@ _SIGS = {
     "gf_histogram_scratch_bytes": [_U64, _VP],
     "gf_histogram_u32": [_VP, _VP, _U64, _VP, _U64, _VP, _VP, _VP, _VP],
     "gf_run_dense_chain": [_U64, _U64, _U32, _U32, _I32, C.c_double, _U32, _U32, _U32, _I32, _I32, _VP, _VP],
+    "gf_run_dense_chain_device": [_U64, _U64, _U32, _U32, _I32, C.c_double, _VP, _VP, _VP, _VP],
+    "gf_device_pool_bytes": [_U32, C.POINTER(_U64)],
+    "gf_device_pool_init": [_VP, _VP, _U32],
+    "gf_device_pool_acquire": [_VP, _VP, _U32, _VP, _VP],
+    "gf_device_pool_settle": [_VP, _VP, _VP, _U32, _VP, _U32, _VP, _U32, _VP, _U32, _VP],
+    "gf_device_pool_read": [_VP, _VP, _VP],
     "gf_run_photon": [_U64, _U64, _U64, _VP, _I32, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                       _VP],
     "gf_run_photon_traced": [_U64, _U64, _U64, _VP, _I32, _U32, _U32, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
@@ -375,6 +381,36 @@ def run_dense_chain(seed, n, bins, nodes=1, dist="uniform", zipf_s=1.1, chunk_ca
     if rc != GF_OK:
         raise GfError(rc, "dense chain: " + last_error())
     return (port_of[:n] if want_ports else None), stats
+
+
+class DevicePoolStats(C.Structure):
+    """gf_device_pool_stats: counters of a device-resident chunk pool."""
+    _fields_ = [("num_chunks", C.c_uint32), ("free_chunks", C.c_uint32), ("peak_live", C.c_uint32),
+                ("status", C.c_uint32), ("acquired", C.c_uint64), ("released", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def run_dense_chain_device(seed, n, bins, nodes=1, dist="uniform", zipf_s=1.1, want_ports=True):
+    """The dense chain of run_dense_chain run entirely on the device with a device-resident chunk
+    pool. Returns (port_of, node_totals[nodes, bins], pool_stats, flow_stats)."""
+    import numpy as np
+    port_of = np.zeros(max(n, 1), np.uint32) if want_ports else None
+    totals = np.zeros((nodes, bins), np.uint32)
+    pool, stats = DevicePoolStats(), FlowStats()
+    rc = lib().gf_run_dense_chain_device(seed, n, bins, nodes, DIST_NAMES[dist], zipf_s,
+                                         port_of.ctypes.data if want_ports else None, totals.ctypes.data,
+                                         C.byref(pool), C.byref(stats))
+    if rc != GF_OK:
+        raise GfError(rc, "device dense chain: " + last_error())
+    return (port_of[:n] if want_ports else None), totals, pool, stats
+
+
+def device_pool_bytes(num_chunks):
+    out = C.c_uint64(0)
+    check(lib().gf_device_pool_bytes(num_chunks, C.byref(out)), "device pool bytes")
+    return out.value
 
 
 class Rec16Columns(C.Structure):

@@ -19,6 +19,7 @@
 
 #include "../examples/dense_chain.cuh"
 #include "../examples/particle_feedback.cuh"
+#include "gf_device_chain.cuh"
 
 gf_status gf_flows_guard(const std::function<void()>& body); // gf_flows.cu
 void gf_photon_enqueue_f32(cudaStream_t stream, const gf_photon_params& P, std::uint64_t seed, std::uint64_t n,
@@ -31,8 +32,6 @@ namespace {
 using namespace graphflow;
 
 constexpr std::uint32_t kChainNodes = 2u;
-constexpr std::uint32_t kChainCapacity = 8192u;
-constexpr std::uint32_t kChainTile = 4096u;
 constexpr std::uint32_t kFeedbackVisits = 64u;
 constexpr std::uint64_t kGolden = 0x9E3779B97F4A7C15ull;
 
@@ -102,182 +101,20 @@ __global__ void fill_u32_kernel(std::uint32_t* p, std::uint64_t n, std::uint32_t
         p[i] = v;
 }
 
-// ---- the two-node dense chain on the device ----
-struct KeyIdColumns { // {u32 id, u32 key} in two pool columns; a batch reads and writes distinct chunks
-    using Payload = dense::KeyRecord;
-    std::uint32_t* id;
-    std::uint32_t* key;
-    GF_D Payload load(std::uint64_t s) const { return Payload{id[s], key[s]}; }
-    GF_D void store(std::uint64_t s, const Payload& p) const
-    {
-        id[s] = p.id;
-        key[s] = p.key;
-    }
-};
-
-struct ShiftPort { // node i: port = (key >> 8 i) mod B (dense_chain.cuh's PortOfKey)
-    std::uint32_t shift;
-    gf::FastDiv fd;
-    GF_D std::uint32_t operator()(const dense::KeyRecord& r) const { return fd.mod(r.key >> shift); }
-};
-
-// Source: ids 0..n-1 with the chain's keys, in chunks 0.. of the request's pool (slot = id).
-__global__ void chain_source_kernel(std::uint64_t seedMixed, std::uint32_t bins, std::uint64_t n, std::uint32_t* id,
-                                    std::uint32_t* key)
+// ---- the two-node dense chain: gf_device_chain.cuh with a device-resident chunk pool ----
+gf::DeviceChainLayout chainLayout(std::uint64_t n, std::uint32_t bins)
 {
-    const std::uint64_t stride = static_cast<std::uint64_t>(gridDim.x) * blockDim.x;
-    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-        id[i] = static_cast<std::uint32_t>(i);
-        key[i] = gf::synthetic_key(GF_DIST_UNIFORM, seedMixed, i, bins, nullptr);
-    }
+    return gf::DeviceChainLayout(n, bins, kChainNodes, outputChunkBound(n, gf::kChainCapacity, bins));
 }
 
-// Two tiles per chunk: the source's full chunks, or a node's published output chunks.
-__global__ void chain_tiles_kernel(std::uint64_t n, std::uint32_t nChunks, const gf_out_desc* descs,
-                                   const std::uint32_t* numOut, gf_tile* tiles)
-{
-    for (std::uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < nChunks; f += gridDim.x * blockDim.x) {
-        std::uint32_t chunk = 0, fill = 0;
-        if (descs == nullptr) {
-            chunk = f;
-            const std::uint64_t left = n - static_cast<std::uint64_t>(f) * kChainCapacity;
-            fill = static_cast<std::uint32_t>(left < kChainCapacity ? left : kChainCapacity);
-        } else if (f < *numOut) {
-            chunk = descs[f].chunk_index;
-            fill = descs[f].fill;
-        }
-        tiles[2u * f] = gf_tile{chunk, 0u, fill < kChainTile ? fill : kChainTile};
-        tiles[2u * f + 1u] = gf_tile{chunk, kChainTile, fill > kChainTile ? fill - kChainTile : 0u};
-    }
-}
-
-__global__ void iota_kernel(std::uint32_t* p, std::uint32_t n, std::uint32_t first)
-{
-    for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        p[i] = first + i;
-}
-
-// Sink: each published output chunk of the last node records its port for every id in it.
-__global__ void chain_sink_kernel(const gf_out_desc* descs, const std::uint32_t* numOut, const std::uint32_t* id,
-                                  std::uint32_t* portOf, std::uint64_t n)
-{
-    for (std::uint32_t f = blockIdx.x; f < *numOut; f += gridDim.x) {
-        const gf_out_desc d = descs[f];
-        const std::uint64_t base = static_cast<std::uint64_t>(d.chunk_index) * kChainCapacity;
-        for (std::uint32_t i = threadIdx.x; i < d.fill; i += blockDim.x) {
-            const std::uint32_t who = id[base + i];
-            if (who < n)
-                portOf[who] = d.bin;
-        }
-    }
-}
-
-using ChainShape = gf::TileShape<256, 16, 3>;
-
-struct ChainLayout { // byte offsets of one chain request's buffers inside its arena block
-    std::uint64_t n, nIn, bound, slots, tiles, maxK, descBytes;
-    std::uint64_t id, key, tile, reserved, scratch, totals, portChunks, table, descs, numOut, portOf, total;
-    explicit ChainLayout(std::uint64_t n_, std::uint32_t bins) : n(n_)
-    {
-        nIn = (n + kChainCapacity - 1u) / kChainCapacity;
-        bound = outputChunkBound(n, kChainCapacity, bins);
-        const std::uint64_t chunks = nIn + kChainNodes * bound;
-        slots = chunks * kChainCapacity;
-        tiles = 2u * std::max<std::uint64_t>(nIn, bound);
-        maxK = std::max<std::uint64_t>(nIn, 1u);
-        auto up = [](std::uint64_t v) { return (v + 255u) & ~std::uint64_t(255u); };
-        std::uint64_t o = 0;
-        id = o;
-        o += up(slots * 4u);
-        key = o;
-        o += up(slots * 4u);
-        tile = o;
-        o += up(tiles * sizeof(gf_tile));
-        reserved = o;
-        o += up(kChainNodes * bound * 4u);
-        scratch = o;
-        o += up(64u + tiles * bins * 8u);
-        totals = o;
-        o += up(bins * 4u);
-        portChunks = o;
-        o += up(bins * maxK * 8u);
-        table = o;
-        o += up((bins + bound) * 4u);
-        descs = o;
-        o += up(bound * sizeof(gf_out_desc));
-        numOut = o;
-        o += 256u;
-        portOf = o;
-        o += up(std::max<std::uint64_t>(n, 1u) * 4u);
-        total = o;
-    }
-};
-
-// Enqueues the whole two-node chain of one request on `s` (digest into *acc, failures in *status).
-void enqueueChain(cudaStream_t s, char* base, const ChainLayout& L, std::uint32_t bins, std::uint64_t seed,
+void enqueueChain(cudaStream_t s, char* base, const gf::DeviceChainLayout& L, std::uint64_t seed,
                   std::uint32_t* status, unsigned long long* acc, std::uint32_t sms)
 {
-    auto P = [&](std::uint64_t off) { return base + off; };
-    auto* id = reinterpret_cast<std::uint32_t*>(P(L.id));
-    auto* key = reinterpret_cast<std::uint32_t*>(P(L.key));
-    auto* tiles = reinterpret_cast<gf_tile*>(P(L.tile));
-    auto* reserved = reinterpret_cast<std::uint32_t*>(P(L.reserved));
-    auto* ctl = reinterpret_cast<gf::FusedCtl*>(P(L.scratch));
-    auto* desc = reinterpret_cast<unsigned long long*>(ctl + 1);
-    auto* totals = reinterpret_cast<std::uint32_t*>(P(L.totals));
-    auto* portChunks = reinterpret_cast<unsigned long long*>(P(L.portChunks));
-    auto* table = reinterpret_cast<std::uint32_t*>(P(L.table));
-    auto* descs = reinterpret_cast<gf_out_desc*>(P(L.descs));
-    auto* numOut = reinterpret_cast<std::uint32_t*>(P(L.numOut));
-    auto* portOf = reinterpret_cast<std::uint32_t*>(P(L.portOf));
-    const unsigned g = static_cast<unsigned>(std::min<std::uint64_t>((L.slots + 255u) / 256u, sms * 8u)) + 1u;
-    fill_u32_kernel<<<g, 256, 0, s>>>(portOf, std::max<std::uint64_t>(L.n, 1u), 0xFFFFFFFFu);
-    // A fresh control block restarts the launch epochs at 1, so the epoch-tagged look-back
-    // descriptors and chunk claims left in this arena block by an earlier request are cleared too
-    // (tag 0 never matches a launch epoch).
-    cuda::check(cudaMemsetAsync(ctl, 0, 64u + L.tiles * bins * 8u, s), "memset");
-    cuda::check(cudaMemsetAsync(portChunks, 0, bins * L.maxK * 8u, s), "memset");
-    iota_kernel<<<std::min<std::uint32_t>(static_cast<std::uint32_t>((kChainNodes * L.bound + 255u) / 256u), 1024u) + 1u,
-                  256, 0, s>>>(reserved, static_cast<std::uint32_t>(kChainNodes * L.bound),
-                               static_cast<std::uint32_t>(L.nIn));
-    chain_source_kernel<<<g, 256, 0, s>>>(gf::mix64(seed), bins, L.n, id, key);
-    const KeyIdColumns acc_cols{id, key};
-    auto kernel = gf::fused_partition_kernel<ChainShape, KeyIdColumns, ShiftPort, gf::NoUpdate>;
-    constexpr int W = ChainShape::kWarps;
-    const std::size_t smem = sizeof(dense::KeyRecord) * ChainShape::kTile + 4u * ChainShape::kTile + 4u * W * bins +
-                             4u * bins * 6u + 4u * (W + 2u) + 16u + 4u * (4u + 2u * ChainShape::kThreads);
-    cuda::check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
-                "chain partition attribute");
-    constexpr int FT = 1024;
-    const std::size_t fsmem = sizeof(std::uint32_t) * (4096u * 2u + FT / 32 + 1);
-    cuda::check(cudaFuncSetAttribute(gf::fused_finish_kernel<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(fsmem)),
-                "finish attribute");
-    const gf::FastDiv fdc(kChainCapacity);
-    for (std::uint32_t node = 0; node < kChainNodes; ++node) {
-        const std::uint32_t nChunks = node == 0u ? static_cast<std::uint32_t>(L.nIn) : static_cast<std::uint32_t>(L.bound);
-        const std::uint32_t nTiles = 2u * nChunks;
-        chain_tiles_kernel<<<(nChunks + 255u) / 256u + 1u, 256, 0, s>>>(L.n, nChunks, node == 0u ? nullptr : descs,
-                                                                        numOut, tiles);
-        if (nTiles != 0u) {
-            cuda::check(cudaMemsetAsync(ctl, 0, gf::kFusedCtlResetBytes, s), "memset");
-            // the last CTA builds this node's table and descriptors (no separate finish launch)
-            kernel<<<nTiles, ChainShape::kThreads, smem, s>>>(
-                acc_cols, ShiftPort{8u * node, gf::FastDiv(bins)}, gf::NoUpdate{}, 0u, kChainCapacity, fdc, L.slots,
-                tiles, nTiles, bins, reserved + node * L.bound, static_cast<std::uint32_t>(L.bound), totals,
-                portChunks, static_cast<std::uint32_t>(L.maxK), ctl, desc, status,
-                gf::InlineFinish{table, descs, static_cast<std::uint32_t>(L.bound), numOut});
-        } else {
-            cuda::check(cudaMemsetAsync(totals, 0, bins * 4u, s), "memset");
-            gf::fused_finish_kernel<FT><<<1, FT, fsmem, s>>>(totals, portChunks, bins, kChainCapacity, fdc,
-                                                              static_cast<std::uint32_t>(L.maxK), ctl, table, descs,
-                                                              static_cast<std::uint32_t>(L.bound), numOut, status);
-        }
-    }
-    chain_sink_kernel<<<static_cast<unsigned>(std::min<std::uint64_t>(std::max<std::uint64_t>(L.bound, 1u), 4096u)),
-                        256, 0, s>>>(descs, numOut, id, portOf, L.n);
-    digest_port_kernel<<<g, 256, 0, s>>>(portOf, L.n, acc);
-    cuda::check(cudaGetLastError(), "chain launch");
+    gf::enqueueDeviceChain(s, base, L, GF_DIST_UNIFORM, nullptr, seed, status, sms);
+    const unsigned g = static_cast<unsigned>(std::min<std::uint64_t>((std::max<std::uint64_t>(L.n, 1u) + 255u) / 256u,
+                                                                     sms * 8u));
+    digest_port_kernel<<<g, 256, 0, s>>>(reinterpret_cast<const std::uint32_t*>(base + L.portOf), L.n, acc);
+    cuda::check(cudaGetLastError(), "chain digest launch");
 }
 
 // ---- requests ----
@@ -308,7 +145,7 @@ std::uint64_t footprint(const gf_request& r)
     case GF_REQ_PHOTON:
         return up(m * gf_photon_record_bytes_f32()) + up(m * 4u);
     default:
-        return ChainLayout(r.n, r.bins).total;
+        return chainLayout(r.n, r.bins).total;
     }
 }
 
@@ -344,7 +181,7 @@ void enqueueRequest(cudaStream_t s, const gf_request& r, char* block, unsigned l
         gf_photon_enqueue_f32(s, servedPhotonParams(), r.seed, r.n, rec, visits, status, sms);
         digest_photon_kernel<<<g, 256, 0, s>>>(reinterpret_cast<const PhotonRecordF32*>(rec), r.n, acc);
     } else {
-        enqueueChain(s, block, ChainLayout(r.n, r.bins), r.bins, r.seed, status, acc, sms);
+        enqueueChain(s, block, chainLayout(r.n, r.bins), r.seed, status, acc, sms);
     }
     cuda::check(cudaGetLastError(), "request launch");
     cuda::check(cudaMemcpyAsync(host, dev, 16u, cudaMemcpyDeviceToHost, s), "D2H");
@@ -454,7 +291,7 @@ gf_status runPlain(const gf_request& r, std::uint64_t& digest)
     }
     std::vector<std::uint32_t> port(m);
     gf_flow_stats st{};
-    const gf_status rc = gf_run_dense_chain(r.seed, r.n, r.bins, kChainNodes, GF_DIST_UNIFORM, 1.0, kChainCapacity,
+    const gf_status rc = gf_run_dense_chain(r.seed, r.n, r.bins, kChainNodes, GF_DIST_UNIFORM, 1.0, gf::kChainCapacity,
                                             16384u, 8u, 0, GF_LAYOUT_SOA, port.data(), &st);
     std::uint64_t d = 0;
     for (std::uint64_t i = 0; i < r.n; ++i)

@@ -523,6 +523,53 @@ gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins, uint32_t 
                              uint32_t chunk_capacity, uint32_t live_particles, uint32_t batch_chunks, int fused,
                              int layout, uint32_t* h_port_of, gf_flow_stats* h_stats);
 
+/* ---- device-resident chunk pool ----------------------------------------------------------------
+ * The host pool's free list, per-chunk ledger and reservation credits (core/ChunkPool.hpp:88-190,
+ * core/ChunkLedger.hpp:33-150, sched/GraphRunner.hpp:1014-1037) in device memory, for flows whose
+ * nodes run on the device without host round trips. One allocation of gf_device_pool_bytes(S)
+ * bytes (16-byte aligned) holds chunks 0..S-1; every operation is one kernel on `stream`, and the
+ * operations on one pool must be stream-ordered.
+ *   acquire  pops k chunks into d_ids[k] in the host pool's order (a fresh pool hands out 0, 1, ...;
+ *            the chunk released last comes out first). Fewer than k free: GF_OVERFLOW in *d_status
+ *            and in the pool, nothing taken, d_ids filled with 0xFFFFFFFF.
+ *   settle   after a batch that reserved d_reserved[reserved_n] (its outputChunkBound, from one
+ *            acquire) and used the first *d_used (or `used` when d_used is NULL) of them: the
+ *            unused ones go back exactly where they were, then the input chunks
+ *            d_in[j * in_stride], j < *d_in_count (or in_count), are released (in_stride 1 for an
+ *            id array, 3 for the chunk_index field of gf_out_desc records). A chunk that is not
+ *            live, out of range, named twice or one of the unused reservations, or unused
+ *            reservations no longer at the front of the free list: GF_INVALID, nothing changed.
+ * A chunk's ledger word is generation << 1 | live; releases step the generation. */
+typedef struct gf_device_pool_stats {
+    uint32_t num_chunks;
+    uint32_t free_chunks;
+    uint32_t peak_live; /* most chunks out of the pool at once */
+    uint32_t status;    /* GF_OK or the first failed operation's code */
+    uint64_t acquired;  /* chunks acquired over the pool's life (returned reservations excluded) */
+    uint64_t released;
+} gf_device_pool_stats;
+
+gf_status gf_device_pool_bytes(uint32_t num_chunks, uint64_t* h_bytes);
+gf_status gf_device_pool_init(void* stream, void* d_pool, uint32_t num_chunks);
+gf_status gf_device_pool_acquire(void* stream, void* d_pool, uint32_t k, uint32_t* d_ids, uint32_t* d_status);
+gf_status gf_device_pool_settle(void* stream, void* d_pool, const uint32_t* d_reserved, uint32_t reserved_n,
+                                const uint32_t* d_used, uint32_t used, const uint32_t* d_in, uint32_t in_stride,
+                                const uint32_t* d_in_count, uint32_t in_count, uint32_t* d_status);
+/* Synchronises `stream` and reads the pool's counters. */
+gf_status gf_device_pool_read(void* stream, const void* d_pool, gf_device_pool_stats* h_stats);
+
+/* The same dense chain as gf_run_dense_chain (same records, keys, ports and results) run entirely on
+ * the device: one stream, the host enqueues every launch up front and synchronises once. Each node
+ * is one fused partition launch over its whole input, with its output chunks reserved from a
+ * device-resident pool (outputChunkBound per node, the unused ones returned and the node's input
+ * chunks released after it): C = 8192, tiles of 4096, pool S = max(ceil(n / C), bound) + bound
+ * chunks. h_port_of[n], h_node_totals[nodes * bins] (node i's per-port counts), h_pool (the pool's
+ * counters at the end: every chunk free again) and h_stats are optional; h_stats->loop_seconds is
+ * the device time from the first launch to the last. Errors as gf_run_dense_chain. */
+gf_status gf_run_dense_chain_device(uint64_t seed, uint64_t n, uint32_t bins, uint32_t nodes, int dist,
+                                    double zipf_s, uint32_t* h_port_of, uint32_t* h_node_totals,
+                                    gf_device_pool_stats* h_pool, gf_flow_stats* h_stats);
+
 /* examples/particle_feedback/ParticleFeedback.hpp:41-108 runParticleFeedback: the
  * Generate -> Filter -> {A, B} -> sink feedback graph with the example's functors, on the GPU.
  * h_weights[n] receives each particle's final weight (0xDEADBEEF if it never reached a sink),

@@ -88,3 +88,21 @@ def test_tuning_knobs():
             assert L.gf_set_tuning(b"sink_batch_chunks", good) == capi.GF_OK
     finally:
         assert L.gf_set_tuning(b"sink_batch_chunks", 256) == capi.GF_OK
+
+
+def test_device_pool_host_checks():
+    """Device-resident pool: size formula (64-byte header, an id and a ledger word per chunk) and
+    argument errors reported before any launch."""
+    L = capi.lib()
+    assert capi.device_pool_bytes(0) == 64 and capi.device_pool_bytes(1000) == 64 + 8 * 1000
+    assert L.gf_device_pool_bytes(4, None) == capi.GF_ERR_ARGUMENT
+    assert L.gf_device_pool_init(None, None, 4) == capi.GF_ERR_ARGUMENT
+    assert L.gf_device_pool_init(None, 8, 4) == capi.GF_ERR_ARGUMENT          # not 16-byte aligned
+    assert L.gf_device_pool_acquire(None, None, 1, None, None) == capi.GF_ERR_ARGUMENT
+    assert L.gf_device_pool_acquire(None, 16, 1, None, None) == capi.GF_ERR_ARGUMENT  # k ids, no output
+    assert L.gf_device_pool_settle(None, 16, None, 2, None, 0, None, 1, None, 0, None) == capi.GF_ERR_ARGUMENT
+    assert L.gf_device_pool_settle(None, 16, None, 0, None, 0, None, 0, None, 0, None) == capi.GF_ERR_ARGUMENT
+    assert L.gf_device_pool_settle(None, 16, None, 0, None, 0, None, 1, None, 3, None) == capi.GF_ERR_ARGUMENT
+    assert L.gf_device_pool_read(None, None, None) == capi.GF_ERR_ARGUMENT
+    assert L.gf_run_dense_chain_device(1, 10, 5, 1, 0, 1.1, None, None, None, None) == capi.GF_ERR_ARGUMENT
+    assert L.gf_run_dense_chain_device(1, 10, 8, 5, 0, 1.1, None, None, None, None) == capi.GF_ERR_ARGUMENT
