@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -272,10 +273,11 @@ def reference_arm(args):
 
 
 def workload_config(args):
-    return {"workload": f"dense classify+plan+scatter, N={args.n} u32 keys, B={args.bins}, {args.dist} keys, "
-                        f"C={CAPACITY}, one whole-array batch",
+    return {"workload": f"dense classify+plan+scatter, N={args.n:.0e} u32 keys, B={args.bins}, {args.dist}, "
+                        f"C={CAPACITY}, one batch",
             "n": args.n, "bins": args.bins, "dist": args.dist, "capacity": CAPACITY, "tile": args.tile,
-            "l2": "inputs and outputs (400 MB each) exceed the 126 MB L2: no flush"}
+            "l2": (f"input and output {args.n * 4 / 1e6:.0f} MB each, "
+                   + ("above the 126 MB L2: no flush" if args.n * 4 > 126e6 else "within L2"))}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -530,7 +532,7 @@ def gpu_arm(args):
         sample_n = min(args.n, 20_000_000)
         v, t = cpu_pool_pass(sample_n, args.bins, args.dist, threads=threads)
         cpu = {"value": v, "unit": "particles/s", "cores": threads, "kind": "port",
-               "sample": f"{sample_n} keys, same B/dist/C, T=128 tiles, median of 3 pool passes ({t:.3f} s)"}
+               "sample": f"{sample_n:.0e} keys, same B/dist/C, median of 3 pool passes ({t:.3f} s)"}
     extra = None
     if rank == 0 and world == 1 and not args.no_extra:
         extra = other_configs(peak)
@@ -545,7 +547,7 @@ def gpu_arm(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": (MEASURED_TRAFFIC_PER_KEY[(args.bins, args.dist)] * args.n
                                  if (args.bins, args.dist) in MEASURED_TRAFFIC_PER_KEY and args.tile <= 4096 else None),
-                     "traffic_source": "ncu, 5e7-key launch, scaled", "peak_source": peak_kind,
+                     "traffic_source": "ncu, 5e7 keys, scaled", "peak_source": peak_kind,
                      "kernel": "fused_partition_coop_kernel", "kernel_ms": kernel_ms,
                      "algorithmic_bytes": f"{BYTES_PER_PARTICLE} B/particle"},
         "cpu_baseline": cpu,
@@ -559,7 +561,7 @@ def gpu_arm(args):
                   "form": "classify, host plan, scatter"},
         # every output slot of the timed batch (and of every sweep case) against the stable partition
         "correct": bool(correct and plain_correct and all(e["correct"] for e in sweep)),
-        "correct_check": "every output slot vs a stable partition on the device",
+        "correct_check": "all slots vs a stable partition",
     }
     if sweep:
         fr = [e["hbm_frac"] for e in sweep]
@@ -570,7 +572,25 @@ def gpu_arm(args):
         # the full record of the other configurations first, on its own line; the result line last
         print("# configs " + json.dumps({"sweep": sweep, "configs": extra}), flush=True)
         line["serving"] = extra.get("serving", {}).get("summary")
-    print(json.dumps(line), flush=True)
+        chain = extra.get("dense_flow", {}).get("nodes4_device_chain")
+        if chain:
+            line["dense_chain_4nodes_1e8_on_device"] = {"particles_per_s": chain["particles_per_s"],
+                                                        "all_chunks_free": chain["all_chunks_free"]}
+    print(json.dumps(_compact(line), separators=(",", ":")), flush=True)
+
+
+def _compact(obj, keep=("value", "ms_per_step")):
+    """The result line with every float but the headline figures rounded to 4 significant digits,
+    so that the whole line stays short."""
+    def walk(x, top):
+        if isinstance(x, dict):
+            return {k: (v if top and k in keep else walk(v, False)) for k, v in x.items()}
+        if isinstance(x, list):
+            return [walk(v, False) for v in x]
+        if isinstance(x, float) and x != 0.0 and math.isfinite(x):
+            return float(f"{x:.4g}")
+        return x
+    return walk(obj, True)
 
 
 # ------------------------------------------------------------------------------------------------
@@ -829,23 +849,23 @@ def _cfg_serving():
                                                               np.array_equal(p1["digest"], pp["digest"]))}
     a, b, c = (out["stream256_n1e3_1e5"][k] for k in ("served_batched32", "served_one_at_a_time", "plain"))
     d, e = (out["stream4096_n1e3_1e7"][k] for k in ("served_batched32", "served_one_at_a_time"))
-    out["summary"] = {
-        "fields": "[flows/s, p50 ms, p99 ms]",
-        "s256": {"batched32": short(a), "one_at_a_time": short(b), "plain": short(c),
-                 "identical": out["stream256_n1e3_1e5"]["results_identical"],
-                 "batched_over_plain": round(a["flows_per_s"] / c["flows_per_s"], 1),
-                 "batching_over_one_at_a_time": round(a["flows_per_s"] / b["flows_per_s"], 2)},
-        "s4096": {"batched32": short(d), "one_at_a_time": short(e),
-                  "identical": out["stream4096_n1e3_1e7"]["results_identical"],
-                  "batching_over_one_at_a_time": round(d["flows_per_s"] / e["flows_per_s"], 2)}}
     g, h = out["stream4096_all_at_once_batched32"], out["stream4096_all_at_once_one_at_a_time"]
     i, j, k2 = (out["stream256_all_at_once"][k] for k in ("served_batched32", "served_one_at_a_time", "plain"))
-    out["summary"]["saturated"] = {
-        "s256": {"batched32": short(i), "one_at_a_time": short(j), "plain": short(k2),
-                 "batched_over_plain": round(i["flows_per_s"] / k2["flows_per_s"], 1),
-                 "batching_over_one_at_a_time": round(i["flows_per_s"] / j["flows_per_s"], 2)},
-        "s4096": {"batched32": short(g), "one_at_a_time": short(h),
-                  "batching_over_one_at_a_time": round(g["flows_per_s"] / h["flows_per_s"], 2)}}
+    # short keys: b32 = served with up to 32 requests in flight, one = served one request at a time,
+    # plain = the Flow one request at a time; x_plain = b32 / plain, x_one = b32 / one (flows/s)
+    out["summary"] = {
+        "cols": "flows/s,p50 ms,p99 ms",
+        "s256": {"b32": short(a), "one": short(b), "plain": short(c),
+                 "x_plain": round(a["flows_per_s"] / c["flows_per_s"], 1),
+                 "x_one": round(a["flows_per_s"] / b["flows_per_s"], 2)},
+        "s4096": {"x_one": round(d["flows_per_s"] / e["flows_per_s"], 2)},
+        "sat256": {"b32": short(i), "one": short(j), "plain": short(k2),
+                   "x_plain": round(i["flows_per_s"] / k2["flows_per_s"], 1),
+                   "x_one": round(i["flows_per_s"] / j["flows_per_s"], 2)},
+        "sat4096": {"x_one": round(g["flows_per_s"] / h["flows_per_s"], 2)},
+        "identical": bool(out["stream256_n1e3_1e5"]["results_identical"] and
+                          out["stream4096_n1e3_1e7"]["results_identical"] and
+                          out["stream256_all_at_once"]["results_identical"])}
     return out
 
 
