@@ -30,6 +30,9 @@ int g_sink_batch = 256;
 // partition group (one multi-batch launch drains every member's ready batches); 0 = one runner node
 // per partition node.
 int g_group_partitions = 1;
+// Tuning knob: 1 = the flow entry points run their Flow device-resident (Tuning::deviceResident:
+// waves of whole-list batches on one stream with a device chunk pool); 0 = the host runner (default).
+int g_device_resident = 0;
 
 constexpr int kThreads = 256;
 constexpr uint32_t kMaxDenseBins = 65535u;
@@ -130,6 +133,10 @@ gf_status gf_set_tuning(const char* name, int value)
     }
     if (std::string(name) == "group_partitions") {
         g_group_partitions = value != 0;
+        return GF_OK;
+    }
+    if (std::string(name) == "device_resident") {
+        g_device_resident = value != 0;
         return GF_OK;
     }
     if (std::string(name) == "hash_persistent") {
@@ -486,5 +493,6 @@ bool gf_runner_batched() { return gf::g_runner_batched != 0; }
 uint32_t gf_runner_sink_batch() { return (uint32_t)gf::g_sink_batch; }
 // Read by the flow entry points (gf_dense_flow.cu, gf_flows.cu).
 bool gf_group_partitions() { return gf::g_group_partitions != 0; }
+bool gf_device_resident() { return gf::g_device_resident != 0; }
 // Read by the hash entry points (gf_capi_hash.cu).
 bool gf_hash_persistent() { return gf::g_hash_persistent != 0; }

@@ -97,6 +97,10 @@ struct Tuning {
     // batches of at most Q chunks per member) in one multi-batch kernel.
     bool groupPartitions = false;
     std::uint32_t groupChunks = 1024u;
+    // B200: the whole run on the device (device_flow.cuh): waves of every node's whole input as
+    // one batch on one stream, chunks from a device-resident pool, one host read per wave. P, Q and
+    // the runner options do not apply; partitions run the dense fused kernel.
+    bool deviceResident = false;
     static constexpr std::uint32_t kMaxSinkBatchChunks = 256u;
 
     void validate() const

@@ -1,0 +1,358 @@
+// Device-resident execution of a Flow (Tuning::deviceResident): the same graph, functors, keyed
+// RNG streams and per-particle results as the host runner (runner.hpp), with the chunk pool on the
+// device (gf_device_pool.cuh) and no host decision inside a wave.
+//
+// The run advances in waves. Every node owns an input list of chunks (id and fill) in device
+// memory, in two sets: at a wave's start the host reads one small block (each list's chunk and
+// particle counts, the status word) and then, for every node whose list holds chunks, enqueues the
+// node's whole input as one batch on one stream; outputs are appended to the other set, which the
+// next wave consumes. The reference's runner (sched/GraphRunner.hpp:762-1171) instead dispatches
+// batches of at most Q chunks and decides per batch on the host; both reach every particle with the
+// same functor calls, since every draw is keyed by the particle (rng/ParticleRng.hpp:57-94).
+//   source     wave 0: reserves ceil(n / C) chunks, generates ids 0..n-1 into them;
+//   partition  tiles of 1024 particles from the list; outputChunkBound(particles, C, B) chunks
+//              reserved from the device pool (the credit of GraphRunner.hpp:1014-1037); one fused
+//              classify -> scan -> scatter launch (gf_partition.cuh) that also publishes the
+//              output descriptors; a route kernel appends every output chunk to the list of the
+//              node its port feeds; the settle kernel returns the unused reservations and releases
+//              the input chunks;
+//   transform  the functor applied in place (the reference's TransformKernel copies into a dense
+//              concatenation, Execution.hpp:694-776; the particles and their order inside a chunk
+//              are the same), the chunks forwarded to the next node;
+//   sink       the functor over every particle, then the chunks are released.
+// Pool: 2 (ceil(n / C) + sum of port counts + 2) + max ports + 16 chunks cover the chunks that hold
+// particles at a wave boundary (full chunks and at most one partial chunk per port and producer)
+// plus one batch's reservation. Exhaustion fails the run with GF_OVERFLOW (no waiting).
+#pragma once
+
+#include <algorithm>
+#include <chrono>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "gf_device_pool.cuh"
+#include "kernels.cuh"
+
+namespace graphflow {
+namespace devflow {
+
+inline constexpr std::uint32_t kNoList = 0xFFFFFFFFu;
+inline constexpr std::uint32_t kTile = 1024u;
+
+// Chunk lists: set s, list j at (s * N + j) * cap.
+struct Lists {
+    std::uint32_t* ids = nullptr;
+    std::uint32_t* fills = nullptr;
+    std::uint32_t* counts = nullptr;           // [2][N] chunks
+    unsigned long long* particles = nullptr;   // [2][N]
+    std::uint32_t N = 0u, cap = 0u;
+    __host__ __device__ std::size_t at(std::uint32_t set, std::uint32_t j) const
+    {
+        return (static_cast<std::size_t>(set) * N + j) * cap;
+    }
+};
+
+__device__ inline void appendChunk(const Lists& L, std::uint32_t set, std::uint32_t j, std::uint32_t id,
+                                   std::uint32_t fill, std::uint32_t* status)
+{
+    if (j >= L.N) {
+        gf::set_status(status, GF_INVALID);
+        return;
+    }
+    const std::uint32_t pos = atomicAdd(&L.counts[set * L.N + j], 1u);
+    if (pos >= L.cap) {
+        gf::set_status(status, GF_OVERFLOW);
+        return;
+    }
+    L.ids[L.at(set, j) + pos] = id;
+    L.fills[L.at(set, j) + pos] = fill;
+    atomicAdd(&L.particles[set * L.N + j], static_cast<unsigned long long>(fill));
+}
+
+// Source: particle i (id i) at slot i mod C of chunk chunk_of[i / C].
+template <typename TFunctor, typename TView>
+__global__ void __launch_bounds__(256)
+    wave_source_kernel(TFunctor f, TView view, std::uint64_t seed_mixed, std::uint32_t purpose, std::uint64_t n,
+                       const std::uint32_t* chunk_of, std::uint32_t num_chunks, std::uint32_t C, std::uint32_t* status)
+{
+    const std::uint64_t stride = static_cast<std::uint64_t>(gridDim.x) * blockDim.x;
+    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const std::uint32_t chunk = chunk_of[i / C];
+        if (chunk >= num_chunks)
+            continue; // a failed reservation: the status word already says so
+        rng::Engine engine = rng::makeEngine(seed_mixed, i, 0u, purpose);
+        Status st(status);
+        auto payload = invokeWithContext(f, engine, st, i);
+        view.store(static_cast<std::uint64_t>(chunk) * C + i % C, static_cast<typename TView::Payload>(payload));
+    }
+}
+
+namespace { // internal linkage: every translation unit that runs a Flow has its own kernels
+
+// The source's chunks (fills C, the last one the rest of n) into list `dst` of `set`.
+__global__ void wave_source_list_kernel(const std::uint32_t* chunk_of, std::uint32_t k, std::uint64_t n,
+                                        std::uint32_t C, Lists L, std::uint32_t set, std::uint32_t dst,
+                                        std::uint32_t* status)
+{
+    for (std::uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < k; f += gridDim.x * blockDim.x) {
+        const std::uint64_t left = n - static_cast<std::uint64_t>(f) * C;
+        appendChunk(L, set, dst, chunk_of[f], static_cast<std::uint32_t>(left < C ? left : C), status);
+    }
+}
+
+// A partition's published output chunks to the lists their ports feed (route[bin]).
+__global__ void wave_route_kernel(const gf_out_desc* descs, const std::uint32_t* num_out, std::uint32_t cap_out,
+                                  const std::uint32_t* route, std::uint32_t bins, Lists L, std::uint32_t set,
+                                  std::uint32_t* status)
+{
+    const std::uint32_t m = *num_out < cap_out ? *num_out : cap_out;
+    for (std::uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < m; f += gridDim.x * blockDim.x) {
+        const gf_out_desc d = descs[f];
+        if (d.bin >= bins || d.fill == 0u) {
+            if (d.bin >= bins)
+                gf::set_status(status, GF_INVALID);
+            continue;
+        }
+        appendChunk(L, set, route[d.bin], d.chunk_index, d.fill, status);
+    }
+}
+
+// A whole list (set `from_set`, list `from`, k entries) appended to list `to` of `to_set`.
+__global__ void wave_forward_kernel(Lists L, std::uint32_t from_set, std::uint32_t from, std::uint32_t k,
+                                    std::uint32_t to_set, std::uint32_t to, std::uint32_t* status)
+{
+    const std::size_t base = L.at(from_set, from);
+    for (std::uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < k; f += gridDim.x * blockDim.x)
+        appendChunk(L, to_set, to, L.ids[base + f], L.fills[base + f], status);
+}
+
+// tp tiles per list entry: entry f's tile j covers [j T, min(fill, (j + 1) T)) (empty past the fill).
+__global__ void wave_tiles_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
+                                  std::uint32_t T, std::uint32_t tp, gf_tile* tiles)
+{
+    const std::uint32_t total = k * tp;
+    for (std::uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const std::uint32_t f = t / tp, j = t - f * tp, off = j * T, fill = fills[f];
+        tiles[t] = gf_tile{ids[f], off, fill > off ? (fill - off < T ? fill - off : T) : 0u};
+    }
+}
+
+// The same tiles as MoveTile with out_pos = f C + offset: with out_chunks = ids, the transform
+// kernel writes every particle back to its own slot.
+__global__ void wave_move_tiles_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
+                                       std::uint32_t C, std::uint32_t T, std::uint32_t tp, MoveTile* tiles)
+{
+    const std::uint32_t total = k * tp;
+    for (std::uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const std::uint32_t f = t / tp, j = t - f * tp, off = j * T, fill = fills[f];
+        tiles[t] = MoveTile{ids[f], off, fill > off ? (fill - off < T ? fill - off : T) : 0u, f * C + off};
+    }
+}
+
+} // namespace
+
+inline unsigned gridFor(std::uint64_t items, unsigned threads = 256u, unsigned cap = 4096u)
+{
+    const std::uint64_t g = (items + threads - 1u) / threads;
+    return static_cast<unsigned>(std::max<std::uint64_t>(1u, std::min<std::uint64_t>(g, cap)));
+}
+
+// Buffers shared by every node of a run (one stream: a node's batch uses them and is done before
+// the next node's batch starts).
+struct WaveContext {
+    cudaStream_t s = nullptr;
+    gf::DevicePoolHdr* pool = nullptr;
+    Lists L;
+    std::uint32_t* status = nullptr;
+    std::uint32_t C = 0u, T = kTile, tp = 1u;
+    std::uint32_t numChunks = 0u;
+    std::uint64_t slots = 0u;
+    std::uint64_t seedMixed = 0u;
+    gf_tile* tiles = nullptr;
+    MoveTile* moveTiles = nullptr;
+    std::uint32_t* reserved = nullptr;
+    std::uint32_t* totals = nullptr;
+    unsigned long long* portChunks = nullptr;
+    std::uint32_t maxK = 0u;
+    gf::FusedCtl* ctl = nullptr;
+    std::uint32_t* table = nullptr;
+    gf_out_desc* descs = nullptr;
+    std::uint32_t descCap = 0u;
+    std::uint32_t* numOut = nullptr;
+    std::uint64_t launches = 0u, partitionBatches = 0u, batches = 0u, sunk = 0u;
+};
+
+// One node's wave step. `routes` are the list indices its ports feed (device copy in routesDev).
+class WaveNode {
+public:
+    virtual ~WaveNode() = default;
+    // source only: generate n particles into reserved chunks, append them to list `to` of `set`
+    virtual void generate(WaveContext&, std::uint64_t, std::uint32_t, std::uint32_t)
+    {
+        throw std::logic_error("graphflow: only a source generates");
+    }
+    // the node's whole input (k chunks, `particles` particles, list `self` of set `cur`) as one batch
+    virtual void run(WaveContext& w, std::uint32_t self, std::uint32_t k, std::uint64_t particles,
+                     std::uint32_t cur, std::uint32_t next, const std::vector<std::uint32_t>& routes,
+                     const std::uint32_t* routesDev) = 0;
+    virtual std::uint32_t bins() const { return 1u; }
+    virtual void bind(std::uint32_t) {}
+};
+
+template <typename TStorage, typename TFunctor>
+class SourceWave final : public WaveNode {
+public:
+    SourceWave(TStorage& st, TFunctor f, std::uint32_t purpose) : m_st(st), m_f(std::move(f)), m_purpose(purpose) {}
+    void generate(WaveContext& w, std::uint64_t n, std::uint32_t set, std::uint32_t to) override
+    {
+        const std::uint32_t k = static_cast<std::uint32_t>((n + w.C - 1u) / w.C);
+        // the reservation lands in this run's source list, which no route targets
+        std::uint32_t* ids = w.L.ids + w.L.at(0u, m_self);
+        gf::pool_acquire_kernel<<<1, gf::kPoolThreads, 0, w.s>>>(w.pool, k, ids, w.status);
+        wave_source_kernel<<<gridFor(n, 256u, 148u * 16u), 256, 0, w.s>>>(m_f, m_st.view(), w.seedMixed, m_purpose,
+                                                                        n, ids, w.numChunks, w.C, w.status);
+        wave_source_list_kernel<<<gridFor(k), 256, 0, w.s>>>(ids, k, n, w.C, w.L, set, to, w.status);
+        cuda::check(cudaGetLastError(), "device-resident source launch");
+        w.launches += 3u;
+        ++w.batches;
+    }
+    void run(WaveContext&, std::uint32_t, std::uint32_t, std::uint64_t, std::uint32_t, std::uint32_t,
+             const std::vector<std::uint32_t>&, const std::uint32_t*) override
+    {
+        throw std::logic_error("graphflow: a source has no input");
+    }
+    void bind(std::uint32_t self) override { m_self = self; }
+
+private:
+    TStorage& m_st;
+    TFunctor m_f;
+    std::uint32_t m_purpose;
+    std::uint32_t m_self = 0u;
+};
+
+template <typename TStorage, typename TFunctor>
+class TransformWave final : public WaveNode {
+public:
+    TransformWave(TStorage& st, TFunctor f, std::uint32_t purpose) : m_st(st), m_f(std::move(f)), m_purpose(purpose) {}
+    void run(WaveContext& w, std::uint32_t self, std::uint32_t k, std::uint64_t, std::uint32_t cur,
+             std::uint32_t next, const std::vector<std::uint32_t>& routes, const std::uint32_t*) override
+    {
+        const std::uint32_t* ids = w.L.ids + w.L.at(cur, self);
+        const std::uint32_t* fills = w.L.fills + w.L.at(cur, self);
+        const std::uint32_t nt = k * w.tp;
+        wave_move_tiles_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.C, w.T, w.tp, w.moveTiles);
+        transform_kernel<<<nt, 256, 0, w.s>>>(m_f, m_st.view(), w.seedMixed, m_purpose, w.moveTiles, nt, ids, k, w.C,
+                                              gf::FastDiv(w.C), w.slots, w.status);
+        wave_forward_kernel<<<gridFor(k), 256, 0, w.s>>>(w.L, cur, self, k, next, routes[0], w.status);
+        cuda::check(cudaGetLastError(), "device-resident transform launch");
+        w.launches += 3u;
+        ++w.batches;
+    }
+
+private:
+    TStorage& m_st;
+    TFunctor m_f;
+    std::uint32_t m_purpose;
+};
+
+template <typename TStorage, typename TFunctor>
+class SinkWave final : public WaveNode {
+public:
+    SinkWave(TStorage& st, TFunctor f, std::uint32_t purpose) : m_st(st), m_f(std::move(f)), m_purpose(purpose) {}
+    void run(WaveContext& w, std::uint32_t self, std::uint32_t k, std::uint64_t particles, std::uint32_t cur,
+             std::uint32_t, const std::vector<std::uint32_t>&, const std::uint32_t*) override
+    {
+        const std::uint32_t* ids = w.L.ids + w.L.at(cur, self);
+        const std::uint32_t* fills = w.L.fills + w.L.at(cur, self);
+        const std::uint32_t nt = k * w.tp;
+        wave_move_tiles_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.C, w.T, w.tp, w.moveTiles);
+        sink_kernel<<<nt, 256, 0, w.s>>>(m_f, m_st.view(), w.seedMixed, m_purpose, w.moveTiles, nt, w.C, w.slots,
+                                         w.status);
+        gf::pool_settle_kernel<<<1, gf::kPoolThreads, 0, w.s>>>(w.pool, nullptr, 0u, nullptr, 0u, ids, 1u, nullptr, k,
+                                                                w.status);
+        cuda::check(cudaGetLastError(), "device-resident sink launch");
+        w.launches += 3u;
+        w.sunk += particles;
+        ++w.batches;
+    }
+
+private:
+    TStorage& m_st;
+    TFunctor m_f;
+    std::uint32_t m_purpose;
+};
+
+template <typename TStorage, typename TClassifier, typename TUpdate, typename TBin>
+class PartitionWave final : public WaveNode {
+    using View = typename TStorage::View;
+    using P = typename TStorage::Payload;
+    using Acc = ViewAccess<View>;
+    using Cls = ClassifyAdapter<TClassifier, P>;
+    using Upd = UpdateAdapter<TUpdate, TBin, P>;
+    using Shape = gf::TileShape<256, 4, 2>; // 1024-particle tiles, as PartitionStage
+    static_assert(Shape::kTile == kTile, "tile size");
+
+public:
+    PartitionWave(TStorage& st, TClassifier cls, TUpdate upd, std::uint32_t bins, std::uint32_t purpose)
+        : m_st(st), m_cls(std::move(cls)), m_upd(std::move(upd)), m_bins(bins), m_purpose(purpose)
+    {
+        m_smem = smemBytes(bins);
+        int dev = 0, limit = 0;
+        cuda::check(cudaGetDevice(&dev), "cudaGetDevice");
+        cuda::check(cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "smem limit");
+        if (m_smem > static_cast<std::size_t>(limit))
+            throw std::invalid_argument("graphflow: deviceResident runs dense fused partitions only; " +
+                                        std::to_string(bins) + " ports do not fit one block's shared memory");
+        cuda::check(cudaFuncSetAttribute(gf::fused_partition_kernel<Shape, Acc, Cls, Upd>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(m_smem)),
+                    "device-resident partition attribute");
+    }
+    static std::size_t smemBytes(std::uint32_t bins)
+    {
+        return sizeof(P) * Shape::kTile + 4u * Shape::kTile + 4u * Shape::kWarps * bins + 4u * bins * 6u +
+               4u * (2u * Shape::kThreads + Shape::kWarps + 8u);
+    }
+    std::uint32_t bins() const override { return m_bins; }
+    void run(WaveContext& w, std::uint32_t self, std::uint32_t k, std::uint64_t particles, std::uint32_t cur,
+             std::uint32_t next, const std::vector<std::uint32_t>&, const std::uint32_t* routesDev) override
+    {
+        const std::uint32_t* ids = w.L.ids + w.L.at(cur, self);
+        const std::uint32_t* fills = w.L.fills + w.L.at(cur, self);
+        const std::uint32_t nt = k * w.tp;
+        const std::uint64_t b64 = checkedOutputChunkBound(particles, w.C, m_bins);
+        if (b64 > w.descCap)
+            throw BatchError("graphflow: deviceResident batch needs more output chunks than the run reserved");
+        const std::uint32_t bound = static_cast<std::uint32_t>(b64);
+        wave_tiles_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.T, w.tp, w.tiles);
+        gf::pool_acquire_kernel<<<1, gf::kPoolThreads, 0, w.s>>>(w.pool, bound, w.reserved, w.status);
+        cuda::check(cudaMemsetAsync(w.ctl, 0, gf::kFusedCtlResetBytes, w.s), "memset");
+        const Acc acc{m_st.view()};
+        const Cls cls{m_cls, w.seedMixed, m_purpose, w.status};
+        const Upd upd{m_upd, m_purpose + 1u, w.status};
+        auto* desc = reinterpret_cast<unsigned long long*>(w.ctl + 1);
+        // the launch's last CTA builds the table and the output descriptors
+        gf::fused_partition_kernel<Shape, Acc, Cls, Upd><<<nt, Shape::kThreads, m_smem, w.s>>>(
+            acc, cls, upd, w.seedMixed, w.C, gf::FastDiv(w.C), w.slots, w.tiles, nt, m_bins, w.reserved, bound,
+            w.totals, w.portChunks, w.maxK, w.ctl, desc, w.status,
+            gf::InlineFinish{w.table, w.descs, bound, w.numOut});
+        wave_route_kernel<<<gridFor(bound), 256, 0, w.s>>>(w.descs, w.numOut, bound, routesDev, m_bins, w.L, next,
+                                                          w.status);
+        gf::pool_settle_kernel<<<1, gf::kPoolThreads, 0, w.s>>>(w.pool, w.reserved, bound, w.numOut, 0u, ids, 1u,
+                                                                nullptr, k, w.status);
+        cuda::check(cudaGetLastError(), "device-resident partition launch");
+        w.launches += 5u;
+        ++w.partitionBatches;
+        ++w.batches;
+    }
+
+private:
+    TStorage& m_st;
+    TClassifier m_cls;
+    TUpdate m_upd;
+    std::uint32_t m_bins, m_purpose;
+    std::size_t m_smem = 0u;
+};
+
+} // namespace devflow
+} // namespace graphflow

@@ -24,6 +24,7 @@
 #include <string>
 #include <vector>
 
+#include "device_flow.cuh"
 #include "record.hpp"
 #include "runner.hpp"
 #include "stages.cuh"
@@ -152,6 +153,9 @@ public:
                           [f](TStorage& st, const Config& c, std::uint32_t purpose) -> std::unique_ptr<Stage> {
                               return std::make_unique<SourceStage<TStorage, F>>(st, c, f, purpose);
                           });
+        m_nodes[key].makeWave = [f](TStorage& st, std::uint32_t purpose) -> std::unique_ptr<devflow::WaveNode> {
+            return std::make_unique<devflow::SourceWave<TStorage, F>>(st, f, purpose);
+        };
         m_sourceKey = key;
         return NodeHandle(m_identity, key, 1u, m_nodes[key].name);
     }
@@ -169,6 +173,10 @@ public:
                                   st, c, cls, upd, static_cast<std::uint32_t>(TClassifier::maxBins), purpose);
                           });
         m_nodes[key].partition = true;
+        m_nodes[key].makeWave = [cls, upd](TStorage& st, std::uint32_t purpose) -> std::unique_ptr<devflow::WaveNode> {
+            return std::make_unique<devflow::PartitionWave<TStorage, TClassifier, TUpdate, TBin>>(
+                st, cls, upd, static_cast<std::uint32_t>(TClassifier::maxBins), purpose);
+        };
         m_nodes[key].groupKey = &detail::PartitionGroupKey<TClassifier, TUpdate>::id;
         m_nodes[key].makeGroup = [](TStorage& st, const Config& c, std::uint32_t b) -> std::unique_ptr<Stage> {
             using G = PartitionGroupStage<TStorage, TClassifier, TUpdate, TBin>;
@@ -190,6 +198,9 @@ public:
                           [f](TStorage& st, const Config& c, std::uint32_t purpose) -> std::unique_ptr<Stage> {
                               return std::make_unique<TransformStage<TStorage, F>>(st, c, f, purpose);
                           });
+        m_nodes[key].makeWave = [f](TStorage& st, std::uint32_t purpose) -> std::unique_ptr<devflow::WaveNode> {
+            return std::make_unique<devflow::TransformWave<TStorage, F>>(st, f, purpose);
+        };
         return NodeHandle(m_identity, key, 1u, m_nodes[key].name);
     }
 
@@ -210,6 +221,9 @@ public:
                           [f](TStorage& st, const Config& c, std::uint32_t purpose) -> std::unique_ptr<Stage> {
                               return std::make_unique<SinkStage<TStorage, F>>(st, c, f, purpose);
                           });
+        m_nodes[key].makeWave = [f](TStorage& st, std::uint32_t purpose) -> std::unique_ptr<devflow::WaveNode> {
+            return std::make_unique<devflow::SinkWave<TStorage, F>>(st, f, purpose);
+        };
         return NodeHandle(m_identity, key, 0u, m_nodes[key].name);
     }
 
@@ -237,6 +251,8 @@ public:
         validateForRun(source);
         if (itemCount != 0u && itemCount - 1u > rng::maxStreamId)
             throw std::overflow_error("graphflow: item count exceeds the 32 bit RNG stream-id range");
+        if (m_tuning.deviceResident)
+            return runDeviceResident(itemCount);
         const auto t0 = std::chrono::steady_clock::now();
         const Config config = resolveConfig(itemCount);
         m_device.makeCurrent();
@@ -331,6 +347,168 @@ public:
     Config resolvedConfig(std::uint64_t itemCount) const { return resolveConfig(itemCount); }
 
 private:
+    // Tuning::deviceResident (device_flow.cuh): waves of whole-list batches on one stream, chunks
+    // from a device-resident pool, one read of the list counters per wave.
+    Stats runDeviceResident(std::uint64_t itemCount)
+    {
+        using namespace devflow;
+        const auto t0 = std::chrono::steady_clock::now();
+        const Config config = resolveConfig(itemCount);
+        if (config.effectiveBinPath() == BinPath::hash || config.scatterMode == ScatterMode::Direct)
+            throw std::invalid_argument("graphflow: deviceResident runs the fused dense partition; the hash bin path "
+                                        "and the direct scatter need the host runner");
+        m_device.makeCurrent();
+        const std::uint32_t C = config.chunkCapacity;
+        const auto N = static_cast<std::uint32_t>(m_nodes.size());
+        std::uint64_t sumBins = 0u;
+        std::uint32_t maxBins = 1u;
+        for (const auto& n : m_nodes)
+            if (n.partition) {
+                sumBins += n.bins;
+                maxBins = std::max(maxBins, n.bins);
+            }
+        const std::uint64_t nIn = (itemCount + C - 1u) / C;
+        const std::uint64_t S64 = 2u * (nIn + sumBins + 2u) + maxBins + 16u;
+        if (S64 * C > 0xFFFFFFFFull)
+            throw std::overflow_error("graphflow: the device-resident pool would exceed 2^32 slots");
+        const auto S = static_cast<std::uint32_t>(S64);
+        const std::uint32_t tp = (C + kTile - 1u) / kTile;
+        TStorage storage(m_device, S, C);
+        std::vector<std::unique_ptr<WaveNode>> waves;
+        for (std::uint32_t k = 0; k < N; ++k) {
+            waves.push_back(m_nodes[k].makeWave(storage, rng::streamPurposeForNode(k)));
+            waves.back()->bind(k);
+        }
+        // routes: port b of node k feeds node routes[k][b]; one device copy of all of them
+        std::vector<std::vector<std::uint32_t>> routes(N);
+        std::vector<std::uint32_t> routeOffset(N, 0u), flat;
+        for (std::uint32_t k = 0; k < N; ++k) {
+            routeOffset[k] = static_cast<std::uint32_t>(flat.size());
+            for (auto r : m_nodes[k].routes)
+                routes[k].push_back(static_cast<std::uint32_t>(r));
+            flat.insert(flat.end(), routes[k].begin(), routes[k].end());
+        }
+        cuda::Buffer<std::uint32_t> routesDev(std::max<std::size_t>(flat.size(), 1u));
+        if (!flat.empty())
+            cuda::check(cudaMemcpy(routesDev.data(), flat.data(), flat.size() * 4u, cudaMemcpyHostToDevice), "H2D");
+        // device buffers of the run
+        const std::size_t listWords = 2u * static_cast<std::size_t>(N) * S;
+        cuda::Buffer<std::uint32_t> ids(listWords), fills(listWords);
+        // meta: particles [2N] (u64) | counts [2N] | status, read by the host once per wave
+        const std::size_t metaWords = 4u * N + 2u * N + 2u;
+        cuda::Buffer<std::uint32_t> meta(metaWords);
+        cuda::HostBuffer<std::uint32_t> metaHost(metaWords);
+        cuda::Buffer<unsigned char> pool(gf::device_pool_bytes(S));
+        const std::size_t tiles = static_cast<std::size_t>(S) * tp;
+        cuda::Buffer<gf_tile> tileBuf(tiles);
+        cuda::Buffer<MoveTile> moveBuf(tiles);
+        const std::uint32_t descCap = S + maxBins;
+        cuda::Buffer<std::uint32_t> reserved(descCap), table(maxBins + descCap), totals(maxBins), numOut(1);
+        cuda::Buffer<gf_out_desc> descs(descCap);
+        cuda::Buffer<unsigned long long> portChunks(static_cast<std::size_t>(maxBins) * S);
+        const std::size_t scratchBytes = 64u + tiles * maxBins * 8u;
+        cuda::Buffer<unsigned char> scratch(scratchBytes);
+        cudaStream_t s = nullptr;
+        cuda::check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard()
+            {
+                cudaStreamSynchronize(s);
+                cudaStreamDestroy(s);
+            }
+        } guard{s};
+        cuda::check(cudaMemsetAsync(meta.data(), 0, metaWords * 4u, s), "memset");
+        cuda::check(cudaMemsetAsync(portChunks.data(), 0, portChunks.size() * 8u, s), "memset");
+        cuda::check(cudaMemsetAsync(scratch.data(), 0, scratchBytes, s), "memset");
+        auto* poolHdr = reinterpret_cast<gf::DevicePoolHdr*>(pool.data());
+        gf::pool_init_kernel<<<gridFor(S, gf::kPoolThreads, 148u), gf::kPoolThreads, 0, s>>>(poolHdr, S);
+        WaveContext w;
+        w.s = s;
+        w.pool = poolHdr;
+        w.L.ids = ids.data();
+        w.L.fills = fills.data();
+        w.L.particles = reinterpret_cast<unsigned long long*>(meta.data());
+        w.L.counts = meta.data() + 4u * N;
+        w.L.N = N;
+        w.L.cap = S;
+        w.status = meta.data() + 6u * N;
+        w.C = C;
+        w.tp = tp;
+        w.numChunks = S;
+        w.slots = storage.slotCount();
+        w.seedMixed = gf::mix64(config.seed);
+        w.tiles = tileBuf.data();
+        w.moveTiles = moveBuf.data();
+        w.reserved = reserved.data();
+        w.totals = totals.data();
+        w.portChunks = portChunks.data();
+        w.maxK = S;
+        w.ctl = reinterpret_cast<gf::FusedCtl*>(scratch.data());
+        w.table = table.data();
+        w.descs = descs.data();
+        w.descCap = descCap;
+        w.numOut = numOut.data();
+        w.launches = 1u;
+        std::uint32_t next = 1u;
+        if (itemCount != 0u)
+            waves[*m_sourceKey]->generate(w, itemCount, next, routes[*m_sourceKey][0]);
+        const auto t1 = std::chrono::steady_clock::now();
+        constexpr std::uint64_t kMaxWaves = 1u << 20;
+        std::uint64_t wavesRun = 0u;
+        for (;;) {
+            cuda::check(cudaMemcpyAsync(metaHost.data(), meta.data(), metaWords * 4u, cudaMemcpyDeviceToHost, s), "D2H");
+            cuda::check(cudaStreamSynchronize(s), "device-resident wave");
+            const std::uint32_t st = metaHost.data()[6u * N];
+            if (st != 0u)
+                throw BatchError("graphflow: device-resident run failed: " +
+                                 std::string(st == GF_OVERFLOW ? "overflow" : statusCodeName(decodeStatus(st))) +
+                                 " (code " + std::to_string(st) + ")");
+            const std::uint32_t* counts = metaHost.data() + 4u * N;
+            const auto* parts = reinterpret_cast<const unsigned long long*>(metaHost.data());
+            bool any = false;
+            for (std::uint32_t k = 0; k < N; ++k)
+                any = any || counts[next * N + k] != 0u;
+            if (!any)
+                break;
+            if (++wavesRun > kMaxWaves ||
+                (m_tuning.stallTimeout && std::chrono::steady_clock::now() - t1 > *m_tuning.stallTimeout))
+                throw SchedulerStallError("graphflow: device-resident run still has particles in flight after " +
+                                          std::to_string(wavesRun - 1u) + " waves");
+            const std::uint32_t cur = next;
+            next = 1u - cur;
+            cuda::check(cudaMemsetAsync(w.L.counts + next * N, 0, N * 4u, s), "memset");
+            cuda::check(cudaMemsetAsync(w.L.particles + next * N, 0, N * 8u, s), "memset");
+            for (std::uint32_t k = 0; k < N; ++k)
+                if (counts[cur * N + k] != 0u)
+                    waves[k]->run(w, k, counts[cur * N + k], parts[cur * N + k], cur, next, routes[k],
+                                  routesDev.data() + routeOffset[k]);
+        }
+        gf::DevicePoolHdr hdr{};
+        cuda::check(cudaMemcpyAsync(&hdr, poolHdr, sizeof(hdr), cudaMemcpyDeviceToHost, s), "D2H");
+        cuda::check(cudaStreamSynchronize(s), "device-resident run");
+        if (hdr.status != 0u || hdr.base != 0u)
+            throw BatchError("graphflow: device-resident run ended with " + std::to_string(hdr.base) +
+                             " chunks out of the pool (status " + std::to_string(hdr.status) + ")");
+        Stats stats;
+        stats.completedBatches = w.batches;
+        stats.loopIterations = wavesRun;
+        stats.poolChunks = S;
+        stats.poolSlots = storage.slotCount();
+        stats.poolBytes = stats.poolSlots * TStorage::slotBytes();
+        stats.peakLiveChunks = hdr.peak_live;
+        stats.sourceParticles = itemCount;
+        stats.sourceGenerated = itemCount;
+        stats.sourceSunk = w.sunk;
+        stats.chunkCapacity = C;
+        stats.kernelLaunches = w.launches;
+        stats.partitionBatches = w.partitionBatches;
+        stats.partitionLaunches = w.partitionBatches;
+        stats.setupSeconds = std::chrono::duration<double>(t1 - t0).count();
+        stats.loopSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+        return stats;
+    }
+
     static constexpr std::size_t kInvalid = static_cast<std::size_t>(-1);
     using Factory = std::function<std::unique_ptr<Stage>(TStorage&, const Config&, std::uint32_t)>;
 
@@ -344,6 +522,7 @@ private:
         const void* groupKey = nullptr; // partition nodes: classifier/updater type identity
         std::function<std::unique_ptr<Stage>(TStorage&, const Config&, std::uint32_t)> makeGroup;
         std::function<std::uint32_t(Stage&, std::uint32_t)> joinGroup;
+        std::function<std::unique_ptr<devflow::WaveNode>(TStorage&, std::uint32_t)> makeWave;
     };
 
     std::size_t append(std::string name, NodeRole role, std::uint32_t bins, Factory make)
