@@ -659,6 +659,28 @@ def _cfg_particle_feedback():
         "histogram_sha256_matches_published": hashlib.sha256(text.encode()).hexdigest()
         == "21ab0aeb9ec72d380af2ce6e9631f8fa7b9111d24ff7831f272aa9f6a7be9dab",
         "reference_published_particles_per_s": 1.3e7}
+    # the same Flow run device-resident (Tuning::deviceResident): Cfg1 and the published configuration
+    capi.check(capi.lib().gf_set_tuning(b"device_resident", 1), "tuning")
+    try:
+        capi.run_particle_feedback(42, 10_000, chunk_capacity=1024, live_particles=4096, batch_chunks=1)
+        runs = [capi.run_particle_feedback(42, n, chunk_capacity=1024, live_particles=4096, batch_chunks=1)
+                for _ in range(3)]
+        wd8, _, sd8 = capi.run_particle_feedback(42, n8, chunk_capacity=8192, live_particles=16384, batch_chunks=8)
+    finally:
+        capi.check(capi.lib().gf_set_tuning(b"device_resident", 0), "tuning")
+    sd = sorted((r[2] for r in runs), key=lambda x: x.seconds)[1]
+    vd, cd = O.histogram_u32(wd8)
+    text_d = "".join(f"{int(v)},{int(c)}\n" for v, c in zip(vd, cd))
+    out["flow_device_resident"] = {
+        "seconds": sd.seconds, "particles_per_s": n / sd.seconds, "waves": sd.loop_iterations,
+        "kernel_launches": sd.kernel_launches,
+        "identical_to_host_runner": all(bool(np.array_equal(r[0], w) and np.array_equal(r[1], c)) for r in runs)}
+    out["published_config_flow_device_resident"] = {
+        "seconds": sd8.seconds, "particles_per_s": n8 / sd8.seconds, "waves": sd8.loop_iterations,
+        "kernel_launches": sd8.kernel_launches, "peak_live_chunks": sd8.peak_live_chunks,
+        "pool_chunks": sd8.pool_chunks,
+        "histogram_sha256_matches_published": hashlib.sha256(text_d.encode()).hexdigest()
+        == "21ab0aeb9ec72d380af2ce6e9631f8fa7b9111d24ff7831f272aa9f6a7be9dab"}
     return out
 
 
@@ -690,6 +712,15 @@ def _cfg_dense_flow():
     out["nodes4_plain_reference_runner"] = run(4, 200_000, False, False)
     # the same chain run entirely on the device (device-resident chunk pool, one launch per node,
     # no host round trip): device time over three runs, and the wall time of the whole call
+    capi.check(L.gf_set_tuning(b"device_resident", 1), "tuning")
+    try:
+        _, st = capi.run_dense_chain(42, 100_000_000, 64, nodes=4, dist="uniform", chunk_capacity=8192,
+                                     live_particles=16384, batch_chunks=8, want_ports=False)
+    finally:
+        capi.check(L.gf_set_tuning(b"device_resident", 0), "tuning")
+    out["nodes4_flow_device_resident"] = {"n": 100_000_000, "seconds": st.seconds,
+                                          "particles_per_s": 1e8 / st.seconds, "waves": st.loop_iterations,
+                                          "kernel_launches": st.kernel_launches}
     runs = [capi.run_dense_chain_device(42, 100_000_000, 64, nodes=4, want_ports=False) for _ in range(3)]
     dev = sorted(r[3].loop_seconds for r in runs)[1]
     out["nodes4_device_chain"] = {"n": 100_000_000, "device_seconds": dev, "particles_per_s": 1e8 / dev,

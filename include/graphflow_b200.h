@@ -106,6 +106,14 @@ uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap);
  *                port runs with bulk copies (shared -> global) when the scratch also holds one
  *                histogram per tile (gf_fused_scratch_bytes sizes it so); 0 = warp stores.
  *                Results are identical.
+ *   "device_resident" 0 (default) = the flow entry points run their Flow with the host runner;
+ *                1 = device-resident (Tuning::deviceResident): in waves, every node takes its whole
+ *                input as one batch on one stream, output chunks come from a device-resident pool
+ *                and each output chunk is appended on the device to the list of the node its port
+ *                feeds; the host reads one block of list counters per wave. P, Q and the runner
+ *                options do not apply; partitions run the fused dense kernel (the kernel workload's
+ *                plain, direct-scatter and hash-path forms keep the host runner). Results are
+ *                identical.
  *   "runner_batched" 1 (default) = the flow entry points (gf_run_particle_feedback,
  *                gf_run_dense_chain, gf_run_photon) let a sink take up to "sink_batch_chunks"
  *                ready chunks per launch and dispatch every idle node in one scheduler iteration;
