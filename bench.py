@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--hash", type=int, default=0, metavar="K",
                    help="only run the device-planned hash partition of --n records over K keys (Zipf 1.2, "
                         "tiles of 2048) --steps times after --warmup batches and print its timing; for profiling")
+    p.add_argument("--feedback-device-resident", action="store_true",
+                   help="one particle_feedback run through the Flow device-resident at N=--n, C=8192 (profiling)")
     p.add_argument("--flow-chain", type=int, default=0, metavar="NODES",
                    help="only run the dense chain of NODES partition nodes through the Flow on --n keys (--bins, "
                         "--dist, C=8192, P=16384, Q=8, partition groups) and print its counters; for profiling")
@@ -1087,8 +1089,26 @@ def flow_chain_only(args):
                       "kernel_launches": st.kernel_launches, "sunk": st.sunk}))
 
 
+def feedback_device_resident_only(args):
+    """One particle_feedback run through the Flow device-resident (seed 42, C = 8192, 64 visits), for
+    profiling its launches."""
+    from graphflow_b200 import capi
+    capi.check(capi.lib().gf_set_tuning(b"device_resident", 1), "tuning")
+    try:
+        _, _, st = capi.run_particle_feedback(SEED, args.n, 64, chunk_capacity=8192, live_particles=16384,
+                                              batch_chunks=8)
+    finally:
+        capi.check(capi.lib().gf_set_tuning(b"device_resident", 0), "tuning")
+    print(json.dumps({"workload": f"particle_feedback through the Flow device-resident, N={args.n}, C=8192",
+                      "seconds": st.seconds, "waves": st.loop_iterations, "kernel_launches": st.kernel_launches,
+                      "partition_batches": st.partition_batches, "sunk": st.sunk}))
+
+
 def main():
     args = parse()
+    if args.feedback_device_resident:
+        feedback_device_resident_only(args)
+        return
     if args.flow_chain:
         flow_chain_only(args)
         return
