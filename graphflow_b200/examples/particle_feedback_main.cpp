@@ -59,6 +59,7 @@ struct Options {
     std::vector<std::string> kernelOnly; // flags of the kernel workload
     std::string scatter = "shared", binPath = "dense", distribution = "balanced"; // KernelOptions defaults
     std::uint32_t bins = 64u;
+    bool deviceResident = false; // B200 extension: the Flow run device-resident
 };
 
 void usage(std::ostream& out)
@@ -67,7 +68,7 @@ void usage(std::ostream& out)
            "                                        [--particles N] [--chunk-size C]\n"
            "                                        [--live-particles P] [--tile-size T]\n"
            "                                        [--batch-chunks Q] [--seed S] [--max-visits M]\n"
-           "                                        [--workload feedback|kernel]\n"
+           "                                        [--workload feedback|kernel] [--device-resident]\n"
            "       kernel workload only: [--scatter shared|direct] [--bin-path dense|hash]\n"
            "                             [--bins 64|1024|4096|65536]\n"
            "                             [--distribution balanced|one-hot|skewed|sparse]\n"
@@ -113,6 +114,8 @@ Options parse(int argc, char** argv)
             o.maxVisits = parseU32(flag, next());
         } else if (flag == "--device") {
             o.device = parseU32(flag, next(), true);
+        } else if (flag == "--device-resident") {
+            o.deviceResident = true;
         } else if (flag == "--workload") {
             o.workload = next();
             expectOneOf(flag, o.workload, {"feedback", "kernel"});
@@ -227,6 +230,8 @@ int run(const Options& o)
         std::cerr << kName << ": note: " << f << " has no effect in this build\n";
 
     cudaOrThrow(cudaSetDevice(static_cast<int>(o.device)), "cudaSetDevice");
+    if (o.deviceResident && gf_set_tuning("device_resident", 1) != GF_OK)
+        throw std::runtime_error("device_resident: " + lastError());
     const bool wideChunk = !o.chunkSize || *o.chunkSize >= kLogicalTileWidth;
     gf_policy pol{};
     if (gf_device_policy(nullptr, o.particles, o.chunkSize.value_or(0u), o.liveParticles.value_or(0u),

@@ -128,6 +128,17 @@ def test_cli_config1_matches_the_scalar_model():
 
 
 @pytest.mark.gpu
+def test_cli_device_resident_prints_the_same_rows():
+    """--device-resident (a B200 extension) runs the Flow device-resident: the rows equal the host
+    runner's."""
+    args = ["--backend", "cuda", "--particles", "200000", "--chunk-size", "1024", "--live-particles", "4096",
+            "--batch-chunks", "1", "--seed", "42", "--max-visits", "64"]
+    a, b = _run(*args), _run(*args, "--device-resident")
+    assert a.returncode == 0 and b.returncode == 0, b.stderr
+    assert _rows(a.stdout)[3] == _rows(b.stdout)[3] and _rows(a.stdout)[2] == _rows(b.stdout)[2]
+
+
+@pytest.mark.gpu
 def test_cli_inert_flags_are_noted_and_change_nothing():
     base = ["--backend", "cuda", "--particles", "20000", "--chunk-size", "1024", "--live-particles", "4096",
             "--seed", "7"]

@@ -108,3 +108,14 @@ def test_kernel_workload_with_the_hash_path_runs_on_the_host_runner():
     with device_resident():
         dev = capi.run_kernel_axes(3, n, 64, "balanced", bin_path="hash", fused=False)
     assert np.array_equal(host[0], dev[0]) and dev[1].partition_batches == host[1].partition_batches > 1
+
+
+@pytest.mark.parametrize("n,c", [(50_001, 1024), (0, 1024)])
+def test_set_transform_device_resident(n, c):
+    """transform<Set<WeightTag, VisitTag>> on a Record payload, run device-resident (the transform
+    is applied in place)."""
+    with device_resident():
+        weights, visits, st = capi.run_set_transform(7, n, 1234, chunk_capacity=c, live_particles=4 * c,
+                                                     batch_chunks=1)
+    assert st.sunk == n
+    assert np.all(weights == 1234) and np.all(visits == 1)
