@@ -33,6 +33,9 @@ int g_group_partitions = 1;
 // Tuning knob: 1 = the flow entry points run their Flow device-resident (Tuning::deviceResident:
 // waves of whole-list batches on one stream with a device chunk pool); 0 = the host runner (default).
 int g_device_resident = 0;
+// Tuning knob: 1 = device-resident partition batches of at least 64 tiles and up to 64 ports run the
+// cooperative kernel of gf_fused_any.cuh (default); 0 = always the per-tile look-back kernel.
+int g_device_coop = 1;
 
 constexpr int kThreads = 256;
 constexpr uint32_t kMaxDenseBins = 65535u;
@@ -137,6 +140,10 @@ gf_status gf_set_tuning(const char* name, int value)
     }
     if (std::string(name) == "device_resident") {
         g_device_resident = value != 0;
+        return GF_OK;
+    }
+    if (std::string(name) == "device_coop") {
+        g_device_coop = value != 0;
         return GF_OK;
     }
     if (std::string(name) == "hash_persistent") {
@@ -494,5 +501,6 @@ uint32_t gf_runner_sink_batch() { return (uint32_t)gf::g_sink_batch; }
 // Read by the flow entry points (gf_dense_flow.cu, gf_flows.cu).
 bool gf_group_partitions() { return gf::g_group_partitions != 0; }
 bool gf_device_resident() { return gf::g_device_resident != 0; }
+bool gf_device_coop() { return gf::g_device_coop != 0; }
 // Read by the hash entry points (gf_capi_hash.cu).
 bool gf_hash_persistent() { return gf::g_hash_persistent != 0; }

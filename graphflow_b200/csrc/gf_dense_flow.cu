@@ -11,6 +11,7 @@ bool gf_runner_batched();                                       // gf_capi.cu
 uint32_t gf_runner_sink_batch();
 bool gf_group_partitions();                                // gf_capi.cu
 bool gf_device_resident();                                 // gf_capi.cu
+bool gf_device_coop();     // gf_capi.cu
 
 namespace {
 
@@ -71,6 +72,7 @@ extern "C" gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins
             t.groupPartitions = gf_group_partitions();
         }
         t.deviceResident = gf_device_resident();
+        t.deviceCoop = gf_device_coop();
         const auto t0 = std::chrono::steady_clock::now();
         const SchedulerStats s =
             layout == GF_LAYOUT_SOA

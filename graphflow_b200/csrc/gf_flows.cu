@@ -68,6 +68,7 @@ bool gf_runner_batched();        // gf_capi.cu
 uint32_t gf_runner_sink_batch();
 bool gf_group_partitions(); // gf_capi.cu
 bool gf_device_resident();  // gf_capi.cu
+bool gf_device_coop();     // gf_capi.cu
 
 // Runs a front-end call, mapping its exceptions to gf_status and the last-error message.
 gf_status gf_flows_guard(const std::function<void()>& body) { return guarded(body); }
@@ -158,6 +159,7 @@ gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visit
             t.groupPartitions = gf_group_partitions();
         }
         t.deviceResident = gf_device_resident();
+        t.deviceCoop = gf_device_coop();
         return gf_run_particle_feedback_record_form(n, max_visits, t, h_weights, h_capped, h_stats);
     }
     return guarded([&] {
@@ -184,6 +186,7 @@ gf_status gf_run_particle_feedback(uint64_t seed, uint64_t n, uint32_t max_visit
             t.groupPartitions = gf_group_partitions();
         }
         t.deviceResident = gf_device_resident();
+        t.deviceCoop = gf_device_coop();
         const auto t0 = std::chrono::steady_clock::now();
         SchedulerStats s = layout == GF_LAYOUT_SOA
                                ? runParticleFeedback<SoAStorage<Particle>>(device, n, max_visits, t, weights.data(),
@@ -238,6 +241,7 @@ gf_status gf_run_kernel_axes(uint64_t seed, uint64_t n, uint32_t bins, int distr
         }
         // device-resident runs take the fused dense partition: the fused form of the workload only
         t.deviceResident = gf_device_resident() && t.fused && hash_path == 0 && scatter_mode != GF_SCATTER_DIRECT;
+        t.deviceCoop = gf_device_coop();
         const auto d = static_cast<Distribution>(distribution);
         const auto t0 = std::chrono::steady_clock::now();
         SchedulerStats s;

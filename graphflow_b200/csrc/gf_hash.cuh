@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(kHashPThreads, PPT == 8u ? 3 : 4) hash_scatter
     constexpr uint32_t T = kHashPThreads, W = T / 32u, RPT = 2048u / T; // rows per unit: unit / T <= RPT
     static_assert((PPT == 4u || PPT == 8u) && PPT * T >= kHashGroupBins / 2u && (!kTail || PPT * T >= kHashGroupBins),
                   "owned ports: PPT per thread cover the grouped ports");
-    extern __shared__ __align__(16) uint32_t sm[];
+    extern __shared__ __align__(128) uint32_t sm[];
     const uint32_t GB = B < kHashGroupBins ? B : kHashGroupBins;
     P* stage = reinterpret_cast<P*>(sm);                              // [unit]
     uint64_t* rbase = reinterpret_cast<uint64_t*>(stage + unit);      // [2][RPT]

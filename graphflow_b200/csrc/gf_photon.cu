@@ -14,6 +14,7 @@ uint32_t gf_runner_sink_batch();                                // gf_capi.cu
 
 bool gf_group_partitions(); // gf_capi.cu
 bool gf_device_resident();  // gf_capi.cu
+bool gf_device_coop();     // gf_capi.cu
 
 namespace {
 
@@ -80,6 +81,7 @@ void runTyped(std::uint64_t seed, std::uint64_t firstId, std::uint64_t n, const 
                 t.groupPartitions = gf_group_partitions();
             }
             t.deviceResident = gf_device_resident();
+            t.deviceCoop = gf_device_coop();
             stats = runPhotonFlow<T, SoAStorage<PhotonT<T>>>(device, n, propose, slab, scatter, terminal, t);
         } else if (n != 0u) {
             const unsigned blocks = static_cast<unsigned>(std::min<std::uint64_t>((n + 255u) / 256u, 148u * 64u));

@@ -39,6 +39,7 @@ gf_status gf_run_particle_feedback_record_form(std::uint64_t n, std::uint32_t ma
 }
 
 bool gf_device_resident(); // gf_capi.cu
+bool gf_device_coop();     // gf_capi.cu
 
 extern "C" gf_status gf_run_set_transform(uint64_t seed, uint64_t n, uint32_t increment, uint32_t chunk_capacity,
                                           uint32_t live_particles, uint32_t batch_chunks, uint32_t* h_weights,
@@ -63,6 +64,7 @@ extern "C" gf_status gf_run_set_transform(uint64_t seed, uint64_t n, uint32_t in
             t.liveParticles = live_particles;
         t.batchChunks = batch_chunks;
         t.deviceResident = gf_device_resident();
+        t.deviceCoop = gf_device_coop();
         const auto t0 = std::chrono::steady_clock::now();
         const SchedulerStats s = runSetTransform(device, n, increment, t, weights.data(), visits.data());
         const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -101,6 +101,9 @@ struct Tuning {
     // one batch on one stream, chunks from a device-resident pool, one host read per wave. P, Q and
     // the runner options do not apply; partitions run the dense fused kernel.
     bool deviceResident = false;
+    // B200, device-resident runs: a partition batch of at least 64 tiles and up to 64 ports runs
+    // the cooperative count -> grid barrier -> scatter kernel instead of the per-tile look-back one.
+    bool deviceCoop = true;
     static constexpr std::uint32_t kMaxSinkBatchChunks = 256u;
 
     void validate() const

@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "gf_device_pool.cuh"
+#include "gf_fused_any.cuh"
 #include "kernels.cuh"
 
 namespace graphflow {
@@ -180,8 +181,15 @@ struct WaveContext {
     gf_out_desc* descs = nullptr;
     std::uint32_t descCap = 0u;
     std::uint32_t* numOut = nullptr;
-    std::uint64_t launches = 0u, partitionBatches = 0u, batches = 0u, sunk = 0u;
+    // cooperative partitions (gf_fused_any.cuh) for batches of at least kCoopMinTiles tiles
+    void* coopScratch = nullptr;
+    std::uint64_t coopScratchBytes = 0u;
+    std::uint32_t coopMaxCtas = 0u;
+    int sms = 1;
+    std::uint64_t launches = 0u, partitionBatches = 0u, batches = 0u, sunk = 0u, coopBatches = 0u;
 };
+
+inline constexpr std::uint32_t kCoopMinTiles = 64u;
 
 // One node's wave step. `routes` are the list indices its ports feed (device copy in routesDev).
 class WaveNode {
@@ -326,16 +334,25 @@ public:
         const std::uint32_t bound = static_cast<std::uint32_t>(b64);
         wave_tiles_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.T, w.tp, w.tiles);
         gf::pool_acquire_kernel<<<1, gf::kPoolThreads, 0, w.s>>>(w.pool, bound, w.reserved, w.status);
-        cuda::check(cudaMemsetAsync(w.ctl, 0, gf::kFusedCtlResetBytes, w.s), "memset");
         const Acc acc{m_st.view()};
         const Cls cls{m_cls, w.seedMixed, m_purpose, w.status};
         const Upd upd{m_upd, m_purpose + 1u, w.status};
-        auto* desc = reinterpret_cast<unsigned long long*>(w.ctl + 1);
-        // the launch's last CTA builds the table and the output descriptors
-        gf::fused_partition_kernel<Shape, Acc, Cls, Upd><<<nt, Shape::kThreads, m_smem, w.s>>>(
-            acc, cls, upd, w.seedMixed, w.C, gf::FastDiv(w.C), w.slots, w.tiles, nt, m_bins, w.reserved, bound,
-            w.totals, w.portChunks, w.maxK, w.ctl, desc, w.status,
-            gf::InlineFinish{w.table, w.descs, bound, w.numOut});
+        const gf::InlineFinish fin{w.table, w.descs, bound, w.numOut};
+        if (w.coopScratch != nullptr && m_bins <= gf::kAnyCoopMaxBins && nt >= kCoopMinTiles) {
+            // a large batch: count, one grid barrier, plan, scatter (no per-tile look-back)
+            cuda::check(gf::launch_fused_any_coop<Shape>(w.s, acc, cls, upd, w.seedMixed, w.C, w.slots, w.tiles, nt,
+                                                         m_bins, w.reserved, bound, w.totals, w.coopScratch,
+                                                         w.coopScratchBytes, w.coopMaxCtas, w.status, fin, w.sms),
+                        "device-resident cooperative partition launch");
+            ++w.coopBatches;
+        } else {
+            cuda::check(cudaMemsetAsync(w.ctl, 0, gf::kFusedCtlResetBytes, w.s), "memset");
+            auto* desc = reinterpret_cast<unsigned long long*>(w.ctl + 1);
+            // the launch's last CTA builds the table and the output descriptors
+            gf::fused_partition_kernel<Shape, Acc, Cls, Upd><<<nt, Shape::kThreads, m_smem, w.s>>>(
+                acc, cls, upd, w.seedMixed, w.C, gf::FastDiv(w.C), w.slots, w.tiles, nt, m_bins, w.reserved, bound,
+                w.totals, w.portChunks, w.maxK, w.ctl, desc, w.status, fin);
+        }
         wave_route_kernel<<<gridFor(bound), 256, 0, w.s>>>(w.descs, w.numOut, bound, routesDev, m_bins, w.L, next,
                                                           w.status);
         gf::pool_settle_kernel<<<1, gf::kPoolThreads, 0, w.s>>>(w.pool, w.reserved, bound, w.numOut, 0u, ids, 1u,

@@ -408,6 +408,16 @@ private:
         cuda::Buffer<unsigned long long> portChunks(static_cast<std::size_t>(maxBins) * S);
         const std::size_t scratchBytes = 64u + tiles * maxBins * 8u;
         cuda::Buffer<unsigned char> scratch(scratchBytes);
+        int sms = 1;
+        {
+            int dev = 0;
+            cuda::check(cudaGetDevice(&dev), "cudaGetDevice");
+            cuda::check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+        }
+        const std::uint32_t coopCtas = static_cast<std::uint32_t>(sms) * 16u;
+        const std::uint64_t coopBytes =
+            m_tuning.deviceCoop ? gf::any_coop_scratch_bytes(static_cast<std::uint32_t>(tiles), kTile, coopCtas) : 0u;
+        cuda::Buffer<unsigned char> coopScratch(coopBytes);
         cudaStream_t s = nullptr;
         cuda::check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
         struct StreamGuard {
@@ -449,6 +459,10 @@ private:
         w.descs = descs.data();
         w.descCap = descCap;
         w.numOut = numOut.data();
+        w.coopScratch = coopBytes ? coopScratch.data() : nullptr;
+        w.coopScratchBytes = coopBytes;
+        w.coopMaxCtas = coopCtas;
+        w.sms = sms;
         w.launches = 1u;
         std::uint32_t next = 1u;
         if (itemCount != 0u)
