@@ -19,6 +19,7 @@
 
 #include "../examples/dense_chain.cuh"
 #include "gf_device_pool.cuh"
+#include "gf_fused_any.cuh"
 #include "gf_partition.cuh"
 
 namespace gf {
@@ -119,9 +120,12 @@ struct DeviceChainLayout {
     std::uint32_t bins, nodes;
     std::uint64_t nIn, bound, chunks, slots, tiles, maxK;
     std::uint64_t pool, id, key, tile, srcIds, reserved, scratch, totals, portChunks, table, descs[2], numOut,
-        sunk, portOf, total;
-    DeviceChainLayout(std::uint64_t n_, std::uint32_t bins_, std::uint32_t nodes_, std::uint64_t bound_)
-        : n(n_), bins(bins_), nodes(nodes_)
+        sunk, portOf, coop, coopBytes, total;
+    std::uint32_t coopCtas;
+    // coop_ctas: rows of the cooperative kernel's scratch (0: every node runs the per-tile kernel)
+    DeviceChainLayout(std::uint64_t n_, std::uint32_t bins_, std::uint32_t nodes_, std::uint64_t bound_,
+                      std::uint32_t coop_ctas = 0u)
+        : n(n_), bins(bins_), nodes(nodes_), coopCtas(coop_ctas)
     {
         nIn = (n + kChainCapacity - 1u) / kChainCapacity;
         bound = bound_;
@@ -150,6 +154,8 @@ struct DeviceChainLayout {
         take(numOut, 256u);
         take(sunk, 256u);
         take(portOf, std::max<std::uint64_t>(n, 1u) * 4u);
+        coopBytes = coopCtas ? any_coop_scratch_bytes(static_cast<std::uint32_t>(tiles), kChainTile, coopCtas) : 0u;
+        take(coop, coopBytes);
         total = o;
     }
 };
@@ -224,7 +230,14 @@ inline std::uint32_t enqueueDeviceChain(cudaStream_t s, char* base, const Device
         chain_tiles_kernel<<<(nChunks + 255u) / 256u + 1u, 256, 0, s>>>(L.n, nChunks, srcIds, in, inCount, tiles);
         pool_acquire_kernel<<<1, kPoolThreads, 0, s>>>(pool, bound, reserved, status);
         std::uint32_t* nodeTotals = totals + static_cast<std::size_t>(node) * bins;
-        if (nTiles != 0u) {
+        if (nTiles != 0u && L.coopBytes != 0u && nTiles >= 64u && bins <= kAnyCoopMaxBins) {
+            // count, one grid barrier, plan, scatter over the node's whole input
+            check(launch_fused_any_coop<ChainShape>(s, cols, ShiftPort{8u * node, FastDiv(bins)}, NoUpdate{}, 0u,
+                                                    kChainCapacity, L.slots, tiles, nTiles, bins, reserved, bound,
+                                                    nodeTotals, P(L.coop), L.coopBytes, L.coopCtas, status,
+                                                    InlineFinish{table, out, bound, outCount}, static_cast<int>(sms)),
+                  "device chain cooperative partition");
+        } else if (nTiles != 0u) {
             check(cudaMemsetAsync(ctl, 0, kFusedCtlResetBytes, s), "memset");
             // the last CTA builds this node's table and descriptors (no separate finish launch)
             kernel<<<nTiles, ChainShape::kThreads, smem, s>>>(

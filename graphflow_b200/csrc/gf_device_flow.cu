@@ -8,6 +8,7 @@
 #include "gf_device_chain.cuh"
 
 gf_status gf_flows_guard(const std::function<void()>& body); // gf_flows.cu
+bool gf_device_coop();                                        // gf_capi.cu
 void gf_set_last_error(const char* message);                 // gf_flows.cu
 
 namespace {
@@ -112,7 +113,8 @@ gf_status gf_run_dense_chain_device(uint64_t seed, uint64_t n, uint32_t bins, ui
         cuda::Device device = cuda::Device::current();
         device.makeCurrent();
         const std::uint64_t bound = outputChunkBound(n, gf::kChainCapacity, bins);
-        const gf::DeviceChainLayout L(n, bins, nodes, bound);
+        const std::uint32_t sms = current_sms();
+        const gf::DeviceChainLayout L(n, bins, nodes, bound, gf_device_coop() ? sms * 16u : 0u);
         if (L.slots > 0xFFFFFFFFull)
             throw std::overflow_error("graphflow::dense: the device chain's pool exceeds 2^32 slots");
         cuda::Buffer<unsigned char> block(L.total);
@@ -137,7 +139,7 @@ gf_status gf_run_dense_chain_device(uint64_t seed, uint64_t n, uint32_t bins, ui
         cudaError_t e = cudaEventRecord(ev[0], s);
         try {
             launches = gf::enqueueDeviceChain(s, base, L, dist, dist == GF_DIST_ZIPF ? cdf.data() : nullptr, seed,
-                                              status.data(), current_sms());
+                                              status.data(), sms);
         } catch (...) {
             cudaStreamSynchronize(s);
             cudaStreamDestroy(s);

@@ -114,6 +114,10 @@ uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap);
  *                options do not apply; partitions run the fused dense kernel (the kernel workload's
  *                plain, direct-scatter and hash-path forms keep the host runner). Results are
  *                identical.
+ *   "device_coop" 1 (default) = in device-resident runs and gf_run_dense_chain_device, a partition
+ *                batch of at least 64 tiles and up to 64 ports runs the cooperative count -> grid
+ *                barrier -> scatter kernel (bins kept from the count pass); 0 = the per-tile
+ *                look-back kernel. Results are identical.
  *   "runner_batched" 1 (default) = the flow entry points (gf_run_particle_feedback,
  *                gf_run_dense_chain, gf_run_photon) let a sink take up to "sink_batch_chunks"
  *                ready chunks per launch and dispatch every idle node in one scheduler iteration;
