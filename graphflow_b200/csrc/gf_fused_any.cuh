@@ -6,8 +6,8 @@
 // descriptors), every port's particles in input order, and no per-tile look-back:
 //   phase 1  CTA c owns the contiguous tiles [n c / G, n (c + 1) / G); it loads and classifies
 //            every particle once, keeps the bin (16 bits per particle, in the scratch) and counts
-//            ports in shared memory (warp-aggregated); its per-port counts go to its row of the
-//            scratch and are added to the batch totals;
+//            ports in shared memory (warp-aggregated up to 16 ports); its per-port counts go to
+//            its row of the scratch and are added to the batch totals;
 //   barrier  cooperative launch, bounded wait (coop_grid_barrier);
 //   plan     per-port base of this CTA (the rows before it, or the batch total minus the rows
 //            after it, whichever is fewer), binBase[b] = sum_{b' < b} ceil(total_b' / C); port b's
@@ -112,9 +112,14 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
                     set_status(status, GF_INVALID);
                 bins16[(size_t)t * Shape::kTile + i] = (uint16_t)b;
             }
-            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
-            if (b != kNoBin16 && lane == __ffs(peers) - 1)
-                atomicAdd(&cnt[b], (uint32_t)__popc(peers));
+            if (B > 16u) { // many ports: few lanes share one, a plain shared atomic each
+                if (b != kNoBin16)
+                    atomicAdd(&cnt[b], 1u);
+            } else { // few ports: one atomic per distinct port of the warp
+                const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
+                if (b != kNoBin16 && lane == __ffs(peers) - 1)
+                    atomicAdd(&cnt[b], (uint32_t)__popc(peers));
+            }
         }
     }
     __syncthreads();
