@@ -29,6 +29,7 @@
 #include <chrono>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "gf_device_pool.cuh"
@@ -299,7 +300,10 @@ class PartitionWave final : public WaveNode {
     using Cls = ClassifyAdapter<TClassifier, P>;
     using Upd = UpdateAdapter<TUpdate, TBin, P>;
     using Shape = gf::TileShape<256, 4, 2>; // 1024-particle tiles, as PartitionStage
-    static_assert(Shape::kTile == kTile, "tile size");
+    // the cooperative kernel: the same tiles; payloads of up to 32 bytes at three CTAs per SM (at
+    // most 85 registers per thread), wider ones (the FP64 photon) at two, which keeps them unspilled
+    using CoopShape = std::conditional_t<(sizeof(P) <= 32u), gf::TileShape<256, 4, 3>, gf::TileShape<256, 4, 2>>;
+    static_assert(Shape::kTile == kTile && CoopShape::kTile == kTile, "tile size");
 
 public:
     PartitionWave(TStorage& st, TClassifier cls, TUpdate upd, std::uint32_t bins, std::uint32_t purpose)
@@ -340,9 +344,9 @@ public:
         const gf::InlineFinish fin{w.table, w.descs, bound, w.numOut};
         if (w.coopScratch != nullptr && m_bins <= gf::kAnyCoopMaxBins && nt >= kCoopMinTiles) {
             // a large batch: count, one grid barrier, plan, scatter (no per-tile look-back)
-            cuda::check(gf::launch_fused_any_coop<Shape>(w.s, acc, cls, upd, w.seedMixed, w.C, w.slots, w.tiles, nt,
-                                                         m_bins, w.reserved, bound, w.totals, w.coopScratch,
-                                                         w.coopScratchBytes, w.coopMaxCtas, w.status, fin, w.sms),
+            cuda::check(gf::launch_fused_any_coop<CoopShape>(w.s, acc, cls, upd, w.seedMixed, w.C, w.slots, w.tiles, nt,
+                                                             m_bins, w.reserved, bound, w.totals, w.coopScratch,
+                                                             w.coopScratchBytes, w.coopMaxCtas, w.status, fin, w.sms),
                         "device-resident cooperative partition launch");
             ++w.coopBatches;
         } else {
