@@ -70,6 +70,7 @@ struct Options {
     std::uint32_t batchChunks = 1u;
     std::uint32_t device = 0u;
     std::string exec = "fused";
+    bool deviceResident = false; // with --exec flow: the Flow run device-resident
     std::uint32_t frameCap = 8u; // LaunchPolicy.hpp:18 defaultFrameCap (inert here, recorded in metadata)
     std::optional<std::string> outputDir;
     std::uint32_t tracePhotons = 0u, traceVertices = 64u; // PhotonCli.hpp:46-47
@@ -86,7 +87,7 @@ void usage(std::ostream& out)
            "                                        [--max-scatters M] [--seed S]\n"
            "                                        [--chunk-size C] [--live-particles P]\n"
            "                                        [--tile-size T] [--batch-chunks Q]\n"
-           "                                        [--exec fused|flow]\n"
+           "                                        [--exec fused|flow] [--device-resident]\n"
            "       accepted for parity with graphFlow_photon_scattering, no effect here:\n"
            "       [--occupancy-target D] [--frame-cap F] [--pool-budget-bytes B]\n"
            "       [--pool-mode fixed|slotArena] [--slot-arena-budget BYTES]\n"
@@ -142,6 +143,8 @@ Options parse(int argc, char** argv)
             o.batchChunks = parseU32(flag, next());
         } else if (flag == "--device") {
             o.device = parseU32(flag, next(), true);
+        } else if (flag == "--device-resident") {
+            o.deviceResident = true;
         } else if (flag == "--exec") {
             o.exec = next();
             expectOneOf(flag, o.exec, {"fused", "flow"});
@@ -179,6 +182,8 @@ Options parse(int argc, char** argv)
             throw std::invalid_argument("unknown argument '" + flag + "'");
         }
     }
+    if (o.deviceResident && o.exec != "flow")
+        throw std::invalid_argument("--device-resident requires --exec flow");
     return o;
 }
 
@@ -196,6 +201,8 @@ int run(const Options& o)
         std::cerr << kName << ": note: " << f << " has no effect in this build\n";
 
     cudaOrThrow(cudaSetDevice(static_cast<int>(o.device)), "cudaSetDevice");
+    if (o.deviceResident && gf_set_tuning("device_resident", 1) != GF_OK)
+        throw std::runtime_error("device_resident: " + lastError());
     cudaDeviceProp prop{};
     cudaOrThrow(cudaGetDeviceProperties(&prop, static_cast<int>(o.device)), "cudaGetDeviceProperties");
     const bool wideChunk = !o.chunkSize || *o.chunkSize >= kLogicalTileWidth;

@@ -88,6 +88,9 @@ def test_tuning_knobs():
             assert L.gf_set_tuning(b"sink_batch_chunks", good) == capi.GF_OK
     finally:
         assert L.gf_set_tuning(b"sink_batch_chunks", 256) == capi.GF_OK
+    for knob, default in ((b"device_resident", 0), (b"device_coop", 1), (b"fused_coop_bulk", 1)):
+        assert L.gf_set_tuning(knob, 1 - default) == capi.GF_OK
+        assert L.gf_set_tuning(knob, default) == capi.GF_OK
 
 
 def test_device_pool_host_checks():

@@ -228,6 +228,7 @@ def test_photon_cli_help():
     ["--backend", "cuda", "--trace-vertices", "-1"],
     ["--backend", "cuda", "--pool-mode", "arena"],
     ["--backend", "cuda", "--exec", "both"],
+    ["--backend", "cuda", "--device-resident"],                   # a Flow option: needs --exec flow
 ])
 def test_photon_cli_rejects_bad_command_lines(args):
     r = _prun(*args)
@@ -255,9 +256,11 @@ def test_photon_cli_report_matches_the_library_and_both_execution_forms(mode):
     args = ["--backend", "cuda", "--photons", str(n), "--thickness", "1", "--sigma-s", "2", "--sigma-a", "0.5",
             "--mode", mode, "--max-scatters", "64", "--seed", str(seed)]
     fused, flow = _prun(*args), _prun(*args, "--exec", "flow", "--chunk-size", "4096", "--batch-chunks", "4")
-    assert fused.returncode == 0 and flow.returncode == 0, fused.stderr + flow.stderr
+    dev = _prun(*args, "--exec", "flow", "--chunk-size", "4096", "--device-resident")
+    assert fused.returncode == 0 and flow.returncode == 0 and dev.returncode == 0, fused.stderr + flow.stderr
     ev, rows, term, bad = _photon_report(fused.stdout)
     assert _photon_report(flow.stdout) == (ev, rows, term, bad)
+    assert _photon_report(dev.stdout) == (ev, rows, term, bad)
     p = capi.photon_params(model=capi.PHOTON_ANALOG, thickness=1.0, sigma_s=2.0, sigma_a=0.5, max_scatters=64,
                            isotropic=(mode == "isotropic"), fp64=True)
     got = capi.run_photon(seed, n, p, exec_mode=capi.EXEC_FUSED)
