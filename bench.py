@@ -550,7 +550,8 @@ def gpu_arm(args):
                      "traffic": (MEASURED_TRAFFIC_PER_KEY[(args.bins, args.dist)] * args.n
                                  if (args.bins, args.dist) in MEASURED_TRAFFIC_PER_KEY and args.tile <= 4096 else None),
                      "traffic_source": "ncu, 5e7 keys, scaled", "peak_source": peak_kind,
-                     "kernel": "fused_partition_coop_kernel", "kernel_ms": kernel_ms,
+                     "kernel": ("fused_partition_coop_bulk_kernel" if args.bins <= 16 else "fused_partition_coop_kernel"),
+                     "kernel_ms": kernel_ms,
                      "algorithmic_bytes": f"{BYTES_PER_PARTICLE} B/particle"},
         "cpu_baseline": cpu,
         "e2e": {"value": world * args.n / (e2e_ms / 1e3), "unit": "particles/s",
