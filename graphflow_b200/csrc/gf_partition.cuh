@@ -113,6 +113,10 @@ GF_D uint32_t block_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n
 // Stable in-tile ranking. bp[r] holds the bin of item (w, r, lane) in its low half (kNoBin16 for
 // none). On return its high half holds the item's rank among the items of its bin inside its
 // warp's slice, and warp_cnt[w*B + b] holds the number of items of bin b in warp w's slice.
+// The lanes that share an item's bin: match.any, whose cost grows with the number of distinct
+// values in the warp, except for 17 to 64 bins: one ballot for "has a bin" and one per bin bit
+// (7 ballots at 64 bins, about a third of match.any's cost there; at 16 bins and fewer match.any
+// measured cheaper).
 template <typename Shape>
 GF_D void warp_rank(uint32_t (&bp)[Shape::kIpt], uint32_t* warp_cnt, uint32_t B)
 {
@@ -122,10 +126,23 @@ GF_D void warp_rank(uint32_t (&bp)[Shape::kIpt], uint32_t* warp_cnt, uint32_t B)
         cnt[b] = 0u;
     __syncwarp();
     const uint32_t lt = lanemask_lt();
+    // bits of a bin, or -1: match.any
+    const int nbits = B > 16u && B <= 64u ? 32 - __clz((int)(B - 1u)) : -1;
 #pragma unroll
     for (int r = 0; r < Shape::kIpt; ++r) {
         const uint32_t bin = bp_bin(bp[r]);
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, bin);
+        uint32_t peers;
+        if (nbits >= 0) {
+            const uint32_t valid = __ballot_sync(0xFFFFFFFFu, bin != kNoBin16);
+            peers = bin != kNoBin16 ? valid : ~valid;
+            for (int k = 0; k < nbits; ++k) {
+                const uint32_t bit = (bin >> k) & 1u;
+                const uint32_t set = __ballot_sync(0xFFFFFFFFu, bit != 0u);
+                peers &= bit != 0u ? set : ~set;
+            }
+        } else {
+            peers = __match_any_sync(0xFFFFFFFFu, bin);
+        }
         uint32_t base = 0;
         if (bin != kNoBin16)
             base = cnt[bin];
