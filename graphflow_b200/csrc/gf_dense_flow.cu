@@ -4,7 +4,7 @@
 #include <functional>
 #include <vector>
 
-#include "../examples/dense_chain.cuh"
+#include "gf_device_chain.cuh" // dense_chain.cuh and chain_expand_kernel
 
 gf_status gf_flows_guard(const std::function<void()>& body); // gf_flows.cu
 bool gf_runner_batched();                                       // gf_capi.cu
@@ -20,7 +20,7 @@ using namespace graphflow::dense;
 
 template <typename TStorage>
 SchedulerStats dispatchBins(std::uint32_t bins, cuda::Device device, std::uint64_t n, std::uint32_t nodes, int dist,
-                            std::uint64_t seed, const double* cdf, const Tuning& t, std::uint32_t* portOf)
+                            std::uint64_t seed, const double* cdf, const Tuning& t, std::uint8_t* portOf)
 {
     switch (bins) {
     case 2u:
@@ -49,8 +49,8 @@ extern "C" gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins
         cuda::Device device = cuda::Device::current();
         device.makeCurrent();
         const std::size_t m = n ? n : 1u;
-        cuda::Buffer<std::uint32_t> portOf(m);
-        cuda::check(cudaMemset(portOf.data(), 0xFF, m * 4u), "memset");
+        cuda::Buffer<std::uint8_t> portOf(m); // one byte per id, widened to the caller's words below
+        cuda::check(cudaMemset(portOf.data(), 0xFF, m), "memset");
         cuda::Buffer<double> cdf(bins);
         if (dist == GF_DIST_ZIPF) {
             std::vector<double> h(bins);
@@ -79,8 +79,13 @@ extern "C" gf_status gf_run_dense_chain(uint64_t seed, uint64_t n, uint32_t bins
                 ? dispatchBins<SoAStorage<KeyRecord>>(bins, device, n, nodes, dist, seed, cdf.data(), t, portOf.data())
                 : dispatchBins<AoSStorage<KeyRecord>>(bins, device, n, nodes, dist, seed, cdf.data(), t, portOf.data());
         const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        if (h_port_of != nullptr && n != 0u)
-            cuda::check(cudaMemcpy(h_port_of, portOf.data(), n * 4u, cudaMemcpyDeviceToHost), "D2H");
+        if (h_port_of != nullptr && n != 0u) {
+            cuda::Buffer<std::uint32_t> wide(n);
+            gf::chain_expand_kernel<<<static_cast<unsigned>(std::min<std::uint64_t>((n + 1023u) / 1024u, 148u * 16u)),
+                                      256>>>(portOf.data(), wide.data(), n);
+            cuda::check(cudaGetLastError(), "port expand launch");
+            cuda::check(cudaMemcpy(h_port_of, wide.data(), n * 4u, cudaMemcpyDeviceToHost), "D2H");
+        }
         if (h_stats != nullptr) {
             h_stats->completed_batches = s.completedBatches;
             h_stats->partition_batches = s.partitionBatches;

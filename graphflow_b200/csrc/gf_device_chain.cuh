@@ -88,8 +88,11 @@ __global__ void chain_tiles_kernel(std::uint64_t n, std::uint32_t nChunks, const
 
 // Sink: each published output chunk of the last node records its port for every id in it and
 // counts the records it saw (a chunk id numChunks or above, from a failed reservation, is skipped).
+// The ports (below 255) go to a byte per id: the ids arrive in no order, and N bytes fit the
+// 126 MB L2 at N = 1e8 where N words do not, so the scattered writes merge in L2 instead of each
+// costing a DRAM sector; chain_expand_kernel widens them afterwards with streaming stores.
 __global__ void chain_sink_kernel(const gf_out_desc* descs, const std::uint32_t* numOut, std::uint32_t numChunks,
-                                  const std::uint32_t* id, std::uint32_t* portOf, std::uint64_t n,
+                                  const std::uint32_t* id, std::uint8_t* port8, std::uint64_t n,
                                   unsigned long long* sunk)
 {
     for (std::uint32_t f = blockIdx.x; f < *numOut; f += gridDim.x) {
@@ -100,18 +103,27 @@ __global__ void chain_sink_kernel(const gf_out_desc* descs, const std::uint32_t*
         for (std::uint32_t i = threadIdx.x; i < d.fill; i += blockDim.x) {
             const std::uint32_t who = id[base + i];
             if (who < n)
-                portOf[who] = d.bin;
+                port8[who] = static_cast<std::uint8_t>(d.bin);
         }
         if (threadIdx.x == 0 && sunk != nullptr)
             atomicAdd(sunk, static_cast<unsigned long long>(d.fill));
     }
 }
 
-__global__ void chain_fill_kernel(std::uint32_t* p, std::uint64_t n, std::uint32_t v)
+// portOf[i] = port8[i], 0xFF (no port recorded) widened to 0xFFFFFFFF; four ids per thread step.
+__global__ void chain_expand_kernel(const std::uint8_t* port8, std::uint32_t* portOf, std::uint64_t n)
 {
+    auto widen = [](std::uint32_t b) { return b == 0xFFu ? 0xFFFFFFFFu : b; };
     const std::uint64_t stride = static_cast<std::uint64_t>(gridDim.x) * blockDim.x;
-    for (std::uint64_t i = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
-        p[i] = v;
+    const std::uint64_t n4 = n / 4u;
+    for (std::uint64_t q = static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; q < n4; q += stride) {
+        const std::uint32_t v = reinterpret_cast<const std::uint32_t*>(port8)[q];
+        reinterpret_cast<uint4*>(portOf)[q] =
+            make_uint4(widen(v & 0xFFu), widen((v >> 8) & 0xFFu), widen((v >> 16) & 0xFFu), widen(v >> 24));
+    }
+    for (std::uint64_t i = 4u * n4 + static_cast<std::uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += stride)
+        portOf[i] = widen(port8[i]);
 }
 
 // Byte offsets of one chain run's buffers inside one device block (every buffer 256-byte aligned).
@@ -120,7 +132,7 @@ struct DeviceChainLayout {
     std::uint32_t bins, nodes;
     std::uint64_t nIn, bound, chunks, slots, tiles, maxK;
     std::uint64_t pool, id, key, tile, srcIds, reserved, scratch, totals, portChunks, table, descs[2], numOut,
-        sunk, portOf, coop, coopBytes, total;
+        sunk, portOf, port8, coop, coopBytes, total;
     std::uint32_t coopCtas;
     // coop_ctas: rows of the cooperative kernel's scratch (0: every node runs the per-tile kernel)
     DeviceChainLayout(std::uint64_t n_, std::uint32_t bins_, std::uint32_t nodes_, std::uint64_t bound_,
@@ -154,6 +166,7 @@ struct DeviceChainLayout {
         take(numOut, 256u);
         take(sunk, 256u);
         take(portOf, std::max<std::uint64_t>(n, 1u) * 4u);
+        take(port8, std::max<std::uint64_t>(n, 1u));
         coopBytes = coopCtas ? any_coop_scratch_bytes(static_cast<std::uint32_t>(tiles), kChainTile, coopCtas) : 0u;
         take(coop, coopBytes);
         total = o;
@@ -190,8 +203,8 @@ inline std::uint32_t enqueueDeviceChain(cudaStream_t s, char* base, const Device
                                                                      sms * 8u));
     pool_init_kernel<<<static_cast<unsigned>(std::min<std::uint64_t>((L.chunks + 1023u) / 1024u + 1u, sms)),
                        kPoolThreads, 0, s>>>(pool, static_cast<std::uint32_t>(L.chunks));
-    chain_fill_kernel<<<g, 256, 0, s>>>(portOf, std::max<std::uint64_t>(L.n, 1u), 0xFFFFFFFFu);
-    launches += 2u;
+    check(cudaMemsetAsync(P(L.port8), 0xFF, std::max<std::uint64_t>(L.n, 1u), s), "memset");
+    launches += 1u;
     // A fresh control block restarts the launch epochs at 1, so epoch-tagged look-back descriptors
     // and chunk claims left in this block by an earlier run are cleared too (tag 0 never matches).
     check(cudaMemsetAsync(ctl, 0, 64u + L.tiles * bins * 8u, s), "memset");
@@ -259,11 +272,12 @@ inline std::uint32_t enqueueDeviceChain(cudaStream_t s, char* base, const Device
     const gf_out_desc* last = descs[(L.nodes - 1u) & 1u];
     const std::uint32_t* lastCount = numOut + ((L.nodes - 1u) & 1u);
     chain_sink_kernel<<<static_cast<unsigned>(std::min<std::uint64_t>(std::max<std::uint64_t>(L.bound, 1u), 4096u)),
-                        256, 0, s>>>(last, lastCount, static_cast<std::uint32_t>(L.chunks), id, portOf, L.n,
-                                     sunk);
+                        256, 0, s>>>(last, lastCount, static_cast<std::uint32_t>(L.chunks), id,
+                                     reinterpret_cast<std::uint8_t*>(P(L.port8)), L.n, sunk);
+    chain_expand_kernel<<<g, 256, 0, s>>>(reinterpret_cast<const std::uint8_t*>(P(L.port8)), portOf, L.n);
     pool_settle_kernel<<<1, kPoolThreads, 0, s>>>(pool, nullptr, 0u, nullptr, 0u, &last->chunk_index, 3u, lastCount,
                                                   0u, status);
-    launches += 2u;
+    launches += 3u;
     check(cudaGetLastError(), "device chain launch");
     return launches;
 }
