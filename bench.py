@@ -55,6 +55,9 @@ def parse():
     p.add_argument("--hash", type=int, default=0, metavar="K",
                    help="only run the device-planned hash partition of --n records over K keys (Zipf 1.2, "
                         "tiles of 2048) --steps times after --warmup batches and print its timing; for profiling")
+    p.add_argument("--device-chain", type=int, default=0, metavar="NODES",
+                   help="one run of the dense chain entirely on the device (gf_run_dense_chain_device) at N=--n, "
+                        "B=--bins (profiling)")
     p.add_argument("--feedback-device-resident", action="store_true",
                    help="one particle_feedback run through the Flow device-resident at N=--n, C=8192 (profiling)")
     p.add_argument("--flow-chain", type=int, default=0, metavar="NODES",
@@ -1105,8 +1108,22 @@ def feedback_device_resident_only(args):
                       "partition_batches": st.partition_batches, "sunk": st.sunk}))
 
 
+def device_chain_only(args):
+    """One run of the dense chain on the device (seed 42, C = 8192), for profiling its launches."""
+    from graphflow_b200 import capi
+    _, _, pool, st = capi.run_dense_chain_device(SEED, args.n, args.bins, nodes=args.device_chain, dist=args.dist,
+                                                 want_ports=False)
+    print(json.dumps({"workload": f"dense chain on the device, {args.device_chain} nodes, N={args.n}, B={args.bins}, "
+                                  f"{args.dist}, C=8192", "device_seconds": st.loop_seconds,
+                      "kernel_launches": st.kernel_launches, "pool_chunks": pool.num_chunks,
+                      "peak_live_chunks": pool.peak_live}))
+
+
 def main():
     args = parse()
+    if args.device_chain:
+        device_chain_only(args)
+        return
     if args.feedback_device_resident:
         feedback_device_resident_only(args)
         return
