@@ -882,24 +882,29 @@ def _cfg_serving():
     p32, pt32 = capi.serve(sburst, capi.SERVE_BATCHED, max_inflight=32)
     p1, pt1 = capi.serve(sburst, capi.SERVE_BATCHED, max_inflight=1)
     pp, ptp = capi.serve(sburst, capi.SERVE_PLAIN)
+    pd, ptd = capi.serve(sburst, capi.SERVE_FLOW_DEVICE)
     out["stream256_all_at_once"] = {"served_batched32": summary(sburst, p32, pt32),
                                     "served_one_at_a_time": summary(sburst, p1, pt1),
                                     "plain": summary(sburst, pp, ptp),
+                                    "flow_device_resident": summary(sburst, pd, ptd),
                                     "results_identical": bool(np.array_equal(p32["digest"], pp["digest"]) and
-                                                              np.array_equal(p1["digest"], pp["digest"]))}
+                                                              np.array_equal(p1["digest"], pp["digest"]) and
+                                                              np.array_equal(pd["digest"], pp["digest"]))}
     a, b, c = (out["stream256_n1e3_1e5"][k] for k in ("served_batched32", "served_one_at_a_time", "plain"))
     d, e = (out["stream4096_n1e3_1e7"][k] for k in ("served_batched32", "served_one_at_a_time"))
     g, h = out["stream4096_all_at_once_batched32"], out["stream4096_all_at_once_one_at_a_time"]
-    i, j, k2 = (out["stream256_all_at_once"][k] for k in ("served_batched32", "served_one_at_a_time", "plain"))
+    i, j, k2, fd = (out["stream256_all_at_once"][k]
+                    for k in ("served_batched32", "served_one_at_a_time", "plain", "flow_device_resident"))
     # short keys: b32 = served with up to 32 requests in flight, one = served one request at a time,
-    # plain = the Flow one request at a time; x_plain = b32 / plain, x_one = b32 / one (flows/s)
+    # plain = the Flow one request at a time, flowdev = the same Flow one request at a time run
+    # device-resident; x_plain = b32 / plain, x_one = b32 / one (flows/s)
     out["summary"] = {
         "cols": "flows/s,p50 ms,p99 ms",
         "s256": {"b32": short(a), "one": short(b), "plain": short(c),
                  "x_plain": round(a["flows_per_s"] / c["flows_per_s"], 1),
                  "x_one": round(a["flows_per_s"] / b["flows_per_s"], 2)},
         "s4096": {"x_one": round(d["flows_per_s"] / e["flows_per_s"], 2)},
-        "sat256": {"b32": short(i), "one": short(j), "plain": short(k2),
+        "sat256": {"b32": short(i), "one": short(j), "plain": short(k2), "flowdev": short(fd),
                    "x_plain": round(i["flows_per_s"] / k2["flows_per_s"], 1),
                    "x_one": round(i["flows_per_s"] / j["flows_per_s"], 2)},
         "sat4096": {"x_one": round(g["flows_per_s"] / h["flows_per_s"], 2)},

@@ -313,7 +313,7 @@ def histogram_u32(values, stream=None):
 
 # ---- request server ----
 REQ_PARTICLE_FEEDBACK, REQ_PHOTON, REQ_DENSE_CHAIN = 0, 1, 2
-SERVE_PLAIN, SERVE_BATCHED = 0, 1
+SERVE_PLAIN, SERVE_BATCHED, SERVE_FLOW_DEVICE = 0, 1, 2
 REQUEST_DTYPE = None
 RESULT_DTYPE = None
 

@@ -302,13 +302,15 @@ gf_status runPlain(const gf_request& r, std::uint64_t& digest)
 
 } // namespace
 
-bool gf_runner_batched(); // gf_capi.cu
+bool gf_runner_batched();  // gf_capi.cu
+bool gf_device_resident(); // gf_capi.cu
 
 extern "C" gf_status gf_serve(const gf_request* h_requests, uint32_t n_requests, int mode, uint64_t memory_cap_bytes,
                               uint32_t max_inflight, gf_request_result* h_results, gf_serve_stats* h_stats)
 {
     if ((n_requests != 0u && (h_requests == nullptr || h_results == nullptr)) ||
-        (mode != GF_SERVE_PLAIN && mode != GF_SERVE_BATCHED) || max_inflight == 0u || max_inflight > 256u)
+        (mode != GF_SERVE_PLAIN && mode != GF_SERVE_BATCHED && mode != GF_SERVE_FLOW_DEVICE) || max_inflight == 0u ||
+        max_inflight > 256u)
         return GF_ERR_ARGUMENT;
     for (uint32_t i = 0; i < n_requests; ++i) {
         const gf_request& r = h_requests[i];
@@ -326,9 +328,20 @@ extern "C" gf_status gf_serve(const gf_request* h_requests, uint32_t n_requests,
         if (n_requests != 0u)
             std::memset(h_results, 0, sizeof(gf_request_result) * n_requests);
         gf_serve_stats stats{};
-        if (mode == GF_SERVE_PLAIN) {
-            const int saved = gf_runner_batched() ? 1 : 0;
-            gf_set_tuning("runner_batched", 0); // the reference runner: one-chunk sinks, one dispatch per iteration
+        if (mode == GF_SERVE_PLAIN || mode == GF_SERVE_FLOW_DEVICE) {
+            // one request at a time through the Flow: the reference runner (one-chunk sinks, one
+            // dispatch per iteration), or the same graphs run device-resident
+            const int saved = gf_runner_batched() ? 1 : 0, savedDevice = gf_device_resident() ? 1 : 0;
+            auto restore = [&] {
+                gf_set_tuning("runner_batched", saved);
+                gf_set_tuning("device_resident", savedDevice);
+            };
+            if (mode == GF_SERVE_PLAIN) {
+                gf_set_tuning("runner_batched", 0);
+                gf_set_tuning("device_resident", 0);
+            } else {
+                gf_set_tuning("device_resident", 1);
+            }
             try {
                 const auto t0 = std::chrono::steady_clock::now();
                 for (uint32_t i = 0; i < n_requests; ++i) {
@@ -342,10 +355,10 @@ extern "C" gf_status gf_serve(const gf_request* h_requests, uint32_t n_requests,
                 stats.seconds = secondsSince(t0);
                 stats.peak_inflight = n_requests ? 1u : 0u;
             } catch (...) {
-                gf_set_tuning("runner_batched", saved);
+                restore();
                 throw;
             }
-            gf_set_tuning("runner_batched", saved);
+            restore();
             if (h_stats)
                 *h_stats = stats;
             return;

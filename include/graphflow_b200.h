@@ -490,8 +490,10 @@ enum { GF_REQ_PARTICLE_FEEDBACK = 0, GF_REQ_PHOTON = 1, GF_REQ_DENSE_CHAIN = 2 }
 /* GF_SERVE_PLAIN: one request at a time in arrival order through the C++ Flow with plain partitions
  * and the reference runner. GF_SERVE_BATCHED: continuous batching, every admitted request's whole
  * flow on the device on its own stream, admitted while others run as stream slots and device
- * memory (an arena capped at memory_cap_bytes) free up. */
-enum { GF_SERVE_PLAIN = 0, GF_SERVE_BATCHED = 1 };
+ * memory (an arena capped at memory_cap_bytes) free up. GF_SERVE_FLOW_DEVICE: one request at a
+ * time through the same Flow graphs as GF_SERVE_PLAIN, run device-resident (knob
+ * "device_resident"). */
+enum { GF_SERVE_PLAIN = 0, GF_SERVE_BATCHED = 1, GF_SERVE_FLOW_DEVICE = 2 };
 
 typedef struct gf_request {
     uint32_t kind;    /* GF_REQ_* */

@@ -50,8 +50,9 @@ def test_each_result_is_the_same_alone_in_the_mix_and_in_both_forms():
     req = _stream()
     mixed, st = capi.serve(req, capi.SERVE_BATCHED, max_inflight=8)
     plain, _ = capi.serve(req, capi.SERVE_PLAIN)
-    assert np.all(mixed["status"] == 0) and np.all(plain["status"] == 0)
-    assert np.array_equal(mixed["digest"], plain["digest"])
+    flowdev, _ = capi.serve(req, capi.SERVE_FLOW_DEVICE)
+    assert np.all(mixed["status"] == 0) and np.all(plain["status"] == 0) and np.all(flowdev["status"] == 0)
+    assert np.array_equal(mixed["digest"], plain["digest"]) and np.array_equal(flowdev["digest"], plain["digest"])
     for i in range(len(req)):
         alone, _ = capi.serve(req[i:i + 1], capi.SERVE_BATCHED, max_inflight=1)
         assert alone["digest"][0] == mixed["digest"][i], f"request {i}"
