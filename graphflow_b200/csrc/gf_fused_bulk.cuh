@@ -76,7 +76,8 @@ struct CoopBulkShape {
     static constexpr uint32_t kPc = kMbar + 8u;    // [2 * kMaxBins] x uint4 pieces {slot, stage pos, n, -}
     static constexpr uint32_t kWords = kPc + 8u * kMaxBins;
     static constexpr size_t kSmemBytes = sizeof(uint32_t) * kWords;
-    static_assert(kPc % 4u == 0u && kHist % 4u == 0u && kStage % 4u == 0u && kCnt % 4u == 0u && kMbar % 2u == 0u, "alignment");
+    static_assert(kPc % 4u == 0u && kHist % 4u == 0u && kStage % 4u == 0u && kCnt % 4u == 0u && kMbar % 2u == 0u,
+                  "alignment");
     static_assert(kStageWords >= kMaxCount, "stage doubles as a phase-1 buffer");
 };
 

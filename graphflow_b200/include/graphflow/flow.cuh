@@ -471,7 +471,8 @@ private:
         constexpr std::uint64_t kMaxWaves = 1u << 20;
         std::uint64_t wavesRun = 0u;
         for (;;) {
-            cuda::check(cudaMemcpyAsync(metaHost.data(), meta.data(), metaWords * 4u, cudaMemcpyDeviceToHost, s), "D2H");
+            cuda::check(cudaMemcpyAsync(metaHost.data(), meta.data(), metaWords * 4u, cudaMemcpyDeviceToHost, s),
+                        "D2H");
             cuda::check(cudaStreamSynchronize(s), "device-resident wave");
             const std::uint32_t st = metaHost.data()[6u * N];
             if (st != 0u)
