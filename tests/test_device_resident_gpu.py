@@ -43,6 +43,19 @@ def test_feedback_matches_oracle(layout, n, c, seed):
         assert st.peak_live_chunks <= st.pool_chunks
 
 
+@pytest.mark.parametrize("c", [1000, 3000, 2048])
+def test_feedback_chunk_capacities_off_the_tile_size(c):
+    """Chunk capacities that are not a multiple of the 1024-particle tile (a chunk's last tile is
+    partial) and one that is."""
+    n, seed = 150_001, 5
+    with device_resident():
+        w, capped, st = capi.run_particle_feedback(seed, n, 64, chunk_capacity=c, live_particles=4 * c,
+                                                   batch_chunks=1)
+    ew, ecapped, _ = O.particle_scalar(seed, n, 64)
+    assert np.array_equal(w, ew) and np.array_equal(capped.astype(np.uint8), ecapped)
+    assert st.sunk == n
+
+
 def test_feedback_equals_host_runner():
     n, seed = 300_007, 11
     host = capi.run_particle_feedback(seed, n, 16, chunk_capacity=1024, live_particles=4096, batch_chunks=2)
