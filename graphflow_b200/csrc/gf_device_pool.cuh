@@ -21,8 +21,9 @@
 //              free list ends exactly as if only the used chunks had been taken (their ledger
 //              state returns to free without a generation step), then releases the batch's input
 //              chunks.
-// Each operation is one single-CTA kernel on the caller's stream. Operations on one pool must be
-// stream-ordered, like the launches that share a fused partition's scratch.
+// Each operation is one single-CTA kernel on the caller's stream (or the same work in block 0 of a
+// larger kernel). Operations on one pool must be stream-ordered, like the launches that share a
+// fused partition's scratch.
 #pragma once
 
 #include "gf_device.cuh"
@@ -79,8 +80,8 @@ __global__ void __launch_bounds__(kPoolThreads) pool_init_kernel(DevicePoolHdr* 
 // Reserves k chunks: pops ids[base .. base + k) into out[0..k) and marks them live. Fewer than k
 // free: GF_OVERFLOW, nothing taken, out[] filled with kNoChunk (every kernel that writes through
 // a reservation rejects that id).
-__global__ void __launch_bounds__(kPoolThreads)
-    pool_acquire_kernel(DevicePoolHdr* h, uint32_t k, uint32_t* out, uint32_t* status)
+// The work of one CTA (all of its threads take part); other kernels may run it in their block 0.
+GF_D void pool_acquire_block(DevicePoolHdr* h, uint32_t k, uint32_t* out, uint32_t* status)
 {
     __shared__ uint32_t s_base, s_ok, s_bad;
     if (threadIdx.x == 0) {
@@ -119,6 +120,12 @@ __global__ void __launch_bounds__(kPoolThreads)
     }
 }
 
+__global__ void __launch_bounds__(kPoolThreads)
+    pool_acquire_kernel(DevicePoolHdr* h, uint32_t k, uint32_t* out, uint32_t* status)
+{
+    pool_acquire_block(h, k, out, status);
+}
+
 // Settles a batch: of its reservation `reserved[0..reserved_n)` the first *d_used (or `used` when
 // d_used is null, clamped to reserved_n) were used; the rest go back where they were. Then the
 // input chunks in[j * in_stride], j < *d_in_count (or in_count), are released (in_stride 1 for an
@@ -126,10 +133,10 @@ __global__ void __launch_bounds__(kPoolThreads)
 // reserved_n = 0, in may be null with a zero count. Any misuse (unused ids no longer just in front
 // of base, a released chunk that is out of range, not live, one of the unused reservations or named
 // twice) changes nothing and records GF_INVALID.
-__global__ void __launch_bounds__(kPoolThreads)
-    pool_settle_kernel(DevicePoolHdr* h, const uint32_t* reserved, uint32_t reserved_n, const uint32_t* d_used,
-                       uint32_t used, const uint32_t* in, uint32_t in_stride, const uint32_t* d_in_count,
-                       uint32_t in_count, uint32_t* status)
+// The work of one CTA (all of its threads take part); other kernels may run it in their block 0.
+GF_D void pool_settle_block(DevicePoolHdr* h, const uint32_t* reserved, uint32_t reserved_n, const uint32_t* d_used,
+                            uint32_t used, const uint32_t* in, uint32_t in_stride, const uint32_t* d_in_count,
+                            uint32_t in_count, uint32_t* status)
 {
     constexpr uint32_t kMark = 0x80000000u; // set only inside this kernel: "released by this call"
     __shared__ uint32_t s_base, s_unused, s_k, s_bad;
@@ -195,6 +202,14 @@ __global__ void __launch_bounds__(kPoolThreads)
         h->acquired -= unused;
         h->released += k;
     }
+}
+
+__global__ void __launch_bounds__(kPoolThreads)
+    pool_settle_kernel(DevicePoolHdr* h, const uint32_t* reserved, uint32_t reserved_n, const uint32_t* d_used,
+                       uint32_t used, const uint32_t* in, uint32_t in_stride, const uint32_t* d_in_count,
+                       uint32_t in_count, uint32_t* status)
+{
+    pool_settle_block(h, reserved, reserved_n, d_used, used, in, in_stride, d_in_count, in_count, status);
 }
 
 } // namespace

@@ -103,34 +103,13 @@ __global__ void wave_source_list_kernel(const std::uint32_t* chunk_of, std::uint
     }
 }
 
-// A partition's published output chunks to the lists their ports feed (route[bin]).
-__global__ void wave_route_kernel(const gf_out_desc* descs, const std::uint32_t* num_out, std::uint32_t cap_out,
-                                  const std::uint32_t* route, std::uint32_t bins, Lists L, std::uint32_t set,
-                                  std::uint32_t* status)
-{
-    const std::uint32_t m = *num_out < cap_out ? *num_out : cap_out;
-    for (std::uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < m; f += gridDim.x * blockDim.x) {
-        const gf_out_desc d = descs[f];
-        if (d.bin >= bins || d.fill == 0u) {
-            if (d.bin >= bins)
-                gf::set_status(status, GF_INVALID);
-            continue;
-        }
-        appendChunk(L, set, route[d.bin], d.chunk_index, d.fill, status);
-    }
-}
-
-// A whole list (set `from_set`, list `from`, k entries) appended to list `to` of `to_set`.
-__global__ void wave_forward_kernel(Lists L, std::uint32_t from_set, std::uint32_t from, std::uint32_t k,
-                                    std::uint32_t to_set, std::uint32_t to, std::uint32_t* status)
-{
-    const std::size_t base = L.at(from_set, from);
-    for (std::uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < k; f += gridDim.x * blockDim.x)
-        appendChunk(L, to_set, to, L.ids[base + f], L.fills[base + f], status);
-}
+// Per-node kernels of a wave. Each folds a node's small steps into as few launches as stream order
+// allows (a wave's tail is a few chunks per node, where every launch costs more than its work):
+// the pool steps run in block 0 (pool_acquire_block / pool_settle_block), the list and tile steps
+// in every block.
 
 // tp tiles per list entry: entry f's tile j covers [j T, min(fill, (j + 1) T)) (empty past the fill).
-__global__ void wave_tiles_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
+__device__ inline void buildTiles(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
                                   std::uint32_t T, std::uint32_t tp, gf_tile* tiles)
 {
     const std::uint32_t total = k * tp;
@@ -142,14 +121,75 @@ __global__ void wave_tiles_kernel(const std::uint32_t* ids, const std::uint32_t*
 
 // The same tiles as MoveTile with out_pos = f C + offset: with out_chunks = ids, the transform
 // kernel writes every particle back to its own slot.
-__global__ void wave_move_tiles_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
-                                       std::uint32_t C, std::uint32_t T, std::uint32_t tp, MoveTile* tiles)
+__device__ inline void buildMoveTiles(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
+                                      std::uint32_t C, std::uint32_t T, std::uint32_t tp, MoveTile* tiles)
 {
     const std::uint32_t total = k * tp;
     for (std::uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         const std::uint32_t f = t / tp, j = t - f * tp, off = j * T, fill = fills[f];
         tiles[t] = MoveTile{ids[f], off, fill > off ? (fill - off < T ? fill - off : T) : 0u, f * C + off};
     }
+}
+
+// Partition, before the partition kernel: its tiles; in block 0 the reservation of `bound` output
+// chunks and, for the per-tile kernel, the control block's three reset words.
+__global__ void wave_partition_prep_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
+                                           std::uint32_t T, std::uint32_t tp, gf_tile* tiles, gf::DevicePoolHdr* pool,
+                                           std::uint32_t bound, std::uint32_t* reserved, gf::FusedCtl* ctl,
+                                           std::uint32_t* status)
+{
+    buildTiles(ids, fills, k, T, tp, tiles);
+    if (blockIdx.x == 0) {
+        if (ctl != nullptr && threadIdx.x < gf::kFusedCtlResetBytes / 4u)
+            reinterpret_cast<std::uint32_t*>(ctl)[threadIdx.x] = 0u;
+        gf::pool_acquire_block(pool, bound, reserved, status);
+    }
+}
+
+// Partition, after the partition kernel: its published output chunks appended to the lists their
+// ports feed (route[bin]); in block 0 the unused reservations returned and the k input chunks
+// released (the partition kernel, earlier in the stream, has read them).
+__global__ void wave_partition_post_kernel(const gf_out_desc* descs, const std::uint32_t* num_out,
+                                           std::uint32_t cap_out, const std::uint32_t* route, std::uint32_t bins,
+                                           Lists L, std::uint32_t set, gf::DevicePoolHdr* pool,
+                                           const std::uint32_t* reserved, const std::uint32_t* ids, std::uint32_t k,
+                                           std::uint32_t* status)
+{
+    const std::uint32_t m = *num_out < cap_out ? *num_out : cap_out;
+    for (std::uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < m; f += gridDim.x * blockDim.x) {
+        const gf_out_desc d = descs[f];
+        if (d.bin >= bins || d.fill == 0u) {
+            if (d.bin >= bins)
+                gf::set_status(status, GF_INVALID);
+            continue;
+        }
+        appendChunk(L, set, route[d.bin], d.chunk_index, d.fill, status);
+    }
+    if (blockIdx.x == 0)
+        gf::pool_settle_block(pool, reserved, cap_out, num_out, 0u, ids, 1u, nullptr, k, status);
+}
+
+// Sink, before the sink kernel: its tiles; in block 0 the k input chunks released. Releasing them
+// before the sink reads them is safe in stream order: the next acquisition, which could hand them
+// out again, comes after the sink kernel.
+__global__ void wave_sink_prep_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
+                                      std::uint32_t C, std::uint32_t T, std::uint32_t tp, MoveTile* tiles,
+                                      gf::DevicePoolHdr* pool, std::uint32_t* status)
+{
+    buildMoveTiles(ids, fills, k, C, T, tp, tiles);
+    if (blockIdx.x == 0)
+        gf::pool_settle_block(pool, nullptr, 0u, nullptr, 0u, ids, 1u, nullptr, k, status);
+}
+
+// Transform, before the transform kernel: its tiles, and the k chunks (changed in place by the
+// kernel that follows) appended to list `to` of set `to_set` for the next wave.
+__global__ void wave_transform_prep_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
+                                           std::uint32_t C, std::uint32_t T, std::uint32_t tp, MoveTile* tiles,
+                                           Lists L, std::uint32_t to_set, std::uint32_t to, std::uint32_t* status)
+{
+    buildMoveTiles(ids, fills, k, C, T, tp, tiles);
+    for (std::uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < k; f += gridDim.x * blockDim.x)
+        appendChunk(L, to_set, to, ids[f], fills[f], status);
 }
 
 } // namespace
@@ -250,12 +290,12 @@ public:
         const std::uint32_t* ids = w.L.ids + w.L.at(cur, self);
         const std::uint32_t* fills = w.L.fills + w.L.at(cur, self);
         const std::uint32_t nt = k * w.tp;
-        wave_move_tiles_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.C, w.T, w.tp, w.moveTiles);
+        wave_transform_prep_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.C, w.T, w.tp, w.moveTiles, w.L,
+                                                                 next, routes[0], w.status);
         transform_kernel<<<nt, 256, 0, w.s>>>(m_f, m_st.view(), w.seedMixed, m_purpose, w.moveTiles, nt, ids, k, w.C,
                                               gf::FastDiv(w.C), w.slots, w.status);
-        wave_forward_kernel<<<gridFor(k), 256, 0, w.s>>>(w.L, cur, self, k, next, routes[0], w.status);
         cuda::check(cudaGetLastError(), "device-resident transform launch");
-        w.launches += 3u;
+        w.launches += 2u;
         ++w.batches;
     }
 
@@ -275,13 +315,12 @@ public:
         const std::uint32_t* ids = w.L.ids + w.L.at(cur, self);
         const std::uint32_t* fills = w.L.fills + w.L.at(cur, self);
         const std::uint32_t nt = k * w.tp;
-        wave_move_tiles_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.C, w.T, w.tp, w.moveTiles);
+        wave_sink_prep_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.C, w.T, w.tp, w.moveTiles, w.pool,
+                                                            w.status);
         sink_kernel<<<nt, 256, 0, w.s>>>(m_f, m_st.view(), w.seedMixed, m_purpose, w.moveTiles, nt, w.C, w.slots,
                                          w.status);
-        gf::pool_settle_kernel<<<1, gf::kPoolThreads, 0, w.s>>>(w.pool, nullptr, 0u, nullptr, 0u, ids, 1u, nullptr, k,
-                                                                w.status);
         cuda::check(cudaGetLastError(), "device-resident sink launch");
-        w.launches += 3u;
+        w.launches += 2u;
         w.sunk += particles;
         ++w.batches;
     }
@@ -336,13 +375,15 @@ public:
         if (b64 > w.descCap)
             throw BatchError("graphflow: deviceResident batch needs more output chunks than the run reserved");
         const std::uint32_t bound = static_cast<std::uint32_t>(b64);
-        wave_tiles_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.T, w.tp, w.tiles);
-        gf::pool_acquire_kernel<<<1, gf::kPoolThreads, 0, w.s>>>(w.pool, bound, w.reserved, w.status);
+        const bool coop =
+            w.coopScratch != nullptr && m_bins <= gf::kAnyCoopMaxBins && nt >= kCoopMinTiles;
+        wave_partition_prep_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.T, w.tp, w.tiles, w.pool, bound,
+                                                                 w.reserved, coop ? nullptr : w.ctl, w.status);
         const Acc acc{m_st.view()};
         const Cls cls{m_cls, w.seedMixed, m_purpose, w.status};
         const Upd upd{m_upd, m_purpose + 1u, w.status};
         const gf::InlineFinish fin{w.table, w.descs, bound, w.numOut};
-        if (w.coopScratch != nullptr && m_bins <= gf::kAnyCoopMaxBins && nt >= kCoopMinTiles) {
+        if (coop) {
             // a large batch: count, one grid barrier, plan, scatter (no per-tile look-back)
             cuda::check(gf::launch_fused_any_coop<CoopShape>(w.s, acc, cls, upd, w.seedMixed, w.C, w.slots, w.tiles, nt,
                                                              m_bins, w.reserved, bound, w.totals, w.coopScratch,
@@ -350,19 +391,16 @@ public:
                         "device-resident cooperative partition launch");
             ++w.coopBatches;
         } else {
-            cuda::check(cudaMemsetAsync(w.ctl, 0, gf::kFusedCtlResetBytes, w.s), "memset");
-            auto* desc = reinterpret_cast<unsigned long long*>(w.ctl + 1);
+            auto* desc = reinterpret_cast<unsigned long long*>(w.ctl + 1); // reset words zeroed by the prep kernel
             // the launch's last CTA builds the table and the output descriptors
             gf::fused_partition_kernel<Shape, Acc, Cls, Upd><<<nt, Shape::kThreads, m_smem, w.s>>>(
                 acc, cls, upd, w.seedMixed, w.C, gf::FastDiv(w.C), w.slots, w.tiles, nt, m_bins, w.reserved, bound,
                 w.totals, w.portChunks, w.maxK, w.ctl, desc, w.status, fin);
         }
-        wave_route_kernel<<<gridFor(bound), 256, 0, w.s>>>(w.descs, w.numOut, bound, routesDev, m_bins, w.L, next,
-                                                          w.status);
-        gf::pool_settle_kernel<<<1, gf::kPoolThreads, 0, w.s>>>(w.pool, w.reserved, bound, w.numOut, 0u, ids, 1u,
-                                                                nullptr, k, w.status);
+        wave_partition_post_kernel<<<gridFor(bound), 256, 0, w.s>>>(w.descs, w.numOut, bound, routesDev, m_bins, w.L,
+                                                                   next, w.pool, w.reserved, ids, k, w.status);
         cuda::check(cudaGetLastError(), "device-resident partition launch");
-        w.launches += 5u;
+        w.launches += 3u;
         ++w.partitionBatches;
         ++w.batches;
     }
