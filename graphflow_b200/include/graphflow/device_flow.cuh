@@ -10,16 +10,17 @@
 // batches of at most Q chunks and decides per batch on the host; both reach every particle with the
 // same functor calls, since every draw is keyed by the particle (rng/ParticleRng.hpp:57-94).
 //   source     wave 0: reserves ceil(n / C) chunks, generates ids 0..n-1 into them;
-//   partition  tiles of 1024 particles from the list; outputChunkBound(particles, C, B) chunks
-//              reserved from the device pool (the credit of GraphRunner.hpp:1014-1037); one fused
-//              classify -> scan -> scatter launch (gf_partition.cuh) that also publishes the
-//              output descriptors; a route kernel appends every output chunk to the list of the
-//              node its port feeds; the settle kernel returns the unused reservations and releases
-//              the input chunks;
-//   transform  the functor applied in place (the reference's TransformKernel copies into a dense
-//              concatenation, Execution.hpp:694-776; the particles and their order inside a chunk
-//              are the same), the chunks forwarded to the next node;
-//   sink       the functor over every particle, then the chunks are released.
+//   partition  three launches: tiles of 1024 particles from the list with the reservation of
+//              outputChunkBound(particles, C, B) chunks from the device pool (the credit of
+//              GraphRunner.hpp:1014-1037); one fused classify -> scan -> scatter launch that also
+//              publishes the output descriptors (the cooperative any-payload kernel of
+//              gf_fused_any.cuh for large batches, the per-tile kernel of gf_partition.cuh
+//              otherwise); every output chunk appended to the list of the node its port feeds, with
+//              the unused reservations returned and the input chunks released;
+//   transform  two launches: tiles with the chunks forwarded to the next node, then the functor
+//              applied in place (the reference's TransformKernel copies into a dense concatenation,
+//              Execution.hpp:694-776; the particles and their order inside a chunk are the same);
+//   sink       two launches: tiles with the chunks released, then the functor over every particle.
 // Pool: 2 (ceil(n / C) + sum of port counts + 2) + max ports + 16 chunks cover the chunks that hold
 // particles at a wave boundary (full chunks and at most one partial chunk per port and producer)
 // plus one batch's reservation. Exhaustion fails the run with GF_OVERFLOW (no waiting).
