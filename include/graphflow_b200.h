@@ -135,7 +135,11 @@ uint32_t gf_supported_tile_sizes(uint32_t* h_sizes, uint32_t cap);
  *                the scatter groups each tile's records of ports below 2048 by port and places
  *                rarer ports one record at a time); 0 = the per-tile open-addressing table
  *                kernels (graph/BinTable.hpp design). Counts, the plan and every port's record
- *                multiset are identical; the order inside a port is arrival order either way. */
+ *                multiset are identical; the order inside a port is arrival order either way.
+ *   "spin_limit" polls (default 2^20; 0 or less restores it) = how often a wait between CTAs of the
+ *                fused partition kernels polls before it gives up with GF_ERR_TIMEOUT (a short
+ *                limit lets a test make a wait run out); sets a device variable, so it needs a GPU.
+ * Unknown names and out-of-range values return GF_ERR_ARGUMENT. */
 gf_status gf_set_tuning(const char* name, int value);
 
 /* ---- dense partition: the reference's two-launch form --------------------------------------- */

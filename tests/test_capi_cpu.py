@@ -1,6 +1,7 @@
 """CPU-side checks of the C ABI: the library loads, exports every symbol the public header
 declares, and its host planning entry points agree with the oracle (no device work here)."""
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -109,3 +110,23 @@ def test_device_pool_host_checks():
     assert L.gf_device_pool_read(None, None, None) == capi.GF_ERR_ARGUMENT
     assert L.gf_run_dense_chain_device(1, 10, 5, 1, 0, 1.1, None, None, None, None) == capi.GF_ERR_ARGUMENT
     assert L.gf_run_dense_chain_device(1, 10, 8, 5, 0, 1.1, None, None, None, None) == capi.GF_ERR_ARGUMENT
+
+
+def test_every_documented_knob_is_accepted():
+    """Each tuning knob the public header documents is a name gf_set_tuning accepts (set to its
+    documented default here; spin_limit writes a device variable and is left to the GPU tests)."""
+    import re
+    header = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                               "graphflow_b200.h")).read()
+    section = header[header.index("Process-wide tuning knobs"):header.index("gf_status gf_set_tuning")]
+    knobs = re.findall(r'\*\s+"([a-z_]+)"\s+([0-9.]+)?', section)
+    assert len(knobs) >= 9
+    L = capi.lib()
+    for name, default in knobs:
+        if name == "spin_limit":
+            continue
+        m = re.search(r'"%s"\s+\S*\s*\(default (\d+)\)' % name, section) or \
+            re.search(r'"%s"\s+(\d+)\s+\(default\)' % name, section)
+        assert m, name
+        assert L.gf_set_tuning(name.encode(), int(m.group(1))) == capi.GF_OK, name
+
