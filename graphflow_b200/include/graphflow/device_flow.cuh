@@ -6,7 +6,10 @@
 // memory, in two sets: at a wave's start the host reads one small block (each list's chunk and
 // particle counts, the status word) and then, for every node whose list holds chunks, enqueues the
 // node's whole input as one batch on one stream; outputs are appended to the other set, which the
-// next wave consumes. The reference's runner (sched/GraphRunner.hpp:762-1171) instead dispatches
+// next wave consumes. A transform forwards all its chunks to one node, so when that node comes later
+// in the wave's node order (the runner orders every transform before its successor where the graph
+// allows) the chunks join the successor's input of the same wave instead: a run of transforms and
+// the node after them take one wave. The reference's runner (sched/GraphRunner.hpp:762-1171) instead dispatches
 // batches of at most Q chunks and decides per batch on the host; both reach every particle with the
 // same functor calls, since every draw is keyed by the particle (rng/ParticleRng.hpp:57-94).
 //   source     wave 0: reserves ceil(n / C) chunks, generates ids 0..n-1 into them;
@@ -73,6 +76,19 @@ __device__ inline void appendChunk(const Lists& L, std::uint32_t set, std::uint3
     atomicAdd(&L.particles[set * L.N + j], static_cast<unsigned long long>(fill));
 }
 
+// Zeroes the counters of list set `set` (kNoList: none) for its use as the next wave's output set.
+// The first prep kernel of a wave runs it on the set the wave reads: the host has copied those
+// counters before the wave's launches, and no kernel of the wave reads them on the device.
+__device__ inline void clearSet(const Lists& L, std::uint32_t set)
+{
+    if (set >= 2u)
+        return;
+    for (std::uint32_t j = threadIdx.x; j < L.N; j += blockDim.x) {
+        L.counts[set * L.N + j] = 0u;
+        L.particles[set * L.N + j] = 0ull;
+    }
+}
+
 // Source: particle i (id i) at slot i mod C of chunk chunk_of[i / C].
 template <typename TFunctor, typename TView>
 __global__ void __launch_bounds__(256)
@@ -133,16 +149,17 @@ __device__ inline void buildMoveTiles(const std::uint32_t* ids, const std::uint3
 }
 
 // Partition, before the partition kernel: its tiles; in block 0 the reservation of `bound` output
-// chunks and, for the per-tile kernel, the control block's three reset words.
+// chunks, for the per-tile kernel the control block's three reset words, and clearSet(clear).
 __global__ void wave_partition_prep_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
                                            std::uint32_t T, std::uint32_t tp, gf_tile* tiles, gf::DevicePoolHdr* pool,
-                                           std::uint32_t bound, std::uint32_t* reserved, gf::FusedCtl* ctl,
-                                           std::uint32_t* status)
+                                           std::uint32_t bound, std::uint32_t* reserved, gf::FusedCtl* ctl, Lists L,
+                                           std::uint32_t clear, std::uint32_t* status)
 {
     buildTiles(ids, fills, k, T, tp, tiles);
     if (blockIdx.x == 0) {
         if (ctl != nullptr && threadIdx.x < gf::kFusedCtlResetBytes / 4u)
             reinterpret_cast<std::uint32_t*>(ctl)[threadIdx.x] = 0u;
+        clearSet(L, clear);
         gf::pool_acquire_block(pool, bound, reserved, status);
     }
 }
@@ -170,27 +187,41 @@ __global__ void wave_partition_post_kernel(const gf_out_desc* descs, const std::
         gf::pool_settle_block(pool, reserved, cap_out, num_out, 0u, ids, 1u, nullptr, k, status);
 }
 
-// Sink, before the sink kernel: its tiles; in block 0 the k input chunks released. Releasing them
-// before the sink reads them is safe in stream order: the next acquisition, which could hand them
-// out again, comes after the sink kernel.
+// Sink, before the sink kernel: its tiles; in block 0 clearSet(clear) and the k input chunks
+// released. Releasing them before the sink reads them is safe in stream order: the next
+// acquisition, which could hand them out again, comes after the sink kernel.
 __global__ void wave_sink_prep_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
                                       std::uint32_t C, std::uint32_t T, std::uint32_t tp, MoveTile* tiles,
-                                      gf::DevicePoolHdr* pool, std::uint32_t* status)
+                                      gf::DevicePoolHdr* pool, Lists L, std::uint32_t clear, std::uint32_t* status)
+{
+    buildMoveTiles(ids, fills, k, C, T, tp, tiles);
+    if (blockIdx.x == 0) {
+        clearSet(L, clear);
+        gf::pool_settle_block(pool, nullptr, 0u, nullptr, 0u, ids, 1u, nullptr, k, status);
+    }
+}
+
+// Transform, before the transform kernel: its tiles, the k chunks (changed in place by the kernel
+// that follows) forwarded to list `to` of set `to_set`, and in block 0 clearSet(clear). With base
+// == kNoList the chunks are appended (counters of to_set, the next wave's set); otherwise they are
+// written at entries base .. base + k - 1 of the list, whose count the host keeps (the successor
+// runs later in the same wave).
+__global__ void wave_transform_prep_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
+                                           std::uint32_t C, std::uint32_t T, std::uint32_t tp, MoveTile* tiles,
+                                           Lists L, std::uint32_t to_set, std::uint32_t to, std::uint32_t base,
+                                           std::uint32_t clear, std::uint32_t* status)
 {
     buildMoveTiles(ids, fills, k, C, T, tp, tiles);
     if (blockIdx.x == 0)
-        gf::pool_settle_block(pool, nullptr, 0u, nullptr, 0u, ids, 1u, nullptr, k, status);
-}
-
-// Transform, before the transform kernel: its tiles, and the k chunks (changed in place by the
-// kernel that follows) appended to list `to` of set `to_set` for the next wave.
-__global__ void wave_transform_prep_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
-                                           std::uint32_t C, std::uint32_t T, std::uint32_t tp, MoveTile* tiles,
-                                           Lists L, std::uint32_t to_set, std::uint32_t to, std::uint32_t* status)
-{
-    buildMoveTiles(ids, fills, k, C, T, tp, tiles);
-    for (std::uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < k; f += gridDim.x * blockDim.x)
-        appendChunk(L, to_set, to, ids[f], fills[f], status);
+        clearSet(L, clear);
+    for (std::uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < k; f += gridDim.x * blockDim.x) {
+        if (base == kNoList) {
+            appendChunk(L, to_set, to, ids[f], fills[f], status);
+        } else {
+            L.ids[L.at(to_set, to) + base + f] = ids[f];
+            L.fills[L.at(to_set, to) + base + f] = fills[f];
+        }
+    }
 }
 
 } // namespace
@@ -228,6 +259,19 @@ struct WaveContext {
     std::uint64_t coopScratchBytes = 0u;
     std::uint32_t coopMaxCtas = 0u;
     int sms = 1;
+    // the host's copy of the counts of the set the wave reads, and every node's position in the
+    // wave's order: a transform whose successor comes later forwards into that set (same wave)
+    std::uint32_t* waveCounts = nullptr;
+    unsigned long long* waveParticles = nullptr;
+    const std::uint32_t* order = nullptr;
+    // the list set the wave's first prep kernel zeroes (clearSet), kNoList once one has
+    std::uint32_t pendingClear = kNoList;
+    std::uint32_t takeClearSet()
+    {
+        const std::uint32_t c = pendingClear;
+        pendingClear = kNoList;
+        return c;
+    }
     std::uint64_t launches = 0u, partitionBatches = 0u, batches = 0u, sunk = 0u, coopBatches = 0u;
 };
 
@@ -248,6 +292,8 @@ public:
                      const std::uint32_t* routesDev) = 0;
     virtual std::uint32_t bins() const { return 1u; }
     virtual void bind(std::uint32_t) {}
+    // true when every input chunk goes on, unchanged in count, to routes[0] (a transform)
+    virtual bool forwardsAll() const { return false; }
 };
 
 template <typename TStorage, typename TFunctor>
@@ -285,14 +331,26 @@ template <typename TStorage, typename TFunctor>
 class TransformWave final : public WaveNode {
 public:
     TransformWave(TStorage& st, TFunctor f, std::uint32_t purpose) : m_st(st), m_f(std::move(f)), m_purpose(purpose) {}
-    void run(WaveContext& w, std::uint32_t self, std::uint32_t k, std::uint64_t, std::uint32_t cur,
+    bool forwardsAll() const override { return true; }
+    void run(WaveContext& w, std::uint32_t self, std::uint32_t k, std::uint64_t particles, std::uint32_t cur,
              std::uint32_t next, const std::vector<std::uint32_t>& routes, const std::uint32_t*) override
     {
         const std::uint32_t* ids = w.L.ids + w.L.at(cur, self);
         const std::uint32_t* fills = w.L.fills + w.L.at(cur, self);
         const std::uint32_t nt = k * w.tp;
+        const std::uint32_t to = routes[0];
+        std::uint32_t toSet = next, base = kNoList;
+        if (w.waveCounts != nullptr && to < w.L.N && w.order[to] > w.order[self]) {
+            // the successor runs later in this wave: its input list of this wave grows by k chunks
+            base = w.waveCounts[to];
+            if (static_cast<std::uint64_t>(base) + k > w.L.cap)
+                throw BatchError("graphflow: device-resident list overflow");
+            toSet = cur;
+            w.waveCounts[to] = base + k;
+            w.waveParticles[to] += particles;
+        }
         wave_transform_prep_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.C, w.T, w.tp, w.moveTiles, w.L,
-                                                                 next, routes[0], w.status);
+                                                                 toSet, to, base, w.takeClearSet(), w.status);
         transform_kernel<<<nt, 256, 0, w.s>>>(m_f, m_st.view(), w.seedMixed, m_purpose, w.moveTiles, nt, ids, k, w.C,
                                               gf::FastDiv(w.C), w.slots, w.status);
         cuda::check(cudaGetLastError(), "device-resident transform launch");
@@ -317,7 +375,7 @@ public:
         const std::uint32_t* fills = w.L.fills + w.L.at(cur, self);
         const std::uint32_t nt = k * w.tp;
         wave_sink_prep_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.C, w.T, w.tp, w.moveTiles, w.pool,
-                                                            w.status);
+                                                            w.L, w.takeClearSet(), w.status);
         sink_kernel<<<nt, 256, 0, w.s>>>(m_f, m_st.view(), w.seedMixed, m_purpose, w.moveTiles, nt, w.C, w.slots,
                                          w.status);
         cuda::check(cudaGetLastError(), "device-resident sink launch");
@@ -379,7 +437,8 @@ public:
         const bool coop =
             w.coopScratch != nullptr && m_bins <= gf::kAnyCoopMaxBins && nt >= kCoopMinTiles;
         wave_partition_prep_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.T, w.tp, w.tiles, w.pool, bound,
-                                                                 w.reserved, coop ? nullptr : w.ctl, w.status);
+                                                                 w.reserved, coop ? nullptr : w.ctl, w.L,
+                                                                 w.takeClearSet(), w.status);
         const Acc acc{m_st.view()};
         const Cls cls{m_cls, w.seedMixed, m_purpose, w.status};
         const Upd upd{m_upd, m_purpose + 1u, w.status};

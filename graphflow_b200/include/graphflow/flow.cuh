@@ -464,6 +464,33 @@ private:
         w.coopMaxCtas = coopCtas;
         w.sms = sms;
         w.launches = 1u;
+        // the wave's node order: along every transform edge (a transform forwards all its chunks to
+        // one node) the successor comes later, so a particle passes a run of transforms and the
+        // node after them in one wave; nodes on a cycle of transforms alone keep their index order
+        std::vector<std::uint32_t> order(N, 0u), seq;
+        {
+            std::vector<std::uint32_t> indeg(N, 0u);
+            for (std::uint32_t k = 0; k < N; ++k)
+                if (waves[k]->forwardsAll() && !routes[k].empty() && routes[k][0] < N && routes[k][0] != k)
+                    ++indeg[routes[k][0]];
+            std::vector<char> placed(N, 0);
+            for (std::uint32_t k = 0; k < N; ++k)
+                for (std::uint32_t v = k; v < N && indeg[v] == 0u && !placed[v];) {
+                    placed[v] = 1;
+                    seq.push_back(v);
+                    if (!waves[v]->forwardsAll() || routes[v].empty() || routes[v][0] >= N || routes[v][0] == v)
+                        break;
+                    v = routes[v][0];
+                    --indeg[v];
+                }
+            for (std::uint32_t k = 0; k < N; ++k)
+                if (!placed[k])
+                    seq.push_back(k);
+            for (std::uint32_t i = 0; i < N; ++i)
+                order[seq[i]] = i;
+        }
+        std::vector<std::uint32_t> waveCounts(N, 0u);
+        std::vector<unsigned long long> waveParticles(N, 0u);
         std::uint32_t next = 1u;
         if (itemCount != 0u)
             waves[*m_sourceKey]->generate(w, itemCount, next, routes[*m_sourceKey][0]);
@@ -492,11 +519,19 @@ private:
                                           std::to_string(wavesRun - 1u) + " waves");
             const std::uint32_t cur = next;
             next = 1u - cur;
-            cuda::check(cudaMemsetAsync(w.L.counts + next * N, 0, N * 4u, s), "memset");
-            cuda::check(cudaMemsetAsync(w.L.particles + next * N, 0, N * 8u, s), "memset");
-            for (std::uint32_t k = 0; k < N; ++k)
-                if (counts[cur * N + k] != 0u)
-                    waves[k]->run(w, k, counts[cur * N + k], parts[cur * N + k], cur, next, routes[k],
+            // set `next` was cleared by the previous wave (or the initial memset); the first prep
+            // kernel of this wave clears set `cur`, whose counters the host has just read
+            w.pendingClear = cur;
+            for (std::uint32_t k = 0; k < N; ++k) {
+                waveCounts[k] = counts[cur * N + k];
+                waveParticles[k] = parts[cur * N + k];
+            }
+            w.waveCounts = waveCounts.data();
+            w.waveParticles = waveParticles.data();
+            w.order = order.data();
+            for (const std::uint32_t k : seq)
+                if (waveCounts[k] != 0u)
+                    waves[k]->run(w, k, waveCounts[k], waveParticles[k], cur, next, routes[k],
                                   routesDev.data() + routeOffset[k]);
         }
         gf::DevicePoolHdr hdr{};

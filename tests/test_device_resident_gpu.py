@@ -87,6 +87,9 @@ def test_photon_flow_equals_fused_transport(model, fp64):
     for k in ("event", "scatter_count", "weight", "cos_exit", "position"):
         assert np.array_equal(a[k], b[k]), k
     assert a["stats"].generated == n and a["stats"].sunk == n
+    # scatter -> propose flight -> advance and route run in one wave (transforms forward into the
+    # same wave), so a photon takes one wave per scattering plus its first flight and its sink
+    assert a["stats"].loop_iterations <= int(b["scatter_count"].max()) + 2
 
 
 @pytest.mark.parametrize("bins,dist", [(64, "balanced"), (1024, "one-hot")])
@@ -132,3 +135,5 @@ def test_set_transform_device_resident(n, c):
                                                      batch_chunks=1)
     assert st.sunk == n
     assert np.all(weights == 1234) and np.all(visits == 1)
+    # the transform forwards into the sink's input of the same wave: one wave for the whole run
+    assert st.loop_iterations == (1 if n else 0)
