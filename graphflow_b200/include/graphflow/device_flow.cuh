@@ -9,9 +9,10 @@
 // next wave consumes. A transform forwards all its chunks to one node, so when that node comes later
 // in the wave's node order (the runner orders every transform before its successor where the graph
 // allows) the chunks join the successor's input of the same wave instead: a run of transforms and
-// the node after them take one wave. The reference's runner (sched/GraphRunner.hpp:762-1171) instead dispatches
-// batches of at most Q chunks and decides per batch on the host; both reach every particle with the
-// same functor calls, since every draw is keyed by the particle (rng/ParticleRng.hpp:57-94).
+// the node after them take one wave. The reference's runner (sched/GraphRunner.hpp:762-1171)
+// instead dispatches batches of at most Q chunks and decides per batch on the host; both reach
+// every particle with the same functor calls, since every draw is keyed by the particle
+// (rng/ParticleRng.hpp:57-94).
 //   source     wave 0: reserves ceil(n / C) chunks, generates ids 0..n-1 into them;
 //   partition  three launches: tiles of 1024 particles from the list with the reservation of
 //              outputChunkBound(particles, C, B) chunks from the device pool (the credit of
@@ -20,10 +21,10 @@
 //              gf_fused_any.cuh for large batches, the per-tile kernel of gf_partition.cuh
 //              otherwise); every output chunk appended to the list of the node its port feeds, with
 //              the unused reservations returned and the input chunks released;
-//   transform  two launches: tiles with the chunks forwarded to the next node, then the functor
-//              applied in place (the reference's TransformKernel copies into a dense concatenation,
+//   transform  one launch: the functor applied in place and the chunks forwarded to the next node
+//              (the reference's TransformKernel copies into a dense concatenation,
 //              Execution.hpp:694-776; the particles and their order inside a chunk are the same);
-//   sink       two launches: tiles with the chunks released, then the functor over every particle.
+//   sink       one launch: the functor over every particle and the chunks released.
 // Pool: 2 (ceil(n / C) + sum of port counts + 2) + max ports + 16 chunks cover the chunks that hold
 // particles at a wave boundary (full chunks and at most one partial chunk per port and producer)
 // plus one batch's reservation. Exhaustion fails the run with GF_OVERFLOW (no waiting).
@@ -136,18 +137,6 @@ __device__ inline void buildTiles(const std::uint32_t* ids, const std::uint32_t*
     }
 }
 
-// The same tiles as MoveTile with out_pos = f C + offset: with out_chunks = ids, the transform
-// kernel writes every particle back to its own slot.
-__device__ inline void buildMoveTiles(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
-                                      std::uint32_t C, std::uint32_t T, std::uint32_t tp, MoveTile* tiles)
-{
-    const std::uint32_t total = k * tp;
-    for (std::uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        const std::uint32_t f = t / tp, j = t - f * tp, off = j * T, fill = fills[f];
-        tiles[t] = MoveTile{ids[f], off, fill > off ? (fill - off < T ? fill - off : T) : 0u, f * C + off};
-    }
-}
-
 // Partition, before the partition kernel: its tiles; in block 0 the reservation of `bound` output
 // chunks, for the per-tile kernel the control block's three reset words, and clearSet(clear).
 __global__ void wave_partition_prep_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
@@ -187,40 +176,77 @@ __global__ void wave_partition_post_kernel(const gf_out_desc* descs, const std::
         gf::pool_settle_block(pool, reserved, cap_out, num_out, 0u, ids, 1u, nullptr, k, status);
 }
 
-// Sink, before the sink kernel: its tiles; in block 0 clearSet(clear) and the k input chunks
-// released. Releasing them before the sink reads them is safe in stream order: the next
-// acquisition, which could hand them out again, comes after the sink kernel.
-__global__ void wave_sink_prep_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
-                                      std::uint32_t C, std::uint32_t T, std::uint32_t tp, MoveTile* tiles,
-                                      gf::DevicePoolHdr* pool, Lists L, std::uint32_t clear, std::uint32_t* status)
+// The transform in one launch: block t runs tile t of the k entries (entry f = t / tp, particles
+// [j T, min(fill, (j + 1) T)) of chunk ids[f], j = t - f tp), applying the functor in place (each
+// particle back to its own slot, as transform_kernel with out_chunks = ids); block 0 runs
+// clearSet(clear). Thread 0 of entry f's first tile forwards the entry to list `to` of set
+// `to_set`: with base == kNoList appended (counters of to_set, the next wave's set), otherwise
+// written at entry base + f of the list, whose count the host keeps (the successor runs later in
+// the same wave). The successor reads the chunk in a later launch.
+template <typename TFunctor, typename TView>
+__global__ void __launch_bounds__(256)
+    wave_transform_kernel(TFunctor f, TView view, std::uint64_t seed_mixed, std::uint32_t purpose,
+                          const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k, std::uint32_t C,
+                          std::uint32_t T, std::uint32_t tp, std::uint64_t slots, Lists L, std::uint32_t to_set,
+                          std::uint32_t to, std::uint32_t base, std::uint32_t clear, std::uint32_t* status)
 {
-    buildMoveTiles(ids, fills, k, C, T, tp, tiles);
-    if (blockIdx.x == 0) {
+    if (blockIdx.x == 0)
         clearSet(L, clear);
-        gf::pool_settle_block(pool, nullptr, 0u, nullptr, 0u, ids, 1u, nullptr, k, status);
+    for (std::uint32_t t = blockIdx.x; t < k * tp; t += gridDim.x) {
+        const std::uint32_t e = t / tp, off = (t - e * tp) * T, fill = fills[e], chunk = ids[e];
+        const std::uint32_t count = fill > off ? (fill - off < T ? fill - off : T) : 0u;
+        if (off == 0u && threadIdx.x == 0u) {
+            if (base == kNoList) {
+                appendChunk(L, to_set, to, chunk, fill, status);
+            } else {
+                L.ids[L.at(to_set, to) + base + e] = chunk;
+                L.fills[L.at(to_set, to) + base + e] = fill;
+            }
+        }
+        const std::uint64_t in_base = static_cast<std::uint64_t>(chunk) * C + off;
+        for (std::uint32_t i = threadIdx.x; i < count; i += blockDim.x) {
+            if (in_base + i >= slots) {
+                gf::set_status(status, GF_INVALID);
+                continue;
+            }
+            auto p = view.load(in_base + i);
+            rng::Engine engine = rng::engineFor(seed_mixed, p, purpose);
+            Status st(status);
+            applyTransform(f, engine, st, p);
+            view.store(in_base + i, p);
+        }
     }
 }
 
-// Transform, before the transform kernel: its tiles, the k chunks (changed in place by the kernel
-// that follows) forwarded to list `to` of set `to_set`, and in block 0 clearSet(clear). With base
-// == kNoList the chunks are appended (counters of to_set, the next wave's set); otherwise they are
-// written at entries base .. base + k - 1 of the list, whose count the host keeps (the successor
-// runs later in the same wave).
-__global__ void wave_transform_prep_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
-                                           std::uint32_t C, std::uint32_t T, std::uint32_t tp, MoveTile* tiles,
-                                           Lists L, std::uint32_t to_set, std::uint32_t to, std::uint32_t base,
-                                           std::uint32_t clear, std::uint32_t* status)
+// The sink in one launch: tiles as wave_transform_kernel, the functor over every particle; block 0
+// runs clearSet(clear) and releases the k input chunks. Releasing them while other blocks still
+// read them is safe in stream order: the next acquisition, which could hand them out again, comes
+// after this launch.
+template <typename TFunctor, typename TView>
+__global__ void __launch_bounds__(256)
+    wave_sink_kernel(TFunctor f, TView view, std::uint64_t seed_mixed, std::uint32_t purpose,
+                     const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k, std::uint32_t C,
+                     std::uint32_t T, std::uint32_t tp, std::uint64_t slots, gf::DevicePoolHdr* pool, Lists L,
+                     std::uint32_t clear, std::uint32_t* status)
 {
-    buildMoveTiles(ids, fills, k, C, T, tp, tiles);
-    if (blockIdx.x == 0)
-        clearSet(L, clear);
-    for (std::uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < k; f += gridDim.x * blockDim.x) {
-        if (base == kNoList) {
-            appendChunk(L, to_set, to, ids[f], fills[f], status);
-        } else {
-            L.ids[L.at(to_set, to) + base + f] = ids[f];
-            L.fills[L.at(to_set, to) + base + f] = fills[f];
+    for (std::uint32_t t = blockIdx.x; t < k * tp; t += gridDim.x) {
+        const std::uint32_t e = t / tp, off = (t - e * tp) * T, fill = fills[e];
+        const std::uint32_t count = fill > off ? (fill - off < T ? fill - off : T) : 0u;
+        const std::uint64_t in_base = static_cast<std::uint64_t>(ids[e]) * C + off;
+        for (std::uint32_t i = threadIdx.x; i < count; i += blockDim.x) {
+            if (in_base + i >= slots) {
+                gf::set_status(status, GF_INVALID);
+                continue;
+            }
+            const auto p = view.load(in_base + i);
+            rng::Engine engine = rng::engineFor(seed_mixed, p, purpose);
+            Status st(status);
+            invokeWithContext(f, engine, st, p);
         }
+    }
+    if (blockIdx.x == 0) {
+        clearSet(L, clear);
+        gf::pool_settle_block(pool, nullptr, 0u, nullptr, 0u, ids, 1u, nullptr, k, status);
     }
 }
 
@@ -244,7 +270,6 @@ struct WaveContext {
     std::uint64_t slots = 0u;
     std::uint64_t seedMixed = 0u;
     gf_tile* tiles = nullptr;
-    MoveTile* moveTiles = nullptr;
     std::uint32_t* reserved = nullptr;
     std::uint32_t* totals = nullptr;
     unsigned long long* portChunks = nullptr;
@@ -349,12 +374,10 @@ public:
             w.waveCounts[to] = base + k;
             w.waveParticles[to] += particles;
         }
-        wave_transform_prep_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.C, w.T, w.tp, w.moveTiles, w.L,
-                                                                 toSet, to, base, w.takeClearSet(), w.status);
-        transform_kernel<<<nt, 256, 0, w.s>>>(m_f, m_st.view(), w.seedMixed, m_purpose, w.moveTiles, nt, ids, k, w.C,
-                                              gf::FastDiv(w.C), w.slots, w.status);
+        wave_transform_kernel<<<nt, 256, 0, w.s>>>(m_f, m_st.view(), w.seedMixed, m_purpose, ids, fills, k, w.C, w.T,
+                                                   w.tp, w.slots, w.L, toSet, to, base, w.takeClearSet(), w.status);
         cuda::check(cudaGetLastError(), "device-resident transform launch");
-        w.launches += 2u;
+        ++w.launches;
         ++w.batches;
     }
 
@@ -374,12 +397,10 @@ public:
         const std::uint32_t* ids = w.L.ids + w.L.at(cur, self);
         const std::uint32_t* fills = w.L.fills + w.L.at(cur, self);
         const std::uint32_t nt = k * w.tp;
-        wave_sink_prep_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.C, w.T, w.tp, w.moveTiles, w.pool,
-                                                            w.L, w.takeClearSet(), w.status);
-        sink_kernel<<<nt, 256, 0, w.s>>>(m_f, m_st.view(), w.seedMixed, m_purpose, w.moveTiles, nt, w.C, w.slots,
-                                         w.status);
+        wave_sink_kernel<<<nt, 256, 0, w.s>>>(m_f, m_st.view(), w.seedMixed, m_purpose, ids, fills, k, w.C, w.T, w.tp,
+                                              w.slots, w.pool, w.L, w.takeClearSet(), w.status);
         cuda::check(cudaGetLastError(), "device-resident sink launch");
-        w.launches += 2u;
+        ++w.launches;
         w.sunk += particles;
         ++w.batches;
     }

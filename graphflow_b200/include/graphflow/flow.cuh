@@ -401,7 +401,6 @@ private:
         cuda::Buffer<unsigned char> pool(gf::device_pool_bytes(S));
         const std::size_t tiles = static_cast<std::size_t>(S) * tp;
         cuda::Buffer<gf_tile> tileBuf(tiles);
-        cuda::Buffer<MoveTile> moveBuf(tiles);
         const std::uint32_t descCap = S + maxBins;
         cuda::Buffer<std::uint32_t> reserved(descCap), table(maxBins + descCap), totals(maxBins), numOut(1);
         cuda::Buffer<gf_out_desc> descs(descCap);
@@ -449,7 +448,6 @@ private:
         w.slots = storage.slotCount();
         w.seedMixed = gf::mix64(config.seed);
         w.tiles = tileBuf.data();
-        w.moveTiles = moveBuf.data();
         w.reserved = reserved.data();
         w.totals = totals.data();
         w.portChunks = portChunks.data();
