@@ -60,6 +60,8 @@ def parse():
                         "B=--bins (profiling)")
     p.add_argument("--feedback-device-resident", action="store_true",
                    help="one particle_feedback run through the Flow device-resident at N=--n, C=8192 (profiling)")
+    p.add_argument("--photon-device-resident", action="store_true",
+                   help="one photon run through the Flow device-resident at N=--n (profiling)")
     p.add_argument("--flow-chain", type=int, default=0, metavar="NODES",
                    help="only run the dense chain of NODES partition nodes through the Flow on --n keys (--bins, "
                         "--dist, C=8192, P=16384, Q=8, partition groups) and print its counters; for profiling")
@@ -1126,6 +1128,21 @@ def feedback_device_resident_only(args):
                       "partition_batches": st.partition_batches, "sunk": st.sunk}))
 
 
+def photon_device_resident_only(args):
+    """One photon_scattering run (weighted HG slab, FP32, seed 42) through the Flow device-resident,
+    for profiling its launches."""
+    from graphflow_b200 import capi
+    p = capi.photon_params()
+    capi.check(capi.lib().gf_set_tuning(b"device_resident", 1), "tuning")
+    try:
+        st = capi.run_photon(SEED, args.n, p, exec_mode=capi.EXEC_FLOW, records=False)["stats"]
+    finally:
+        capi.check(capi.lib().gf_set_tuning(b"device_resident", 0), "tuning")
+    print(json.dumps({"workload": f"photon slab through the Flow device-resident, N={args.n}",
+                      "seconds": st.seconds, "waves": st.loop_iterations, "kernel_launches": st.kernel_launches,
+                      "partition_batches": st.partition_batches, "sunk": st.sunk}))
+
+
 def device_chain_only(args):
     """One run of the dense chain on the device (seed 42, C = 8192), for profiling its launches."""
     from graphflow_b200 import capi
@@ -1144,6 +1161,9 @@ def main():
         return
     if args.feedback_device_resident:
         feedback_device_resident_only(args)
+        return
+    if args.photon_device_resident:
+        photon_device_resident_only(args)
         return
     if args.flow_chain:
         flow_chain_only(args)
