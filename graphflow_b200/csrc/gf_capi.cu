@@ -323,7 +323,7 @@ gf_status fused_u32(void* stream, const uint32_t* d_keys_in, uint32_t* d_keys_ou
         KeyClassify<Acc> cls{key_classifier(classifier, bins)};
         kernel<<<n_tiles, Shape::kThreads, smem, as_stream(stream)>>>(
             acc, cls, NoUpdate{}, 0u, capacity, FastDiv(capacity), pool_slots, d_tiles, n_tiles, bins, d_reserved,
-            n_reserved, d_totals, d_port_chunks, max_chunks_per_port, ctl, desc, d_status, fin);
+            n_reserved, d_totals, d_port_chunks, max_chunks_per_port, ctl, desc, d_status, fin, NoPost{});
         return cuda_status(cudaGetLastError());
     });
 }

@@ -256,7 +256,7 @@ inline std::uint32_t enqueueDeviceChain(cudaStream_t s, char* base, const Device
             kernel<<<nTiles, ChainShape::kThreads, smem, s>>>(
                 cols, ShiftPort{8u * node, FastDiv(bins)}, NoUpdate{}, 0u, kChainCapacity, fdc, L.slots, tiles, nTiles,
                 bins, reserved, bound, nodeTotals, portChunks, static_cast<std::uint32_t>(L.maxK), ctl, desc, status,
-                InlineFinish{table, out, bound, outCount});
+                InlineFinish{table, out, bound, outCount}, NoPost{});
         } else {
             check(cudaMemsetAsync(nodeTotals, 0, bins * 4u, s), "memset");
             fused_finish_kernel<FT><<<1, FT, fsmem, s>>>(nodeTotals, portChunks, bins, kChainCapacity, fdc,

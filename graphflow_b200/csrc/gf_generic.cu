@@ -439,7 +439,7 @@ extern "C" gf_status gf_partition_fused(void* stream, const gf_columns* h_cols, 
                     ViewAccess<V>{ViewOf<T, Layout>::make(*h_cols)}, cls, upd, gf::mix64(prm.seed), capacity,
                     gf::FastDiv(capacity), pool_slots, d_tiles, n_tiles, bins, d_reserved, n_reserved, d_totals,
                     d_port_chunks, max_chunks_per_port, ctl, reinterpret_cast<unsigned long long*>(ctl + 1), d_status,
-                    gf::InlineFinish{d_table, d_descs, desc_cap, d_num_out});
+                    gf::InlineFinish{d_table, d_descs, desc_cap, d_num_out}, gf::NoPost{});
                 return cuda_status(cudaGetLastError());
             });
         });

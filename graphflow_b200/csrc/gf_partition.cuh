@@ -607,12 +607,19 @@ GF_D void finish_plan(const uint32_t* totals, const unsigned long long* port_chu
         *num_out = carry;
 }
 
-template <typename Shape, typename Access, typename Classify, typename Update>
+// Work of the finishing CTA after an inline finish (all of its threads call it once the table,
+// descriptors and output count are written): none by default.
+struct NoPost {
+    static constexpr bool kActive = false;
+    GF_D void operator()(const InlineFinish&, uint32_t*) const {}
+};
+
+template <typename Shape, typename Access, typename Classify, typename Update, typename Post = NoPost>
 __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_partition_kernel(
     Access acc, Classify classify, Update update, uint64_t seed_mixed, uint32_t capacity, FastDiv fdc,
     uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B, const uint32_t* reserved,
     uint32_t n_reserved, uint32_t* totals, unsigned long long* port_chunks, uint32_t max_k, FusedCtl* ctl,
-    unsigned long long* desc, uint32_t* status, InlineFinish fin)
+    unsigned long long* desc, uint32_t* status, InlineFinish fin, Post post)
 {
     using P = typename Access::Payload;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -672,6 +679,10 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
                                      fin.desc_cap, fin.num_out, status, scratch, scratch + kSeg, kSeg, lb_flag);
         if (fin.done_rec != nullptr)
             publish_done(fin, ctl, totals, B, status);
+        if constexpr (Post::kActive) {
+            __syncthreads();
+            post(fin, status);
+        }
     };
     if (t >= n_tiles) {
         retire();

@@ -14,13 +14,14 @@
 // every particle with the same functor calls, since every draw is keyed by the particle
 // (rng/ParticleRng.hpp:57-94).
 //   source     wave 0: reserves ceil(n / C) chunks, generates ids 0..n-1 into them;
-//   partition  three launches: tiles of 1024 particles from the list with the reservation of
+//   partition  tiles of 1024 particles from the list with the reservation of
 //              outputChunkBound(particles, C, B) chunks from the device pool (the credit of
 //              GraphRunner.hpp:1014-1037); one fused classify -> scan -> scatter launch that also
-//              publishes the output descriptors (the cooperative any-payload kernel of
-//              gf_fused_any.cuh for large batches, the per-tile kernel of gf_partition.cuh
-//              otherwise); every output chunk appended to the list of the node its port feeds, with
-//              the unused reservations returned and the input chunks released;
+//              publishes the output descriptors; every output chunk appended to the list of the
+//              node its port feeds, with the unused reservations returned and the input chunks
+//              released. Large batches: three launches (the cooperative any-payload kernel of
+//              gf_fused_any.cuh between the tile and the routing launch); others two (the per-tile
+//              kernel of gf_partition.cuh, whose finishing CTA also routes and settles);
 //   transform  one launch: the functor applied in place and the chunks forwarded to the next node
 //              (the reference's TransformKernel copies into a dense concatenation,
 //              Execution.hpp:694-776; the particles and their order inside a chunk are the same);
@@ -250,6 +251,34 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// The routing and settle of wave_partition_post_kernel as the work of the per-tile partition
+// kernel's finishing CTA (after its inline finish): one launch fewer per partition batch.
+struct WavePost {
+    static constexpr bool kActive = true;
+    const std::uint32_t* route = nullptr;
+    std::uint32_t bins = 0u;
+    Lists L;
+    std::uint32_t set = 0u;
+    gf::DevicePoolHdr* pool = nullptr;
+    const std::uint32_t* reserved = nullptr;
+    const std::uint32_t* ids = nullptr;
+    std::uint32_t k = 0u;
+    __device__ void operator()(const gf::InlineFinish& fin, std::uint32_t* status) const
+    {
+        const std::uint32_t n = *fin.num_out, m = n < fin.desc_cap ? n : fin.desc_cap;
+        for (std::uint32_t f = threadIdx.x; f < m; f += blockDim.x) {
+            const gf_out_desc d = fin.descs[f];
+            if (d.bin >= bins || d.fill == 0u) {
+                if (d.bin >= bins)
+                    gf::set_status(status, GF_INVALID);
+                continue;
+            }
+            appendChunk(L, set, route[d.bin], d.chunk_index, d.fill, status);
+        }
+        gf::pool_settle_block(pool, reserved, fin.desc_cap, fin.num_out, 0u, ids, 1u, nullptr, k, status);
+    }
+};
+
 } // namespace
 
 inline unsigned gridFor(std::uint64_t items, unsigned threads = 256u, unsigned cap = 4096u)
@@ -432,10 +461,13 @@ public:
         int dev = 0, limit = 0;
         cuda::check(cudaGetDevice(&dev), "cudaGetDevice");
         cuda::check(cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "smem limit");
-        if (m_smem > static_cast<std::size_t>(limit))
+        cudaFuncAttributes fa{}; // the finishing CTA's settle adds a few bytes of static shared memory
+        cuda::check(cudaFuncGetAttributes(&fa, gf::fused_partition_kernel<Shape, Acc, Cls, Upd, WavePost>),
+                    "device-resident partition attributes");
+        if (m_smem + fa.sharedSizeBytes > static_cast<std::size_t>(limit))
             throw std::invalid_argument("graphflow: deviceResident runs dense fused partitions only; " +
                                         std::to_string(bins) + " ports do not fit one block's shared memory");
-        cuda::check(cudaFuncSetAttribute(gf::fused_partition_kernel<Shape, Acc, Cls, Upd>,
+        cuda::check(cudaFuncSetAttribute(gf::fused_partition_kernel<Shape, Acc, Cls, Upd, WavePost>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(m_smem)),
                     "device-resident partition attribute");
     }
@@ -471,17 +503,20 @@ public:
                                                              w.coopScratchBytes, w.coopMaxCtas, w.status, fin, w.sms),
                         "device-resident cooperative partition launch");
             ++w.coopBatches;
+            wave_partition_post_kernel<<<gridFor(bound), 256, 0, w.s>>>(w.descs, w.numOut, bound, routesDev, m_bins,
+                                                                       w.L, next, w.pool, w.reserved, ids, k, w.status);
+            ++w.launches;
         } else {
             auto* desc = reinterpret_cast<unsigned long long*>(w.ctl + 1); // reset words zeroed by the prep kernel
-            // the launch's last CTA builds the table and the output descriptors
-            gf::fused_partition_kernel<Shape, Acc, Cls, Upd><<<nt, Shape::kThreads, m_smem, w.s>>>(
+            // the launch's last CTA builds the table and the output descriptors, then routes them
+            // and settles the pool (WavePost)
+            const WavePost post{routesDev, m_bins, w.L, next, w.pool, w.reserved, ids, k};
+            gf::fused_partition_kernel<Shape, Acc, Cls, Upd, WavePost><<<nt, Shape::kThreads, m_smem, w.s>>>(
                 acc, cls, upd, w.seedMixed, w.C, gf::FastDiv(w.C), w.slots, w.tiles, nt, m_bins, w.reserved, bound,
-                w.totals, w.portChunks, w.maxK, w.ctl, desc, w.status, fin);
+                w.totals, w.portChunks, w.maxK, w.ctl, desc, w.status, fin, post);
         }
-        wave_partition_post_kernel<<<gridFor(bound), 256, 0, w.s>>>(w.descs, w.numOut, bound, routesDev, m_bins, w.L,
-                                                                   next, w.pool, w.reserved, ids, k, w.status);
         cuda::check(cudaGetLastError(), "device-resident partition launch");
-        w.launches += 3u;
+        w.launches += 2u;
         ++w.partitionBatches;
         ++w.batches;
     }

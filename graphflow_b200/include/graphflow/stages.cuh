@@ -438,7 +438,7 @@ public:
                 gf::fused_partition_kernel<Shape, Acc, Cls, Upd><<<m_numTiles, Shape::kThreads, m_smemFused, s>>>(
                     acc, cls, upd, m_seed, m_C, gf::FastDiv(m_C), m_st.slotCount(), tiles, m_numTiles, m_bins,
                     m_hinDev + 3u * m_tileCap, bound, io + m_oTotals, m_portChunks.data(), m_maxK, ctl, desc, status,
-                    fin);
+                    fin, gf::NoPost{});
                 cuda::check(cudaGetLastError(), "fused partition kernel launch");
             } else {
                 // an empty batch: nothing to run, the record is complete at once
