@@ -154,9 +154,10 @@ __global__ void wave_partition_prep_kernel(const std::uint32_t* ids, const std::
     }
 }
 
-// Partition, after the partition kernel: its published output chunks appended to the lists their
-// ports feed (route[bin]); in block 0 the unused reservations returned and the k input chunks
-// released (the partition kernel, earlier in the stream, has read them).
+// Partition, after the cooperative partition kernel (the per-tile kernel does the same in its
+// finishing CTA, WavePost): its published output chunks appended to the lists their ports feed
+// (route[bin]); in block 0 the unused reservations returned and the k input chunks released (the
+// partition kernel, earlier in the stream, has read them).
 __global__ void wave_partition_post_kernel(const gf_out_desc* descs, const std::uint32_t* num_out,
                                            std::uint32_t cap_out, const std::uint32_t* route, std::uint32_t bins,
                                            Lists L, std::uint32_t set, gf::DevicePoolHdr* pool,
