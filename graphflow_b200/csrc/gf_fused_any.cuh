@@ -26,11 +26,13 @@ namespace { // internal linkage: see gf_partition.cuh
 
 constexpr uint32_t kAnyCoopMaxBins = 64u;
 
-// Batch totals and the grid-barrier counter; zeroed by the launcher before every launch.
+// Batch totals, the grid-barrier counter and the count of finished CTAs; zeroed before every
+// launch (by the launcher, or by the caller's previous launch on the stream).
 struct AnyCoopHdr {
     unsigned long long total[kAnyCoopMaxBins];
     unsigned long long done;
-    unsigned long long pad[7];
+    unsigned long long finished;
+    unsigned long long pad[6];
 };
 static_assert(sizeof(AnyCoopHdr) % 64u == 0u, "row alignment");
 
@@ -47,12 +49,12 @@ constexpr size_t any_coop_smem_bytes(uint32_t B)
            4u * (Shape::kWarps + 1u + 8u);
 }
 
-template <typename Shape, typename Access, typename Classify, typename Update>
+template <typename Shape, typename Access, typename Classify, typename Update, typename Post>
 __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_partition_any_coop_kernel(
     Access acc, Classify classify, Update update, uint64_t seed_mixed, uint32_t capacity, FastDiv fdc,
     uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles, uint32_t B, const uint32_t* reserved,
     uint32_t n_reserved, uint32_t* totals, AnyCoopHdr* hdr, uint32_t* cta_cnt, uint16_t* bins16,
-    uint32_t* status, InlineFinish fin)
+    uint32_t* status, InlineFinish fin, Post post)
 {
     using P = typename Access::Payload;
     constexpr int T = Shape::kThreads, W = Shape::kWarps, IPT = Shape::kIpt;
@@ -236,24 +238,39 @@ __global__ void __launch_bounds__(Shape::kThreads, Shape::kMinBlocks) fused_part
             run_base[b] += bin_tot[b];
         __syncthreads();
     }
+    // the last CTA to finish runs the caller's post step over the published descriptors (every
+    // other CTA's descriptors, output count and reads of its input are done before its arrival)
+    if constexpr (Post::kActive) {
+        if (threadIdx.x == 0) {
+            __threadfence();
+            misc[1] = atomicAdd(&hdr->finished, 1ull) + 1ull == (unsigned long long)G ? 1u : 0u;
+        }
+        __syncthreads();
+        if (misc[1] != 0u) {
+            __threadfence();
+            post(fin, status);
+        }
+    }
 }
 
 // Host side: one cooperative launch over n_tiles tiles; the grid is as many CTAs as fit on the
 // device at once (at most n_tiles and max_ctas). The scratch (any_coop_scratch_bytes) holds the
 // header, zeroed here on the stream, the per-CTA rows and the bins.
-template <typename Shape, typename Access, typename Classify, typename Update>
+// post: work of the last CTA after the whole batch (NoPost: none); zero_hdr false when an earlier
+// launch on the stream has zeroed the header (sizeof(AnyCoopHdr) bytes at the scratch's start).
+template <typename Shape, typename Access, typename Classify, typename Update, typename Post = NoPost>
 cudaError_t launch_fused_any_coop(cudaStream_t stream, Access acc, Classify cls, Update upd, uint64_t seed_mixed,
                                   uint32_t capacity, uint64_t pool_slots, const gf_tile* tiles, uint32_t n_tiles,
                                   uint32_t B, const uint32_t* reserved, uint32_t n_reserved, uint32_t* totals,
                                   void* scratch, uint64_t scratch_bytes, uint32_t max_ctas, uint32_t* status,
-                                  InlineFinish fin, int sms)
+                                  InlineFinish fin, int sms, Post post = Post{}, bool zero_hdr = true)
 {
     using P = typename Access::Payload;
     if (B == 0u || B > kAnyCoopMaxBins || fin.table == nullptr || n_tiles == 0u || scratch == nullptr ||
         (reinterpret_cast<uintptr_t>(scratch) & 15u) != 0u ||
         scratch_bytes < any_coop_scratch_bytes(n_tiles, Shape::kTile, max_ctas))
         return cudaErrorInvalidValue;
-    auto kernel = fused_partition_any_coop_kernel<Shape, Access, Classify, Update>;
+    auto kernel = fused_partition_any_coop_kernel<Shape, Access, Classify, Update, Post>;
     const size_t smem = any_coop_smem_bytes<Shape, P>(B);
     cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess)
@@ -270,13 +287,15 @@ cudaError_t launch_fused_any_coop(cudaStream_t stream, Access acc, Classify cls,
     auto* hdr = static_cast<AnyCoopHdr*>(scratch);
     auto* cta_cnt = reinterpret_cast<uint32_t*>(hdr + 1);
     auto* bins16 = reinterpret_cast<uint16_t*>(cta_cnt + (size_t)kAnyCoopMaxBins * max_ctas);
-    err = cudaMemsetAsync(hdr, 0, sizeof(AnyCoopHdr), stream);
-    if (err != cudaSuccess)
-        return err;
+    if (zero_hdr) {
+        err = cudaMemsetAsync(hdr, 0, sizeof(AnyCoopHdr), stream);
+        if (err != cudaSuccess)
+            return err;
+    }
     FastDiv fd(capacity);
     void* args[] = {&acc,      &cls,      &upd,    &seed_mixed, &capacity, &fd,     &pool_slots,
                     &tiles,    &n_tiles,  &B,      &reserved,   &n_reserved, &totals, &hdr,
-                    &cta_cnt,  &bins16,   &status, &fin};
+                    &cta_cnt,  &bins16,   &status, &fin,        &post};
     return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3((uint32_t)g),
                                        dim3(Shape::kThreads), args, smem, stream);
 }

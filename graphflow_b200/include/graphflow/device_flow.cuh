@@ -19,9 +19,9 @@
 //              GraphRunner.hpp:1014-1037); one fused classify -> scan -> scatter launch that also
 //              publishes the output descriptors; every output chunk appended to the list of the
 //              node its port feeds, with the unused reservations returned and the input chunks
-//              released. Large batches: three launches (the cooperative any-payload kernel of
-//              gf_fused_any.cuh between the tile and the routing launch); others two (the per-tile
-//              kernel of gf_partition.cuh, whose finishing CTA also routes and settles);
+//              released: two launches, the tiles and reservation, then the cooperative
+//              any-payload kernel of gf_fused_any.cuh (large batches) or the per-tile kernel of
+//              gf_partition.cuh, whose finishing CTA also routes and settles;
 //   transform  one launch: the functor applied in place and the chunks forwarded to the next node
 //              (the reference's TransformKernel copies into a dense concatenation,
 //              Execution.hpp:694-776; the particles and their order inside a chunk are the same);
@@ -139,43 +139,24 @@ __device__ inline void buildTiles(const std::uint32_t* ids, const std::uint32_t*
 }
 
 // Partition, before the partition kernel: its tiles; in block 0 the reservation of `bound` output
-// chunks, for the per-tile kernel the control block's three reset words, and clearSet(clear).
+// chunks, the control block's three reset words (per-tile kernel) or the header of the
+// cooperative kernel's scratch, and clearSet(clear).
 __global__ void wave_partition_prep_kernel(const std::uint32_t* ids, const std::uint32_t* fills, std::uint32_t k,
                                            std::uint32_t T, std::uint32_t tp, gf_tile* tiles, gf::DevicePoolHdr* pool,
-                                           std::uint32_t bound, std::uint32_t* reserved, gf::FusedCtl* ctl, Lists L,
-                                           std::uint32_t clear, std::uint32_t* status)
+                                           std::uint32_t bound, std::uint32_t* reserved, gf::FusedCtl* ctl,
+                                           gf::AnyCoopHdr* coop_hdr, Lists L, std::uint32_t clear,
+                                           std::uint32_t* status)
 {
     buildTiles(ids, fills, k, T, tp, tiles);
     if (blockIdx.x == 0) {
         if (ctl != nullptr && threadIdx.x < gf::kFusedCtlResetBytes / 4u)
             reinterpret_cast<std::uint32_t*>(ctl)[threadIdx.x] = 0u;
+        if (coop_hdr != nullptr)
+            for (std::uint32_t i = threadIdx.x; i < sizeof(gf::AnyCoopHdr) / 8u; i += blockDim.x)
+                reinterpret_cast<unsigned long long*>(coop_hdr)[i] = 0ull;
         clearSet(L, clear);
         gf::pool_acquire_block(pool, bound, reserved, status);
     }
-}
-
-// Partition, after the cooperative partition kernel (the per-tile kernel does the same in its
-// finishing CTA, WavePost): its published output chunks appended to the lists their ports feed
-// (route[bin]); in block 0 the unused reservations returned and the k input chunks released (the
-// partition kernel, earlier in the stream, has read them).
-__global__ void wave_partition_post_kernel(const gf_out_desc* descs, const std::uint32_t* num_out,
-                                           std::uint32_t cap_out, const std::uint32_t* route, std::uint32_t bins,
-                                           Lists L, std::uint32_t set, gf::DevicePoolHdr* pool,
-                                           const std::uint32_t* reserved, const std::uint32_t* ids, std::uint32_t k,
-                                           std::uint32_t* status)
-{
-    const std::uint32_t m = *num_out < cap_out ? *num_out : cap_out;
-    for (std::uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < m; f += gridDim.x * blockDim.x) {
-        const gf_out_desc d = descs[f];
-        if (d.bin >= bins || d.fill == 0u) {
-            if (d.bin >= bins)
-                gf::set_status(status, GF_INVALID);
-            continue;
-        }
-        appendChunk(L, set, route[d.bin], d.chunk_index, d.fill, status);
-    }
-    if (blockIdx.x == 0)
-        gf::pool_settle_block(pool, reserved, cap_out, num_out, 0u, ids, 1u, nullptr, k, status);
 }
 
 // The transform in one launch: block t runs tile t of the k entries (entry f = t / tp, particles
@@ -252,8 +233,11 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// The routing and settle of wave_partition_post_kernel as the work of the per-tile partition
-// kernel's finishing CTA (after its inline finish): one launch fewer per partition batch.
+// A partition batch's routing and settle, run by the partition kernel's finishing CTA after the
+// output descriptors are published (the per-tile kernel's last CTA after its inline finish, the
+// cooperative kernel's last CTA to finish): every output chunk appended to the list of the node
+// its port feeds (route[bin]), the unused reservations returned and the k input chunks released
+// (every CTA has read them by then).
 struct WavePost {
     static constexpr bool kActive = true;
     const std::uint32_t* route = nullptr;
@@ -490,28 +474,27 @@ public:
         const std::uint32_t bound = static_cast<std::uint32_t>(b64);
         const bool coop =
             w.coopScratch != nullptr && m_bins <= gf::kAnyCoopMaxBins && nt >= kCoopMinTiles;
-        wave_partition_prep_kernel<<<gridFor(nt), 256, 0, w.s>>>(ids, fills, k, w.T, w.tp, w.tiles, w.pool, bound,
-                                                                 w.reserved, coop ? nullptr : w.ctl, w.L,
-                                                                 w.takeClearSet(), w.status);
+        wave_partition_prep_kernel<<<gridFor(nt), 256, 0, w.s>>>(
+            ids, fills, k, w.T, w.tp, w.tiles, w.pool, bound, w.reserved, coop ? nullptr : w.ctl,
+            coop ? static_cast<gf::AnyCoopHdr*>(w.coopScratch) : nullptr, w.L, w.takeClearSet(), w.status);
         const Acc acc{m_st.view()};
         const Cls cls{m_cls, w.seedMixed, m_purpose, w.status};
         const Upd upd{m_upd, m_purpose + 1u, w.status};
         const gf::InlineFinish fin{w.table, w.descs, bound, w.numOut};
+        // the partition kernel's finishing CTA routes the outputs and settles the pool
+        const WavePost post{routesDev, m_bins, w.L, next, w.pool, w.reserved, ids, k};
         if (coop) {
-            // a large batch: count, one grid barrier, plan, scatter (no per-tile look-back)
+            // a large batch: count, one grid barrier, plan, scatter (no per-tile look-back); the
+            // prep kernel zeroed the scratch header
             cuda::check(gf::launch_fused_any_coop<CoopShape>(w.s, acc, cls, upd, w.seedMixed, w.C, w.slots, w.tiles, nt,
                                                              m_bins, w.reserved, bound, w.totals, w.coopScratch,
-                                                             w.coopScratchBytes, w.coopMaxCtas, w.status, fin, w.sms),
+                                                             w.coopScratchBytes, w.coopMaxCtas, w.status, fin, w.sms,
+                                                             post, false),
                         "device-resident cooperative partition launch");
             ++w.coopBatches;
-            wave_partition_post_kernel<<<gridFor(bound), 256, 0, w.s>>>(w.descs, w.numOut, bound, routesDev, m_bins,
-                                                                       w.L, next, w.pool, w.reserved, ids, k, w.status);
-            ++w.launches;
         } else {
             auto* desc = reinterpret_cast<unsigned long long*>(w.ctl + 1); // reset words zeroed by the prep kernel
-            // the launch's last CTA builds the table and the output descriptors, then routes them
-            // and settles the pool (WavePost)
-            const WavePost post{routesDev, m_bins, w.L, next, w.pool, w.reserved, ids, k};
+            // the launch's last CTA builds the table and the output descriptors
             gf::fused_partition_kernel<Shape, Acc, Cls, Upd, WavePost><<<nt, Shape::kThreads, m_smem, w.s>>>(
                 acc, cls, upd, w.seedMixed, w.C, gf::FastDiv(w.C), w.slots, w.tiles, nt, m_bins, w.reserved, bound,
                 w.totals, w.portChunks, w.maxK, w.ctl, desc, w.status, fin, post);
