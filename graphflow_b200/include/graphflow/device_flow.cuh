@@ -41,6 +41,7 @@
 #include "gf_device_pool.cuh"
 #include "gf_fused_any.cuh"
 #include "kernels.cuh"
+#include "wave_order.hpp"
 
 namespace graphflow {
 namespace devflow {

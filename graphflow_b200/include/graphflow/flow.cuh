@@ -462,31 +462,17 @@ private:
         w.coopMaxCtas = coopCtas;
         w.sms = sms;
         w.launches = 1u;
-        // the wave's node order: along every transform edge (a transform forwards all its chunks to
-        // one node) the successor comes later, so a particle passes a run of transforms and the
-        // node after them in one wave; nodes on a cycle of transforms alone keep their index order
-        std::vector<std::uint32_t> order(N, 0u), seq;
-        {
-            std::vector<std::uint32_t> indeg(N, 0u);
-            for (std::uint32_t k = 0; k < N; ++k)
-                if (waves[k]->forwardsAll() && !routes[k].empty() && routes[k][0] < N && routes[k][0] != k)
-                    ++indeg[routes[k][0]];
-            std::vector<char> placed(N, 0);
-            for (std::uint32_t k = 0; k < N; ++k)
-                for (std::uint32_t v = k; v < N && indeg[v] == 0u && !placed[v];) {
-                    placed[v] = 1;
-                    seq.push_back(v);
-                    if (!waves[v]->forwardsAll() || routes[v].empty() || routes[v][0] >= N || routes[v][0] == v)
-                        break;
-                    v = routes[v][0];
-                    --indeg[v];
-                }
-            for (std::uint32_t k = 0; k < N; ++k)
-                if (!placed[k])
-                    seq.push_back(k);
-            for (std::uint32_t i = 0; i < N; ++i)
-                order[seq[i]] = i;
+        // the wave's node order (waveOrder): a transform's successor after it where the graph allows
+        std::vector<char> forwards(N, 0);
+        std::vector<std::uint32_t> succ(N, kNoList), order(N, 0u);
+        for (std::uint32_t k = 0; k < N; ++k) {
+            forwards[k] = waves[k]->forwardsAll() ? 1 : 0;
+            if (!routes[k].empty())
+                succ[k] = routes[k][0];
         }
+        const std::vector<std::uint32_t> seq = waveOrder(forwards, succ);
+        for (std::uint32_t i = 0; i < N; ++i)
+            order[seq[i]] = i;
         std::vector<std::uint32_t> waveCounts(N, 0u);
         std::vector<unsigned long long> waveParticles(N, 0u);
         std::uint32_t next = 1u;
